@@ -1,0 +1,179 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY -- ctypes access to the CPU checkers.
+
+* ``Restatement``  -- oracle/_build/liboracle.so, the project's plain-C
+  restatement of ccpsdv3/cpsd.c (cpsd_oracle.c + fft3d.c).
+* ``ReferenceBuild`` -- oracle/_ref/libcpsd_ref.so, the reference's own
+  ccpsdv3/*.c compiled unmodified (oracle/Makefile target ``ref``).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  Both classes run the same state machine as the reference's
+driver: ``run(inputs, inner, state)`` performs one ``cpsd()`` call and
+updates ``state`` (c1, c2, cpsi, dn, hml, lmd, r1, r2, fion, E) in place.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATEMENT_SO = os.path.join(HERE, "_build", "liboracle.so")
+REFERENCE_SO = os.path.join(HERE, "_ref", "libcpsd_ref.so")
+
+_P = ctypes.c_void_p
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def build_restatement() -> str:
+    subprocess.run(["make", "-s", "-C", HERE, "restatement"], check=True)
+    return RESTATEMENT_SO
+
+
+class State:
+    """Mutable arrays cpsd() reads and writes, sized like main.c:124-136."""
+
+    def __init__(self, inp):
+        nb = inp.nbands
+        ne0 = int(inp.ne[0])
+        ne1 = int(inp.ne[1])
+        self.c2 = inp.c2.copy()
+        self.c1 = inp.c2.copy()
+        self.cpsi = np.zeros_like(inp.c2)
+        self.dn = np.zeros(inp.ispin * inp.n2ft3d)
+        self.hml = np.zeros(ne0 * ne0 + ne1 * ne1)
+        self.lmd = np.zeros(ne0 * ne0 + ne1 * ne1)
+        self.r2 = inp.r2.copy()
+        self.r1 = inp.r2.copy()
+        self.fion = np.zeros(3 * inp.nion)
+        self.E = np.zeros(10)
+        self.deltae = 0.0
+        self.deltac = 0.0
+        self.deltar = 0.0
+        self.lagrange_fail = 0
+        assert self.c2.size == nb * inp.n2ft3d
+
+
+def _common_args(inp, inner: int, move: int):
+    ne = np.ascontiguousarray(inp.ne, dtype=np.int32)
+    return ne, [
+        ctypes.c_int(inner), ctypes.c_int(move), ctypes.c_int(inp.nion), ctypes.c_int(inp.ispin),
+        _ptr(ne), ctypes.c_int(inp.nfft), ctypes.c_int(inp.nfft3d), ctypes.c_int(inp.n2ft3d),
+        _ptr(inp.unitg), ctypes.c_double(inp.omega), ctypes.c_double(inp.dt),
+        ctypes.c_double(inp.fmass), _ptr(inp.katm), _ptr(inp.amass), _ptr(inp.zv),
+        ctypes.c_int(inp.nsh), _ptr(inp.rcell), ctypes.c_double(inp.cewald),
+        ctypes.c_double(inp.rcut), _ptr(inp.masker), _ptr(inp.G), _ptr(inp.tg), _ptr(inp.vc),
+        _ptr(inp.vg), _ptr(inp.lmmax), _ptr(inp.vnlnrm), _ptr(inp.vl), _ptr(inp.vnl),
+    ]
+
+
+class Restatement:
+    def __init__(self, path: str = RESTATEMENT_SO):
+        if not os.path.exists(path):
+            build_restatement()
+        self.lib = ctypes.CDLL(path)
+        self.lib.oracle_cpsd.restype = ctypes.c_int
+        self.lib.oracle_gcdotc.restype = ctypes.c_double
+        self.lib.oracle_gsdot.restype = ctypes.c_double
+        self.lib.oracle_gssum.restype = ctypes.c_double
+
+    def run(self, inp, inner: int, st: State, move: Optional[int] = None) -> State:
+        move = inp.spec.move if move is None else move
+        ne, args = _common_args(inp, inner, move)
+        dd = [ctypes.c_double() for _ in range(3)]
+        fail = ctypes.c_int()
+        rc = self.lib.oracle_cpsd(*args, _ptr(st.r1), _ptr(st.r2), _ptr(st.fion), _ptr(st.c1),
+                                  _ptr(st.c2), _ptr(st.cpsi), _ptr(st.dn), _ptr(st.hml),
+                                  _ptr(st.lmd), _ptr(st.E), ctypes.byref(dd[0]),
+                                  ctypes.byref(dd[1]), ctypes.byref(dd[2]), ctypes.byref(fail))
+        if rc != 0:
+            raise MemoryError("oracle_cpsd could not allocate scratch")
+        st.deltae, st.deltac, st.deltar = dd[0].value, dd[1].value, dd[2].value
+        st.lagrange_fail += fail.value
+        return st
+
+    # FFT and helper entry points (same argument conventions as the reference)
+    def cr_fft3b(self, A: np.ndarray, nfft: int) -> None:
+        _fft(self.lib.cr_fft3b_, A, nfft)
+
+    def rc_fft3f(self, A: np.ndarray, nfft: int) -> None:
+        _fft(self.lib.rc_fft3f_, A, nfft)
+
+    def gcdotc(self, nfft: int, a: np.ndarray, b: np.ndarray) -> float:
+        return self.lib.oracle_gcdotc(ctypes.c_int(nfft), _ptr(a), _ptr(b))
+
+    def xc(self, ispin: int, n2ft3d: int, dn: np.ndarray):
+        xcp = np.zeros(ispin * n2ft3d)
+        xce = np.zeros(n2ft3d)
+        self.lib.oracle_xc(ctypes.c_int(ispin), ctypes.c_int(n2ft3d), _ptr(dn), _ptr(xcp), _ptr(xce))
+        return xcp, xce
+
+
+def _fft(fn, A: np.ndarray, nfft: int) -> None:
+    assert A.dtype == np.float64 and A.flags.c_contiguous
+    i = lambda v: ctypes.byref(ctypes.c_int(v))  # noqa: E731
+    nh = nfft // 2 + 1
+    fn(_ptr(A), i(nh), i(nh * nfft), i(nfft + 2), i((nfft + 2) * nfft), i(nfft), i(nfft), i(nfft),
+       None, i(0))
+
+
+class ReferenceBuild:
+    """The reference's own cpsd() (oracle/_ref/libcpsd_ref.so)."""
+
+    def __init__(self, path: str = REFERENCE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path + " (build with: make -C oracle ref)")
+        self.lib = ctypes.CDLL(path)
+        self.lib.gcdotc.restype = ctypes.c_double
+        self.lib.gssum.restype = ctypes.c_double
+
+    @staticmethod
+    def work_size(inp) -> int:
+        """cpsdwork length, main.c:317-320 (+nion for dti when move, cpsd.c:119)."""
+        ne0 = int(inp.ne[0])
+        return ((6 + inp.ispin) * inp.n2ft3d + inp.nion * (5 * inp.nfft + 3) + 7 * ne0 * ne0)
+
+    def run(self, inp, inner: int, st: State, move: Optional[int] = None) -> State:
+        move = inp.spec.move if move is None else move
+        ne, args = _common_args(inp, inner, move)
+        work = np.zeros(self.work_size(inp))
+        dd = [ctypes.c_double() for _ in range(3)]
+        self.lib.cpsd(*args, _ptr(st.r1), _ptr(st.r2), _ptr(st.fion), _ptr(st.c1), _ptr(st.c2),
+                      _ptr(st.cpsi), _ptr(st.dn), _ptr(st.hml), _ptr(st.lmd), _ptr(work),
+                      _ptr(st.E), ctypes.byref(dd[0]), ctypes.byref(dd[1]), ctypes.byref(dd[2]))
+        st.deltae, st.deltac, st.deltar = dd[0].value, dd[1].value, dd[2].value
+        return st
+
+    def cr_fft3b(self, A: np.ndarray, nfft: int) -> None:
+        _fft(self.lib.cr_fft3b_, A, nfft)
+
+    def rc_fft3f(self, A: np.ndarray, nfft: int) -> None:
+        _fft(self.lib.rc_fft3f_, A, nfft)
+
+    def get_g(self, nfft: int, unitg: np.ndarray) -> np.ndarray:
+        nh = nfft // 2 + 1
+        G = np.zeros(3 * nh * nfft * nfft)
+        self.lib.get_g(ctypes.c_int(nfft), _ptr(unitg), _ptr(G))
+        return G
+
+    def get_masker(self, nfft: int, ggcut: float, unitg: np.ndarray) -> np.ndarray:
+        nh = nfft // 2 + 1
+        m = np.zeros(nh * nfft * nfft, dtype=np.int32)
+        self.lib.get_masker(ctypes.c_int(nfft), ctypes.c_double(ggcut), _ptr(unitg), _ptr(m))
+        return m
+
+    def get_cube(self, icube: int, unit: float):
+        vol = ctypes.c_double()
+        unita = np.zeros(9)
+        unitg = np.zeros(9)
+        self.lib.get_cube(ctypes.c_int(icube), ctypes.c_double(unit), ctypes.byref(vol),
+                          _ptr(unita), _ptr(unitg))
+        return vol.value, unita, unitg
+
+    def gssum(self, nfft: int, x: np.ndarray) -> float:
+        return self.lib.gssum(ctypes.c_int(nfft), _ptr(x))
