@@ -1,0 +1,152 @@
+/*
+ * cpsd_b200.h -- C ABI of the B200 (sm_100a) steepest-descent engine.
+ *
+ * Drop-in for the serial Simple-CPSD electronic minimisation
+ * (Cpsd-mpi-bamboo/ccpsdv3): a program that linked cpsd.o and the FFTPACK
+ * 3-D wrapper links this library instead and runs the same loop on the GPU.
+ * All pointers are host pointers in the reference's layouts (half box of
+ * (nfft/2+1) x nfft x nfft complex per band = n2ft3d doubles; real-space
+ * arrays padded to (nfft+2) x nfft x nfft).  Supported grids: nfft in
+ * {16, 24, 32, 48, 64, 128}; bands per spin <= 256.  There is no CPU
+ * fallback: without a usable GPU every call fails.
+ */
+#ifndef CPSD_B200_H
+#define CPSD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+    CPSD_OK = 0,
+    CPSD_ERR_CUDA = 1,          /* a CUDA call failed (no device, out of memory, ...) */
+    CPSD_ERR_ARG = 2,           /* an argument is out of range or inconsistent */
+    CPSD_ERR_GRID = 3,          /* nfft not one of the supported sizes */
+    CPSD_ERR_BANDS = 4,         /* more than 256 bands in a spin channel */
+    CPSD_ERR_EMPTY_MASK = 5,    /* the cutoff mask selects no G vector */
+    CPSD_ERR_UNMASKED_PSI = 6,  /* input orbitals have coefficients outside the mask */
+    CPSD_ERR_MOVE = 7,          /* move=1 (ionic forces) requested but not built in */
+    CPSD_WARN_LAGRANGE = 10     /* (positive warning) Lagrange iteration hit 30 steps; the
+                                   reference prints "ierr=10" and continues (cpsd.c:477) */
+};
+
+/* Human-readable text for a status code. */
+const char *cpsd_gpu_strerror(int status);
+
+/* ------------------------------------------------------ drop-in entry points */
+
+/*
+ * Replaces void cpsd(...) of ccpsdv3/cpsd.c:33-71 (prototype repeated at
+ * ccpsdv3/main.c:18-56), same arguments and meanings: runs `inner`
+ * steepest-descent steps from c2, then the energies E[0..9] and the
+ * convergence measures.  On exit c1 holds the orbitals of the last step, c2
+ * the next iterate, cpsi = c2 - c1, dn the spin densities of the last step,
+ * hml/lmd the Hamiltonian and Lagrange matrices.  cpsdwork is accepted and
+ * not used (scratch lives on the GPU).  Errors are printed like the
+ * reference's and the call returns; use cpsd_gpu_cpsd() for a status.
+ */
+void cpsd(const int inner, const int move, const int nion, const int ispin, const int *ne,
+          const int nfft, const int nfft3d, const int n2ft3d, const double *unitg,
+          const double omega, const double dt, const double fmass, const int *katm,
+          const double *amass, const double *zv, const int nsh, const double *rcell,
+          const double cewald, const double rcut, const int *masker, const double *G,
+          const double *tg, const double *vc, const double *vg, int *lmmax, double *vnlnrm,
+          double *vl, double *vnl, double *r1, double *r2, double *fion, double *c1, double *c2,
+          double *cpsi, double *dn, double *hml, double *lmd, double *cpsdwork, double *E,
+          double *deltae, double *deltac, double *deltar);
+
+/* cpsd() returning a status (CPSD_OK, an error, or CPSD_WARN_LAGRANGE). */
+int cpsd_gpu_cpsd(const int inner, const int move, const int nion, const int ispin, const int *ne,
+                  const int nfft, const int nfft3d, const int n2ft3d, const double *unitg,
+                  const double omega, const double dt, const double fmass, const int *katm,
+                  const double *amass, const double *zv, const int nsh, const double *rcell,
+                  const double cewald, const double rcut, const int *masker, const double *G,
+                  const double *tg, const double *vc, const double *vg, const int *lmmax,
+                  const double *vnlnrm, const double *vl, const double *vnl, double *r1, double *r2,
+                  double *fion, double *c1, double *c2, double *cpsi, double *dn, double *hml,
+                  double *lmd, double *E, double *deltae, double *deltac, double *deltar);
+
+/*
+ * Replace the Fortran-ABI cr_fft3b / rc_fft3f of fftpack3d/fftpack3d.f:22-96
+ * and :107-196 (called from ccpsdv3/cpsd.c:179,201,380,390): in-place,
+ * unnormalised complex->real inverse and real->complex forward 3-D FFTs of
+ * one (nx+2) x ny x nz array.  Only cubic nx = ny = nz with the reference's
+ * strides (inc2c = nx/2+1, inc3c = (nx/2+1)*ny, inc2r = nx+2, inc3r =
+ * (nx+2)*ny) are accepted; tmp/ntmp are ignored.  The whole box is
+ * transformed (no sphere pruning).
+ */
+void cr_fft3b_(double *A, int *inc2c, int *inc3c, int *inc2r, int *inc3r, int *nx, int *ny,
+               int *nz, double *tmp, int *ntmp);
+void rc_fft3f_(double *A, int *inc2c, int *inc3c, int *inc2r, int *inc3r, int *nx, int *ny,
+               int *nz, double *tmp, int *ntmp);
+
+/* Status of the last cr_fft3b_/rc_fft3f_ call on this thread. */
+int cpsd_gpu_fft_status(void);
+
+/* ------------------------------------------------------ persistent context */
+
+typedef struct cpsd_gpu_ctx cpsd_gpu_ctx;
+
+enum { CPSD_PREC_FP64 = 0, CPSD_PREC_MIXED = 1 };
+
+typedef struct {
+    int nfft;        /* grid edge */
+    int ispin;       /* 1 or 2 */
+    int ne[2];       /* bands per spin */
+    int nion;        /* ions */
+    int nkatm;       /* ion kinds */
+    int nsh;         /* real-space Ewald image cells (27 in the reference) */
+    int precision;   /* CPSD_PREC_FP64 (parity path) or CPSD_PREC_MIXED */
+    int device;      /* CUDA device ordinal */
+    double unitg[9]; /* reciprocal lattice, ccpsdv3/get_cube.c */
+    double omega, dt, fmass, cewald, rcut;
+} cpsd_gpu_params;
+
+/*
+ * Create a context for one cell.  masker1 is the nfft3d-long cutoff mask of
+ * ccpsdv3/get_masker.c (one int per half-box G, not the duplicated
+ * n2ft3d-long array cpsd() takes).  All GPU memory is allocated here.
+ */
+int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx **out);
+
+/* Change the per-call scalars cpsd() receives (lattice, volume, time step,
+ * fictitious mass, Ewald constant and cut radius) without rebuilding. */
+int cpsd_gpu_set_scalars(cpsd_gpu_ctx *c, const double *unitg, double omega, double dt, double fmass,
+                         double cewald, double rcut);
+
+/* Upload the per-cell tables in the layouts cpsd() takes. */
+int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, const double *zv,
+                        const double *rcell, const double *G, const double *tg, const double *vc,
+                        const double *vg, const int *lmmax, const double *vnlnrm, const double *vl,
+                        const double *vnl);
+
+/* Upload orbitals (half box, (ne0+ne1) x n2ft3d doubles) and ion positions. */
+int cpsd_gpu_set_state(cpsd_gpu_ctx *c, const double *c2, const double *r2);
+
+/*
+ * Run `inner` SD steps and the energy evaluation, the body of cpsd().
+ * E[0] must hold the previous total energy (for deltae), as in cpsd().
+ */
+int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae, double *deltac,
+                 double *deltar);
+
+/* Download the state cpsd() returns; any pointer may be NULL to skip it. */
+int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double *dn,
+                       double *hml, double *lmd, double *r1, double *r2, double *fion);
+
+/* Sphere size (packed G vectors per band) and the kernel launches of one SD step. */
+int cpsd_gpu_npw(const cpsd_gpu_ctx *c);
+int cpsd_gpu_launches_per_step(const cpsd_gpu_ctx *c);
+/* Steps whose Lagrange iteration stopped at 30 iterations, since creation. */
+int cpsd_gpu_lagrange_failures(cpsd_gpu_ctx *c);
+
+/* CUDA stream the context runs on (a cudaStream_t), for timing with events. */
+void *cpsd_gpu_stream(cpsd_gpu_ctx *c);
+
+void cpsd_gpu_destroy(cpsd_gpu_ctx *c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,181 @@
+"""Python mirror of the reference's entry points, backed by the CUDA library.
+
+* ``cpsd(inp, state, inner)`` -- one call of the drop-in ``cpsd()`` of
+  ccpsdv3/cpsd.c:33-71 with host numpy buffers (``state`` is updated in
+  place exactly as the reference updates its arrays).
+* ``GpuCell`` -- a persistent context: tables and orbitals stay resident in
+  HBM between calls; ``run(inner)`` is the body of ``cpsd()``.
+* ``cr_fft3b`` / ``rc_fft3f`` -- the fftpack3d 3-D FFT drop-ins.
+
+Errors raise ``CpsdError``; the Lagrange non-convergence warning of the
+reference (``ierr=10``, cpsd.c:477) is counted, not raised.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import lib as _l
+from .lib import CpsdError
+
+_P = ctypes.c_void_p
+
+
+def _ptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.flags.c_contiguous, "arrays must be C-contiguous"
+    return a.ctypes.data_as(_P)
+
+
+class State:
+    """The arrays cpsd() reads and writes (sizes as ccpsdv3/main.c:124-136)."""
+
+    def __init__(self, inp):
+        ne0, ne1 = int(inp.ne[0]), int(inp.ne[1])
+        self.c2 = inp.c2.copy()
+        self.c1 = inp.c2.copy()
+        self.cpsi = np.zeros_like(inp.c2)
+        self.dn = np.zeros(inp.ispin * inp.n2ft3d)
+        self.hml = np.zeros(ne0 * ne0 + ne1 * ne1)
+        self.lmd = np.zeros(ne0 * ne0 + ne1 * ne1)
+        self.r2 = inp.r2.copy()
+        self.r1 = inp.r2.copy()
+        self.fion = np.zeros(3 * max(inp.nion, 1))
+        self.E = np.zeros(10)
+        self.deltae = 0.0
+        self.deltac = 0.0
+        self.deltar = 0.0
+        self.lagrange_fail = 0
+
+
+def cpsd(inp, st: State, inner: int, move: int = 0) -> State:
+    """The drop-in: exactly the reference's cpsd() call with host buffers."""
+    L = _l.load()
+    ne = np.ascontiguousarray(inp.ne, dtype=np.int32)
+    dd = [ctypes.c_double() for _ in range(3)]
+    rc = L.cpsd_gpu_cpsd(
+        ctypes.c_int(inner), ctypes.c_int(move), ctypes.c_int(inp.nion), ctypes.c_int(inp.ispin),
+        _ptr(ne), ctypes.c_int(inp.nfft), ctypes.c_int(inp.nfft3d), ctypes.c_int(inp.n2ft3d),
+        _ptr(inp.unitg), ctypes.c_double(inp.omega), ctypes.c_double(inp.dt),
+        ctypes.c_double(inp.fmass), _ptr(inp.katm), _ptr(inp.amass), _ptr(inp.zv),
+        ctypes.c_int(inp.nsh), _ptr(inp.rcell), ctypes.c_double(inp.cewald),
+        ctypes.c_double(inp.rcut), _ptr(inp.masker), _ptr(inp.G), _ptr(inp.tg), _ptr(inp.vc),
+        _ptr(inp.vg), _ptr(inp.lmmax), _ptr(inp.vnlnrm), _ptr(inp.vl), _ptr(inp.vnl),
+        _ptr(st.r1), _ptr(st.r2), _ptr(st.fion), _ptr(st.c1), _ptr(st.c2), _ptr(st.cpsi),
+        _ptr(st.dn), _ptr(st.hml), _ptr(st.lmd), _ptr(st.E), ctypes.byref(dd[0]),
+        ctypes.byref(dd[1]), ctypes.byref(dd[2]))
+    if rc == _l.CPSD_WARN_LAGRANGE:
+        st.lagrange_fail += 1
+    elif rc != _l.CPSD_OK:
+        raise CpsdError(rc, "cpsd")
+    st.deltae, st.deltac, st.deltar = dd[0].value, dd[1].value, dd[2].value
+    return st
+
+
+class GpuCell:
+    """A cell resident on one GPU (the persistent-context API)."""
+
+    def __init__(self, inp, precision: int = _l.CPSD_PREC_FP64, device: int = 0):
+        L = _l.load()
+        self._L = L
+        self.inp = inp
+        p = _l.Params()
+        p.nfft = inp.nfft
+        p.ispin = inp.ispin
+        p.ne[0] = int(inp.ne[0])
+        p.ne[1] = int(inp.ne[1])
+        p.nion = inp.nion
+        p.nkatm = len(inp.zv)
+        p.nsh = inp.nsh
+        p.precision = precision
+        p.device = device
+        for i in range(9):
+            p.unitg[i] = float(inp.unitg[i])
+        p.omega, p.dt, p.fmass, p.cewald, p.rcut = inp.omega, inp.dt, inp.fmass, inp.cewald, inp.rcut
+        h = ctypes.c_void_p()
+        m1 = np.ascontiguousarray(inp.masker1, dtype=np.int32)
+        rc = L.cpsd_gpu_create(ctypes.byref(p), _ptr(m1), ctypes.byref(h))
+        if rc:
+            raise CpsdError(rc, "cpsd_gpu_create")
+        self.h = h
+        self._check(L.cpsd_gpu_set_tables(
+            h, _ptr(inp.katm), _ptr(inp.amass), _ptr(inp.zv), _ptr(inp.rcell), _ptr(inp.G),
+            _ptr(inp.tg), _ptr(inp.vc), _ptr(inp.vg), _ptr(inp.lmmax), _ptr(inp.vnlnrm),
+            _ptr(inp.vl), _ptr(inp.vnl)), "cpsd_gpu_set_tables")
+        self.E = np.zeros(10)
+        self.deltae = self.deltac = self.deltar = 0.0
+        self.lagrange_warnings = 0
+
+    def _check(self, rc: int, what: str) -> int:
+        if rc not in (_l.CPSD_OK, _l.CPSD_WARN_LAGRANGE):
+            raise CpsdError(rc, what)
+        return rc
+
+    @property
+    def npw(self) -> int:
+        return self._L.cpsd_gpu_npw(self.h)
+
+    @property
+    def launches_per_step(self) -> int:
+        return self._L.cpsd_gpu_launches_per_step(self.h)
+
+    @property
+    def stream(self) -> int:
+        return self._L.cpsd_gpu_stream(self.h) or 0
+
+    def set_state(self, c2: np.ndarray, r2: np.ndarray) -> None:
+        self._check(self._L.cpsd_gpu_set_state(self.h, _ptr(np.ascontiguousarray(c2)),
+                                               _ptr(np.ascontiguousarray(r2))), "cpsd_gpu_set_state")
+
+    def run(self, inner: int, move: int = 0) -> np.ndarray:
+        dd = [ctypes.c_double() for _ in range(3)]
+        rc = self._check(self._L.cpsd_gpu_run(self.h, inner, move, _ptr(self.E), ctypes.byref(dd[0]),
+                                              ctypes.byref(dd[1]), ctypes.byref(dd[2])), "cpsd_gpu_run")
+        if rc == _l.CPSD_WARN_LAGRANGE:
+            self.lagrange_warnings += 1
+        self.deltae, self.deltac, self.deltar = dd[0].value, dd[1].value, dd[2].value
+        return self.E
+
+    def get_state(self, st: State) -> State:
+        self._check(self._L.cpsd_gpu_get_state(self.h, _ptr(st.c1), _ptr(st.c2), _ptr(st.cpsi),
+                                                _ptr(st.dn), _ptr(st.hml), _ptr(st.lmd), _ptr(st.r1),
+                                                _ptr(st.r2), _ptr(st.fion)), "cpsd_gpu_get_state")
+        st.E[:] = self.E
+        st.deltae, st.deltac, st.deltar = self.deltae, self.deltac, self.deltar
+        return st
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self._L.cpsd_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _fft(fn, A: np.ndarray, nfft: int) -> None:
+    assert A.dtype == np.float64 and A.flags.c_contiguous
+    L = _l.load()
+    i = lambda v: ctypes.byref(ctypes.c_int(v))  # noqa: E731
+    nh = nfft // 2 + 1
+    fn(_ptr(A), i(nh), i(nh * nfft), i(nfft + 2), i((nfft + 2) * nfft), i(nfft), i(nfft), i(nfft),
+       None, i(0))
+    rc = L.cpsd_gpu_fft_status()
+    if rc:
+        raise CpsdError(rc, "3-D FFT")
+
+
+def cr_fft3b(A: np.ndarray, nfft: int) -> None:
+    """In place: half box (complex) -> real (padded x lines), unnormalised."""
+    _fft(_l.load().cr_fft3b_, A, nfft)
+
+
+def rc_fft3f(A: np.ndarray, nfft: int) -> None:
+    """In place: real (padded x lines) -> half box (complex), unnormalised."""
+    _fft(_l.load().rc_fft3f_, A, nfft)

@@ -1,0 +1,92 @@
+"""ctypes binding of include/cpsd_b200.h (the in-tree libcpsd_b200.so).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .build import LIB
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+
+CPSD_OK = 0
+CPSD_ERR_CUDA = 1
+CPSD_ERR_ARG = 2
+CPSD_ERR_GRID = 3
+CPSD_ERR_BANDS = 4
+CPSD_ERR_EMPTY_MASK = 5
+CPSD_ERR_UNMASKED_PSI = 6
+CPSD_ERR_MOVE = 7
+CPSD_WARN_LAGRANGE = 10
+
+CPSD_PREC_FP64 = 0
+CPSD_PREC_MIXED = 1
+
+# every symbol include/cpsd_b200.h declares
+EXPORTS = [
+    "cpsd_gpu_strerror", "cpsd", "cpsd_gpu_cpsd", "cr_fft3b_", "rc_fft3f_", "cpsd_gpu_fft_status",
+    "cpsd_gpu_create", "cpsd_gpu_set_scalars", "cpsd_gpu_set_tables", "cpsd_gpu_set_state",
+    "cpsd_gpu_run", "cpsd_gpu_get_state", "cpsd_gpu_npw", "cpsd_gpu_launches_per_step",
+    "cpsd_gpu_lagrange_failures", "cpsd_gpu_stream", "cpsd_gpu_destroy",
+]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("nfft", _I), ("ispin", _I), ("ne", _I * 2), ("nion", _I), ("nkatm", _I), ("nsh", _I),
+        ("precision", _I), ("device", _I), ("unitg", _D * 9), ("omega", _D), ("dt", _D),
+        ("fmass", _D), ("cewald", _D), ("rcut", _D),
+    ]
+
+
+class CpsdError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__("%s: status %d (%s)" % (what, status, strerror(status)))
+
+
+_lib = None
+
+
+def load(path: str = LIB) -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            "%s is missing: build it with `python -m cpsd_b200.build` "
+            "(there is no CPU fallback)" % path)
+    lib = ctypes.CDLL(path)
+    lib.cpsd_gpu_strerror.restype = ctypes.c_char_p
+    lib.cpsd_gpu_strerror.argtypes = [_I]
+    lib.cpsd_gpu_create.argtypes = [ctypes.POINTER(Params), _P, ctypes.POINTER(_P)]
+    lib.cpsd_gpu_set_scalars.argtypes = [_P, _P, _D, _D, _D, _D, _D]
+    lib.cpsd_gpu_set_tables.argtypes = [_P] + [_P] * 12
+    lib.cpsd_gpu_set_state.argtypes = [_P, _P, _P]
+    lib.cpsd_gpu_run.argtypes = [_P, _I, _I, _P, _P, _P, _P]
+    lib.cpsd_gpu_get_state.argtypes = [_P] + [_P] * 9
+    lib.cpsd_gpu_npw.argtypes = [_P]
+    lib.cpsd_gpu_launches_per_step.argtypes = [_P]
+    lib.cpsd_gpu_lagrange_failures.argtypes = [_P]
+    lib.cpsd_gpu_stream.argtypes = [_P]
+    lib.cpsd_gpu_stream.restype = _P
+    lib.cpsd_gpu_destroy.argtypes = [_P]
+    lib.cpsd_gpu_destroy.restype = None
+    lib.cpsd_gpu_fft_status.restype = _I
+    lib.cr_fft3b_.restype = None
+    lib.rc_fft3f_.restype = None
+    lib.cpsd.restype = None
+    lib.cpsd_gpu_cpsd.restype = _I
+    _lib = lib
+    return lib
+
+
+def strerror(status: int) -> str:
+    try:
+        return load().cpsd_gpu_strerror(int(status)).decode()
+    except FileNotFoundError:
+        return "library not built"

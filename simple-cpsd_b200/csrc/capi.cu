@@ -1,0 +1,303 @@
+// capi.cu -- the reference-facing entry points of include/cpsd_b200.h:
+// cpsd() / cpsd_gpu_cpsd() (ccpsdv3/cpsd.c:33-71) and the Fortran-ABI
+// cr_fft3b_ / rc_fft3f_ (fftpack3d/fftpack3d.f:22-196).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+#include "cpsd_b200.h"
+#include "fft.cuh"
+
+namespace {
+
+std::mutex g_mu;
+cpsd_gpu_ctx *g_ctx = nullptr;
+struct Signature {
+    int nfft = 0, ispin = 0, ne0 = 0, ne1 = 0, nion = 0, nkatm = 0, nsh = 0, device = -1;
+    std::vector<int> masker1;
+    bool operator==(const Signature &o) const
+    {
+        return nfft == o.nfft && ispin == o.ispin && ne0 == o.ne0 && ne1 == o.ne1 && nion == o.nion &&
+               nkatm == o.nkatm && nsh == o.nsh && device == o.device && masker1 == o.masker1;
+    }
+};
+Signature g_sig;
+
+}  // namespace
+
+extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, const int ispin, const int *ne,
+                             const int nfft, const int nfft3d, const int n2ft3d, const double *unitg,
+                             const double omega, const double dt, const double fmass, const int *katm,
+                             const double *amass, const double *zv, const int nsh, const double *rcell,
+                             const double cewald, const double rcut, const int *masker, const double *G,
+                             const double *tg, const double *vc, const double *vg, const int *lmmax,
+                             const double *vnlnrm, const double *vl, const double *vnl, double *r1, double *r2,
+                             double *fion, double *c1, double *c2, double *cpsi, double *dn, double *hml,
+                             double *lmd, double *E, double *deltae, double *deltac, double *deltar)
+{
+    if (!ne || !unitg || !masker || !c2 || !E) return CPSD_ERR_ARG;
+    const int nh = nfft / 2 + 1;
+    if (nfft <= 0 || nfft3d != nh * nfft * nfft || n2ft3d != (nfft + 2) * nfft * nfft) return CPSD_ERR_ARG;
+    if (move) return CPSD_ERR_MOVE;
+    int nkatm = 1;
+    for (int ii = 0; ii < nion; ++ii) nkatm = std::max(nkatm, katm[ii] + 1);
+    Signature sig;
+    sig.nfft = nfft;
+    sig.ispin = ispin;
+    sig.ne0 = ne[0];
+    sig.ne1 = ispin == 2 ? ne[1] : 0;
+    sig.nion = nion;
+    sig.nkatm = nkatm;
+    sig.nsh = nsh;
+    cudaGetDevice(&sig.device);
+    sig.masker1.resize(nfft3d);
+    for (int k = 0; k < nfft3d; ++k) sig.masker1[k] = masker[2 * k];  // main.c:189-195 duplicates it
+
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx || !(sig == g_sig)) {
+        if (g_ctx) cpsd_gpu_destroy(g_ctx);
+        g_ctx = nullptr;
+        cpsd_gpu_params p{};
+        p.nfft = nfft;
+        p.ispin = ispin;
+        p.ne[0] = sig.ne0;
+        p.ne[1] = sig.ne1;
+        p.nion = nion;
+        p.nkatm = nkatm;
+        p.nsh = nsh;
+        p.precision = CPSD_PREC_FP64;
+        p.device = sig.device;
+        memcpy(p.unitg, unitg, sizeof(p.unitg));
+        p.omega = omega;
+        p.dt = dt;
+        p.fmass = fmass;
+        p.cewald = cewald;
+        p.rcut = rcut;
+        int rc = cpsd_gpu_create(&p, sig.masker1.data(), &g_ctx);
+        if (rc) return rc;
+        g_sig = sig;
+    }
+    // per-call scalars (the reference passes them every call)
+    cpsd_gpu_ctx *c = g_ctx;
+    int rc = cpsd_gpu_set_scalars(c, unitg, omega, dt, fmass, cewald, rcut);
+    if (rc) return rc;
+    rc = cpsd_gpu_set_tables(c, katm, amass, zv, rcell, G, tg, vc, vg, lmmax, vnlnrm, vl, vnl);
+    if (rc) return rc;
+    rc = cpsd_gpu_set_state(c, c2, r2);
+    if (rc) return rc;
+    const int run = cpsd_gpu_run(c, inner, move, E, deltae, deltac, deltar);
+    if (run != CPSD_OK && run != CPSD_WARN_LAGRANGE) return run;
+    rc = cpsd_gpu_get_state(c, c1, c2, cpsi, dn, hml, lmd, r1, r2, fion);
+    return rc ? rc : run;
+}
+
+extern "C" void cpsd(const int inner, const int move, const int nion, const int ispin, const int *ne,
+                     const int nfft, const int nfft3d, const int n2ft3d, const double *unitg, const double omega,
+                     const double dt, const double fmass, const int *katm, const double *amass, const double *zv,
+                     const int nsh, const double *rcell, const double cewald, const double rcut,
+                     const int *masker, const double *G, const double *tg, const double *vc, const double *vg,
+                     int *lmmax, double *vnlnrm, double *vl, double *vnl, double *r1, double *r2, double *fion,
+                     double *c1, double *c2, double *cpsi, double *dn, double *hml, double *lmd,
+                     double *cpsdwork, double *E, double *deltae, double *deltac, double *deltar)
+{
+    (void)cpsdwork;
+    const int rc = cpsd_gpu_cpsd(inner, move, nion, ispin, ne, nfft, nfft3d, n2ft3d, unitg, omega, dt, fmass,
+                                 katm, amass, zv, nsh, rcell, cewald, rcut, masker, G, tg, vc, vg, lmmax, vnlnrm,
+                                 vl, vnl, r1, r2, fion, c1, c2, cpsi, dn, hml, lmd, E, deltae, deltac, deltar);
+    if (rc == CPSD_WARN_LAGRANGE)
+        printf("ierr=10\n");  // the reference's message for the same condition (cpsd.c:477)
+    else if (rc != CPSD_OK)
+        printf("cpsd (B200): error %d: %s\n", rc, cpsd_gpu_strerror(rc));
+}
+
+// ====================================================================== 3-D FFT drop-ins
+namespace {
+
+// unpadded real grid from the reference's (n+2)-padded x lines
+__global__ void unpad_real_kernel(int n, const double *__restrict__ src, double *__restrict__ dst)
+{
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long n3 = (long)n * n * n;
+    if (id >= n3) return;
+    const int x = (int)(id % n);
+    const long yz = id / n;
+    dst[id] = src[yz * (n + 2) + x];
+}
+
+__global__ void copy_pad_kernel(int n, const double *__restrict__ src, double *__restrict__ dst)
+{
+    const long n2r = (long)(n + 2) * n * n;
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n2r) return;
+    const int x = (int)(id % (n + 2));
+    const long yz = id / (n + 2);
+    dst[id] = (x < n) ? src[yz * n + x] : 0.0;
+}
+
+// half box -> packed (full geometry: every point), and back
+__global__ void perm_kernel(long count, const int *__restrict__ idx, const cx<double> *__restrict__ src,
+                            cx<double> *__restrict__ dst, int to_packed)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    if (to_packed)
+        dst[p] = src[idx[p]];
+    else
+        dst[idx[p]] = src[p];
+}
+
+struct FftCtx {
+    int n = 0, device = -1;
+    long nfft3d = 0, n2ft3d = 0, n3 = 0;
+    cudaStream_t st = nullptr;
+    double *buf = nullptr, *grid = nullptr;
+    cx<double> *packed = nullptr;
+    void *Taux = nullptr;
+    int *pt_idx = nullptr, *col_i = nullptr, *col_j = nullptr, *col_ptr = nullptr, *pt_k = nullptr,
+        *colidx = nullptr;
+    Geom g{};
+    std::vector<void *> allocs;
+    ~FftCtx()
+    {
+        for (void *p : allocs) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+thread_local int t_fft_status = CPSD_OK;
+std::mutex f_mu;
+std::unique_ptr<FftCtx> f_ctx;
+
+}  // namespace
+
+// engine.cu provides the transform instantiations through this factory
+int cpsd_fft_run_full(int n, int dir, const Geom &g, double *grid, cx<double> *packed, void *Taux,
+                      cudaStream_t st, int init_kx, int *ok);
+
+namespace {
+
+template <typename X>
+int dalloc(FftCtx &f, X **p, size_t count)
+{
+    void *q = nullptr;
+    if (cudaMalloc(&q, count * sizeof(X)) != cudaSuccess) return CPSD_ERR_CUDA;
+    f.allocs.push_back(q);
+    *p = (X *)q;
+    return CPSD_OK;
+}
+
+int fft_setup(int n)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CPSD_ERR_CUDA;
+    if (f_ctx && f_ctx->n == n && f_ctx->device == dev) return CPSD_OK;
+    f_ctx.reset();
+    std::unique_ptr<FftCtx> f(new FftCtx());
+    f->n = n;
+    f->device = dev;
+    const int nh = n / 2 + 1;
+    f->nfft3d = (long)nh * n * n;
+    f->n2ft3d = 2 * f->nfft3d;
+    f->n3 = (long)n * n * n;
+    if (cudaStreamCreateWithFlags(&f->st, cudaStreamNonBlocking) != cudaSuccess) return CPSD_ERR_CUDA;
+    // full geometry: columns (kx, ky) for every kx <= n/2, every kz
+    std::vector<int> col_i, col_j, col_ptr{0}, pt_k, pt_idx, colidx((size_t)nh * n);
+    for (int i = 0; i < nh; ++i)
+        for (int j = 0; j < n; ++j) {
+            colidx[(size_t)i * n + j] = (int)col_i.size();
+            col_i.push_back(i);
+            col_j.push_back(j);
+            for (int k = 0; k < n; ++k) {
+                pt_k.push_back(k);
+                pt_idx.push_back(i + j * nh + k * nh * n);
+            }
+            col_ptr.push_back((int)pt_k.size());
+        }
+    auto up = [&](int **d, const std::vector<int> &v) -> int {
+        if (dalloc(*f, d, v.size())) return CPSD_ERR_CUDA;
+        return cudaMemcpy(*d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess
+                   ? CPSD_OK
+                   : CPSD_ERR_CUDA;
+    };
+    if (up(&f->col_i, col_i) || up(&f->col_j, col_j) || up(&f->col_ptr, col_ptr) || up(&f->pt_k, pt_k) ||
+        up(&f->pt_idx, pt_idx) || up(&f->colidx, colidx))
+        return CPSD_ERR_CUDA;
+    if (dalloc(*f, &f->buf, f->n2ft3d) || dalloc(*f, &f->grid, f->n3) || dalloc(*f, &f->packed, f->nfft3d))
+        return CPSD_ERR_CUDA;
+    unsigned char *t = nullptr;
+    if (dalloc(*f, &t, sizeof(cx<double>) * (size_t)n * nh * n)) return CPSD_ERR_CUDA;
+    f->Taux = t;
+    f->g.n = n;
+    f->g.nh = nh;
+    f->g.KX = nh;
+    f->g.ncol = (int)col_i.size();
+    f->g.npw = (int)pt_k.size();
+    f->g.npw_pad = f->g.npw;
+    f->g.col_i = f->col_i;
+    f->g.col_j = f->col_j;
+    f->g.col_ptr = f->col_ptr;
+    f->g.pt_k = f->pt_k;
+    f->g.colidx = f->colidx;
+    f_ctx = std::move(f);
+    return CPSD_OK;
+}
+
+int fft_call(double *A, int *inc2c, int *inc3c, int *inc2r, int *inc3r, int *nx, int *ny, int *nz, int dir)
+{
+    if (!A || !nx || !ny || !nz || !inc2c || !inc3c || !inc2r || !inc3r) return CPSD_ERR_ARG;
+    const int n = *nx;
+    if (*ny != n || *nz != n) return CPSD_ERR_ARG;
+    const int nh = n / 2 + 1;
+    if (*inc2c != nh || *inc3c != nh * n || *inc2r != n + 2 || *inc3r != (n + 2) * n) return CPSD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(f_mu);
+    int rc = fft_setup(n);
+    if (rc) return rc;
+    FftCtx &f = *f_ctx;
+    cudaStream_t s = f.st;
+    const size_t bytes = sizeof(double) * f.n2ft3d;
+    if (cudaMemcpyAsync(f.buf, A, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return CPSD_ERR_CUDA;
+    const unsigned gb = (unsigned)((f.nfft3d + 255) / 256);
+    int ok = 0;
+    if (dir > 0) {  // cr_fft3b: half box -> real
+        perm_kernel<<<gb, 256, 0, s>>>(f.nfft3d, f.pt_idx, (const cx<double> *)f.buf, f.packed, 1);
+        rc = cpsd_fft_run_full(n, +1, f.g, f.grid, f.packed, f.Taux, s, nh, &ok);
+        if (rc) return rc;
+        copy_pad_kernel<<<(unsigned)((f.n2ft3d + 255) / 256), 256, 0, s>>>(n, f.grid, f.buf);
+    } else {  // rc_fft3f: real -> half box
+        unpad_real_kernel<<<(unsigned)((f.n3 + 255) / 256), 256, 0, s>>>(n, f.buf, f.grid);
+        rc = cpsd_fft_run_full(n, -1, f.g, f.grid, f.packed, f.Taux, s, nh, &ok);
+        if (rc) return rc;
+        perm_kernel<<<gb, 256, 0, s>>>(f.nfft3d, f.pt_idx, f.packed, (cx<double> *)f.buf, 0);
+    }
+    if (cudaGetLastError() != cudaSuccess) return CPSD_ERR_CUDA;
+    if (cudaMemcpyAsync(A, f.buf, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess) return CPSD_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return CPSD_ERR_CUDA;
+    return ok ? CPSD_OK : CPSD_ERR_GRID;
+}
+
+}  // namespace
+
+extern "C" void cr_fft3b_(double *A, int *inc2c, int *inc3c, int *inc2r, int *inc3r, int *nx, int *ny, int *nz,
+                          double *tmp, int *ntmp)
+{
+    (void)tmp;
+    (void)ntmp;
+    t_fft_status = fft_call(A, inc2c, inc3c, inc2r, inc3r, nx, ny, nz, +1);
+    if (t_fft_status) printf("cr_fft3b (B200): error %d: %s\n", t_fft_status, cpsd_gpu_strerror(t_fft_status));
+}
+
+extern "C" void rc_fft3f_(double *A, int *inc2c, int *inc3c, int *inc2r, int *inc3r, int *nx, int *ny, int *nz,
+                          double *tmp, int *ntmp)
+{
+    (void)tmp;
+    (void)ntmp;
+    t_fft_status = fft_call(A, inc2c, inc3c, inc2r, inc3r, nx, ny, nz, -1);
+    if (t_fft_status) printf("rc_fft3f (B200): error %d: %s\n", t_fft_status, cpsd_gpu_strerror(t_fft_status));
+}
+
+extern "C" int cpsd_gpu_fft_status(void) { return t_fft_status; }

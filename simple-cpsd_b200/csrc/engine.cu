@@ -1,0 +1,941 @@
+// engine.cu -- context, geometry, step orchestration and the C ABI of
+// include/cpsd_b200.h.  One context = one cell resident on one GPU; every SD
+// step is a fixed sequence of kernel launches on the context's stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "cpsd_b200.h"
+#include "fft.cuh"
+#include "kernels.cuh"
+
+namespace {
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) {                                   \
+            last_cuda_error() = e_;                                \
+            return CPSD_ERR_CUDA;                                  \
+        }                                                          \
+    } while (0)
+
+cudaError_t &last_cuda_error()
+{
+    static thread_local cudaError_t e = cudaSuccess;
+    return e;
+}
+
+inline long cdiv(long a, long b) { return (a + b - 1) / b; }
+
+// ------------------------------------------------------------ geometry
+struct HostGeom {
+    int n = 0, nh = 0, KX = 0, ncol = 0, npw = 0, npw_pad = 0;
+    std::vector<int> col_i, col_j, col_ptr, pt_k, pt_i, pt_j, pt_idx, colidx, inv_idx;
+    std::vector<double> w;
+};
+
+// Columns (kx, ky) holding mask points, ordered kx then ky; points ordered by
+// column then kz.  full=true takes every half-box point (no pruning).
+HostGeom build_geom(int n, const int *masker1, bool full)
+{
+    HostGeom h;
+    h.n = n;
+    h.nh = n / 2 + 1;
+    const long nfft3d = (long)h.nh * n * n;
+    h.inv_idx.assign(nfft3d, -1);
+    h.col_ptr.push_back(0);
+    for (int i = 0; i < h.nh; ++i)
+        for (int j = 0; j < n; ++j) {
+            int cnt = 0;
+            for (int k = 0; k < n; ++k) {
+                const long idx = i + (long)j * h.nh + (long)k * h.nh * n;
+                if (full || masker1[idx]) {
+                    h.inv_idx[idx] = (int)h.pt_k.size();
+                    h.pt_k.push_back(k);
+                    h.pt_i.push_back(i);
+                    h.pt_j.push_back(j);
+                    h.pt_idx.push_back((int)idx);
+                    h.w.push_back(i == 0 ? 1.0 : 2.0);
+                    ++cnt;
+                }
+            }
+            if (cnt) {
+                h.col_i.push_back(i);
+                h.col_j.push_back(j);
+                h.col_ptr.push_back((int)h.pt_k.size());
+                h.KX = std::max(h.KX, i + 1);
+            }
+        }
+    h.ncol = (int)h.col_i.size();
+    h.npw = (int)h.pt_k.size();
+    h.npw_pad = (int)cdiv(std::max(h.npw, 1), 32) * 32;
+    h.w.resize(h.npw_pad, 0.0);
+    h.colidx.assign((size_t)std::max(h.KX, 1) * n, -1);
+    for (int c = 0; c < h.ncol; ++c) h.colidx[(size_t)h.col_i[c] * n + h.col_j[c]] = c;
+    return h;
+}
+
+// ------------------------------------------------------------ device memory
+struct DevArena {
+    std::vector<void *> ptrs;
+    ~DevArena() { release(); }
+    void release()
+    {
+        for (void *p : ptrs) cudaFree(p);
+        ptrs.clear();
+    }
+    template <typename X>
+    cudaError_t alloc(X **p, size_t count)
+    {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(X));
+        if (e != cudaSuccess) return e;
+        ptrs.push_back(q);
+        *p = static_cast<X *>(q);
+        return cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(X));
+    }
+};
+
+template <typename X>
+cudaError_t upload(DevArena &ar, X **d, const std::vector<X> &h)
+{
+    cudaError_t e = ar.alloc(d, h.size());
+    if (e != cudaSuccess) return e;
+    if (h.empty()) return cudaSuccess;
+    return cudaMemcpy(*d, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice);
+}
+
+// ------------------------------------------------------------ transform engines
+struct FftOps {
+    virtual ~FftOps() = default;
+    virtual size_t elem() const = 0;
+    virtual int init(DevArena &ar, int KX) = 0;
+    virtual void inv_z(const Geom &g, const cx<double> *psi, long ldp, void *Tb, int nb, cudaStream_t s) = 0;
+    virtual void fwd_z_store(const Geom &g, const void *Tb, cx<double> *out, long ldo, double scale,
+                             int nb, cudaStream_t s) = 0;
+    virtual void fwd_z_sd(const Geom &g, const void *Tb, const ZEpilogue &e, int nb, cudaStream_t s) = 0;
+    virtual void plane(int mode, const Geom &g, void *Tb, const PlaneArgs &a, int nchunks, cudaStream_t s) = 0;
+};
+
+template <typename T, int NF>
+struct FftOpsT final : FftOps {
+    Twiddles<T> tw{};
+    int KX = 0;
+    size_t zsmem = 0;
+    size_t psmem[4] = {0, 0, 0, 0};
+
+    size_t elem() const override { return sizeof(cx<T>); }
+
+    static void fill(std::vector<cx<T>> &v, int N, int sign, int count)
+    {
+        for (int m = 0; m < count; ++m) {
+            long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)N;
+            v.push_back(cx<T>{(T)cosl(a), (T)(sign * sinl(a))});
+        }
+    }
+
+    int init(DevArena &ar, int kx) override
+    {
+        KX = kx;
+        constexpr int H = NF / 2;
+        std::vector<cx<T>> tab;
+        size_t o_ninv = tab.size();
+        fill(tab, NF, +1, NF);
+        size_t o_nfwd = tab.size();
+        fill(tab, NF, -1, NF);
+        size_t o_hinv = tab.size();
+        fill(tab, H, +1, H);
+        size_t o_hfwd = tab.size();
+        fill(tab, H, -1, H);
+        size_t o_rinv = tab.size();
+        fill(tab, NF, +1, H + 1);
+        size_t o_rfwd = tab.size();
+        fill(tab, NF, -1, H + 1);
+        cx<T> *d = nullptr;
+        CK(upload(ar, &d, tab));
+        tw.n_inv = d + o_ninv;
+        tw.n_fwd = d + o_nfwd;
+        tw.h_inv = d + o_hinv;
+        tw.h_fwd = d + o_hfwd;
+        tw.r_inv = d + o_rinv;
+        tw.r_fwd = d + o_rfwd;
+
+        using L = Line<NF>;
+        constexpr int P = L::P, CPB = kThreads / P;
+        constexpr int TILE = (CPB * (NF + 1) > NF * (CPB + 1)) ? CPB * (NF + 1) : NF * (CPB + 1);
+        zsmem = sizeof(cx<T>) * ((size_t)TILE + (size_t)CPB * L::XB);
+        int dev = 0, optin = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        CK(cudaFuncSetAttribute(inv_z_kernel<T, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem));
+        CK(cudaFuncSetAttribute(fwd_z_kernel<T, NF, ZEPI_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem));
+        CK(cudaFuncSetAttribute(fwd_z_kernel<T, NF, ZEPI_SD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem));
+        for (int m = 0; m < 4; ++m) psmem[m] = plane_smem_bytes<T, NF>(m, KX);
+        for (int m = 0; m < 4; ++m)
+            if ((int)psmem[m] > optin) psmem[m] = 0;  // mode unavailable for this sphere
+        if (psmem[PM_DENSITY])
+            CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem[PM_DENSITY]));
+        if (psmem[PM_APPLYV])
+            CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_APPLYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem[PM_APPLYV]));
+        if (psmem[PM_INVREAL])
+            CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_INVREAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem[PM_INVREAL]));
+        if (psmem[PM_FWDREAL])
+            CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_FWDREAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem[PM_FWDREAL]));
+        return CPSD_OK;
+    }
+
+    void inv_z(const Geom &g, const cx<double> *psi, long ldp, void *Tb, int nb, cudaStream_t s) override
+    {
+        constexpr int CPB = kThreads / Line<NF>::P;
+        dim3 grid((unsigned)cdiv(g.ncol, CPB), (unsigned)nb);
+        inv_z_kernel<T, NF><<<grid, kThreads, zsmem, s>>>(g, psi, ldp, (cx<T> *)Tb, tw);
+    }
+    void fwd_z_store(const Geom &g, const void *Tb, cx<double> *out, long ldo, double scale, int nb,
+                     cudaStream_t s) override
+    {
+        constexpr int CPB = kThreads / Line<NF>::P;
+        ZEpilogue e{};
+        e.out = out;
+        e.ldo = ldo;
+        e.scale = scale;
+        dim3 grid((unsigned)cdiv(g.ncol, CPB), (unsigned)nb);
+        fwd_z_kernel<T, NF, ZEPI_STORE><<<grid, kThreads, zsmem, s>>>(g, (const cx<T> *)Tb, e, tw);
+    }
+    void fwd_z_sd(const Geom &g, const void *Tb, const ZEpilogue &e, int nb, cudaStream_t s) override
+    {
+        constexpr int CPB = kThreads / Line<NF>::P;
+        dim3 grid((unsigned)cdiv(g.ncol, CPB), (unsigned)nb);
+        fwd_z_kernel<T, NF, ZEPI_SD><<<grid, kThreads, zsmem, s>>>(g, (const cx<T> *)Tb, e, tw);
+    }
+    void plane(int mode, const Geom &g, void *Tb, const PlaneArgs &a, int nchunks, cudaStream_t s) override
+    {
+        dim3 grid(NF, (unsigned)nchunks);
+        const int nt = plane_threads<T, NF>(mode);
+        switch (mode) {
+        case PM_DENSITY:
+            plane_kernel<T, NF, PM_DENSITY><<<grid, nt, psmem[mode], s>>>(g, (cx<T> *)Tb, a, tw);
+            break;
+        case PM_APPLYV:
+            plane_kernel<T, NF, PM_APPLYV><<<grid, nt, psmem[mode], s>>>(g, (cx<T> *)Tb, a, tw);
+            break;
+        case PM_INVREAL:
+            plane_kernel<T, NF, PM_INVREAL><<<grid, nt, psmem[mode], s>>>(g, (cx<T> *)Tb, a, tw);
+            break;
+        default:
+            plane_kernel<T, NF, PM_FWDREAL><<<grid, nt, psmem[mode], s>>>(g, (cx<T> *)Tb, a, tw);
+            break;
+        }
+    }
+    bool mode_ok(int mode) const { return psmem[mode] != 0; }
+};
+
+bool grid_supported(int n)
+{
+    return n == 16 || n == 24 || n == 32 || n == 48 || n == 64 || n == 128;
+}
+
+std::unique_ptr<FftOps> make_fft(int n)
+{
+    switch (n) {
+    case 16: return std::unique_ptr<FftOps>(new FftOpsT<double, 16>());
+    case 24: return std::unique_ptr<FftOps>(new FftOpsT<double, 24>());
+    case 32: return std::unique_ptr<FftOps>(new FftOpsT<double, 32>());
+    case 48: return std::unique_ptr<FftOps>(new FftOpsT<double, 48>());
+    case 64: return std::unique_ptr<FftOps>(new FftOpsT<double, 64>());
+    case 128: return std::unique_ptr<FftOps>(new FftOpsT<double, 128>());
+    default: return nullptr;
+    }
+}
+
+size_t plane_need(int n, int mode, int KX)
+{
+    switch (n) {
+    case 16: return plane_smem_bytes<double, 16>(mode, KX);
+    case 24: return plane_smem_bytes<double, 24>(mode, KX);
+    case 32: return plane_smem_bytes<double, 32>(mode, KX);
+    case 48: return plane_smem_bytes<double, 48>(mode, KX);
+    case 64: return plane_smem_bytes<double, 64>(mode, KX);
+    default: return plane_smem_bytes<double, 128>(mode, KX);
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ context
+struct cpsd_gpu_ctx {
+    cpsd_gpu_params prm{};
+    int n = 0, nh = 0, nb = 0, ne0 = 0, ne1 = 0, nion = 0, nkatm = 0, nsh = 0, ispin = 1;
+    long nfft3d = 0, n2ft3d = 0, n3 = 0;
+    double scal1 = 0, scal2 = 0, dv = 0, dte = 0;
+    cudaStream_t st = nullptr;
+    DevArena ar;
+    HostGeom hg;
+    Geom g{};
+    std::unique_ptr<FftOps> fft;
+    int npw = 0, npw_pad = 0, nproj = 0;
+    long ldc = 0;  // complex stride between bands
+    int nchunk0 = 0, nchunk1 = 0;
+    int gemm_splits_cap = 0;
+    size_t gemm_ws_elems = 0;
+    int launches_per_step = 0;
+    int lag_fail_total = 0;
+    bool tables_ok = false, state_ok = false, ran = false;
+
+    // device
+    int *pt_i = nullptr, *pt_j = nullptr, *pt_k = nullptr, *pt_idx = nullptr, *inv_idx = nullptr;
+    int *col_i = nullptr, *col_j = nullptr, *col_ptr = nullptr, *colidx = nullptr;
+    double *w = nullptr, *tg = nullptr, *vc = nullptr, *vg = nullptr, *vl = nullptr, *vnl = nullptr;
+    double *zv = nullptr, *rcell = nullptr, *unitg = nullptr, *vnlnrm_p = nullptr;
+    int *katm = nullptr, *lmmax = nullptr, *proj_off = nullptr;
+    cx<double> *cbuf[2] = {nullptr, nullptr};
+    int cur = 0;
+    cx<double> *cpsi = nullptr;
+    double *r1 = nullptr, *r2 = nullptr, *fion = nullptr;
+    void *Tb = nullptr, *Taux = nullptr;
+    double *rho_part = nullptr, *dn = nullptr, *xcp = nullptr, *xce = nullptr, *rfwd = nullptr, *Vr = nullptr;
+    cx<double> *dng = nullptr, *vall = nullptr, *sfac = nullptr, *Vg = nullptr, *proj = nullptr;
+    cx<double> *ex1 = nullptr, *ex2 = nullptr, *ex3 = nullptr;
+    double *beta = nullptr, *coefT = nullptr, *Mov = nullptr, *gws = nullptr, *lag = nullptr;
+    double *lmd = nullptr, *hml = nullptr, *Edev = nullptr, *red = nullptr;
+    int *chunk_dens = nullptr, *chunk_band = nullptr, *flags = nullptr;
+    double *full = nullptr;  // (ne0+ne1) * n2ft3d staging for host layout conversion
+    int pblocks = 0, bblocks = 0, gblocks = 0;
+    double *ppart = nullptr, *bpart = nullptr, *gpart = nullptr;
+};
+
+namespace {
+
+int gemm_tn(cpsd_gpu_ctx *c, int M, int N, int K, const double *A, long lda, const double *B, long ldb,
+            const double *w, double alpha, double beta, double *C, long ldc)
+{
+    if (M <= 0 || N <= 0) return CPSD_OK;
+    const long tiles = cdiv(M, GB) * cdiv(N, GB);
+    long splits = std::max<long>(1, cdiv(2 * 148, tiles));
+    splits = std::min<long>(splits, cdiv(K, GK));
+    splits = std::min<long>(splits, c->gemm_splits_cap);
+    while ((size_t)splits * M * N > c->gemm_ws_elems && splits > 1) --splits;
+    const int kchunk = (int)(cdiv(cdiv(K, splits), GK) * GK);
+    splits = cdiv(K, kchunk);
+    dim3 grid((unsigned)cdiv(M, GB), (unsigned)cdiv(N, GB), (unsigned)splits);
+    gemm_tn_w_kernel<<<grid, 256, 0, c->st>>>(M, N, K, A, lda, B, ldb, w, kchunk, c->gws);
+    splitk_reduce_kernel<<<(unsigned)cdiv((long)M * N, 256), 256, 0, c->st>>>(M, N, (int)splits, c->gws,
+                                                                              alpha, beta, C, ldc);
+    return CPSD_OK;
+}
+
+void gemm_nn(cpsd_gpu_ctx *c, int NJ, int K, int L, double alpha, const double *Mat, long ldm,
+             const double *B, long ldb, double beta, double *Out, long ldo)
+{
+    if (NJ <= 0 || L <= 0) return;
+    dim3 grid((unsigned)cdiv(K, GB), (unsigned)cdiv(NJ, GB));
+    gemm_nn_kernel<<<grid, 256, 0, c->st>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo);
+}
+
+const double *Mblk(cpsd_gpu_ctx *c, int ms, int which)
+{
+    // 4 overlap blocks per spin: 0 M22, 1 M21, 2 M11, 3 hml source
+    return c->Mov + ((long)ms * 4 + which) * (long)c->ne0 * c->ne0;
+}
+
+int one_step(cpsd_gpu_ctx *c)
+{
+    cudaStream_t s = c->st;
+    cx<double> *c1 = c->cbuf[c->cur], *c2 = c->cbuf[c->cur ^ 1];
+    const int K = 2 * c->npw_pad;
+    const long ldr = 2L * c->npw_pad;
+    CK(cudaMemcpyAsync(c->r1, c->r2, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToDevice, s));  // cpsd.c:174
+
+    // psi(G) -> psi(r) and the density, cpsd.c:177-194
+    c->fft->inv_z(c->g, c1, c->ldc, c->Tb, c->nb, s);
+    PlaneArgs pa{};
+    pa.chunk_b0 = c->chunk_dens;
+    pa.rho_part = c->rho_part;
+    c->fft->plane(PM_DENSITY, c->g, c->Tb, pa, c->nchunk0 + c->nchunk1, s);
+    XcArgs xa{c->n3, c->ispin, c->nchunk0, c->nchunk1, c->rho_part, c->scal1, c->scal2,
+              c->dn, c->xcp, c->xce, c->rfwd};
+    density_xc_kernel<<<(unsigned)cdiv(c->n3, 256), 256, 0, s>>>(xa);
+    // rho(G), cpsd.c:198-205
+    PlaneArgs pf{};
+    pf.rin = c->rfwd;
+    c->fft->plane(PM_FWDREAL, c->g, c->Taux, pf, 1, s);
+    c->fft->fwd_z_store(c->g, c->Taux, c->dng, c->ldc, 1.0, 1, s);
+    // phase factors, local psp, projectors, V(G): cpsd.c:208, 224-286, 373-379
+    if (c->nion > 0)
+        phase_tables_kernel<<<(unsigned)cdiv(3 * c->nion, 128), 128, 0, s>>>(c->nion, c->n, c->unitg, c->r1,
+                                                                              c->ex1, c->ex2, c->ex3);
+    VlocArgs va{};
+    va.npw = c->npw;
+    va.npw_pad = c->npw_pad;
+    va.n = c->n;
+    va.nh = c->nh;
+    va.nion = c->nion;
+    va.pt_i = c->pt_i;
+    va.pt_j = c->pt_j;
+    va.pt_k = c->pt_k;
+    va.katm = c->katm;
+    va.zv = c->zv;
+    va.ex1 = c->ex1;
+    va.ex2 = c->ex2;
+    va.ex3 = c->ex3;
+    va.vl = c->vl;
+    va.vnl = c->vnl;
+    va.lmmax = c->lmmax;
+    va.proj_off = c->proj_off;
+    va.vc = c->vc;
+    va.dng = c->dng;
+    va.scal2 = c->scal2;
+    va.s = c->sfac;
+    va.vall = c->vall;
+    va.Vg = c->Vg;
+    va.proj = c->proj;
+    vloc_proj_kernel<<<(unsigned)cdiv(c->npw_pad, 128), 128, 0, s>>>(va);
+    // V_loc + V_H to real space, plus xc per spin (cpsd.c:380-388)
+    c->fft->inv_z(c->g, c->Vg, c->ldc, c->Taux, 1, s);
+    PlaneArgs pv{};
+    pv.rout = c->Vr;
+    pv.xadd = c->xcp;
+    pv.nout = c->ispin;
+    c->fft->plane(PM_INVREAL, c->g, c->Taux, pv, 1, s);
+    // kinetic + nonlocal part of -H psi, cpsd.c:212-221, 287-290
+    kinetic_kernel<<<(unsigned)cdiv((long)c->nb * c->npw_pad, 256), 256, 0, s>>>(c->nb, c->npw_pad, c->ldc,
+                                                                                c->tg, c1, c2);
+    if (c->nproj > 0) {
+        int rc = gemm_tn(c, c->nproj, c->nb, K, (const double *)c->proj, ldr, (const double *)c1, ldr, c->w,
+                         1.0, 0.0, c->beta, c->nb);
+        if (rc) return rc;
+        kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, s>>>(
+            c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT);
+        gemm_nn(c, c->nb, K, c->nproj, 1.0, c->coefT, c->nproj, (const double *)c->proj, ldr, 1.0,
+                (double *)c2, ldr);
+    }
+    // (V + xc) psi back to G, -H psi and the SD step, cpsd.c:384-400
+    PlaneArgs pp{};
+    pp.chunk_b0 = c->chunk_band;
+    pp.V = c->Vr;
+    pp.ne0 = (c->ispin == 2) ? c->ne0 : c->nb;
+    c->fft->plane(PM_APPLYV, c->g, c->Tb, pp, c->nb, s);
+    ZEpilogue e{};
+    e.c2 = c2;
+    e.c1 = c1;
+    e.cpsi = c->cpsi;
+    e.ldc = c->ldc;
+    e.scal1 = c->scal1;
+    e.dte = c->dte;
+    c->fft->fwd_z_sd(c->g, c->Tb, e, c->nb, s);
+    // overlaps and Lagrange multipliers, cpsd.c:415-479
+    LagArgs la{};
+    la.ispin = c->ispin;
+    la.ne0 = c->ne0;
+    la.ne1 = c->ne1;
+    la.dte = c->dte;
+    const long ne02 = (long)c->ne0 * c->ne0;
+    for (int ms = 0; ms < c->ispin; ++ms) {
+        const int m = ms ? c->ne1 : c->ne0;
+        const long off = (long)(ms ? c->ne0 : 0) * ldr;
+        const double *C1 = (const double *)c1 + off, *C2 = (const double *)c2 + off;
+        int rc = gemm_tn(c, m, m, K, C2, ldr, C2, ldr, c->w, 1.0, 0.0, (double *)Mblk(c, ms, 0), m);
+        if (!rc) rc = gemm_tn(c, m, m, K, C2, ldr, C1, ldr, c->w, 1.0, 0.0, (double *)Mblk(c, ms, 1), m);
+        if (!rc) rc = gemm_tn(c, m, m, K, C1, ldr, C1, ldr, c->w, 1.0, 0.0, (double *)Mblk(c, ms, 2), m);
+        if (rc) return rc;
+        la.M22[ms] = Mblk(c, ms, 0);
+        la.M21[ms] = Mblk(c, ms, 1);
+        la.M11[ms] = Mblk(c, ms, 2);
+    }
+    la.s11 = c->lag;
+    la.s12 = c->lag + ne02;
+    la.s21 = c->lag + 2 * ne02;
+    la.s22 = c->lag + 3 * ne02;
+    la.st1 = c->lag + 4 * ne02;
+    la.X0 = c->lag + 5 * ne02;
+    la.X1 = c->lag + 6 * ne02;
+    la.lmd = c->lmd;
+    la.red = c->red;
+    la.fail = c->flags;
+    lagrange_kernel<<<kLagCluster, kLagThreads, 0, s>>>(la);
+    // constraint correction c2 += dte C1 lmd, cpsd.c:482-488
+    for (int ms = 0; ms < c->ispin; ++ms) {
+        const int m = ms ? c->ne1 : c->ne0;
+        const long off = (long)(ms ? c->ne0 : 0) * ldr;
+        gemm_nn(c, m, K, m, c->dte, c->lmd + ms * ne02, m, (const double *)c1 + off, ldr, 1.0,
+                (double *)c2 + off, ldr);
+    }
+    CK(cudaGetLastError());
+    c->cur ^= 1;
+    return CPSD_OK;
+}
+
+int energies(cpsd_gpu_ctx *c, int inner)
+{
+    cudaStream_t s = c->st;
+    const cx<double> *c2 = c->cbuf[c->cur], *c1 = c->cbuf[c->cur ^ 1];
+    const int K = 2 * c->npw_pad;
+    const long ldr = 2L * c->npw_pad;
+    FinalArgs fa{};
+    for (int ms = 0; ms < c->ispin; ++ms) {
+        const int m = ms ? c->ne1 : c->ne0;
+        const long off = (long)(ms ? c->ne0 : 0) * ldr;
+        int rc = gemm_tn(c, m, m, K, (const double *)c1 + off, ldr, (const double *)c->cpsi + off, ldr, c->w,
+                         1.0, 0.0, (double *)Mblk(c, ms, 3), m);
+        if (rc) return rc;
+        fa.Mh[ms] = Mblk(c, ms, 3);
+    }
+    packed_terms_kernel<<<c->pblocks, 256, 0, s>>>(c->npw, c->w, c->sfac, c->vg, c->dng, c->vc, c->vall,
+                                                   c->ppart);
+    band_terms_kernel<<<dim3(c->bblocks, c->nb), 256, 0, s>>>(c->npw, c->ldc, c->w, c->tg, c1, c2, c->bpart);
+    grid_terms_kernel<<<c->gblocks, 256, 0, s>>>(c->n3, c->ispin, c->dn, c->xce, c->xcp, c->gpart);
+    fa.ispin = c->ispin;
+    fa.ne0 = c->ne0;
+    fa.ne1 = c->ne1;
+    fa.nion = c->nion;
+    fa.nsh = c->nsh;
+    fa.nproj = c->nproj;
+    fa.nb = c->nb;
+    fa.inner = inner;
+    fa.pblocks = c->pblocks;
+    fa.bblocks = c->bblocks;
+    fa.gblocks = c->gblocks;
+    fa.ppart = c->ppart;
+    fa.bpart = c->bpart;
+    fa.gpart = c->gpart;
+    fa.hml = c->hml;
+    fa.beta = c->beta;
+    fa.vnlnrm_p = c->vnlnrm_p;
+    fa.r1 = c->r1;
+    fa.rcell = c->rcell;
+    fa.zv = c->zv;
+    fa.katm = c->katm;
+    fa.scal2 = c->scal2;
+    fa.omega = c->prm.omega;
+    fa.dv = c->dv;
+    fa.cewald = c->prm.cewald;
+    fa.rcut = c->prm.rcut;
+    fa.dt = c->prm.dt;
+    fa.dte = c->dte;
+    fa.E = c->Edev;
+    final_energy_kernel<<<1, 32, 0, s>>>(fa);
+    CK(cudaGetLastError());
+    return CPSD_OK;
+}
+
+}  // namespace
+
+// Full-box (unpruned) single-field transform used by the cr_fft3b_ /
+// rc_fft3f_ drop-ins (capi.cu): dir > 0 packed -> real grid, dir < 0 real
+// grid -> packed.  Engines are cached per (grid, device); callers serialise.
+int cpsd_fft_run_full(int n, int dir, const Geom &g, double *grid, cx<double> *packed, void *Taux,
+                      cudaStream_t st, int kx, int *ok)
+{
+    struct Cached {
+        int n, dev;
+        DevArena ar;
+        std::unique_ptr<FftOps> ops;
+        bool inv_ok, fwd_ok;
+    };
+    static std::vector<std::unique_ptr<Cached>> cache;
+    *ok = 0;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    Cached *e = nullptr;
+    for (auto &c : cache)
+        if (c->n == n && c->dev == dev) e = c.get();
+    if (!e) {
+        std::unique_ptr<Cached> c(new Cached());
+        c->n = n;
+        c->dev = dev;
+        c->ops = make_fft(n);
+        if (!c->ops) return CPSD_ERR_GRID;
+        int optin = 0;
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        c->inv_ok = (int)plane_need(n, PM_INVREAL, kx) <= optin;
+        c->fwd_ok = (int)plane_need(n, PM_FWDREAL, kx) <= optin;
+        int rc = c->ops->init(c->ar, kx);
+        if (rc) return rc;
+        e = c.get();
+        cache.push_back(std::move(c));
+    }
+    if (dir > 0) {
+        if (!e->inv_ok) return CPSD_ERR_GRID;
+        e->ops->inv_z(g, packed, g.npw, Taux, 1, st);
+        PlaneArgs pv{};
+        pv.rout = grid;
+        pv.nout = 1;
+        e->ops->plane(PM_INVREAL, g, Taux, pv, 1, st);
+    } else {
+        if (!e->fwd_ok) return CPSD_ERR_GRID;
+        PlaneArgs pf{};
+        pf.rin = grid;
+        e->ops->plane(PM_FWDREAL, g, Taux, pf, 1, st);
+        e->ops->fwd_z_store(g, Taux, packed, g.npw, 1.0, 1, st);
+    }
+    CK(cudaGetLastError());
+    *ok = 1;
+    return CPSD_OK;
+}
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char *cpsd_gpu_strerror(int status)
+{
+    switch (status) {
+    case CPSD_OK: return "ok";
+    case CPSD_ERR_CUDA: return cudaGetErrorString(last_cuda_error());
+    case CPSD_ERR_ARG: return "invalid argument";
+    case CPSD_ERR_GRID: return "unsupported FFT grid (nfft must be 16, 24, 32, 48, 64 or 128, and the sphere must fit the plane kernel)";
+    case CPSD_ERR_BANDS: return "more than 256 bands in a spin channel";
+    case CPSD_ERR_EMPTY_MASK: return "the cutoff mask selects no G vector";
+    case CPSD_ERR_UNMASKED_PSI: return "orbital coefficients outside the cutoff mask";
+    case CPSD_ERR_MOVE: return "ionic motion (move=1) is not available";
+    case CPSD_WARN_LAGRANGE: return "ierr=10: Lagrange-multiplier iteration did not converge in 30 steps";
+    default: return "unknown status";
+    }
+}
+
+int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx **out)
+{
+    if (!p || !masker1 || !out) return CPSD_ERR_ARG;
+    *out = nullptr;
+    if (!grid_supported(p->nfft)) return CPSD_ERR_GRID;
+    if (p->ispin != 1 && p->ispin != 2) return CPSD_ERR_ARG;
+    if (p->ne[0] < 1 || p->ne[1] < 0 || (p->ispin == 2 && p->ne[1] > p->ne[0])) return CPSD_ERR_ARG;
+    if (p->ispin == 1 && p->ne[1] != 0) return CPSD_ERR_ARG;
+    if (p->ne[0] > 256 || p->ne[1] > 256) return CPSD_ERR_BANDS;
+    if (p->nion < 0 || p->nkatm < 1 || p->nsh < 0 || p->omega <= 0 || p->fmass <= 0) return CPSD_ERR_ARG;
+    std::unique_ptr<cpsd_gpu_ctx> c(new cpsd_gpu_ctx());
+    c->prm = *p;
+    c->n = p->nfft;
+    c->nh = c->n / 2 + 1;
+    c->ispin = p->ispin;
+    c->ne0 = p->ne[0];
+    c->ne1 = p->ne[1];
+    c->nb = c->ne0 + c->ne1;
+    c->nion = p->nion;
+    c->nkatm = p->nkatm;
+    c->nsh = p->nsh;
+    c->nfft3d = (long)c->nh * c->n * c->n;
+    c->n2ft3d = 2 * c->nfft3d;
+    c->n3 = (long)c->n * c->n * c->n;
+    c->scal1 = 1.0 / ((double)c->n * c->n * c->n);
+    c->scal2 = 1.0 / p->omega;
+    c->dv = p->omega * c->scal1;
+    c->dte = p->dt / sqrt(p->fmass);
+    c->hg = build_geom(c->n, masker1, false);
+    HostGeom &h = c->hg;
+    if (h.npw == 0) return CPSD_ERR_EMPTY_MASK;
+    c->npw = h.npw;
+    c->npw_pad = h.npw_pad;
+    c->ldc = h.npw_pad;
+    CK(cudaSetDevice(p->device));
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    // the fused density plane must fit in shared memory
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
+    for (int m = 0; m < 4; ++m)
+        if ((int)plane_need(c->n, m, h.KX) > optin) return CPSD_ERR_GRID;
+    c->fft = make_fft(c->n);
+    if (!c->fft) return CPSD_ERR_GRID;
+    DevArena &ar = c->ar;
+    int rc = c->fft->init(ar, h.KX);
+    if (rc) return rc;
+    CK(upload(ar, &c->pt_i, h.pt_i));
+    CK(upload(ar, &c->pt_j, h.pt_j));
+    CK(upload(ar, &c->pt_k, h.pt_k));
+    CK(upload(ar, &c->pt_idx, h.pt_idx));
+    CK(upload(ar, &c->inv_idx, h.inv_idx));
+    CK(upload(ar, &c->col_i, h.col_i));
+    CK(upload(ar, &c->col_j, h.col_j));
+    CK(upload(ar, &c->col_ptr, h.col_ptr));
+    CK(upload(ar, &c->colidx, h.colidx));
+    CK(upload(ar, &c->w, h.w));
+    c->g.n = c->n;
+    c->g.nh = c->nh;
+    c->g.KX = h.KX;
+    c->g.ncol = h.ncol;
+    c->g.npw = h.npw;
+    c->g.npw_pad = h.npw_pad;
+    c->g.col_i = c->col_i;
+    c->g.col_j = c->col_j;
+    c->g.col_ptr = c->col_ptr;
+    c->g.pt_k = c->pt_k;
+    c->g.colidx = c->colidx;
+
+    const long P = c->npw_pad;
+    const int nb = c->nb, nkatm = c->nkatm, nion = c->nion;
+    CK(ar.alloc(&c->tg, P));
+    CK(ar.alloc(&c->vc, P));
+    CK(ar.alloc(&c->vg, P));
+    CK(ar.alloc(&c->vl, (size_t)nkatm * c->npw));
+    CK(ar.alloc(&c->vnl, (size_t)nkatm * 9 * c->npw));
+    CK(ar.alloc(&c->zv, nkatm));
+    CK(ar.alloc(&c->rcell, 3 * std::max(c->nsh, 1)));
+    CK(ar.alloc(&c->unitg, 9));
+    CK(ar.alloc(&c->katm, std::max(nion, 1)));
+    CK(ar.alloc(&c->lmmax, nkatm));
+    CK(ar.alloc(&c->proj_off, std::max(nion, 1)));
+    CK(ar.alloc(&c->cbuf[0], (size_t)nb * P));
+    CK(ar.alloc(&c->cbuf[1], (size_t)nb * P));
+    CK(ar.alloc(&c->cpsi, (size_t)nb * P));
+    CK(ar.alloc(&c->r1, 3 * std::max(nion, 1)));
+    CK(ar.alloc(&c->r2, 3 * std::max(nion, 1)));
+    CK(ar.alloc(&c->fion, 3 * std::max(nion, 1)));
+    const size_t tbytes = c->fft->elem() * (size_t)c->n * h.ncol;
+    {
+        unsigned char *t = nullptr;
+        CK(ar.alloc(&t, tbytes * nb));
+        c->Tb = t;
+        CK(ar.alloc(&t, tbytes));
+        c->Taux = t;
+    }
+    // density chunks: about two CTAs per SM over the z planes, never across spins
+    {
+        const int want = std::max(1, (int)cdiv(2 * 148, c->n));
+        c->nchunk0 = std::min(c->ne0, c->ispin == 2 ? std::max(1, want / 2) : want);
+        c->nchunk1 = (c->ispin == 2 && c->ne1 > 0) ? std::min(c->ne1, std::max(1, want / 2)) : 0;
+        std::vector<int> b0;
+        for (int q = 0; q <= c->nchunk0; ++q) b0.push_back((int)((long)c->ne0 * q / c->nchunk0));
+        for (int q = 1; q <= c->nchunk1; ++q) b0.push_back(c->ne0 + (int)((long)c->ne1 * q / c->nchunk1));
+        CK(upload(ar, &c->chunk_dens, b0));
+        std::vector<int> bb(nb + 1);
+        for (int b = 0; b <= nb; ++b) bb[b] = b;
+        CK(upload(ar, &c->chunk_band, bb));
+    }
+    CK(ar.alloc(&c->rho_part, (size_t)(c->nchunk0 + c->nchunk1) * c->n3));
+    CK(ar.alloc(&c->dn, (size_t)c->ispin * c->n3));
+    CK(ar.alloc(&c->xcp, (size_t)c->ispin * c->n3));
+    CK(ar.alloc(&c->xce, (size_t)c->n3));
+    CK(ar.alloc(&c->rfwd, (size_t)c->n3));
+    CK(ar.alloc(&c->Vr, (size_t)c->ispin * c->n3));
+    CK(ar.alloc(&c->dng, P));
+    CK(ar.alloc(&c->vall, P));
+    CK(ar.alloc(&c->sfac, P));
+    CK(ar.alloc(&c->Vg, P));
+    CK(ar.alloc(&c->ex1, (size_t)std::max(nion, 1) * c->nh));
+    CK(ar.alloc(&c->ex2, (size_t)std::max(nion, 1) * c->n));
+    CK(ar.alloc(&c->ex3, (size_t)std::max(nion, 1) * c->n));
+    const long ne02 = (long)c->ne0 * c->ne0;
+    CK(ar.alloc(&c->Mov, (size_t)8 * ne02));
+    CK(ar.alloc(&c->lag, (size_t)7 * ne02 + 1));
+    CK(ar.alloc(&c->lmd, (size_t)2 * ne02));
+    CK(ar.alloc(&c->hml, (size_t)2 * ne02));
+    CK(ar.alloc(&c->red, 2 * kLagCluster));
+    CK(ar.alloc(&c->Edev, 16));
+    CK(ar.alloc(&c->flags, 4));
+    c->gemm_splits_cap = 512;
+    c->gemm_ws_elems = (size_t)4 << 20;  // 32 MB of split-K partials
+    CK(ar.alloc(&c->gws, c->gemm_ws_elems));
+    c->pblocks = 148;
+    c->bblocks = (int)std::max<long>(1, std::min<long>(64, cdiv(c->npw, 256 * 8)));
+    c->gblocks = 296;
+    CK(ar.alloc(&c->ppart, 3 * c->pblocks));
+    CK(ar.alloc(&c->bpart, (size_t)2 * nb * c->bblocks));
+    CK(ar.alloc(&c->gpart, 2 * c->gblocks));
+    CK(ar.alloc(&c->full, (size_t)std::max(nb, c->ispin) * c->n2ft3d));
+    CK(cudaDeviceSynchronize());  // allocation memsets run on the legacy stream
+    *out = c.release();
+    return CPSD_OK;
+}
+
+int cpsd_gpu_set_scalars(cpsd_gpu_ctx *c, const double *unitg, double omega, double dt, double fmass,
+                         double cewald, double rcut)
+{
+    if (!c || !unitg || omega <= 0 || fmass <= 0) return CPSD_ERR_ARG;
+    memcpy(c->prm.unitg, unitg, sizeof(c->prm.unitg));
+    c->prm.omega = omega;
+    c->prm.dt = dt;
+    c->prm.fmass = fmass;
+    c->prm.cewald = cewald;
+    c->prm.rcut = rcut;
+    c->scal2 = 1.0 / omega;
+    c->dv = omega * c->scal1;
+    c->dte = dt / sqrt(fmass);
+    return CPSD_OK;
+}
+
+int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, const double *zv,
+                        const double *rcell, const double *G, const double *tg, const double *vc,
+                        const double *vg, const int *lmmax, const double *vnlnrm, const double *vl,
+                        const double *vnl)
+{
+    (void)amass;
+    (void)G;
+    if (!c || !zv || !tg || !vc || !vg || !lmmax || !vnlnrm || !vl || !vnl) return CPSD_ERR_ARG;
+    if (c->nion > 0 && (!katm || !rcell)) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    const HostGeom &h = c->hg;
+    const int nkatm = c->nkatm;
+    std::vector<double> ptg(c->npw_pad, 0.0), pvc(c->npw_pad, 0.0), pvg(c->npw_pad, 0.0);
+    for (int p = 0; p < c->npw; ++p) {
+        ptg[p] = tg[h.pt_idx[p]];
+        pvc[p] = vc[h.pt_idx[p]];
+        pvg[p] = vg[h.pt_idx[p]];
+    }
+    std::vector<double> pvl((size_t)nkatm * c->npw), pvnl((size_t)nkatm * 9 * c->npw, 0.0);
+    for (int ia = 0; ia < nkatm; ++ia) {
+        if (lmmax[ia] < 0 || lmmax[ia] > 9) return CPSD_ERR_ARG;
+        for (int p = 0; p < c->npw; ++p) pvl[(size_t)ia * c->npw + p] = vl[(size_t)ia * c->nfft3d + h.pt_idx[p]];
+        for (int l = 0; l < lmmax[ia]; ++l)
+            for (int p = 0; p < c->npw; ++p)
+                pvnl[((size_t)ia * 9 + l) * c->npw + p] = vnl[((size_t)ia * 9 + l) * c->nfft3d + h.pt_idx[p]];
+    }
+    std::vector<int> off(std::max(c->nion, 1), 0), hk(std::max(c->nion, 1), 0);
+    std::vector<double> pn;
+    int np = 0;
+    for (int ii = 0; ii < c->nion; ++ii) {
+        const int ia = katm[ii];
+        if (ia < 0 || ia >= nkatm) return CPSD_ERR_ARG;
+        hk[ii] = ia;
+        off[ii] = np;
+        for (int l = 0; l < lmmax[ia]; ++l) pn.push_back(vnlnrm[ia * 9 + l]);
+        np += lmmax[ia];
+    }
+    if (np != c->nproj || !c->proj) {
+        if (np > 0) {
+            CK(c->ar.alloc(&c->proj, (size_t)np * c->npw_pad));
+            CK(c->ar.alloc(&c->beta, (size_t)np * c->nb));
+            CK(c->ar.alloc(&c->coefT, (size_t)np * c->nb));
+            CK(c->ar.alloc(&c->vnlnrm_p, (size_t)np));
+        }
+        c->nproj = np;
+    }
+    CK(cudaMemcpy(c->tg, ptg.data(), sizeof(double) * c->npw_pad, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->vc, pvc.data(), sizeof(double) * c->npw_pad, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->vg, pvg.data(), sizeof(double) * c->npw_pad, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->vl, pvl.data(), sizeof(double) * pvl.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->vnl, pvnl.data(), sizeof(double) * pvnl.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->zv, zv, sizeof(double) * nkatm, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->lmmax, lmmax, sizeof(int) * nkatm, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->unitg, c->prm.unitg, sizeof(double) * 9, cudaMemcpyHostToDevice));
+    if (c->nion > 0) {
+        CK(cudaMemcpy(c->katm, hk.data(), sizeof(int) * c->nion, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->proj_off, off.data(), sizeof(int) * c->nion, cudaMemcpyHostToDevice));
+    }
+    if (c->nsh > 0) CK(cudaMemcpy(c->rcell, rcell, sizeof(double) * 3 * c->nsh, cudaMemcpyHostToDevice));
+    if (np > 0) CK(cudaMemcpy(c->vnlnrm_p, pn.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
+    CK(cudaDeviceSynchronize());
+    c->tables_ok = true;
+    return CPSD_OK;
+}
+
+int cpsd_gpu_set_state(cpsd_gpu_ctx *c, const double *c2, const double *r2)
+{
+    if (!c || !c2 || (c->nion > 0 && !r2)) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    cudaStream_t s = c->st;
+    CK(cudaMemcpyAsync(c->full, c2, sizeof(double) * c->nb * c->n2ft3d, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(c->flags + 1, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(c->cbuf[c->cur], 0, sizeof(cx<double>) * c->nb * c->npw_pad, s));
+    pack_kernel<<<(unsigned)cdiv((long)c->nb * c->nfft3d, 256), 256, 0, s>>>(
+        c->nb, c->nfft3d, c->ldc, c->npw, c->inv_idx, (const cx<double> *)c->full, c->cbuf[c->cur], c->flags + 1);
+    if (c->nion > 0) CK(cudaMemcpyAsync(c->r2, r2, sizeof(double) * 3 * c->nion, cudaMemcpyHostToDevice, s));
+    int outside = 0;
+    CK(cudaMemcpyAsync(&outside, c->flags + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (outside) return CPSD_ERR_UNMASKED_PSI;
+    c->state_ok = true;
+    return CPSD_OK;
+}
+
+int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae, double *deltac,
+                 double *deltar)
+{
+    if (!c || !E || inner < 1) return CPSD_ERR_ARG;
+    if (move) return CPSD_ERR_MOVE;
+    if (!c->tables_ok || !c->state_ok) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    cudaStream_t s = c->st;
+    CK(cudaMemsetAsync(c->flags, 0, sizeof(int), s));
+    CK(cudaMemcpyAsync(c->Edev, E, sizeof(double), cudaMemcpyHostToDevice, s));
+    for (int it = 0; it < inner; ++it) {
+        int rc = one_step(c);
+        if (rc) return rc;
+    }
+    int rc = energies(c, inner);
+    if (rc) return rc;
+    double Eh[16];
+    int fails = 0;
+    CK(cudaMemcpyAsync(Eh, c->Edev, sizeof(double) * 12, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&fails, c->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < 10; ++i) E[i] = Eh[i];
+    if (deltae) *deltae = Eh[10];
+    if (deltac) *deltac = Eh[11];
+    if (deltar) *deltar = 0.0;
+    c->lag_fail_total += fails;
+    c->ran = true;
+    return fails ? CPSD_WARN_LAGRANGE : CPSD_OK;
+}
+
+int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double *dn, double *hml,
+                       double *lmd, double *r1, double *r2, double *fion)
+{
+    if (!c) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    cudaStream_t s = c->st;
+    const size_t fullb = sizeof(double) * c->nb * c->n2ft3d;
+    const cx<double> *cc2 = c->cbuf[c->cur], *cc1 = c->cbuf[c->cur ^ 1];
+    if (!c->ran) cc1 = cc2;
+    const unsigned ub = (unsigned)cdiv((long)c->nb * c->npw, 256);
+    struct Out {
+        double *host;
+        const cx<double> *a, *sub;
+    } outs[3] = {{c1, cc1, nullptr}, {c2, cc2, nullptr}, {cpsi, cc2, cc1}};
+    for (auto &o : outs) {
+        if (!o.host) continue;
+        CK(cudaMemsetAsync(c->full, 0, fullb, s));
+        unpack_kernel<<<ub, 256, 0, s>>>(c->nb, c->npw, c->ldc, c->pt_idx, o.a, o.sub, (cx<double> *)c->full,
+                                         c->nfft3d);
+        CK(cudaMemcpyAsync(o.host, c->full, fullb, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    if (dn) {
+        const long tot = (long)c->ispin * c->n2ft3d;
+        pad_real_kernel<<<(unsigned)cdiv(tot, 256), 256, 0, s>>>(c->ispin, c->n, c->dn, c->full);
+        CK(cudaMemcpyAsync(dn, c->full, sizeof(double) * tot, cudaMemcpyDeviceToHost, s));
+    }
+    const long ne02 = (long)c->ne0 * c->ne0, ne12 = (long)c->ne1 * c->ne1;
+    if (hml) CK(cudaMemcpyAsync(hml, c->hml, sizeof(double) * (ne02 + ne12), cudaMemcpyDeviceToHost, s));
+    if (lmd) CK(cudaMemcpyAsync(lmd, c->lmd, sizeof(double) * (ne02 + ne12), cudaMemcpyDeviceToHost, s));
+    if (c->nion > 0) {
+        if (r1) CK(cudaMemcpyAsync(r1, c->r1, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
+        if (r2) CK(cudaMemcpyAsync(r2, c->r2, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
+    }
+    (void)fion;  // written only with move=1 (ccpsdv3/cpsd.c:246-364)
+    CK(cudaStreamSynchronize(s));
+    return CPSD_OK;
+}
+
+int cpsd_gpu_npw(const cpsd_gpu_ctx *c) { return c ? c->npw : 0; }
+
+int cpsd_gpu_launches_per_step(const cpsd_gpu_ctx *c)
+{
+    if (!c) return 0;
+    // inv_z, density plane, xc, fwd plane, fwd_z, phase, vloc, inv_z, inv plane,
+    // kinetic, [beta gemm + reduce, coef, nn gemm], applyV plane, fwd_z(SD),
+    // 3 overlap gemms (+reduce) per spin, lagrange, constraint gemm per spin
+    int n = 13 + 2 * 3 * c->ispin + 1 + c->ispin;
+    if (c->nproj > 0) n += 4;
+    return n;
+}
+
+int cpsd_gpu_lagrange_failures(cpsd_gpu_ctx *c) { return c ? c->lag_fail_total : 0; }
+
+void *cpsd_gpu_stream(cpsd_gpu_ctx *c) { return c ? (void *)c->st : nullptr; }
+
+void cpsd_gpu_destroy(cpsd_gpu_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->prm.device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    c->ar.release();
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+}  // extern "C"

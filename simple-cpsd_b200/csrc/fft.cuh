@@ -1,0 +1,383 @@
+// fft.cuh -- sphere-pruned batched 3-D transforms of the half box.
+//
+// Layouts (n = nfft, h = n/2, nh = h+1):
+//   packed   psi[b][p]      complex, p over the cutoff sphere ordered by
+//                           column (kx, ky) then kz (Geom)
+//   columns  T[b][z][c]     complex, after the kz transform: c over the
+//                           (kx, ky) columns that hold sphere points
+//   real     R[z][y][x]     double, x fastest (no padding)
+//
+// A transform G -> r is   inv_z (packed -> T)   then   plane (T -> real),
+// r -> G is               plane (real -> T)     then   fwd_z (T -> packed).
+// The plane kernel owns one z plane per CTA: it transforms the kx <= KX-1
+// lines along y in shared memory, then every x row (c2r / r2c by the
+// half-length complex trick), so the real-space plane never goes to HBM
+// unless asked.  Because the reference keeps psi, the density and every
+// potential masked to the same sphere (ccpsdv3/cpsd.c:205, 233), columns
+// outside the sphere are exact zeros and are skipped.
+//
+// Semantics match fftpack3d/fftpack3d.f: cr_fft3b drops Im(kx=0) and
+// Im(kx=n/2) before the x c2r (:86-89), rc_fft3f sets them to zero after the
+// x r2c (:157-161); both are unnormalised.
+#pragma once
+
+#include "common.cuh"
+
+struct Geom {
+    int n, nh, KX, ncol, npw, npw_pad;
+    const int *col_i, *col_j, *col_ptr;  // ncol, ncol, ncol+1
+    const int *pt_k;                     // npw
+    const int *colidx;                   // KX*n: column of (kx, y) or -1
+};
+
+template <typename T>
+struct Twiddles {
+    // W_N^m for the y/z length n and the half length h, both signs, and the
+    // real-transform factors e^{+-2 pi i k/n}, k <= h
+    const cx<T> *n_inv, *n_fwd, *h_inv, *h_fwd, *r_inv, *r_fwd;
+};
+
+constexpr int kThreads = 256;
+
+// ------------------------------------------------------------------ inv_z
+// packed psi (double) -> T (type T), one CTA = CPB columns of one band
+template <typename T, int NF>
+__global__ void __launch_bounds__(kThreads)
+inv_z_kernel(Geom g, const cx<double> *__restrict__ psi, long ldp, cx<T> *__restrict__ Tb,
+             Twiddles<T> tw)
+{
+    using L = Line<NF>;
+    constexpr int P = L::P, Q = L::Q, U = L::U, CPB = kThreads / P;
+    constexpr int RS = NF + 1, CS = CPB + 1;  // row / column strides of the tile
+    constexpr int TILE = (CPB * RS > NF * CS) ? CPB * RS : NF * CS;
+    extern __shared__ unsigned char smem_raw[];
+    cx<T> *tile = reinterpret_cast<cx<T> *>(smem_raw);
+    cx<T> *xb = tile + TILE;
+
+    const int b = blockIdx.y;
+    const int c0 = blockIdx.x * CPB;
+    const int grp = threadIdx.x / P, t = threadIdx.x % P;
+    const int c = c0 + grp;
+    cx<T> *row = tile + grp * RS;
+    for (int k = t; k < NF; k += P) row[k] = cx<T>{0, 0};
+    __syncwarp();
+    if (c < g.ncol) {
+        const cx<double> *src = psi + (long)b * ldp;
+        for (int p = g.col_ptr[c] + t; p < g.col_ptr[c + 1]; p += P) {
+            cx<double> vv = src[p];
+            row[g.pt_k[p]] = cx<T>{(T)vv.x, (T)vv.y};
+        }
+    }
+    __syncwarp();
+    cx<T> v[Q];
+#pragma unroll
+    for (int m = 0; m < Q; ++m) v[m] = row[L::in_index(t, m)];
+    line_fft<NF, +1, T>(v, t, xb + grp * L::XB, tw.n_inv);
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int s = 0; s < P; ++s) tile[L::out_index(t, u, s) * CS + grp] = v[u * P + s];
+    __syncthreads();
+    cx<T> *dst = Tb + (long)b * NF * g.ncol;
+    for (int idx = threadIdx.x; idx < NF * CPB; idx += kThreads) {
+        int z = idx / CPB, cl = idx % CPB;
+        if (c0 + cl < g.ncol) dst[(long)z * g.ncol + c0 + cl] = tile[z * CS + cl];
+    }
+}
+
+// ------------------------------------------------------------------ fwd_z
+enum { ZEPI_STORE = 0, ZEPI_SD = 1 };
+
+struct ZEpilogue {
+    // STORE: out[b*ldo + p] = scale * F
+    cx<double> *out;
+    long ldo;
+    double scale;
+    // SD (ccpsdv3/cpsd.c:394-400): cpsi = -scal1*F + c2; c2 = c1 + dte*cpsi
+    cx<double> *c2;        // in: kinetic + nonlocal part; out: steepest-descent iterate
+    const cx<double> *c1;
+    cx<double> *cpsi;
+    long ldc;
+    double scal1, dte;
+};
+
+template <typename T, int NF, int EPI>
+__global__ void __launch_bounds__(kThreads)
+fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
+{
+    using L = Line<NF>;
+    constexpr int P = L::P, Q = L::Q, U = L::U, CPB = kThreads / P;
+    constexpr int RS = NF + 1, CS = CPB + 1;
+    constexpr int TILE = (CPB * RS > NF * CS) ? CPB * RS : NF * CS;
+    extern __shared__ unsigned char smem_raw[];
+    cx<T> *tile = reinterpret_cast<cx<T> *>(smem_raw);
+    cx<T> *xb = tile + TILE;
+
+    const int b = blockIdx.y;
+    const int c0 = blockIdx.x * CPB;
+    const int grp = threadIdx.x / P, t = threadIdx.x % P;
+    const int c = c0 + grp;
+    const cx<T> *src = Tb + (long)b * NF * g.ncol;
+    for (int idx = threadIdx.x; idx < NF * CPB; idx += kThreads) {
+        int z = idx / CPB, cl = idx % CPB;
+        tile[z * CS + cl] = (c0 + cl < g.ncol) ? src[(long)z * g.ncol + c0 + cl] : cx<T>{0, 0};
+    }
+    __syncthreads();
+    cx<T> v[Q];
+#pragma unroll
+    for (int m = 0; m < Q; ++m) v[m] = tile[L::in_index(t, m) * CS + grp];
+    line_fft<NF, -1, T>(v, t, xb + grp * L::XB, tw.n_fwd);
+    __syncthreads();
+    cx<T> *row = tile + grp * RS;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int s = 0; s < P; ++s) row[L::out_index(t, u, s)] = v[u * P + s];
+    __syncwarp();
+    if (c < g.ncol) {
+        for (int p = g.col_ptr[c] + t; p < g.col_ptr[c + 1]; p += P) {
+            cx<T> F = row[g.pt_k[p]];
+            if constexpr (EPI == ZEPI_STORE) {
+                e.out[(long)b * e.ldo + p] = cx<double>{e.scale * (double)F.x, e.scale * (double)F.y};
+            } else {
+                long o = (long)b * e.ldc + p;
+                cx<double> c2k = e.c2[o], c1v = e.c1[o];
+                cx<double> cp{-e.scal1 * (double)F.x + c2k.x, -e.scal1 * (double)F.y + c2k.y};
+                e.cpsi[o] = cp;
+                e.c2[o] = cx<double>{c1v.x + e.dte * cp.x, c1v.y + e.dte * cp.y};
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ plane
+enum { PM_DENSITY = 0, PM_APPLYV = 1, PM_INVREAL = 2, PM_FWDREAL = 3 };
+
+struct PlaneArgs {
+    const int *chunk_b0;  // band range of blockIdx.y: [chunk_b0[y], chunk_b0[y+1])
+    double *rho_part;     // DENSITY: [chunk][z][y][x] sums of psi^2
+    const double *V;      // APPLYV: [ispin][z][y][x] total local potential
+    int ne0;              // bands b >= ne0 use V of spin 1
+    double *rout;         // INVREAL: rout[ms] = psi + xadd[ms], ms < nout
+    const double *xadd;
+    int nout;
+    const double *rin;    // FWDREAL: real input grid
+};
+
+template <int NF>
+struct PlaneShape {
+    static constexpr int H = NF / 2;
+    using LY = Line<NF>;
+    using LX = Line<H>;
+    static constexpr int XBMAX = (LY::XB > LX::XB) ? LY::XB : LX::XB;
+};
+
+template <typename T, int NF>
+__host__ __device__ constexpr int plane_threads(int mode)
+{
+    // the density plane (n x n doubles) needs the room of a second CTA at n=128
+    return (mode == PM_DENSITY && NF >= 128) ? 128 : kThreads;
+}
+
+template <typename T, int NF>
+size_t plane_smem_bytes(int mode, int KX)
+{
+    using S = PlaneShape<NF>;
+    int nt = plane_threads<T, NF>(mode);
+    int groups = nt / S::LX::P > nt / S::LY::P ? nt / S::LX::P : nt / S::LY::P;
+    size_t b = sizeof(cx<T>) * ((size_t)KX * (NF + 1) + (size_t)groups * S::XBMAX);
+    if (mode == PM_DENSITY) b += sizeof(double) * NF * NF;
+    return b;
+}
+
+template <typename T, int NF, int MODE>
+__global__ void __launch_bounds__(kThreads)
+plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
+{
+    using S = PlaneShape<NF>;
+    using LY = typename S::LY;
+    using LX = typename S::LX;
+    constexpr int H = S::H;
+    constexpr int NT = plane_threads<T, NF>(MODE);
+    constexpr int YS = NF + 1;  // Ybuf row stride
+    constexpr int PY = LY::P, QY = LY::Q, UY = LY::U, NGY = NT / PY;
+    constexpr int PX = LX::P, QX = LX::Q, UX = LX::U, NGX = NT / PX;
+    constexpr int NGMAX = NGX > NGY ? NGX : NGY;
+    extern __shared__ unsigned char smem_raw[];
+    const int KX = g.KX;
+    cx<T> *Y = reinterpret_cast<cx<T> *>(smem_raw);  // [KX][YS]
+    cx<T> *xball = Y + KX * YS;                       // [NGMAX][XBMAX]
+    double *RHO = reinterpret_cast<double *>(xball + NGMAX * S::XBMAX);  // [NF][NF]
+
+    const int z = blockIdx.x;
+    const int b0 = (MODE == PM_DENSITY || MODE == PM_APPLYV) ? a.chunk_b0[blockIdx.y] : 0;
+    const int b1 = (MODE == PM_DENSITY || MODE == PM_APPLYV) ? a.chunk_b0[blockIdx.y + 1] : 1;
+    const long plane = (long)NF * NF;
+
+    if constexpr (MODE == PM_DENSITY)
+        for (int i = threadIdx.x; i < NF * NF; i += NT) RHO[i] = 0.0;
+
+    const int gy = threadIdx.x / PY, ty = threadIdx.x % PY;
+    const int gx = threadIdx.x / PX, tx = threadIdx.x % PX;
+    cx<T> *xby = xball + gy * S::XBMAX;
+    cx<T> *xbx = xball + gx * S::XBMAX;
+
+    for (int b = b0; b < b1; ++b) {
+        cx<T> *Tplane = Tb + ((long)b * NF + z) * g.ncol;
+        // ---- inverse along y (columns -> lines kx < KX) ------------------
+        if constexpr (MODE != PM_FWDREAL) {
+            for (int base = 0; base < KX; base += NGY) {
+                const int i = base + gy;
+                const bool act = i < KX;
+                cx<T> v[QY];
+#pragma unroll
+                for (int m = 0; m < QY; ++m) {
+                    int c = act ? g.colidx[i * NF + LY::in_index(ty, m)] : -1;
+                    v[m] = (c >= 0) ? Tplane[c] : cx<T>{0, 0};
+                }
+                line_fft<NF, +1, T>(v, ty, xby, tw.n_inv);
+                if (act) {
+#pragma unroll
+                    for (int u = 0; u < UY; ++u)
+#pragma unroll
+                        for (int s = 0; s < PY; ++s) Y[i * YS + LY::out_index(ty, u, s)] = v[u * PY + s];
+                }
+            }
+            __syncthreads();
+        }
+        // ---- x rows --------------------------------------------------------
+        for (int base = 0; base < NF; base += NGX) {
+            const int j = base + gx;
+            const bool act = j < NF;
+            const int jj = act ? j : 0;
+            cx<T> v[QX];
+            if constexpr (MODE != PM_FWDREAL) {
+                // c2r pre-processing: Z_k = E_k + i O_k (half-length packing)
+#pragma unroll
+                for (int m = 0; m < QX; ++m) {
+                    const int k = LX::in_index(tx, m);
+                    const int kk = H - k;
+                    cx<T> xa = (k < KX) ? Y[k * YS + jj] : cx<T>{0, 0};
+                    cx<T> xc = (kk < KX) ? Y[kk * YS + jj] : cx<T>{0, 0};
+                    if (k == 0) {
+                        xa.y = 0;
+                        xc.y = 0;
+                    }
+                    cx<T> E = xa + conj(xc);
+                    cx<T> O = cmul(xa - conj(xc), tw.r_inv[k]);
+                    v[m] = cx<T>{E.x - O.y, E.y + O.x};
+                }
+                line_fft<H, +1, T>(v, tx, xbx, tw.h_inv);
+                // v[u*PX+s] = (psi(2m), psi(2m+1)), m = out_index
+                if constexpr (MODE == PM_DENSITY) {
+                    if (act) {
+#pragma unroll
+                        for (int u = 0; u < UX; ++u)
+#pragma unroll
+                            for (int s = 0; s < PX; ++s) {
+                                const int m = LX::out_index(tx, u, s);
+                                cx<T> w = v[u * PX + s];
+                                double *r = RHO + j * NF + 2 * m;
+                                r[0] += (double)w.x * (double)w.x;
+                                r[1] += (double)w.y * (double)w.y;
+                            }
+                    }
+                } else if constexpr (MODE == PM_INVREAL) {
+                    if (act) {
+#pragma unroll
+                        for (int u = 0; u < UX; ++u)
+#pragma unroll
+                            for (int s = 0; s < PX; ++s) {
+                                const int m = LX::out_index(tx, u, s);
+                                cx<T> w = v[u * PX + s];
+                                const long o = (long)z * plane + (long)j * NF + 2 * m;
+                                for (int ms = 0; ms < a.nout; ++ms) {
+                                    double *ro = a.rout + ms * NF * plane;
+                                    if (a.xadd) {
+                                        const double *xa = a.xadd + ms * NF * plane;
+                                        ro[o] = (double)w.x + xa[o];
+                                        ro[o + 1] = (double)w.y + xa[o + 1];
+                                    } else {
+                                        ro[o] = (double)w.x;
+                                        ro[o + 1] = (double)w.y;
+                                    }
+                                }
+                            }
+                    }
+                } else {  // APPLYV: multiply, then redistribute for the forward
+                    const double *V = a.V + ((b >= a.ne0) ? NF * plane : 0);
+#pragma unroll
+                    for (int u = 0; u < UX; ++u)
+#pragma unroll
+                        for (int s = 0; s < PX; ++s) {
+                            const int m = LX::out_index(tx, u, s);
+                            cx<T> w = v[u * PX + s];
+                            const long o = (long)z * plane + (long)jj * NF + 2 * m;
+                            xbx[m] = cx<T>{(T)((double)w.x * V[o]), (T)((double)w.y * V[o + 1])};
+                        }
+                    __syncwarp();
+#pragma unroll
+                    for (int m = 0; m < QX; ++m) v[m] = xbx[LX::in_index(tx, m)];
+                    __syncwarp();
+                }
+            } else {  // FWDREAL: load the real row directly in DIT order
+                const double *r = a.rin + (long)z * plane + (long)jj * NF;
+#pragma unroll
+                for (int m = 0; m < QX; ++m) {
+                    const int mm = LX::in_index(tx, m);
+                    v[m] = cx<T>{(T)r[2 * mm], (T)r[2 * mm + 1]};
+                }
+            }
+            if constexpr (MODE == PM_APPLYV || MODE == PM_FWDREAL) {
+                line_fft<H, -1, T>(v, tx, xbx, tw.h_fwd);
+#pragma unroll
+                for (int u = 0; u < UX; ++u)
+#pragma unroll
+                    for (int s = 0; s < PX; ++s) xbx[LX::out_index(tx, u, s)] = v[u * PX + s];
+                __syncwarp();
+                // r2c post-processing for the kx < KX that are kept
+                for (int k = tx; k < KX; k += PX) {
+                    cx<T> zk = xbx[k % H];
+                    cx<T> zc = conj(xbx[(H - k) % H]);
+                    cx<T> E = (T)0.5 * (zk + zc);
+                    cx<T> D = (T)0.5 * (zk - zc);
+                    cx<T> O{D.y, -D.x};
+                    cx<T> X = E + cmul(tw.r_fwd[k], O);
+                    if (k == 0 || k == H) X.y = 0;
+                    if (act) Y[k * YS + j] = X;
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // ---- forward along y, keep the columns -----------------------------
+        if constexpr (MODE == PM_APPLYV || MODE == PM_FWDREAL) {
+            for (int base = 0; base < KX; base += NGY) {
+                const int i = base + gy;
+                const bool act = i < KX;
+                const int ii = act ? i : 0;
+                cx<T> v[QY];
+#pragma unroll
+                for (int m = 0; m < QY; ++m) v[m] = Y[ii * YS + LY::in_index(ty, m)];
+                line_fft<NF, -1, T>(v, ty, xby, tw.n_fwd);
+                // each group reads and rewrites only its own line
+                if (act) {
+#pragma unroll
+                    for (int u = 0; u < UY; ++u)
+#pragma unroll
+                        for (int s = 0; s < PY; ++s) Y[i * YS + LY::out_index(ty, u, s)] = v[u * PY + s];
+                }
+            }
+            __syncthreads();
+            for (int c = threadIdx.x; c < g.ncol; c += NT) Tplane[c] = Y[g.col_i[c] * YS + g.col_j[c]];
+            __syncthreads();
+        }
+    }
+
+    if constexpr (MODE == PM_DENSITY) {
+        __syncthreads();
+        double *dst = a.rho_part + ((long)blockIdx.y * NF + z) * plane;
+        for (int i = threadIdx.x; i < NF * NF; i += NT) dst[i] = RHO[i];
+    }
+}

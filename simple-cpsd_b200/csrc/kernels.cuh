@@ -1,0 +1,779 @@
+// kernels.cuh -- pointwise, reduction, GEMM and Lagrange kernels of one SD step.
+//
+// Every routine cites the reference lines (ccpsdv3/, Simple-CPSD) whose
+// arithmetic it carries.  Complex arrays are cx<double>; packed arrays run
+// over the cutoff sphere (see fft.cuh), real grids over n^3 points.
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+
+namespace cg = cooperative_groups;
+
+// ------------------------------------------------------------ reductions
+template <int NT>
+CPSD_D double block_sum(double v, double *sh)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < NT / 32; ++i) r += sh[i];
+    return r;  // valid in thread 0
+}
+
+// ------------------------------------------------------------ phase factors
+// ccpsdv3/strfac.c:10-77: ex_d[k] = e^{-i k (b_d . r + pi)} by recurrence,
+// negative k mirrored as conjugates (ex2, ex3), Nyquist entry zeroed.
+// ex1: [nion][nh], ex2/ex3: [nion][n]
+__global__ void phase_tables_kernel(int nion, int n, const double *__restrict__ unitg,
+                                    const double *__restrict__ r1, cx<double> *ex1,
+                                    cx<double> *ex2, cx<double> *ex3)
+{
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= 3 * nion) return;
+    const int ii = id / 3, d = id % 3;
+    const double pi = 3.14159265358979323846;  // 4 atan(1), strfac's pi argument
+    const double sw = unitg[3 * d] * r1[3 * ii] + unitg[3 * d + 1] * r1[3 * ii + 1] +
+                      unitg[3 * d + 2] * r1[3 * ii + 2] + pi;
+    const double cr = cos(sw), ci = -sin(sw);
+    const int h = n / 2;
+    cx<double> *e = (d == 0) ? ex1 + (long)ii * (h + 1) : ((d == 1) ? ex2 : ex3) + (long)ii * n;
+    e[0] = cx<double>{1.0, 0.0};
+    cx<double> p{1.0, 0.0};
+    for (int k = 1; k <= h; ++k) {
+        cx<double> q{p.x * cr - p.y * ci, p.x * ci + p.y * cr};
+        e[k] = q;
+        if (d > 0) e[n - k] = cx<double>{q.x, -q.y};
+        p = q;
+    }
+    e[h] = cx<double>{0.0, 0.0};
+}
+
+// exi(G) = ex1[i] (ex2[j] ex3[k]) in the reference's multiplication order, strfac.c:112-115
+CPSD_D cx<double> strfac_point(cx<double> e1, cx<double> e2, cx<double> e3)
+{
+    double tr = e2.x * e3.x - e2.y * e3.y;
+    double ti = e2.x * e3.y + e2.y * e3.x;
+    return cx<double>{e1.x * tr - e1.y * ti, e1.y * tr + e1.x * ti};
+}
+
+// ------------------------------------------------------------ local psp, projectors
+// ccpsdv3/cpsd.c:224-245 (s, vall), :260-286 (projectors), :373-379 (V(G))
+struct VlocArgs {
+    int npw, npw_pad, n, nh, nion;
+    const int *pt_i, *pt_j, *pt_k;
+    const int *katm;
+    const double *zv;
+    const cx<double> *ex1, *ex2, *ex3;
+    const double *vl;   // [nkatm][npw]
+    const double *vnl;  // [nkatm][9][npw]
+    const int *lmmax;   // [nkatm]
+    const int *proj_off;  // [nion] first projector row of each ion
+    const double *vc;   // [npw]
+    const cx<double> *dng;
+    double scal2;
+    cx<double> *s, *vall, *Vg;
+    cx<double> *proj;   // [nproj][npw_pad]
+};
+
+__global__ void vloc_proj_kernel(VlocArgs a)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.npw_pad) return;
+    if (p >= a.npw) {  // keep the GEMM padding at zero
+        for (int ii = 0; ii < a.nion; ++ii) {
+            const int nl = a.lmmax[a.katm[ii]];
+            for (int l = 0; l < nl; ++l) a.proj[(long)(a.proj_off[ii] + l) * a.npw_pad + p] = cx<double>{0, 0};
+        }
+        return;
+    }
+    const int i = a.pt_i[p], j = a.pt_j[p], k = a.pt_k[p];
+    cx<double> s{0, 0}, vall{0, 0};
+    for (int ii = 0; ii < a.nion; ++ii) {
+        const int ia = a.katm[ii];
+        cx<double> exi = strfac_point(a.ex1[(long)ii * a.nh + i], a.ex2[(long)ii * a.n + j],
+                                      a.ex3[(long)ii * a.n + k]);
+        const double z = a.zv[ia];
+        s.x += z * exi.x;
+        s.y += z * exi.y;
+        const double v = a.vl[(long)ia * a.npw + p];
+        vall.x += exi.x * v;
+        vall.y += exi.y * v;
+        const int nl = a.lmmax[ia];
+        for (int l = 0; l < nl; ++l) {
+            const double w = a.vnl[((long)ia * 9 + l) * a.npw + p];
+            cx<double> chi = (l == 0 || l >= 4) ? cx<double>{exi.x * w, exi.y * w}
+                                                : cx<double>{-exi.y * w, exi.x * w};
+            a.proj[(long)(a.proj_off[ii] + l) * a.npw_pad + p] = chi;
+        }
+    }
+    a.s[p] = s;
+    a.vall[p] = vall;
+    const double vc = a.vc[p];
+    const cx<double> d = a.dng[p];
+    a.Vg[p] = cx<double>{vall.x * a.scal2 + d.x * vc, vall.y * a.scal2 + d.y * vc};
+}
+
+// kinetic part of -H psi: c2 = -tg c1, ccpsdv3/cpsd.c:212-221
+__global__ void kinetic_kernel(int nb, int npw_pad, long ldc, const double *__restrict__ tg,
+                               const cx<double> *__restrict__ c1, cx<double> *__restrict__ c2)
+{
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (long)nb * npw_pad) return;
+    const int b = (int)(id / npw_pad), p = (int)(id % npw_pad);
+    const double t = tg[p];
+    cx<double> v = c1[(long)b * ldc + p];
+    c2[(long)b * ldc + p] = cx<double>{-t * v.x, -t * v.y};
+}
+
+// coefficients of the KB back-projection, ccpsdv3/cpsd.c:289:
+// coefT[b][P] = -beta[P][b] * scal2 / vnlnrm[P]
+__global__ void kb_coef_kernel(int nproj, int nb, const double *__restrict__ beta,
+                               const double *__restrict__ vnlnrm_p, double scal2,
+                               double *__restrict__ coefT)
+{
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nproj * nb) return;
+    const int P = id / nb, b = id % nb;
+    coefT[(long)b * nproj + P] = -beta[id] * scal2 / vnlnrm_p[P];
+}
+
+// ------------------------------------------------------------ density + xc
+// dn_ms = scal2 * sum_b psi_b^2 (cpsd.c:185-194); Dirac exchange then Vosko
+// correlation (dirac_exchange.c:64-126, vosko.c:99-167); the forward-FFT
+// input (dn_0 + dn_{ispin-1}) * scal1 (cpsd.c:198-199).
+struct XcArgs {
+    long n3;
+    int ispin;
+    int nchunk0, nchunk1;  // chunks of spin 0, then of spin 1
+    const double *part;    // [nchunk][n3]
+    double scal1, scal2;
+    double *dn, *xcp, *xce, *rfwd;
+};
+
+CPSD_D void dirac_vosko(int ispin, double nup_in, double ndn_in, double rho0, double rho1,
+                        double &vx0, double &vx1, double &ex)
+{
+    // --- Dirac exchange, alpha = 2/3 (dirac_exchange.c:14-24, 84-122)
+    const double alpha = 0.6666666666666666667;
+    const double onethird_d = 0.33333333333333333333;
+    const double fourthird_d = 1.33333333333333333333;
+    const double two_to_onethird_d = 1.25992104989487319067;
+    const double A_d = 0.25992104989487319067;
+    const double pi_d = 3.14159265358979311600;
+    if (ispin == 1) {
+        const double n = nup_in + nup_in;
+        const double n13 = pow(3.0 * n / pi_d, onethird_d);
+        ex = -(9.0 / 8.0) * alpha * n13;
+        vx0 = -(3.0 / 2.0) * alpha * n13;
+        vx1 = vx0;
+    } else {
+        const double n = nup_in + ndn_in;
+        const double n13 = pow(3.0 * n / pi_d, onethird_d);
+        // the reference's xi here uses the first two density values (dirac_exchange.c:101)
+        const double xi = (n > 0.0) ? (rho0 - rho1) / n : 1.0;
+        const double ex_p = -(9.0 / 8.0) * alpha * n13;
+        const double ux_p = -(3.0 / 2.0) * alpha * n13;
+        const double ex_f = two_to_onethird_d * ex_p;
+        const double ux_f = fourthird_d * ex_f;
+        const double f = (pow(1.0 + xi, fourthird_d) + pow(1.0 - xi, fourthird_d) - 2.0) / (2.0 * A_d);
+        const double df = fourthird_d * (pow(1.0 + xi, onethird_d) - pow(1.0 - xi, onethird_d)) / (2.0 * A_d);
+        ex = ex_p + f * (ex_f - ex_p);
+        vx0 = ux_p + f * (ux_f - ux_p) + (+1.0 - xi) * (df * (ex_f - ex_p));
+        vx1 = ux_p + f * (ux_f - ux_p) + (-1.0 - xi) * (df * (ex_f - ex_p));
+    }
+    // --- Vosko-Wilk-Nusair, the reference's parameter table (vosko.c:22-57)
+    const double bp = 3.727440e+00, bf = 7.060420e+00;
+    const double cp = 1.293520e+01, cf = 1.805780e+01;
+    const double cp1 = 3.109070e-02, cf1 = 1.554530e-02;
+    const double cp2 = 9.690228e-04, cf2 = 2.247860e-03;
+    const double cp3 = 1.049800e-01, cf3 = 3.250000e-01;
+    const double cp4 = 3.878329e-02, cf4 = 5.249122e-02;
+    const double cp5 = 3.075995e+00, cf5 = 2.365463e+00;
+    const double cp6 = 1.863720e+00, cf6 = 3.530210e+00;
+    const double dp1 = 6.218140e-02, df1 = 3.109060e-02;
+    const double dp2 = 1.938045e-03, df2 = 4.495720e-03;
+    const double dp4 = -3.205972e-02, df4 = -1.779316e-02;
+    const double dp5 = -1.192972e-01, df5 = -1.241661e-01;
+    const double dp6 = 1.863720e+00, df6 = 3.530210e+00;
+    const double dp7 = 9.461748e+00, df7 = 5.595417e+00;
+    const double small_number = 1.0e-30;
+    const double onesixth = 0.166666666666667;
+    const double onethird = 0.333333333333333;
+    const double fourthird = 1.333333333333333;
+    const double A = 0.259921049894873;
+    const double rs_scale = 0.620350490899400;
+    const double nup = nup_in + small_number;
+    const double ndown = ((ispin == 1) ? nup_in : ndn_in) + small_number;
+    const double n = nup + ndown;
+    const double rs = rs_scale / pow(n, onethird);
+    const double xi = (nup - ndown) / n;
+    const double x = sqrt(rs);
+    const double xxp = rs + bp * x + cp;
+    const double dxxp = 2.0 * x + bp;
+    const double ec_p = cp1 * log(rs / xxp) + cp2 * log((x + cp3) * (x + cp3) / xxp) + cp4 * atan(cp5 / (x + cp6));
+    const double uc_p = ec_p - onesixth * x * (dp1 / x + dp2 / (x + cp3) + dp4 * dxxp / xxp +
+                                               dp5 / ((x + dp6) * (x + dp6) + dp7));
+    const double xxf = rs + bf * x + cf;
+    const double dxxf = 2.0 * x + bf;
+    const double ec_f = cf1 * log(rs / xxf) + cf2 * log((x + cf3) * (x + cf3) / xxf) + cf4 * atan(cf5 / (x + cf6));
+    const double uc_f = ec_f - onesixth * x * (df1 / x + df2 / (x + cf3) + df4 * dxxf / xxf +
+                                               df5 / ((x + df6) * (x + df6) + df7));
+    const double f = (pow(1.0 + xi, fourthird) + pow(1.0 - xi, fourthird) - 2.0) / (2.0 * A);
+    const double df = fourthird * (pow(1.0 + xi, onethird) - pow(1.0 - xi, onethird)) / (2.0 * A);
+    ex += ec_p + f * (ec_f - ec_p);
+    vx0 += uc_p + f * (uc_f - uc_p) + (+1.0 - xi) * (df * (ec_f - ec_p));
+    if (ispin == 2) vx1 += uc_p + f * (uc_f - uc_p) + (-1.0 - xi) * (df * (ec_f - ec_p));
+}
+
+__global__ void density_xc_kernel(XcArgs a)
+{
+    const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.n3) return;
+    double d[2] = {0.0, 0.0}, r0 = 0.0, r1 = 0.0;
+    for (int c = 0; c < a.nchunk0; ++c) {
+        d[0] += a.part[(long)c * a.n3 + r];
+        if (a.ispin == 2) {
+            r0 += a.part[(long)c * a.n3 + 0];
+            r1 += a.part[(long)c * a.n3 + 1];
+        }
+    }
+    for (int c = a.nchunk0; c < a.nchunk0 + a.nchunk1; ++c) d[1] += a.part[(long)c * a.n3 + r];
+    d[0] *= a.scal2;
+    d[1] *= a.scal2;
+    r0 *= a.scal2;
+    r1 *= a.scal2;
+    double vx0, vx1, ex;
+    dirac_vosko(a.ispin, d[0], d[1], r0, r1, vx0, vx1, ex);
+    a.dn[r] = d[0];
+    a.xcp[r] = vx0;
+    a.xce[r] = ex;
+    if (a.ispin == 2) {
+        a.dn[a.n3 + r] = d[1];
+        a.xcp[a.n3 + r] = vx1;
+    }
+    a.rfwd[r] = (d[0] + d[a.ispin - 1]) * a.scal1;
+}
+
+// ------------------------------------------------------------ FP64 GEMMs
+// part[split][i][j] = sum_{k in chunk} w(k) A[i*lda+k] B[j*ldb+k]; K counts
+// reals, the weight is per complex pair (w[k/2]); the Gamma-point dot of
+// ccpsdv3/gcdotc.c as a matrix product.
+constexpr int GB = 64, GK = 16;
+
+__global__ void __launch_bounds__(256)
+gemm_tn_w_kernel(int M, int N, int K, const double *__restrict__ A, long lda,
+                 const double *__restrict__ B, long ldb, const double *__restrict__ w, int kchunk,
+                 double *__restrict__ part)
+{
+    __shared__ double As[GK][GB + 1], Bs[GK][GB + 1];
+    const int i0 = blockIdx.x * GB, j0 = blockIdx.y * GB;
+    const int k0 = blockIdx.z * kchunk;
+    const int k1 = min(K, k0 + kchunk);
+    const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
+    double acc[4][4] = {};
+    for (int kk = k0; kk < k1; kk += GK) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = tid + 256 * q;
+            const int row = e / GK, kl = e % GK;
+            const int k = kk + kl;
+            double av = 0.0, bv = 0.0;
+            if (k < k1) {
+                if (i0 + row < M) av = A[(long)(i0 + row) * lda + k] * (w ? w[k >> 1] : 1.0);
+                if (j0 + row < N) bv = B[(long)(j0 + row) * ldb + k];
+            }
+            As[kl][row] = av;
+            Bs[kl][row] = bv;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kl = 0; kl < GK; ++kl) {
+            double a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a[r] = As[kl][ty + 16 * r];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) b[c] = Bs[kl][tx + 16 * c];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        }
+        __syncthreads();
+    }
+    double *out = part + (long)blockIdx.z * M * N;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int i = i0 + ty + 16 * r, j = j0 + tx + 16 * c;
+            if (i < M && j < N) out[(long)i * N + j] = acc[r][c];
+        }
+}
+
+// C[i*ldc+j] = alpha * sum_s part[s][i][j] (+ beta C), summed in split order
+__global__ void splitk_reduce_kernel(int M, int N, int splits, const double *__restrict__ part,
+                                     double alpha, double beta, double *C, long ldc)
+{
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= M * N) return;
+    double s = 0.0;
+    for (int q = 0; q < splits; ++q) s += part[(long)q * M * N + id];
+    const int i = id / N, j = id % N;
+    double *c = C + (long)i * ldc + j;
+    *c = alpha * s + (beta == 0.0 ? 0.0 : beta * *c);
+}
+
+// Out[j*ldo+k] = beta*Out + alpha * sum_l Mat[l + j*ldm] * B[l*ldb + k]
+// (the reference's dgemm('N','N') on column-major psi blocks, cpsd.c:483-488)
+__global__ void __launch_bounds__(256)
+gemm_nn_kernel(int NJ, int K, int L, double alpha, const double *__restrict__ Mat, long ldm,
+               const double *__restrict__ B, long ldb, double beta, double *__restrict__ Out, long ldo)
+{
+    __shared__ double Ms[GK][GB + 1], Bs[GK][GB + 1];
+    const int k0 = blockIdx.x * GB, j0 = blockIdx.y * GB;
+    const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
+    double acc[4][4] = {};
+    for (int l0 = 0; l0 < L; l0 += GK) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = tid + 256 * q;
+            {  // Mat tile: l fastest
+                const int jj = e / GK, ll = e % GK;
+                const int l = l0 + ll, j = j0 + jj;
+                Ms[ll][jj] = (l < L && j < NJ) ? Mat[l + (long)j * ldm] : 0.0;
+            }
+            {  // B tile: k fastest
+                const int ll = e / GB, kk = e % GB;
+                const int l = l0 + ll, k = k0 + kk;
+                Bs[ll][kk] = (l < L && k < K) ? B[(long)l * ldb + k] : 0.0;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ll = 0; ll < GK; ++ll) {
+            double a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a[r] = Ms[ll][ty + 16 * r];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) b[c] = Bs[ll][tx + 16 * c];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int j = j0 + ty + 16 * r, k = k0 + tx + 16 * c;
+            if (j < NJ && k < K) {
+                double *o = Out + (long)j * ldo + k;
+                *o = alpha * acc[r][c] + (beta == 0.0 ? 0.0 : beta * *o);
+            }
+        }
+}
+
+// ------------------------------------------------------------ Lagrange multipliers
+// ccpsdv3/cpsd.c:415-479.  One cluster of kLagCluster CTAs per launch; CTA r
+// owns a contiguous range of columns.  Overlaps come in row-major from the
+// GEMMs: M22[i][j] = <c2_i|c2_j>, M21[i][j] = <c2_i|c1_j>, M11[i][j] = <c1_i|c1_j>.
+constexpr int kLagCluster = 8;
+constexpr int kLagThreads = 256;
+constexpr int kLagMaxPerThread = 32;  // m*ceil(m/8)/256 <= 32  ->  m <= 256
+
+struct LagArgs {
+    int ispin, ne0, ne1;
+    double dte;
+    const double *M22[2], *M21[2], *M11[2];
+    double *s11, *s12, *s21, *s22, *st1, *X0, *X1;  // ne0^2 each, column-major
+    double *lmd;                                     // [ms*ne0^2 + i + j*m]
+    double *red;                                     // [kLagCluster][2]
+    int *fail;                                       // steps whose iteration did not converge
+};
+
+__global__ void __cluster_dims__(kLagCluster, 1, 1) __launch_bounds__(kLagThreads)
+lagrange_kernel(LagArgs a)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int tid = threadIdx.x;
+    __shared__ double shv[kLagThreads / 32];
+    __shared__ int shi[kLagThreads / 32];
+    const long ne02 = (long)a.ne0 * a.ne0;
+    for (int ms = 0; ms < a.ispin; ++ms) {
+        const int m = ms ? a.ne1 : a.ne0;
+        const long kk = (long)m * m;
+        if (m == 0) continue;
+        const double *M22 = a.M22[ms], *M21 = a.M21[ms], *M11 = a.M11[ms];
+        const double dte = a.dte;
+        // s matrices, cpsd.c:420-437 (upper triangles mirrored as the reference does)
+        for (long e = (long)rank * kLagThreads + tid; e < kk; e += (long)kLagCluster * kLagThreads) {
+            const int i = (int)(e % m), j = (int)(e / m);
+            double v22, v21, v12, v11;
+            if (i == j) {
+                v22 = (1.0 - M22[(long)i * m + i]) * 0.5 / dte;
+                v21 = (1.0 - M21[(long)i * m + i]) * 0.5;
+                v12 = v21;
+                v11 = -M11[(long)i * m + i] * 0.5 * dte;
+            } else {
+                const int lo = i < j ? i : j, hi = i < j ? j : i;
+                v22 = -M22[(long)lo * m + hi] * 0.5 / dte;
+                v21 = -M21[(long)lo * m + hi] * 0.5;   // <c2_lo|c1_hi>
+                v12 = -M21[(long)hi * m + lo] * 0.5;   // <c1_lo|c2_hi>
+                v11 = -M11[(long)lo * m + hi] * 0.5 * dte;
+            }
+            a.s22[e] = v22;
+            a.s21[e] = v21;
+            a.s12[e] = v12;
+            a.s11[e] = v11;
+            a.X0[e] = v22;  // sa0 = s22, cpsd.c:441
+        }
+        cl.sync();
+        // my columns
+        const int per = (m + kLagCluster - 1) / kLagCluster;
+        const int jb = rank * per, je = min(m, jb + per);
+        const int mine = (je > jb) ? (je - jb) * m : 0;
+        double *cur = a.X0, *nxt = a.X1;
+        double keep[kLagMaxPerThread];
+        bool done = false;
+        int iter = 0;
+        while (!done && iter < 30) {
+            ++iter;
+            // sa1 = s22 + s21 sa0 + sa0 s12 ; st1 = s11 sa0   (cpsd.c:444-462)
+            int q = 0;
+            for (int e = tid; e < mine; e += kLagThreads, ++q) {
+                const int i = e % m, j = jb + e / m;
+                double t1 = 0.0, t2 = 0.0, t3 = 0.0;
+                for (int l = 0; l < m; ++l) {
+                    const double c_lj = cur[l + (long)j * m];
+                    t1 = fma(a.s21[i + (long)l * m], c_lj, t1);
+                    t2 = fma(cur[i + (long)l * m], a.s12[l + (long)j * m], t2);
+                    t3 = fma(a.s11[i + (long)l * m], c_lj, t3);
+                }
+                double sa1 = t1 + a.s22[i + (long)j * m];
+                sa1 = t2 + sa1;
+                keep[q] = sa1;
+                a.st1[i + (long)j * m] = t3;
+            }
+            __syncthreads();
+            // sa1 += sa0 st1 (cpsd.c:463-468); st1 = sa1 - sa0 (:469-470)
+            q = 0;
+            double bestv = -1.0;
+            int besti = 0x7fffffff;
+            for (int e = tid; e < mine; e += kLagThreads, ++q) {
+                const int i = e % m, j = jb + e / m;
+                double t4 = 0.0;
+                for (int l = 0; l < m; ++l) t4 = fma(cur[i + (long)l * m], a.st1[l + (long)j * m], t4);
+                keep[q] = t4 + keep[q];
+            }
+            __syncthreads();
+            q = 0;
+            for (int e = tid; e < mine; e += kLagThreads, ++q) {
+                const int i = e % m, j = jb + e / m;
+                const long f = i + (long)j * m;
+                nxt[f] = keep[q];
+                const double d = keep[q] - cur[f];
+                a.st1[f] = d;
+                const double ad = fabs(d);
+                if (ad > bestv || (ad == bestv && f < besti)) {
+                    bestv = ad;
+                    besti = (int)f;
+                }
+            }
+            // block argmax (first index of the largest |st1|, as idamax)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                double ov = __shfl_xor_sync(0xffffffffu, bestv, o);
+                int oi = __shfl_xor_sync(0xffffffffu, besti, o);
+                if (ov > bestv || (ov == bestv && oi < besti)) {
+                    bestv = ov;
+                    besti = oi;
+                }
+            }
+            if ((tid & 31) == 0) {
+                shv[tid >> 5] = bestv;
+                shi[tid >> 5] = besti;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                for (int w = 1; w < kLagThreads / 32; ++w)
+                    if (shv[w] > bestv || (shv[w] == bestv && shi[w] < besti)) {
+                        bestv = shv[w];
+                        besti = shi[w];
+                    }
+                a.red[2 * rank] = bestv;
+                a.red[2 * rank + 1] = (double)besti;
+            }
+            cl.sync();
+            // every CTA reduces the cluster's candidates in the same order
+            double gv = -1.0;
+            long gi = 0x7fffffff;
+            for (int r = 0; r < kLagCluster; ++r) {
+                const double v = a.red[2 * r];
+                const long ix = (long)a.red[2 * r + 1];
+                if (v > gv || (v == gv && ix < gi)) {
+                    gv = v;
+                    gi = ix;
+                }
+            }
+            // the reference reads st1 at idamax's 1-based result (cpsd.c:471):
+            // the element after the largest; past the end of st1 lies sa1
+            const long nx = gi + 1;
+            const double adiff = fabs(nx < ne02 ? a.st1[nx] : nxt[nx - ne02]);
+            done = adiff < 1e-15;
+            cl.sync();
+            if (!done) {
+                double *t = cur;
+                cur = nxt;
+                nxt = t;
+            }
+        }
+        if (!done && rank == 0 && tid == 0) atomicAdd(a.fail, 1);
+        // lmd = sa1, cpsd.c:478
+        for (int e = tid; e < mine; e += kLagThreads) {
+            const int i = e % m, j = jb + e / m;
+            a.lmd[ms * ne02 + i + (long)j * m] = nxt[i + (long)j * m];
+        }
+        cl.sync();
+    }
+}
+
+// ------------------------------------------------------------ energies
+// per-block partial sums over packed points of the three single-field terms
+// (cpsd.c:520-526 k-space Ewald, :548-554 Hartree, :590 local)
+__global__ void packed_terms_kernel(int npw, const double *__restrict__ w, const cx<double> *__restrict__ s,
+                                    const double *__restrict__ vg, const cx<double> *__restrict__ dng,
+                                    const double *__restrict__ vc, const cx<double> *__restrict__ vall,
+                                    double *part)
+{
+    __shared__ double sh[32];
+    double e0 = 0, e1 = 0, e2 = 0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npw; p += gridDim.x * blockDim.x) {
+        const double ww = w[p];
+        const cx<double> sv = s[p], d = dng[p], va = vall[p];
+        e0 += ww * (sv.x * sv.x + sv.y * sv.y) * vg[p];
+        e1 += ww * (d.x * d.x + d.y * d.y) * vc[p];
+        e2 += ww * (va.x * d.x + va.y * d.y);
+    }
+    double r0 = block_sum<256>(e0, sh);
+    double r1 = block_sum<256>(e1, sh);
+    double r2 = block_sum<256>(e2, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = r0;
+        part[gridDim.x + blockIdx.x] = r1;
+        part[2 * gridDim.x + blockIdx.x] = r2;
+    }
+}
+
+// per band: eke_b = sum w tg |c1|^2 (cpsd.c:574-586), dc_b = sum w |c2-c1|^2 (:650-659)
+__global__ void band_terms_kernel(int npw, long ldc, const double *__restrict__ w,
+                                  const double *__restrict__ tg, const cx<double> *__restrict__ c1,
+                                  const cx<double> *__restrict__ c2, double *part /* [2][nb][blocks] */)
+{
+    __shared__ double sh[32];
+    const int b = blockIdx.y;
+    const cx<double> *a = c1 + (long)b * ldc, *c = c2 + (long)b * ldc;
+    double ek = 0, dc = 0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npw; p += gridDim.x * blockDim.x) {
+        const double ww = w[p];
+        const cx<double> x = a[p], y = c[p];
+        ek += ww * tg[p] * (x.x * x.x + x.y * x.y);
+        const double dx = y.x - x.x, dy = y.y - x.y;
+        dc += ww * (dx * dx + dy * dy);
+    }
+    double r0 = block_sum<256>(ek, sh);
+    double r1 = block_sum<256>(dc, sh);
+    if (threadIdx.x == 0) {
+        part[(long)b * gridDim.x + blockIdx.x] = r0;
+        part[((long)gridDim.y + b) * gridDim.x + blockIdx.x] = r1;
+    }
+}
+
+// exc, pxc partial sums over the real grid (cpsd.c:557-570)
+__global__ void grid_terms_kernel(long n3, int ispin, const double *__restrict__ dn,
+                                  const double *__restrict__ xce, const double *__restrict__ xcp,
+                                  double *part)
+{
+    __shared__ double sh[32];
+    double ex = 0, px = 0;
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n3; r += (long)gridDim.x * blockDim.x) {
+        const double d0 = dn[r];
+        ex += d0 * xce[r];
+        px += d0 * xcp[r];
+        if (ispin == 2) {
+            const double d1 = dn[n3 + r];
+            ex += d1 * xce[r];
+            px += d1 * xcp[n3 + r];
+        }
+    }
+    double r0 = block_sum<256>(ex, sh);
+    double r1 = block_sum<256>(px, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = r0;
+        part[gridDim.x + blockIdx.x] = r1;
+    }
+}
+
+// hml from M[i][j] = <c1_i|cpsi_j> (row-major per spin), with the reference's
+// mirroring and eorbit reads (cpsd.c:497-515); one thread.
+struct FinalArgs {
+    int ispin, ne0, ne1, nion, nsh, nproj, nb, inner;
+    int pblocks, bblocks, gblocks;
+    const double *ppart, *bpart, *gpart;
+    const double *Mh[2];
+    double *hml;
+    const double *beta, *vnlnrm_p;
+    const double *r1, *rcell, *zv;
+    const int *katm;
+    double scal2, omega, dv, cewald, rcut, dt, dte;
+    double *E;  // in: E[0] previous energy; out: E[0..9], E[10] deltae, E[11] deltac
+};
+
+__global__ void final_energy_kernel(FinalArgs a)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const long ne02 = (long)a.ne0 * a.ne0;
+    // hml and eorbit
+    double eorbit = 0.0;
+    for (int ms = 0; ms < a.ispin; ++ms) {
+        const int m = ms ? a.ne1 : a.ne0;
+        double *H = a.hml + ms * ne02;
+        const double *M = a.Mh[ms];
+        for (int i = 0; i < m; ++i) {
+            H[i + i * m] = -M[(long)i * m + i];
+            eorbit += a.hml[i + i * m];
+            for (int j = i + 1; j < m; ++j) {
+                H[i + j * m] = -M[(long)i * m + j];
+                H[j + i * m] = a.hml[i + j * m];
+            }
+        }
+    }
+    if (a.ispin == 1) eorbit *= 2;
+    // single-field packed terms
+    double t[3] = {0, 0, 0};
+    for (int q = 0; q < 3; ++q)
+        for (int k = 0; k < a.pblocks; ++k) t[q] += a.ppart[q * a.pblocks + k];
+    double eion = t[0] * 0.5 * a.scal2 + a.cewald;
+    // real-space Ewald, cpsd.c:527-545 (A&S 7.1.28 erfc, cpsd.c:11-17)
+    const double B1 = 0.0705230784, B2 = 0.0422820123, B3 = 0.0092705272;
+    const double B4 = 0.0001520143, B5 = 0.0002765672, B6 = 0.0000430638;
+    for (int ii = 0; ii < a.nion; ++ii)
+        for (int jj = ii + 1; jj < a.nion; ++jj) {
+            const double dx = a.r1[3 * ii] - a.r1[3 * jj];
+            const double dy = a.r1[1 + 3 * ii] - a.r1[1 + 3 * jj];
+            const double dz = a.r1[2 + 3 * ii] - a.r1[2 + 3 * jj];
+            const double zz = a.zv[a.katm[ii]] * a.zv[a.katm[jj]];
+            for (int l = 0; l < a.nsh; ++l) {
+                const double x = a.rcell[l] + dx, y = a.rcell[l + a.nsh] + dy, z = a.rcell[l + 2 * a.nsh] + dz;
+                const double r = sqrt(x * x + y * y + z * z);
+                const double w = r / a.rcut;
+                const double aa = (1.0 + w * (B1 + w * (B2 + w * (B3 + w * (B4 + w * (B5 + w * B6))))));
+                const double erfc = 1.0 / (aa * aa * aa * aa);
+                eion += zz * (erfc * erfc * erfc * erfc) / r;
+            }
+        }
+    const double ehartr = t[1] * a.omega * 0.5;
+    const double elocal = t[2];
+    // xc
+    double exc = 0.0, pxc = 0.0;
+    for (int k = 0; k < a.gblocks; ++k) exc += a.gpart[k];
+    for (int k = 0; k < a.gblocks; ++k) pxc += a.gpart[a.gblocks + k];
+    if (a.ispin == 1) {
+        exc += exc;
+        pxc += pxc;
+    }
+    exc *= a.dv;
+    pxc *= a.dv;
+    // kinetic
+    double eke = 0.0;
+    for (int b = 0; b < a.nb; ++b) {
+        double s = 0.0;
+        for (int k = 0; k < a.bblocks; ++k) s += a.bpart[(long)b * a.bblocks + k];
+        eke += s;
+    }
+    if (a.ispin == 1) eke = 2 * eke;
+    // nonlocal from the last step's projections, cpsd.c:593-634
+    double enl = 0.0;
+    for (int P = 0; P < a.nproj; ++P)
+        for (int b = 0; b < a.nb; ++b) {
+            const double sw = a.beta[(long)P * a.nb + b];
+            enl += sw * sw * a.scal2 / a.vnlnrm_p[P];
+        }
+    if (a.ispin == 1) enl = 2 * enl;
+    // deltac
+    double dc = 0.0;
+    for (int b = 0; b < a.nb; ++b) {
+        double s = 0.0;
+        for (int k = 0; k < a.bblocks; ++k) s += a.bpart[((long)a.nb + b) * a.bblocks + k];
+        if (s > dc) dc = s;
+    }
+    const double eold = a.E[0];
+    a.E[0] = eorbit + eion + exc - ehartr - pxc;
+    a.E[1] = eorbit;
+    a.E[2] = ehartr;
+    a.E[3] = exc;
+    a.E[4] = eion;
+    a.E[5] = eke;
+    a.E[6] = elocal;
+    a.E[7] = enl;
+    a.E[8] = 2.0 * ehartr;
+    a.E[9] = pxc;
+    a.E[10] = (a.E[0] - eold) / (a.dt * a.inner);
+    a.E[11] = dc / a.dte;
+}
+
+// ------------------------------------------------------------ layout conversion
+// packed <-> reference half box: full[b][2*idx] <- packed[b][p]
+__global__ void unpack_kernel(int nb, int npw, long ldp, const int *__restrict__ pt_idx,
+                              const cx<double> *__restrict__ a, const cx<double> *__restrict__ sub,
+                              cx<double> *__restrict__ full, long nfft3d)
+{
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (long)nb * npw) return;
+    const int b = (int)(id / npw), p = (int)(id % npw);
+    cx<double> v = a[(long)b * ldp + p];
+    if (sub) {
+        cx<double> u = sub[(long)b * ldp + p];
+        v = cx<double>{v.x - u.x, v.y - u.y};
+    }
+    full[(long)b * nfft3d + pt_idx[p]] = v;
+}
+
+// gather packed from the half box; count entries outside the sphere that are not zero
+__global__ void pack_kernel(int nb, long nfft3d, long ldp, int npw, const int *__restrict__ inv_idx,
+                            const cx<double> *__restrict__ full, cx<double> *__restrict__ packed,
+                            int *outside)
+{
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (long)nb * nfft3d) return;
+    const int b = (int)(id / nfft3d);
+    const long g = id % nfft3d;
+    const cx<double> v = full[id];
+    const int p = inv_idx[g];
+    if (p >= 0)
+        packed[(long)b * ldp + p] = v;
+    else if (v.x != 0.0 || v.y != 0.0)
+        atomicAdd(outside, 1);
+}
+
+// real grid [ms][z][y][x] -> reference padded layout [ms][z][y][x(n+2)] with zero pads
+__global__ void pad_real_kernel(int nsets, int n, const double *__restrict__ src, double *__restrict__ dst)
+{
+    const long n2r = (long)(n + 2) * n * n;
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (long)nsets * n2r) return;
+    const int ms = (int)(id / n2r);
+    const long r = id % n2r;
+    const int x = (int)(r % (n + 2));
+    const long yz = r / (n + 2);
+    dst[id] = (x < n) ? src[(long)ms * n * n * n + yz * n + x] : 0.0;
+}

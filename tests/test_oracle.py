@@ -1,0 +1,174 @@
+"""The oracle, pinned: FFT restatement vs numpy, tables vs the reference's
+own code and its one numeric pin, the cpsd() restatement vs the golden
+vectors generated by the reference build (tests/golden/make_golden.py)."""
+import json
+import sys
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, REPO
+from cpsd_b200 import configs, inputs
+
+import oracle
+
+CASES = {
+    "small_h2_16": (lambda: configs.small_h2(16), 3, 2),
+    "small_diamond_24": (lambda: configs.small_diamond(24, 4), 3, 2),
+    "small_diamond_32": (lambda: configs.small_diamond(32, 5, ecut=25.0), 2, 2),
+    "small_diamond_48": (lambda: configs.small_diamond(48, 6, ecut=30.0), 2, 2),
+    "h2_dimer_32": (lambda: configs.h2_dimer_32(), 200, 1),
+    "diamond8_64": (lambda: configs.diamond8_64(), 4, 2),
+}
+E_TOL = 1e-9  # Ha, total energy parity bar
+
+
+@pytest.mark.parametrize("n", [8, 12, 16, 24, 32, 48, 64])
+def test_fft_restatement_matches_numpy(restatement, n):
+    """cr_fft3b/rc_fft3f restatement == pocketfft up to rounding (fftpack3d.f:22-196)."""
+    rng = np.random.default_rng(n)
+    nh = n // 2 + 1
+    x = rng.standard_normal((n, n, n))
+    A = np.zeros((n, n, n + 2))
+    A[:, :, :n] = x
+    A = A.reshape(-1).copy()
+    restatement.rc_fft3f(A, n)
+    ref = np.fft.rfftn(x)
+    got = A.view(np.complex128).reshape(n, n, nh)
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
+    C = rng.standard_normal((n, n, nh)) + 1j * rng.standard_normal((n, n, nh))
+    B = np.ascontiguousarray(C).view(np.float64).reshape(-1).copy()
+    restatement.cr_fft3b(B, n)
+    refi = np.fft.irfftn(C, s=(n, n, n), axes=(0, 1, 2)) * n ** 3
+    got = B.reshape(n, n, n + 2)
+    assert np.abs(got[:, :, :n] - refi).max() <= 1e-13 * np.abs(refi).max()
+    assert np.all(got[:, :, n:] == 0.0)  # pad zeroed, fftpack3d.f:90-91
+
+
+def test_fft_roundtrip_is_n_cubed(restatement):
+    n = 24
+    rng = np.random.default_rng(1)
+    A = np.zeros((n, n, n + 2))
+    A[:, :, :n] = rng.standard_normal((n, n, n))
+    x0 = A.copy()
+    A = A.reshape(-1)
+    restatement.rc_fft3f(A, n)
+    restatement.cr_fft3b(A, n)
+    assert np.allclose(A.reshape(n, n, n + 2)[:, :, :n], n ** 3 * x0[:, :, :n], rtol=0, atol=1e-10)
+
+
+def test_masker_pins_nwave_8932():
+    """The reference's only numeric pin: NWAVE=8932 for the 32^3 SC examples
+    (Example0-double-serial/aimd.h:1), i.e. get_masker at the grid cutoff."""
+    for a in (20.0, 26.0):
+        _, _, unitg = inputs.get_cube(1, a)
+        h = 16
+        gcut = (unitg[0] * h) ** 2 + (unitg[1] * h) ** 2 + (unitg[2] * h) ** 2
+        assert int(inputs.get_masker(32, gcut, unitg).sum()) == 8932
+
+
+def test_workload_sphere_sizes():
+    """npw of the named workloads (half sphere, get_masker loop bounds)."""
+    got = {}
+    for name in ("h2_dimer_32", "diamond8_64"):
+        spec = configs.NAMED[name]()
+        _, _, unitg = inputs.get_cube(1, spec.unit)
+        got[name] = int(inputs.get_masker(spec.nfft, spec.ecut_ry, unitg).sum())
+    assert got == {"h2_dimer_32": 10924, "diamond8_64": 2483}
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REFERENCE_SO), reason="reference build absent")
+def test_tables_match_reference_functions():
+    """inputs.py get_cube/get_g/get_masker == the reference's C (bit for bit)."""
+    ref = oracle.ReferenceBuild()
+    for icube, a in ((1, 20.0), (1, 10.26), (2, 12.0), (3, 9.0)):
+        v, ua, ug = ref.get_cube(icube, a)
+        v2, ua2, ug2 = inputs.get_cube(icube, a)
+        assert v == v2 and np.array_equal(ua, ua2) and np.array_equal(ug, ug2)
+        for n in (16, 24, 32):
+            assert np.array_equal(ref.get_g(n, ug), inputs.get_g(n, ug2))
+            for cut in (5.0, 12.0, 40.0):
+                assert np.array_equal(ref.get_masker(n, cut, ug), inputs.get_masker(n, cut, ug2))
+
+
+def test_inputs_match_fixture_digests():
+    """The seeded inputs are the ones the fixtures were generated from."""
+    sys.path.insert(0, GOLDEN)
+    from make_golden import input_digest  # noqa: E402
+    with open(os.path.join(GOLDEN, "inputs.json")) as f:
+        want = json.load(f)
+    for name, (mk, _, _) in CASES.items():
+        assert input_digest(inputs.build_inputs(mk())) == want[name], name
+
+
+def test_orbitals_orthonormal_and_hermitian():
+    inp = inputs.build_inputs(configs.small_diamond(24, 4))
+    nh = inp.nfft // 2 + 1
+    w = inputs.gamma_weights(inp.nfft)
+    C = inp.c2.reshape(inp.nbands, -1).view(np.complex128)
+    S = np.einsum("p,ap,bp->ab", w, C.conj(), C).real
+    assert np.allclose(S, np.eye(inp.nbands), atol=1e-13)
+    partner = inputs.hermitian_partner(inp.nfft)
+    plane = np.arange(inp.nfft3d)[::nh]
+    assert np.allclose(C[:, plane], np.conj(C[:, partner[plane]]), atol=0)
+    assert np.all(C[:, inp.masker1 == 0] == 0)
+
+
+def _run(R, mk, ncalls, inner):
+    inp = inputs.build_inputs(mk())
+    st = oracle.State(inp)
+    rows = []
+    for _ in range(ncalls):
+        R.run(inp, inner, st)
+        rows.append((st.E.copy(), st.deltae, st.deltac))
+    return inp, st, rows
+
+
+def packed(inp, c, nbands):
+    pts = np.flatnonzero(inp.masker1)
+    return c.reshape(inp.nbands, inp.nfft3d, 2)[:nbands, pts, :]
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_restatement_matches_reference_build(restatement, golden, name):
+    """The C restatement reproduces the reference's own cpsd() (golden vectors)."""
+    mk, ncalls, inner = CASES[name]
+    g = golden(name)
+    inp, st, rows = _run(restatement, mk, ncalls, inner)
+    E = np.array([r[0] for r in rows])
+    assert np.abs(E[:, 0] - g["E"][:, 0]).max() < E_TOL
+    assert np.abs(E - g["E"]).max() < 10 * E_TOL
+    assert np.abs(np.array([r[1] for r in rows]) - g["deltae"]).max() < 1e-8
+    assert np.abs(np.array([r[2] for r in rows]) - g["deltac"]).max() < 1e-9
+    assert np.abs(st.lmd - g["lmd"]).max() < 1e-9
+    assert np.abs(st.hml - g["hml"]).max() < 1e-9
+    keep = g["c2"].shape[0]
+    assert np.abs(packed(inp, st.c2, keep) - g["c2"]).max() < 1e-10
+    assert np.abs(packed(inp, st.cpsi, keep) - g["cpsi"]).max() < 1e-10
+
+
+def test_restatement_matches_reference_main(restatement):
+    """Same run as the reference's main() from its own files (printed digits)."""
+    g = np.load(os.path.join(GOLDEN, "ref_main_small_diamond_24.npz"))
+    spec = configs.small_diamond(24, 4)
+    spec.ecut_ry = float(g["ecut"])
+    inp = inputs.build_inputs(spec)
+    st = oracle.State(inp)
+    for row in g["rows"]:
+        restatement.run(inp, int(g["inner"]), st)
+        step, e, de, dc, dr = row
+        assert abs(st.E[0] - e) <= 1e-10 * max(1.0, abs(e)) + 1e-9
+        assert abs(st.deltae - de) <= 1e-5 * abs(de) + 1e-12
+        assert abs(st.deltac - dc) <= 1e-5 * abs(dc) + 1e-12
+    assert np.allclose(st.E, g["final"], rtol=1e-9, atol=1e-9)
+
+
+def test_lagrange_off_by_one_quirk_single_band(restatement):
+    """With one band the reference's convergence test reads sa1 (cpsd.c:471)
+    and never passes: every step runs the full 30 iterations ("ierr=10")."""
+    inp = inputs.build_inputs(configs.small_h2(16))
+    st = oracle.State(inp)
+    restatement.run(inp, 3, st)
+    assert st.lagrange_fail == 3
