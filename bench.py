@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 steepest-descent engine (SD steps/s).
+
+One bench *step* is one call of the reference's ``cpsd()`` with inner=10 (one
+outer iteration of ccpsdv3/main.c:417-445): ten steepest-descent steps plus
+the energy evaluation.  ``value`` is SD steps per second of the whole job
+(all replicas), device-timed with CUDA events on the engine's stream, the
+cell resident in HBM and L2 flushed (256 MB write) before every timed call.
+``e2e`` is the same metric through the drop-in ``cpsd()`` C ABI with host
+buffers in the reference's layouts, the host<->device copies inside the
+timed region.  ``--impl reference`` times the reference's own serial C
+(oracle/_ref, ccpsdv3/*.c compiled unmodified) on the host cores.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+Multi-GPU (torchrun, one process per GPU): every rank runs its own replica of
+the cell (the SD loop of one cell has no data-parallel split: replicas only);
+the timed region is bracketed by barriers and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "simple-cpsd_b200"))
+
+METRIC = "SD steps/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ----------------------------------------------------------------- helpers
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def phase_bytes(geo, nb, n, ispin):
+    """Algorithmic bytes per launch of the single-kernel phases (FP64).
+
+    T  = nb*n*ncol complex (column buffer after the kz transform),
+    Pk = nb*npw complex (packed orbitals), R = n^3 doubles (real grid)."""
+    cb = 16
+    T = nb * n * geo["ncol"] * cb
+    Pk = nb * geo["npw"] * cb
+    R = n ** 3 * 8
+    return {
+        "inv_z_bands": Pk + T,                        # packed psi in, columns out
+        "density_plane": T + geo["dens_chunks"] * R,  # columns in, density partials out
+        "density_xc": geo["dens_chunks"] * R + (3 + 2 * ispin) * R,
+        "applyv_plane": 2 * T + ispin * R,            # columns in and out, V(r) in
+        "fwd_z_sd": T + 4 * Pk,                       # columns in; c2, c1 in; cpsi, c2 out
+    }
+
+
+def traffic_from_profile(kernel, workload):
+    """dram bytes per launch from a committed ncu summary, if there is one."""
+    path = os.path.join(REPO, "profiles", "%s_%s.txt" % (kernel, workload))
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def max_over_ranks(x, dist, torch, device):
+    """The slowest rank's time (replicas are timed independently)."""
+    if dist is None:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- CPU reference
+def cpu_reference(inp, budget_s, min_calls=3, inner=1):
+    """Time the reference's own cpsd() (oracle/_ref) on this host's cores."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle  # test infrastructure: only the baseline leg runs it
+    try:
+        impl, kind = oracle.ReferenceBuild(), "reference"
+    except FileNotFoundError:
+        impl, kind = oracle.Restatement(), "port"
+    st = oracle.State(inp)
+    calls, t0 = 0, time.perf_counter()
+    while calls < min_calls or time.perf_counter() - t0 < budget_s:
+        impl.run(inp, inner, st)
+        calls += 1
+    dt = time.perf_counter() - t0
+    return calls * inner / dt, kind, calls, dt
+
+
+# ----------------------------------------------------------------- GPU arm
+def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True):
+    from cpsd_b200 import api
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    if want_phases:
+        cell.phase_timing(True)
+    stream = torch.cuda.ExternalStream(cell.stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(warmup):
+        cell.run(inner)
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+    phases = {}
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = cell.counters()[0]
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()  # L2 flush on the engine's stream, outside the event pair
+        events[k][0].record(stream)
+        cell.run(inner)
+        events[k][1].record(stream)
+        if want_phases:
+            for name, ms in cell.phase_times().items():
+                phases.setdefault(name, []).append(ms)
+    torch.cuda.synchronize()
+    launches = cell.counters()[0] - l0
+    if dist is not None:
+        dist.barrier()
+    total_ms = sum(a.elapsed_time(b) for a, b in events)
+    geo = cell.geometry()
+    E = cell.E.copy()
+    cell.close()
+    ph = {k: sum(v) / len(v) for k, v in phases.items()}
+    return total_ms, launches, ph, geo, E
+
+
+def e2e_dropin(inp, calls, inner):
+    """Through the reference-facing cpsd() with host buffers (copies timed)."""
+    from cpsd_b200 import api
+    st = api.State(inp)
+    api.cpsd(inp, st, inner)  # warm-up: builds the drop-in's context
+    l0, h0, d0 = api.dropin_counters()
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        api.cpsd(inp, st, inner)
+    dt = time.perf_counter() - t0
+    l1, h1, d1 = api.dropin_counters()
+    return calls * inner / dt, (h1 - h0) / calls, (d1 - d0) / calls, l1 - l0
+
+
+def roofline_entry(ph, geo, nb, n, ispin, workload):
+    pb = phase_bytes(geo, nb, n, ispin)
+    cand = {k: v for k, v in ph.items() if k in pb and v > 0}
+    if not cand:
+        return None
+    top = max(cand, key=cand.get)
+    peak, src = peaks()
+    achieved = pb[top] / (cand[top] * 1e-3) / 1e9
+    total = sum(v for v in ph.values() if v > 0)
+    return {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
+            "peak_source": src, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic_from_profile(top, workload), "algorithmic_bytes": pb[top],
+            "launch_ms": round(cand[top], 5), "share_of_step": round(cand[top] / total, 3) if total else None}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="diamond8_64")
+    ap.add_argument("--inner", type=int, default=10)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ncores = os.cpu_count() or 1
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(ncores))
+
+    from cpsd_b200 import configs, inputs
+    spec = configs.NAMED[args.workload]()
+    inp = inputs.build_inputs(spec)
+    config = {"workload": args.workload, "nfft": inp.nfft, "nbands": inp.nbands, "nion": inp.nion,
+              "npw": inp.npw, "ecut_ry": spec.ecut_ry, "inner": args.inner, "precision": "fp64",
+              "step": "one cpsd() call: %d SD steps + energies" % args.inner,
+              "l2": "flushed (256 MB write) before every timed call", "parallelism": "replicas"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        steps_done, t_all = 0, 0.0
+        sample_inner = 1
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle
+        try:
+            impl, kind = oracle.ReferenceBuild(), "reference"
+        except FileNotFoundError:
+            impl, kind = oracle.Restatement(), "port"
+        st = oracle.State(inp)
+        for _ in range(args.warmup):
+            impl.run(inp, sample_inner, st)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            impl.run(inp, sample_inner, st)
+            steps_done += sample_inner
+        t_all = time.perf_counter() - t0
+        v = steps_done / t_all
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "config": dict(config, step="one reference cpsd() call: 1 SD step + energies"),
+                "cpu_baseline": {"value": v, "unit": "steps/s", "cores": ncores, "kind": kind,
+                                 "sample": "%d reference cpsd() calls of inner=1 on %s" % (args.steps, args.workload)},
+                "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                              device_id=torch.device("cuda", local))
+        dist = td
+    else:
+        torch.cuda.set_device(0)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    total_ms, launches, ph, geo, E = time_cell(inp, args.steps, args.warmup, args.inner, torch, dist)
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(total_ms, dist, torch, "cuda")
+    sd_steps = args.steps * args.inner * world
+    value = sd_steps / (total_ms * 1e-3)
+
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": config, "gpu_launches": int(launches), "clocks": clocks,
+            "final_energy": float(E[0])}
+    line["roofline"] = roofline_entry(ph, geo, inp.nbands, inp.nfft, inp.ispin, args.workload)
+    line["phases_ms"] = {k: round(v, 5) for k, v in ph.items()}
+
+    if rank == 0 and not args.no_e2e:
+        ev, hb, db, _ = e2e_dropin(inp, max(3, min(args.steps, 10)), args.inner)
+        line["e2e"] = {"value": ev * world, "unit": "steps/s", "h2d_bytes_per_step": int(hb),
+                       "d2h_bytes_per_step": int(db),
+                       "path": "drop-in cpsd() C ABI, host buffers in the reference layout"}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cv, kind, calls, dt = cpu_reference(inp, args.cpu_budget)
+        line["cpu_baseline"] = {"value": cv, "unit": "steps/s", "cores": ncores, "kind": kind,
+                                "sample": "%d reference cpsd() calls of inner=1 on %s (%.1f s)"
+                                          % (calls, args.workload, dt)}
+    if rank == 0 and world == 1 and not args.no_extra:
+        # the 128^3 / 64-atom / 128-band cell of the precision study, FP64
+        from cpsd_b200 import configs as C
+        big = inputs.build_inputs(C.diamond64_128())
+        tms, lch, ph3, geo3, E3 = time_cell(big, 3, 1, args.inner, torch, None)
+        line["extra"] = {"diamond64_128": {
+            "value": 3 * args.inner / (tms * 1e-3), "unit": "steps/s",
+            "ms_per_sd_step": tms / (3 * args.inner), "npw": big.npw, "nbands": big.nbands,
+            "phases_ms": {k: round(v, 4) for k, v in ph3.items()},
+            "roofline": roofline_entry(ph3, geo3, big.nbands, big.nfft, big.ispin, "diamond64_128"),
+            "cpu_reference_s_per_step": "measured offline: see BASELINE.md"}}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

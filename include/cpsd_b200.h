@@ -138,8 +138,29 @@ int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, do
 /* Sphere size (packed G vectors per band) and the kernel launches of one SD step. */
 int cpsd_gpu_npw(const cpsd_gpu_ctx *c);
 int cpsd_gpu_launches_per_step(const cpsd_gpu_ctx *c);
+/* out[6]: npw, padded npw, (kx,ky) columns of the sphere, kx lines (KX),
+ * KB projectors, density band chunks. */
+int cpsd_gpu_geometry(const cpsd_gpu_ctx *c, int *out);
 /* Steps whose Lagrange iteration stopped at 30 iterations, since creation. */
 int cpsd_gpu_lagrange_failures(cpsd_gpu_ctx *c);
+
+/* Cumulative counters: out[0] kernel launches, out[1] host-to-device bytes,
+ * out[2] device-to-host bytes since the context was created. */
+void cpsd_gpu_counters(const cpsd_gpu_ctx *c, long long *out);
+
+/* SD steps are replayed from captured CUDA graphs unless switched off here
+ * (or with the environment variable CPSD_B200_NO_GRAPHS set at creation). */
+int cpsd_gpu_use_graphs(cpsd_gpu_ctx *c, int on);
+
+/* Phase timing: with it on, CUDA events are recorded between the phases of
+ * every SD step (inside the step graphs); cpsd_gpu_phase_times() returns the
+ * durations (ms) of the phases of the last step and their count. */
+int cpsd_gpu_phase_timing(cpsd_gpu_ctx *c, int on);
+int cpsd_gpu_phase_times(cpsd_gpu_ctx *c, float *ms, int max);
+const char *cpsd_gpu_phase_name(int i);
+
+/* The context the drop-in cpsd() keeps between calls (NULL before the first call). */
+cpsd_gpu_ctx *cpsd_gpu_dropin_context(void);
 
 /* CUDA stream the context runs on (a cudaStream_t), for timing with events. */
 void *cpsd_gpu_stream(cpsd_gpu_ctx *c);

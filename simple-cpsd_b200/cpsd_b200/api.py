@@ -118,9 +118,32 @@ class GpuCell:
     def npw(self) -> int:
         return self._L.cpsd_gpu_npw(self.h)
 
+    def geometry(self) -> dict:
+        out = (ctypes.c_int * 6)()
+        self._check(self._L.cpsd_gpu_geometry(self.h, out), "cpsd_gpu_geometry")
+        return dict(npw=out[0], npw_pad=out[1], ncol=out[2], KX=out[3], nproj=out[4], dens_chunks=out[5])
+
     @property
     def launches_per_step(self) -> int:
         return self._L.cpsd_gpu_launches_per_step(self.h)
+
+    def counters(self):
+        """(kernel launches, host-to-device bytes, device-to-host bytes) so far."""
+        out = (ctypes.c_longlong * 3)()
+        self._L.cpsd_gpu_counters(self.h, out)
+        return int(out[0]), int(out[1]), int(out[2])
+
+    def use_graphs(self, on: bool) -> None:
+        self._check(self._L.cpsd_gpu_use_graphs(self.h, 1 if on else 0), "cpsd_gpu_use_graphs")
+
+    def phase_timing(self, on: bool) -> None:
+        self._check(self._L.cpsd_gpu_phase_timing(self.h, 1 if on else 0), "cpsd_gpu_phase_timing")
+
+    def phase_times(self):
+        """{phase name: ms} of the last SD step (phase timing must be on)."""
+        buf = (ctypes.c_float * 32)()
+        n = self._L.cpsd_gpu_phase_times(self.h, buf, 32)
+        return {self._L.cpsd_gpu_phase_name(i).decode(): float(buf[i]) for i in range(n)}
 
     @property
     def stream(self) -> int:
@@ -157,6 +180,15 @@ class GpuCell:
             self.close()
         except Exception:
             pass
+
+
+def dropin_counters():
+    """Counters of the context the drop-in cpsd() keeps between calls."""
+    L = _l.load()
+    h = L.cpsd_gpu_dropin_context()
+    out = (ctypes.c_longlong * 3)()
+    L.cpsd_gpu_counters(h, out)
+    return int(out[0]), int(out[1]), int(out[2])
 
 
 def _fft(fn, A: np.ndarray, nfft: int) -> None:

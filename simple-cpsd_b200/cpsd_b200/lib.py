@@ -31,7 +31,10 @@ EXPORTS = [
     "cpsd_gpu_strerror", "cpsd", "cpsd_gpu_cpsd", "cr_fft3b_", "rc_fft3f_", "cpsd_gpu_fft_status",
     "cpsd_gpu_create", "cpsd_gpu_set_scalars", "cpsd_gpu_set_tables", "cpsd_gpu_set_state",
     "cpsd_gpu_run", "cpsd_gpu_get_state", "cpsd_gpu_npw", "cpsd_gpu_launches_per_step",
-    "cpsd_gpu_lagrange_failures", "cpsd_gpu_stream", "cpsd_gpu_destroy",
+    "cpsd_gpu_geometry",
+    "cpsd_gpu_lagrange_failures", "cpsd_gpu_counters", "cpsd_gpu_use_graphs",
+    "cpsd_gpu_dropin_context", "cpsd_gpu_phase_timing", "cpsd_gpu_phase_times",
+    "cpsd_gpu_phase_name", "cpsd_gpu_stream", "cpsd_gpu_destroy",
 ]
 
 
@@ -71,7 +74,16 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_gpu_get_state.argtypes = [_P] + [_P] * 9
     lib.cpsd_gpu_npw.argtypes = [_P]
     lib.cpsd_gpu_launches_per_step.argtypes = [_P]
+    lib.cpsd_gpu_geometry.argtypes = [_P, _P]
     lib.cpsd_gpu_lagrange_failures.argtypes = [_P]
+    lib.cpsd_gpu_counters.argtypes = [_P, _P]
+    lib.cpsd_gpu_counters.restype = None
+    lib.cpsd_gpu_use_graphs.argtypes = [_P, _I]
+    lib.cpsd_gpu_dropin_context.restype = _P
+    lib.cpsd_gpu_phase_timing.argtypes = [_P, _I]
+    lib.cpsd_gpu_phase_times.argtypes = [_P, _P, _I]
+    lib.cpsd_gpu_phase_name.argtypes = [_I]
+    lib.cpsd_gpu_phase_name.restype = ctypes.c_char_p
     lib.cpsd_gpu_stream.argtypes = [_P]
     lib.cpsd_gpu_stream.restype = _P
     lib.cpsd_gpu_destroy.argtypes = [_P]

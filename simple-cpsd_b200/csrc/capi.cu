@@ -96,6 +96,12 @@ extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, co
     return rc ? rc : run;
 }
 
+extern "C" cpsd_gpu_ctx *cpsd_gpu_dropin_context(void)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_ctx;
+}
+
 extern "C" void cpsd(const int inner, const int move, const int nion, const int ispin, const int *ne,
                      const int nfft, const int nfft3d, const int n2ft3d, const double *unitg, const double omega,
                      const double dt, const double fmass, const int *katm, const double *amass, const double *zv,

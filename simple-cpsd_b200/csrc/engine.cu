@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -286,6 +287,14 @@ struct cpsd_gpu_ctx {
     size_t gemm_ws_elems = 0;
     int launches_per_step = 0;
     int lag_fail_total = 0;
+    long long nlaunch = 0, h2d = 0, d2h = 0;  // kernel launches and host<->device bytes so far
+    bool use_graph = true;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // one captured SD step per ping-pong parity
+    int graph_launches = 0;
+    // optional phase timing: events recorded between the phases of a step
+    // (captured into the step graphs), read back by cpsd_gpu_phase_times()
+    bool phase_timing = false;
+    cudaEvent_t pev[16] = {};
     bool tables_ok = false, state_ok = false, ran = false;
 
     // device
@@ -325,6 +334,7 @@ int gemm_tn(cpsd_gpu_ctx *c, int M, int N, int K, const double *A, long lda, con
     splits = cdiv(K, kchunk);
     dim3 grid((unsigned)cdiv(M, GB), (unsigned)cdiv(N, GB), (unsigned)splits);
     gemm_tn_w_kernel<<<grid, 256, 0, c->st>>>(M, N, K, A, lda, B, ldb, w, kchunk, c->gws);
+    c->nlaunch += 2;
     splitk_reduce_kernel<<<(unsigned)cdiv((long)M * N, 256), 256, 0, c->st>>>(M, N, (int)splits, c->gws,
                                                                               alpha, beta, C, ldc);
     return CPSD_OK;
@@ -336,12 +346,24 @@ void gemm_nn(cpsd_gpu_ctx *c, int NJ, int K, int L, double alpha, const double *
     if (NJ <= 0 || L <= 0) return;
     dim3 grid((unsigned)cdiv(K, GB), (unsigned)cdiv(NJ, GB));
     gemm_nn_kernel<<<grid, 256, 0, c->st>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo);
+    c->nlaunch += 1;
 }
 
 const double *Mblk(cpsd_gpu_ctx *c, int ms, int which)
 {
     // 4 overlap blocks per spin: 0 M22, 1 M21, 2 M11, 3 hml source
     return c->Mov + ((long)ms * 4 + which) * (long)c->ne0 * c->ne0;
+}
+
+const char *const kPhaseNames[] = {
+    "inv_z_bands", "density_plane", "density_xc", "rho_fft",     "vloc_proj",  "potential_fft",
+    "kinetic_nonlocal", "applyv_plane", "fwd_z_sd", "overlaps", "lagrange", "constraint",
+};
+constexpr int kNumPhases = (int)(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]));
+
+inline void mark(cpsd_gpu_ctx *c, int i)
+{
+    if (c->phase_timing) cudaEventRecord(c->pev[i], c->st);
 }
 
 int one_step(cpsd_gpu_ctx *c)
@@ -352,24 +374,32 @@ int one_step(cpsd_gpu_ctx *c)
     const long ldr = 2L * c->npw_pad;
     CK(cudaMemcpyAsync(c->r1, c->r2, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToDevice, s));  // cpsd.c:174
 
+    mark(c, 0);
     // psi(G) -> psi(r) and the density, cpsd.c:177-194
-    c->fft->inv_z(c->g, c1, c->ldc, c->Tb, c->nb, s);
+    c->fft->inv_z(c->g, c1, c->ldc, c->Tb, c->nb, s); c->nlaunch += 1;
+    mark(c, 1);
     PlaneArgs pa{};
     pa.chunk_b0 = c->chunk_dens;
     pa.rho_part = c->rho_part;
-    c->fft->plane(PM_DENSITY, c->g, c->Tb, pa, c->nchunk0 + c->nchunk1, s);
+    c->fft->plane(PM_DENSITY, c->g, c->Tb, pa, c->nchunk0 + c->nchunk1, s); c->nlaunch += 1;
+    mark(c, 2);
     XcArgs xa{c->n3, c->ispin, c->nchunk0, c->nchunk1, c->rho_part, c->scal1, c->scal2,
               c->dn, c->xcp, c->xce, c->rfwd};
-    density_xc_kernel<<<(unsigned)cdiv(c->n3, 256), 256, 0, s>>>(xa);
+    density_xc_kernel<<<(unsigned)cdiv(c->n3, 256), 256, 0, s>>>(xa); c->nlaunch += 1;
+    mark(c, 3);
     // rho(G), cpsd.c:198-205
     PlaneArgs pf{};
     pf.rin = c->rfwd;
-    c->fft->plane(PM_FWDREAL, c->g, c->Taux, pf, 1, s);
-    c->fft->fwd_z_store(c->g, c->Taux, c->dng, c->ldc, 1.0, 1, s);
+    c->fft->plane(PM_FWDREAL, c->g, c->Taux, pf, 1, s); c->nlaunch += 1;
+    c->fft->fwd_z_store(c->g, c->Taux, c->dng, c->ldc, 1.0, 1, s); c->nlaunch += 1;
+    mark(c, 4);
     // phase factors, local psp, projectors, V(G): cpsd.c:208, 224-286, 373-379
     if (c->nion > 0)
+    {
         phase_tables_kernel<<<(unsigned)cdiv(3 * c->nion, 128), 128, 0, s>>>(c->nion, c->n, c->unitg, c->r1,
                                                                               c->ex1, c->ex2, c->ex3);
+        c->nlaunch += 1;
+    }
     VlocArgs va{};
     va.npw = c->npw;
     va.npw_pad = c->npw_pad;
@@ -395,32 +425,36 @@ int one_step(cpsd_gpu_ctx *c)
     va.vall = c->vall;
     va.Vg = c->Vg;
     va.proj = c->proj;
-    vloc_proj_kernel<<<(unsigned)cdiv(c->npw_pad, 128), 128, 0, s>>>(va);
+    vloc_proj_kernel<<<(unsigned)cdiv(c->npw_pad, 128), 128, 0, s>>>(va); c->nlaunch += 1;
+    mark(c, 5);
     // V_loc + V_H to real space, plus xc per spin (cpsd.c:380-388)
-    c->fft->inv_z(c->g, c->Vg, c->ldc, c->Taux, 1, s);
+    c->fft->inv_z(c->g, c->Vg, c->ldc, c->Taux, 1, s); c->nlaunch += 1;
     PlaneArgs pv{};
     pv.rout = c->Vr;
     pv.xadd = c->xcp;
     pv.nout = c->ispin;
-    c->fft->plane(PM_INVREAL, c->g, c->Taux, pv, 1, s);
+    c->fft->plane(PM_INVREAL, c->g, c->Taux, pv, 1, s); c->nlaunch += 1;
+    mark(c, 6);
     // kinetic + nonlocal part of -H psi, cpsd.c:212-221, 287-290
     kinetic_kernel<<<(unsigned)cdiv((long)c->nb * c->npw_pad, 256), 256, 0, s>>>(c->nb, c->npw_pad, c->ldc,
-                                                                                c->tg, c1, c2);
+                                                                                c->tg, c1, c2); c->nlaunch += 1;
     if (c->nproj > 0) {
         int rc = gemm_tn(c, c->nproj, c->nb, K, (const double *)c->proj, ldr, (const double *)c1, ldr, c->w,
                          1.0, 0.0, c->beta, c->nb);
         if (rc) return rc;
         kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, s>>>(
-            c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT);
+            c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT); c->nlaunch += 1;
         gemm_nn(c, c->nb, K, c->nproj, 1.0, c->coefT, c->nproj, (const double *)c->proj, ldr, 1.0,
                 (double *)c2, ldr);
     }
+    mark(c, 7);
     // (V + xc) psi back to G, -H psi and the SD step, cpsd.c:384-400
     PlaneArgs pp{};
     pp.chunk_b0 = c->chunk_band;
     pp.V = c->Vr;
     pp.ne0 = (c->ispin == 2) ? c->ne0 : c->nb;
-    c->fft->plane(PM_APPLYV, c->g, c->Tb, pp, c->nb, s);
+    c->fft->plane(PM_APPLYV, c->g, c->Tb, pp, c->nb, s); c->nlaunch += 1;
+    mark(c, 8);
     ZEpilogue e{};
     e.c2 = c2;
     e.c1 = c1;
@@ -428,7 +462,8 @@ int one_step(cpsd_gpu_ctx *c)
     e.ldc = c->ldc;
     e.scal1 = c->scal1;
     e.dte = c->dte;
-    c->fft->fwd_z_sd(c->g, c->Tb, e, c->nb, s);
+    c->fft->fwd_z_sd(c->g, c->Tb, e, c->nb, s); c->nlaunch += 1;
+    mark(c, 9);
     // overlaps and Lagrange multipliers, cpsd.c:415-479
     LagArgs la{};
     la.ispin = c->ispin;
@@ -448,6 +483,7 @@ int one_step(cpsd_gpu_ctx *c)
         la.M21[ms] = Mblk(c, ms, 1);
         la.M11[ms] = Mblk(c, ms, 2);
     }
+    mark(c, 10);
     la.s11 = c->lag;
     la.s12 = c->lag + ne02;
     la.s21 = c->lag + 2 * ne02;
@@ -458,7 +494,8 @@ int one_step(cpsd_gpu_ctx *c)
     la.lmd = c->lmd;
     la.red = c->red;
     la.fail = c->flags;
-    lagrange_kernel<<<kLagCluster, kLagThreads, 0, s>>>(la);
+    lagrange_kernel<<<kLagCluster, kLagThreads, 0, s>>>(la); c->nlaunch += 1;
+    mark(c, 11);
     // constraint correction c2 += dte C1 lmd, cpsd.c:482-488
     for (int ms = 0; ms < c->ispin; ++ms) {
         const int m = ms ? c->ne1 : c->ne0;
@@ -466,7 +503,47 @@ int one_step(cpsd_gpu_ctx *c)
         gemm_nn(c, m, K, m, c->dte, c->lmd + ms * ne02, m, (const double *)c1 + off, ldr, 1.0,
                 (double *)c2 + off, ldr);
     }
+    mark(c, 12);
     CK(cudaGetLastError());
+    c->cur ^= 1;
+    return CPSD_OK;
+}
+
+void drop_graphs(cpsd_gpu_ctx *c)
+{
+    for (auto &g : c->gexec)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// One SD step, replayed from a CUDA graph captured on first use (one graph
+// per ping-pong parity of the orbital buffers).
+int run_step(cpsd_gpu_ctx *c)
+{
+    if (!c->use_graph) return one_step(c);
+    const int par = c->cur;
+    if (!c->gexec[par]) {
+        cudaGraph_t g = nullptr;
+        const long long before = c->nlaunch;
+        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+        int rc = one_step(c);
+        cudaError_t e = cudaStreamEndCapture(c->st, &g);
+        c->cur = par;  // capture launched nothing: undo the buffer flip
+        c->graph_launches = (int)(c->nlaunch - before);
+        c->nlaunch = before;
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        CK(e);
+        e = cudaGraphInstantiate(&c->gexec[par], g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+    }
+    CK(cudaGraphLaunch(c->gexec[par], c->st));
+    c->nlaunch += c->graph_launches;
     c->cur ^= 1;
     return CPSD_OK;
 }
@@ -487,9 +564,9 @@ int energies(cpsd_gpu_ctx *c, int inner)
         fa.Mh[ms] = Mblk(c, ms, 3);
     }
     packed_terms_kernel<<<c->pblocks, 256, 0, s>>>(c->npw, c->w, c->sfac, c->vg, c->dng, c->vc, c->vall,
-                                                   c->ppart);
-    band_terms_kernel<<<dim3(c->bblocks, c->nb), 256, 0, s>>>(c->npw, c->ldc, c->w, c->tg, c1, c2, c->bpart);
-    grid_terms_kernel<<<c->gblocks, 256, 0, s>>>(c->n3, c->ispin, c->dn, c->xce, c->xcp, c->gpart);
+                                                   c->ppart); c->nlaunch += 1;
+    band_terms_kernel<<<dim3(c->bblocks, c->nb), 256, 0, s>>>(c->npw, c->ldc, c->w, c->tg, c1, c2, c->bpart); c->nlaunch += 1;
+    grid_terms_kernel<<<c->gblocks, 256, 0, s>>>(c->n3, c->ispin, c->dn, c->xce, c->xcp, c->gpart); c->nlaunch += 1;
     fa.ispin = c->ispin;
     fa.ne0 = c->ne0;
     fa.ne1 = c->ne1;
@@ -519,7 +596,7 @@ int energies(cpsd_gpu_ctx *c, int inner)
     fa.dt = c->prm.dt;
     fa.dte = c->dte;
     fa.E = c->Edev;
-    final_energy_kernel<<<1, 32, 0, s>>>(fa);
+    final_energy_kernel<<<1, 32, 0, s>>>(fa); c->nlaunch += 1;
     CK(cudaGetLastError());
     return CPSD_OK;
 }
@@ -626,6 +703,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     c->scal2 = 1.0 / p->omega;
     c->dv = p->omega * c->scal1;
     c->dte = p->dt / sqrt(p->fmass);
+    c->use_graph = !getenv("CPSD_B200_NO_GRAPHS");
     c->hg = build_geom(c->n, masker1, false);
     HostGeom &h = c->hg;
     if (h.npw == 0) return CPSD_ERR_EMPTY_MASK;
@@ -755,6 +833,7 @@ int cpsd_gpu_set_scalars(cpsd_gpu_ctx *c, const double *unitg, double omega, dou
     c->scal2 = 1.0 / omega;
     c->dv = omega * c->scal1;
     c->dte = dt / sqrt(fmass);
+    drop_graphs(c);  // kernel arguments captured by value change
     return CPSD_OK;
 }
 
@@ -796,6 +875,7 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
         np += lmmax[ia];
     }
     if (np != c->nproj || !c->proj) {
+        drop_graphs(c);
         if (np > 0) {
             CK(c->ar.alloc(&c->proj, (size_t)np * c->npw_pad));
             CK(c->ar.alloc(&c->beta, (size_t)np * c->nb));
@@ -819,6 +899,8 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
     if (c->nsh > 0) CK(cudaMemcpy(c->rcell, rcell, sizeof(double) * 3 * c->nsh, cudaMemcpyHostToDevice));
     if (np > 0) CK(cudaMemcpy(c->vnlnrm_p, pn.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
     CK(cudaDeviceSynchronize());
+    c->h2d += (long long)sizeof(double) * (3 * c->npw_pad + (long)pvl.size() + (long)pvnl.size() + nkatm + 9 + np +
+                                          3 * c->nsh) + (long long)sizeof(int) * (nkatm + 2 * c->nion);
     c->tables_ok = true;
     return CPSD_OK;
 }
@@ -837,6 +919,9 @@ int cpsd_gpu_set_state(cpsd_gpu_ctx *c, const double *c2, const double *r2)
     int outside = 0;
     CK(cudaMemcpyAsync(&outside, c->flags + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    c->h2d += (long long)sizeof(double) * (c->nb * c->n2ft3d + 3 * c->nion);
+    c->d2h += (long long)sizeof(int);
+    c->nlaunch += 1;
     if (outside) return CPSD_ERR_UNMASKED_PSI;
     c->state_ok = true;
     return CPSD_OK;
@@ -853,7 +938,7 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
     CK(cudaMemsetAsync(c->flags, 0, sizeof(int), s));
     CK(cudaMemcpyAsync(c->Edev, E, sizeof(double), cudaMemcpyHostToDevice, s));
     for (int it = 0; it < inner; ++it) {
-        int rc = one_step(c);
+        int rc = run_step(c);
         if (rc) return rc;
     }
     int rc = energies(c, inner);
@@ -863,6 +948,8 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
     CK(cudaMemcpyAsync(Eh, c->Edev, sizeof(double) * 12, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&fails, c->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    c->h2d += sizeof(double);
+    c->d2h += 12 * sizeof(double) + sizeof(int);
     for (int i = 0; i < 10; ++i) E[i] = Eh[i];
     if (deltae) *deltae = Eh[10];
     if (deltac) *deltac = Eh[11];
@@ -893,13 +980,19 @@ int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, do
                                          c->nfft3d);
         CK(cudaMemcpyAsync(o.host, c->full, fullb, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        c->nlaunch += 1;
+        c->d2h += (long long)fullb;
     }
+    const long ne02 = (long)c->ne0 * c->ne0, ne12 = (long)c->ne1 * c->ne1;
     if (dn) {
         const long tot = (long)c->ispin * c->n2ft3d;
         pad_real_kernel<<<(unsigned)cdiv(tot, 256), 256, 0, s>>>(c->ispin, c->n, c->dn, c->full);
         CK(cudaMemcpyAsync(dn, c->full, sizeof(double) * tot, cudaMemcpyDeviceToHost, s));
+        c->nlaunch += 1;
+        c->d2h += (long long)sizeof(double) * tot;
     }
-    const long ne02 = (long)c->ne0 * c->ne0, ne12 = (long)c->ne1 * c->ne1;
+    c->d2h += (long long)sizeof(double) * ((hml ? ne02 + ne12 : 0) + (lmd ? ne02 + ne12 : 0) +
+                                          (c->nion > 0 ? ((r1 ? 3 : 0) + (r2 ? 3 : 0)) * c->nion : 0));
     if (hml) CK(cudaMemcpyAsync(hml, c->hml, sizeof(double) * (ne02 + ne12), cudaMemcpyDeviceToHost, s));
     if (lmd) CK(cudaMemcpyAsync(lmd, c->lmd, sizeof(double) * (ne02 + ne12), cudaMemcpyDeviceToHost, s));
     if (c->nion > 0) {
@@ -913,9 +1006,22 @@ int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, do
 
 int cpsd_gpu_npw(const cpsd_gpu_ctx *c) { return c ? c->npw : 0; }
 
+int cpsd_gpu_geometry(const cpsd_gpu_ctx *c, int *out)
+{
+    if (!c || !out) return CPSD_ERR_ARG;
+    out[0] = c->npw;
+    out[1] = c->npw_pad;
+    out[2] = c->hg.ncol;
+    out[3] = c->hg.KX;
+    out[4] = c->nproj;
+    out[5] = c->nchunk0 + c->nchunk1;
+    return CPSD_OK;
+}
+
 int cpsd_gpu_launches_per_step(const cpsd_gpu_ctx *c)
 {
     if (!c) return 0;
+    if (c->graph_launches) return c->graph_launches;
     // inv_z, density plane, xc, fwd plane, fwd_z, phase, vloc, inv_z, inv plane,
     // kinetic, [beta gemm + reduce, coef, nn gemm], applyV plane, fwd_z(SD),
     // 3 overlap gemms (+reduce) per spin, lagrange, constraint gemm per spin
@@ -926,6 +1032,45 @@ int cpsd_gpu_launches_per_step(const cpsd_gpu_ctx *c)
 
 int cpsd_gpu_lagrange_failures(cpsd_gpu_ctx *c) { return c ? c->lag_fail_total : 0; }
 
+int cpsd_gpu_phase_timing(cpsd_gpu_ctx *c, int on)
+{
+    if (!c) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    drop_graphs(c);  // recapture with (or without) the event records
+    if (on && !c->pev[0])
+        for (int i = 0; i <= kNumPhases; ++i) CK(cudaEventCreate(&c->pev[i]));
+    c->phase_timing = on != 0;
+    return CPSD_OK;
+}
+
+int cpsd_gpu_phase_times(cpsd_gpu_ctx *c, float *ms, int max)
+{
+    if (!c || !c->phase_timing || !ms) return 0;
+    if (cudaEventSynchronize(c->pev[kNumPhases]) != cudaSuccess) return 0;
+    int n = std::min(max, kNumPhases);
+    for (int i = 0; i < n; ++i)
+        if (cudaEventElapsedTime(&ms[i], c->pev[i], c->pev[i + 1]) != cudaSuccess) ms[i] = -1.0f;
+    return n;
+}
+
+const char *cpsd_gpu_phase_name(int i) { return (i >= 0 && i < kNumPhases) ? kPhaseNames[i] : ""; }
+
+void cpsd_gpu_counters(const cpsd_gpu_ctx *c, long long *out)
+{
+    if (!out) return;
+    out[0] = c ? c->nlaunch : 0;
+    out[1] = c ? c->h2d : 0;
+    out[2] = c ? c->d2h : 0;
+}
+
+int cpsd_gpu_use_graphs(cpsd_gpu_ctx *c, int on)
+{
+    if (!c) return CPSD_ERR_ARG;
+    if (!on) drop_graphs(c);
+    c->use_graph = on != 0;
+    return CPSD_OK;
+}
+
 void *cpsd_gpu_stream(cpsd_gpu_ctx *c) { return c ? (void *)c->st : nullptr; }
 
 void cpsd_gpu_destroy(cpsd_gpu_ctx *c)
@@ -933,6 +1078,9 @@ void cpsd_gpu_destroy(cpsd_gpu_ctx *c)
     if (!c) return;
     cudaSetDevice(c->prm.device);
     if (c->st) cudaStreamSynchronize(c->st);
+    drop_graphs(c);
+    for (auto &e : c->pev)
+        if (e) cudaEventDestroy(e);
     c->ar.release();
     if (c->st) cudaStreamDestroy(c->st);
     delete c;

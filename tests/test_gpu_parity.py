@@ -1,0 +1,246 @@
+"""GPU parity: the sm_100a path through the C ABI against the reference's
+golden vectors and the oracle restatement.
+
+Tolerance: the north star's FP64 bar, |E - E_ref| < 1e-9 Ha for the total
+energy of every cpsd() call; matrices and orbitals to ~1e-10.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from cpsd_b200 import api, configs, inputs, lib
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-9
+CASES = {
+    "small_h2_16": (lambda: configs.small_h2(16), 3, 2),
+    "small_diamond_24": (lambda: configs.small_diamond(24, 4), 3, 2),
+    "small_diamond_32": (lambda: configs.small_diamond(32, 5, ecut=25.0), 2, 2),
+    "small_diamond_48": (lambda: configs.small_diamond(48, 6, ecut=30.0), 2, 2),
+    "h2_dimer_32": (lambda: configs.h2_dimer_32(), 200, 1),
+    "diamond8_64": (lambda: configs.diamond8_64(), 4, 2),
+}
+
+
+def packed(inp, c, nbands):
+    pts = np.flatnonzero(inp.masker1)
+    return c.reshape(inp.nbands, inp.nfft3d, 2)[:nbands, pts, :]
+
+
+def check_against_golden(inp, g, rows, st):
+    E = np.array([r[0] for r in rows])
+    assert np.abs(E[:, 0] - g["E"][:, 0]).max() < E_TOL
+    assert np.abs(E - g["E"]).max() < 10 * E_TOL
+    assert np.abs(np.array([r[1] for r in rows]) - g["deltae"]).max() < 1e-8
+    assert np.abs(np.array([r[2] for r in rows]) - g["deltac"]).max() < 1e-9
+    assert np.abs(st.lmd - g["lmd"]).max() < 1e-9
+    assert np.abs(st.hml - g["hml"]).max() < 1e-9
+    keep = g["c2"].shape[0]
+    assert np.abs(packed(inp, st.c2, keep) - g["c2"]).max() < 1e-10
+    assert np.abs(packed(inp, st.cpsi, keep) - g["cpsi"]).max() < 1e-10
+    dn = st.dn.reshape(inp.ispin, inp.nfft, inp.nfft, inp.nfft + 2)
+    assert np.all(dn[..., inp.nfft:] == 0.0)
+    dn = dn[..., :inp.nfft]
+    assert np.allclose(dn.sum(axis=(1, 2, 3)), g["dn_sum"], rtol=1e-12, atol=0)
+    assert np.allclose(dn[:, 0], g["dn_plane0"], rtol=1e-11, atol=1e-15)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_resident_cell_matches_reference(golden, name):
+    """Persistent context (orbitals stay in HBM between calls) == reference build."""
+    mk, ncalls, inner = CASES[name]
+    inp = inputs.build_inputs(mk())
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    rows = []
+    for _ in range(ncalls):
+        cell.run(inner)
+        rows.append((cell.E.copy(), cell.deltae, cell.deltac))
+    st = api.State(inp)
+    cell.get_state(st)
+    cell.close()
+    check_against_golden(inp, golden(name), rows, st)
+
+
+@pytest.mark.parametrize("name", ["small_h2_16", "small_diamond_24", "diamond8_64"])
+def test_dropin_cpsd_matches_reference(golden, name):
+    """The reference-facing cpsd() with host buffers, called like main.c does."""
+    mk, ncalls, inner = CASES[name]
+    inp = inputs.build_inputs(mk())
+    st = api.State(inp)
+    rows = []
+    for _ in range(ncalls):
+        api.cpsd(inp, st, inner)
+        rows.append((st.E.copy(), st.deltae, st.deltac))
+    check_against_golden(inp, golden(name), rows, st)
+    # cpsi leaves as c2 - c1, full box (cpsd.c:650-651)
+    assert np.array_equal(st.cpsi, st.c2 - st.c1) or np.abs(st.cpsi - (st.c2 - st.c1)).max() < 1e-15
+
+
+def test_lagrange_warning_matches_reference_quirk():
+    """One band: the reference never meets its convergence test (cpsd.c:471),
+    every call ends with the ierr=10 warning; so does the drop-in."""
+    inp = inputs.build_inputs(configs.small_h2(16))
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    for _ in range(3):
+        cell.run(2)
+    assert cell.lagrange_warnings == 3
+    assert lib.load().cpsd_gpu_lagrange_failures(cell.h) == 6
+    cell.close()
+
+
+def test_intermediates_match_restatement(restatement):
+    """Density, Hamiltonian and Lagrange matrices after one step, and the
+    orthonormality the constraint restores (<c2|c2> = 1 + O(dte^2))."""
+    inp = inputs.build_inputs(configs.small_diamond(24, 6, ecut=22.0, seed=11))
+    so = oracle.State(inp)
+    restatement.run(inp, 1, so)
+    sg = api.State(inp)
+    api.cpsd(inp, sg, 1)
+    assert np.abs(so.dn - sg.dn).max() < 1e-13
+    assert np.abs(so.hml - sg.hml).max() < 1e-10
+    assert np.abs(so.lmd - sg.lmd).max() < 1e-10
+    assert abs(so.E[0] - sg.E[0]) < E_TOL
+    w = inputs.gamma_weights(inp.nfft)
+    C = sg.c2.reshape(inp.nbands, -1).view(np.complex128)
+    S = np.einsum("p,ap,bp->ab", w, C.conj(), C).real
+    assert np.abs(S - np.eye(inp.nbands)).max() < 1e-4
+
+
+@pytest.mark.parametrize("n", [16, 24, 32, 48, 64, 128])
+def test_fft_dropins_match_oracle(restatement, n):
+    """cr_fft3b_/rc_fft3f_ drop-ins (whole box) == the fftpack3d restatement."""
+    rng = np.random.default_rng(100 + n)
+    nh = n // 2 + 1
+    C = rng.standard_normal((n, n, nh)) + 1j * rng.standard_normal((n, n, nh))
+    A = np.ascontiguousarray(C).view(np.float64).reshape(-1).copy()
+    B = A.copy()
+    api.cr_fft3b(A, n)
+    restatement.cr_fft3b(B, n)
+    assert np.abs(A - B).max() <= 2e-14 * np.abs(B).max()
+    x = rng.standard_normal((n, n, n + 2)).reshape(-1)
+    A, B = x.copy(), x.copy()
+    api.rc_fft3f(A, n)
+    restatement.rc_fft3f(B, n)
+    assert np.abs(A - B).max() <= 2e-14 * np.abs(B).max()
+
+
+def test_fft_roundtrip_full_size():
+    """rc then cr returns n^3 x at the largest supported grid."""
+    n = 128
+    rng = np.random.default_rng(7)
+    A = np.zeros((n, n, n + 2))
+    A[:, :, :n] = rng.standard_normal((n, n, n))
+    x0 = A[:, :, :n].copy()
+    A = A.reshape(-1)
+    api.rc_fft3f(A, n)
+    api.cr_fft3b(A, n)
+    assert np.abs(A.reshape(n, n, n + 2)[:, :, :n] / n ** 3 - x0).max() < 1e-13
+
+
+def test_full_size_cell_properties():
+    """The 128^3 / 64-atom / 128-band cell (too large for the CPU oracle per
+    step): energy decreases, orthonormality holds, hml and lmd symmetric,
+    the density integrates to the electron count, reruns are bitwise equal."""
+    inp = inputs.build_inputs(configs.diamond64_128())
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    Es = []
+    for _ in range(3):
+        cell.run(2)
+        Es.append(cell.E[0])
+    st = api.State(inp)
+    cell.get_state(st)
+    assert Es[0] > Es[1] > Es[2]
+    m = inp.nbands
+    H = st.hml[:m * m].reshape(m, m)
+    assert np.abs(H - H.T).max() < 1e-12 * np.abs(H).max()
+    dv = inp.omega / inp.nfft ** 3
+    dn = st.dn.reshape(inp.nfft, inp.nfft, inp.nfft + 2)[..., :inp.nfft]
+    assert abs(dn.sum() * dv - m) < 1e-8 * m  # ispin=1: dn holds one spin, nb electrons
+    w = inputs.gamma_weights(inp.nfft)
+    pts = np.flatnonzero(inp.masker1)
+    C = st.c1.reshape(m, -1).view(np.complex128)[:, pts]
+    S = (C.conj() * w[pts]) @ C.T
+    assert np.abs(S.real - np.eye(m)).max() < 1e-6
+    # determinism: same inputs, same bits
+    cell.set_state(inp.c2, inp.r2)
+    cell.E[:] = 0
+    cell.run(2)
+    e_again = cell.E[0]
+    cell.close()
+    cell2 = api.GpuCell(inp)
+    cell2.set_state(inp.c2, inp.r2)
+    cell2.run(2)
+    assert cell2.E[0] == e_again
+    cell2.close()
+
+
+def test_error_paths():
+    """Bad inputs come back as status codes, never as a device fault."""
+    inp = inputs.build_inputs(configs.small_h2(16))
+    st = api.State(inp)
+    with pytest.raises(lib.CpsdError) as e:
+        api.cpsd(inp, st, 1, move=1)
+    assert e.value.status == lib.CPSD_ERR_MOVE
+    bad = inputs.build_inputs(configs.small_h2(16))
+    bad.c2 = bad.c2.copy()
+    out_of_mask = np.flatnonzero(bad.masker1 == 0)[5]
+    bad.c2[2 * out_of_mask] = 1.0
+    st = api.State(bad)
+    with pytest.raises(lib.CpsdError) as e:
+        api.cpsd(bad, st, 1)
+    assert e.value.status == lib.CPSD_ERR_UNMASKED_PSI
+    cell = api.GpuCell(inp)
+    with pytest.raises(lib.CpsdError) as e:
+        cell.run(0)
+    assert e.value.status == lib.CPSD_ERR_ARG
+    cell.close()
+    spec = configs.small_h2(16)
+    spec.nfft = 20  # not a supported grid
+    with pytest.raises(lib.CpsdError) as e:
+        api.GpuCell(inputs.build_inputs(spec))
+    assert e.value.status == lib.CPSD_ERR_GRID
+    A = np.zeros((20 + 2) * 20 * 20)
+    with pytest.raises(lib.CpsdError):
+        api.rc_fft3f(A, 20)
+
+
+def test_graphs_and_direct_launches_agree():
+    inp = inputs.build_inputs(configs.small_diamond(32, 5, ecut=25.0))
+    out = []
+    for graphs in (True, False):
+        cell = api.GpuCell(inp)
+        cell.use_graphs(graphs)
+        cell.set_state(inp.c2, inp.r2)
+        cell.run(3)
+        out.append(cell.E.copy())
+        cell.close()
+    assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(oracle.REFERENCE_SO), "dcpsdv3_b200.x")),
+                    reason="drop-in build of the reference main() absent")
+def test_reference_main_linked_against_library(tmp_path):
+    """The reference's unmodified main.c linked with this library's cpsd()
+    (oracle/_ref/dcpsdv3_b200.x) reproduces the reference main()'s run."""
+    import subprocess
+    from cpsd_b200 import refio
+    g = np.load(os.path.join(GOLDEN, "ref_main_small_diamond_24.npz"))
+    spec = configs.small_diamond(24, 4)
+    spec.ecut_ry = float(g["ecut"])
+    inp = inputs.build_inputs(spec)
+    refio.write_reference_inputs(str(tmp_path), inp, inner=int(g["inner"]), outer=int(g["outer"]))
+    exe = os.path.join(os.path.dirname(oracle.REFERENCE_SO), "dcpsdv3_b200.x")
+    out = subprocess.run([exe], cwd=str(tmp_path), capture_output=True, check=True).stdout.decode("utf-8", "replace")
+    rows, final = refio.parse_reference_stdout(out)
+    assert len(rows) == len(g["rows"])
+    for r, w in zip(rows, g["rows"]):
+        assert abs(r[1] - w[1]) <= 1e-9 * max(1.0, abs(w[1]))
+    assert np.allclose([final[i] for i in range(10)], g["final"], rtol=1e-9, atol=1e-9)

@@ -1,0 +1,162 @@
+"""Host-side logic that needs no GPU: the C ABI exports, reference file
+formats, workload generation, bench helpers and the multi-rank reduction."""
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+from cpsd_b200 import build, configs, inputs, lib, refio
+
+
+def header_functions():
+    with open(os.path.join(REPO, "include", "cpsd_b200.h")) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{]*\)\s*;", text)
+    return sorted(set(n for n in names if n not in ("if", "sizeof")))
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    so = build.build_library()
+    out = subprocess.run(["nm", "-D", "--defined-only", so], capture_output=True, text=True, check=True).stdout
+    exported = set(line.split()[-1] for line in out.splitlines() if " T " in line)
+    declared = header_functions()
+    assert declared, "no declarations parsed"
+    assert set(declared) <= exported, sorted(set(declared) - exported)
+    assert set(declared) == set(lib.EXPORTS)
+
+
+def test_library_targets_sm100a_only():
+    """The build compiles for sm_100a alone (no PTX for other targets)."""
+    flags = " ".join(build.NVCC_FLAGS)
+    assert re.findall(r"arch=compute_(\w+),code=(\w+)", flags) == [("100a", "sm_100a")]
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    saved = lib._lib
+    lib._lib = None
+    try:
+        with pytest.raises(FileNotFoundError):
+            lib.load(str(tmp_path / "nope.so"))
+    finally:
+        lib._lib = saved
+
+
+def test_elcin_roundtrip(tmp_path):
+    inp = inputs.build_inputs(configs.small_h2(16))
+    p = str(tmp_path / "ELCIN")
+    refio.write_elcin(p, 1, inp.nfft, 10.0, 1, inp.ne, inp.c2)
+    back = refio.read_elcin(p)
+    assert back["nfft"] == 16 and back["ne"] == (1, 0) and back["unit"] == 10.0
+    assert np.array_equal(back["c"], inp.c2)
+    # the header is the reference's: 4+4+8+4+8 bytes (main.c:116-121)
+    assert os.path.getsize(p) == 28 + 8 * inp.c2.size
+
+
+def test_reference_inputs_written(tmp_path):
+    inp = inputs.build_inputs(configs.small_diamond(16, 2, ecut=10.0))
+    refio.write_reference_inputs(str(tmp_path), inp, inner=2, outer=3)
+    names = sorted(os.listdir(tmp_path))
+    assert names == ["C0.vpp", "CONTROL", "ELCIN", "IONIN"]
+    nfft3d = inp.nfft3d
+    # .vpp: 4+4+8+2+8+8+4 header, rc[lmax+1], vnlnrm[lmmax], vl, vnl[lmmax]
+    want = 38 + 8 * (3 + 4 + nfft3d + 4 * nfft3d)
+    assert os.path.getsize(tmp_path / "C0.vpp") == want
+    ion = open(tmp_path / "IONIN").read().split()
+    assert ion[0] == "1" and ion[1] == "'C0.vpp" and ion[3] == "2" and ion[4] == "8"
+
+
+def test_parse_reference_stdout():
+    text = """          ================ iteration =========================
+          >>>   iteration started on Thu Dec  3 12:00:23 2026    <<<
+       2    8.6420275970e+01  7.45002e+00  4.77763e-01  0.00000e+00
+       4    7.1368710863e+01 -1.29755e+00  4.82470e-01  0.00000e+00
+          *** arrived at the maximum iteration.  iteration terminated.
+ total     energy    : 5.6634818000e+01 ( 7.07935e+00/ion)
+ KS V_xc energy      :-2.0458754790e+00 (-5.11469e-01/electron)
+"""
+    rows, final = refio.parse_reference_stdout(text)
+    assert rows == [(2, 86.42027597, 7.45002, 0.477763, 0.0), (4, 71.368710863, -1.29755, 0.48247, 0.0)]
+    assert final == {0: 56.634818, 9: -2.045875479}
+
+
+def test_batched_cells_follow_the_recipe():
+    cells = configs.batched_cells(seed=0)
+    assert len(cells) == 48
+    for c in cells:
+        assert c.nfft in (32, 48, 64) and c.unit == 0.5 * c.nfft and c.ecut_ry == 30.0
+        assert 2 <= len(c.katm) <= 16 and 4 <= c.ne[0] <= 32
+        z = sum(4.0 if k else 1.0 for k in c.katm)
+        assert c.ne[0] >= min(32, np.ceil(z / 2))
+        p = c.positions
+        for i in range(len(p)):
+            for j in range(i):
+                d = p[i] - p[j]
+                d -= c.unit * np.round(d / c.unit)
+                assert np.sqrt(d @ d) >= 1.5 - 1e-12
+
+
+def test_analytic_psp_limits():
+    """vl(G) -> -4 pi Z/G^2 at small rc, vl(0) = pi Z rc^2, projector norms."""
+    sp = configs.C_SP
+    spec = configs.small_diamond(24, 2, ecut=20.0)
+    inp = inputs.build_inputs(spec)
+    G = inp.G
+    vl, vnl, vnlnrm = inputs.analytic_psp(sp, G, inp.nfft3d)
+    assert vl[0] == pytest.approx(np.pi * sp.zv * sp.rc_loc ** 2)
+    assert np.all(vnlnrm[:4] == [1.0 / sp.ekb[0]] + [1.0 / sp.ekb[1]] * 3)
+    # |p_s>: int |p|^2 = 1  <=>  sum_G |vnl|^2 / Omega (full sphere) -> 1 for a big cell
+    a = 40.0
+    omega, _, unitg = inputs.get_cube(1, a)
+    Gb = inputs.get_g(64, unitg)
+    n3 = (64 // 2 + 1) * 64 * 64
+    _, vb, _ = inputs.analytic_psp(sp, Gb, n3)
+    s = inputs.gssum_np(64, vb[:n3] ** 2) / omega
+    assert s == pytest.approx(1.0, rel=1e-6)
+
+
+def test_bench_roofline_helpers():
+    sys.path.insert(0, REPO)
+    import bench
+    geo = dict(npw=2483, npw_pad=2496, ncol=300, KX=11, nproj=32, dens_chunks=5)
+    pb = bench.phase_bytes(geo, 16, 64, 1)
+    T = 16 * 64 * 300 * 16
+    assert pb["applyv_plane"] == 2 * T + 64 ** 3 * 8
+    r = bench.roofline_entry({"applyv_plane": 0.01, "density_plane": 0.005}, geo, 16, 64, 1, "x")
+    assert r["kernel"] == "applyv_plane" and r["unit"] == "GB/s" and r["bound"] == "hbm"
+    assert r["achieved"] == pytest.approx(pb["applyv_plane"] / 1e-5 / 1e9, rel=1e-3)
+
+
+def _rank_main(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, REPO)
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    got = bench.max_over_ranks(10.0 + rank, dist, torch, "cpu")
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, got))
+
+
+def test_replica_timing_takes_the_slowest_rank():
+    """bench.py's multi-rank path: every rank gets the max over ranks (gloo, 2 ranks)."""
+    import multiprocessing as mp
+    import socket
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    res = dict(q.get(timeout=5) for _ in range(2))
+    assert res == {0: 11.0, 1: 11.0}
