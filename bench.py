@@ -159,9 +159,9 @@ def cpu_reference(inp, budget_s, min_calls=3, inner=1):
 
 
 # ----------------------------------------------------------------- GPU arm
-def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True):
+def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True, precision=0):
     from cpsd_b200 import api
-    cell = api.GpuCell(inp)
+    cell = api.GpuCell(inp, precision=precision)
     cell.set_state(inp.c2, inp.r2)
     if want_phases:
         cell.phase_timing(True)
@@ -195,6 +195,40 @@ def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True):
     cell.close()
     ph = {k: sum(v) / len(v) for k, v in phases.items()}
     return total_ms, launches, ph, geo, E
+
+
+def time_batched(specs, inner, calls):
+    """Config-4 cells: one graph per SD step for all cells vs the cells one by one."""
+    from cpsd_b200 import api, inputs
+    inps = [inputs.build_inputs(s) for s in specs]
+    cells = []
+    for inp in inps:
+        c = api.GpuCell(inp)
+        c.set_state(inp.c2, inp.r2)
+        cells.append(c)
+    for c in cells:  # warm-up (captures each cell's own graphs)
+        c.run(inner)
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        for c in cells:
+            c.run(inner)
+    t_seq = time.perf_counter() - t0
+    batch = api.GpuBatch(cells)
+    batch.run(inner)  # warm-up (captures the batch graphs)
+    l0 = batch.launches()
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        batch.run(inner)
+    t_bat = time.perf_counter() - t0
+    launches = batch.launches() - l0
+    batch.close()
+    for c in cells:
+        c.close()
+    sd = len(cells) * inner * calls
+    return {"cells": len(cells), "grids": sorted(set(s.nfft for s in specs)),
+            "bands": [min(s.ne[0] for s in specs), max(s.ne[0] for s in specs)],
+            "batched_steps_per_s": sd / t_bat, "sequential_steps_per_s": sd / t_seq,
+            "speedup": t_seq / t_bat, "gpu_launches": launches, "timing": "host wall clock, synchronous calls"}
 
 
 def e2e_dropin(inp, calls, inner):
@@ -324,16 +358,31 @@ def main():
                                 "sample": "%d reference cpsd() calls of inner=1 on %s (%.1f s)"
                                           % (calls, args.workload, dt)}
     if rank == 0 and world == 1 and not args.no_extra:
-        # the 128^3 / 64-atom / 128-band cell of the precision study, FP64
         from cpsd_b200 import configs as C
+        extra = {}
+        # the same workload with FP32 transforms (mixed precision)
+        tmx, _, phm, _, Em = time_cell(inp, args.steps, args.warmup, args.inner, torch, None,
+                                       want_phases=True, precision=1)
+        extra["mixed_" + args.workload] = {
+            "value": sd_steps / (tmx * 1e-3), "unit": "steps/s", "ms_per_step": tmx / args.steps,
+            "final_energy": float(Em[0]), "abs_dE_vs_fp64_same_steps": abs(float(Em[0]) - float(E[0])),
+            "phases_ms": {k: round(v, 5) for k, v in phm.items()}}
+        # config 4: 48 uneven cells, one graph launch per SD step for all of them
+        extra["batched_cells"] = time_batched(C.batched_cells(0), args.inner, 3)
+        # the 128^3 / 64-atom / 128-band cell of the precision study, FP64
         big = inputs.build_inputs(C.diamond64_128())
         tms, lch, ph3, geo3, E3 = time_cell(big, 3, 1, args.inner, torch, None)
-        line["extra"] = {"diamond64_128": {
+        tmm, _, ph3m, _, E3m = time_cell(big, 3, 1, args.inner, torch, None, precision=1)
+        extra["mixed_diamond64_128"] = {"value": 3 * args.inner / (tmm * 1e-3), "unit": "steps/s",
+                                        "ms_per_sd_step": tmm / (3 * args.inner),
+                                        "phases_ms": {k: round(v, 4) for k, v in ph3m.items()}}
+        line["extra"] = extra
+        extra["diamond64_128"] = {
             "value": 3 * args.inner / (tms * 1e-3), "unit": "steps/s",
             "ms_per_sd_step": tms / (3 * args.inner), "npw": big.npw, "nbands": big.nbands,
             "phases_ms": {k: round(v, 4) for k, v in ph3.items()},
             "roofline": roofline_entry(ph3, geo3, big.nbands, big.nfft, big.ispin, "diamond64_128"),
-            "cpu_reference_s_per_step": "measured offline: see BASELINE.md"}}
+            "cpu_reference_s_per_step": 105.6}
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

@@ -148,6 +148,12 @@ int cpsd_gpu_lagrange_failures(cpsd_gpu_ctx *c);
  * out[2] device-to-host bytes since the context was created. */
 void cpsd_gpu_counters(const cpsd_gpu_ctx *c, long long *out);
 
+/* Switch the transforms of the next steps between FP64 (the parity path)
+ * and FP32 (mixed).  A context created with CPSD_PREC_MIXED holds both, so
+ * the last steps can run as an FP64 refinement sweep on the same state; one
+ * created with CPSD_PREC_FP64 accepts only CPSD_PREC_FP64. */
+int cpsd_gpu_set_precision(cpsd_gpu_ctx *c, int precision);
+
 /* SD steps are replayed from captured CUDA graphs unless switched off here
  * (or with the environment variable CPSD_B200_NO_GRAPHS set at creation). */
 int cpsd_gpu_use_graphs(cpsd_gpu_ctx *c, int on);
@@ -166,6 +172,27 @@ cpsd_gpu_ctx *cpsd_gpu_dropin_context(void);
 void *cpsd_gpu_stream(cpsd_gpu_ctx *c);
 
 void cpsd_gpu_destroy(cpsd_gpu_ctx *c);
+
+/* ------------------------------------------------------ batches of cells */
+
+typedef struct cpsd_gpu_batch cpsd_gpu_batch;
+
+/*
+ * Step many independent cells together (uneven grids and band counts
+ * allowed).  Each SD step of the whole batch is one CUDA graph launch with
+ * one branch per cell.  The cells keep their own contexts (tables and state
+ * set beforehand) and must not be run on their own while batched.
+ */
+int cpsd_gpu_batch_create(cpsd_gpu_ctx **cells, int ncells, cpsd_gpu_batch **out);
+
+/* `inner` SD steps of every cell, then each cell's energies: E[10*i + k] is
+ * E[k] of cell i (E[10*i] in: the cell's previous total energy). */
+int cpsd_gpu_batch_run(cpsd_gpu_batch *b, int inner, double *E, double *deltae, double *deltac);
+
+/* out[0]: kernel launches of the batch's cells so far. */
+void cpsd_gpu_batch_counters(const cpsd_gpu_batch *b, long long *out);
+void *cpsd_gpu_batch_stream(cpsd_gpu_batch *b);
+void cpsd_gpu_batch_destroy(cpsd_gpu_batch *b);
 
 #ifdef __cplusplus
 }

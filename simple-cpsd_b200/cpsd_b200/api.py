@@ -133,6 +133,10 @@ class GpuCell:
         self._L.cpsd_gpu_counters(self.h, out)
         return int(out[0]), int(out[1]), int(out[2])
 
+    def set_precision(self, precision: int) -> None:
+        """CPSD_PREC_FP64 or CPSD_PREC_MIXED for the following steps."""
+        self._check(self._L.cpsd_gpu_set_precision(self.h, int(precision)), "cpsd_gpu_set_precision")
+
     def use_graphs(self, on: bool) -> None:
         self._check(self._L.cpsd_gpu_use_graphs(self.h, 1 if on else 0), "cpsd_gpu_use_graphs")
 
@@ -173,6 +177,55 @@ class GpuCell:
     def close(self) -> None:
         if getattr(self, "h", None):
             self._L.cpsd_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuBatch:
+    """Many resident cells stepped together: one CUDA graph launch per SD step."""
+
+    def __init__(self, cells):
+        self._L = _l.load()
+        self.cells = list(cells)
+        arr = (ctypes.c_void_p * len(self.cells))(*[c.h for c in self.cells])
+        h = ctypes.c_void_p()
+        rc = self._L.cpsd_gpu_batch_create(arr, len(self.cells), ctypes.byref(h))
+        if rc:
+            raise CpsdError(rc, "cpsd_gpu_batch_create")
+        self.h = h
+        self.E = np.zeros((len(self.cells), 10))
+        self.deltae = np.zeros(len(self.cells))
+        self.deltac = np.zeros(len(self.cells))
+        self.lagrange_warnings = 0
+
+    def run(self, inner: int) -> np.ndarray:
+        rc = self._L.cpsd_gpu_batch_run(self.h, inner, _ptr(self.E), _ptr(self.deltae), _ptr(self.deltac))
+        if rc == _l.CPSD_WARN_LAGRANGE:
+            self.lagrange_warnings += 1
+        elif rc != _l.CPSD_OK:
+            raise CpsdError(rc, "cpsd_gpu_batch_run")
+        for c, e, de, dc in zip(self.cells, self.E, self.deltae, self.deltac):
+            c.E[:] = e
+            c.deltae, c.deltac = float(de), float(dc)
+        return self.E
+
+    def launches(self) -> int:
+        out = (ctypes.c_longlong * 1)()
+        self._L.cpsd_gpu_batch_counters(self.h, out)
+        return int(out[0])
+
+    @property
+    def stream(self) -> int:
+        return self._L.cpsd_gpu_batch_stream(self.h) or 0
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self._L.cpsd_gpu_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -63,11 +63,12 @@ def diamond8_64(seed: int = 0) -> CellSpec:
                     katm=[0] * 8, positions=pos, ne=(16, 0), seed=seed)
 
 
-def diamond64_128(seed: int = 0) -> CellSpec:
+def diamond64_128(seed: int = 0, nbands: int = 128) -> CellSpec:
     a = 20.5
     pos = diamond_positions(a, 2, 0.1, seed)
-    return CellSpec(name="diamond64_128", unit=a, nfft=128, ecut_ry=40.0, species=[C_SP],
-                    katm=[0] * 64, positions=pos, ne=(128, 0), seed=seed)
+    name = "diamond64_128" if nbands == 128 else "diamond64_128_b%d" % nbands
+    return CellSpec(name=name, unit=a, nfft=128, ecut_ry=40.0, species=[C_SP],
+                    katm=[0] * 64, positions=pos, ne=(nbands, 0), seed=seed)
 
 
 def batched_cells(seed: int = 0, count: int = 48) -> List[CellSpec]:
@@ -121,4 +122,6 @@ NAMED = {
     "h2_dimer_32": h2_dimer_32,
     "diamond8_64": diamond8_64,
     "diamond64_128": diamond64_128,
+    # the 128^3 cell with 16 bands: small enough for a full ncu capture
+    "diamond64_128_b16": lambda seed=0: diamond64_128(seed, nbands=16),
 }

@@ -33,8 +33,10 @@ EXPORTS = [
     "cpsd_gpu_run", "cpsd_gpu_get_state", "cpsd_gpu_npw", "cpsd_gpu_launches_per_step",
     "cpsd_gpu_geometry",
     "cpsd_gpu_lagrange_failures", "cpsd_gpu_counters", "cpsd_gpu_use_graphs",
+    "cpsd_gpu_set_precision",
     "cpsd_gpu_dropin_context", "cpsd_gpu_phase_timing", "cpsd_gpu_phase_times",
-    "cpsd_gpu_phase_name", "cpsd_gpu_stream", "cpsd_gpu_destroy",
+    "cpsd_gpu_phase_name", "cpsd_gpu_stream", "cpsd_gpu_destroy", "cpsd_gpu_batch_create",
+    "cpsd_gpu_batch_run", "cpsd_gpu_batch_counters", "cpsd_gpu_batch_stream", "cpsd_gpu_batch_destroy",
 ]
 
 
@@ -79,6 +81,7 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_gpu_counters.argtypes = [_P, _P]
     lib.cpsd_gpu_counters.restype = None
     lib.cpsd_gpu_use_graphs.argtypes = [_P, _I]
+    lib.cpsd_gpu_set_precision.argtypes = [_P, _I]
     lib.cpsd_gpu_dropin_context.restype = _P
     lib.cpsd_gpu_phase_timing.argtypes = [_P, _I]
     lib.cpsd_gpu_phase_times.argtypes = [_P, _P, _I]
@@ -86,6 +89,14 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_gpu_phase_name.restype = ctypes.c_char_p
     lib.cpsd_gpu_stream.argtypes = [_P]
     lib.cpsd_gpu_stream.restype = _P
+    lib.cpsd_gpu_batch_create.argtypes = [_P, _I, ctypes.POINTER(_P)]
+    lib.cpsd_gpu_batch_run.argtypes = [_P, _I, _P, _P, _P]
+    lib.cpsd_gpu_batch_counters.argtypes = [_P, _P]
+    lib.cpsd_gpu_batch_counters.restype = None
+    lib.cpsd_gpu_batch_stream.argtypes = [_P]
+    lib.cpsd_gpu_batch_stream.restype = _P
+    lib.cpsd_gpu_batch_destroy.argtypes = [_P]
+    lib.cpsd_gpu_batch_destroy.restype = None
     lib.cpsd_gpu_destroy.argtypes = [_P]
     lib.cpsd_gpu_destroy.restype = None
     lib.cpsd_gpu_fft_status.restype = _I

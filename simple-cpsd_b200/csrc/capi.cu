@@ -294,6 +294,7 @@ extern "C" void cr_fft3b_(double *A, int *inc2c, int *inc3c, int *inc2r, int *in
     (void)tmp;
     (void)ntmp;
     t_fft_status = fft_call(A, inc2c, inc3c, inc2r, inc3r, nx, ny, nz, +1);
+    if (t_fft_status == CPSD_ERR_CUDA) (void)cudaGetLastError();  // leave no stale error behind
     if (t_fft_status) printf("cr_fft3b (B200): error %d: %s\n", t_fft_status, cpsd_gpu_strerror(t_fft_status));
 }
 
@@ -303,6 +304,7 @@ extern "C" void rc_fft3f_(double *A, int *inc2c, int *inc3c, int *inc2r, int *in
     (void)tmp;
     (void)ntmp;
     t_fft_status = fft_call(A, inc2c, inc3c, inc2r, inc3r, nx, ny, nz, -1);
+    if (t_fft_status == CPSD_ERR_CUDA) (void)cudaGetLastError();  // leave no stale error behind
     if (t_fft_status) printf("rc_fft3f (B200): error %d: %s\n", t_fft_status, cpsd_gpu_strerror(t_fft_status));
 }
 

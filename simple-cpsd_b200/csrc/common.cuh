@@ -260,6 +260,52 @@ CPSD_D void line_fft(cx<T> *v, int t, cx<T> *xb, const cx<T> *__restrict__ tw)
     __syncwarp();
 }
 
+// The transposed algorithm (decimation in frequency): lane t starts with
+// x[(t*U + u) + Q*s] in v[u*P + s] -- the output distribution of line_fft --
+// and ends with X[t + P*m] in v[m], its input distribution.  P-point DFTs,
+// twiddle W_N^{q t'}, one exchange, then the Q-point DFT in registers.
+template <int N, int SIGN, typename T>
+CPSD_D void line_fft_dif(cx<T> *v, int t, cx<T> *xb, const cx<T> *__restrict__ tw)
+{
+    using L = Line<N>;
+    constexpr int P = L::P, Q = L::Q, U = L::U;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        cx<T> w[P];
+#pragma unroll
+        for (int s = 0; s < P; ++s) w[s] = v[u * P + s];
+        DFT<P, SIGN, T>::run(w);
+        const int q = t * U + u;
+#pragma unroll
+        for (int tp = 0; tp < P; ++tp) xb[L::xb_index(q, tp)] = (tp == 0) ? w[0] : cmul(w[tp], tw[q * tp]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) v[q] = xb[L::xb_index(q, t)];
+    __syncwarp();
+    DFT<Q, SIGN, T>::run(v);
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory padding: a 128-byte wavefront holds kSlots<T> complex values;
+// lanes of one access phase must hit distinct slots.
+template <typename T>
+constexpr int kSlots = 128 / (int)sizeof(cx<T>);
+
+// smallest v >= base with v = want (mod m)
+constexpr int pad_to(int base, int m, int want)
+{
+    return base + (((want - base) % m) + m) % m;
+}
+
+// stride between the exchange buffers of consecutive line groups of P lanes:
+// the groups sharing an access phase then start on different slots
+template <typename T, int N>
+constexpr int group_stride()
+{
+    return (Line<N>::P >= kSlots<T>) ? Line<N>::XB : pad_to(Line<N>::XB, kSlots<T>, Line<N>::P);
+}
+
 // ---------------------------------------------------------------------------
 // error flags written by kernels (host reads them after a step)
 enum : int {

@@ -18,11 +18,15 @@
 
 namespace {
 
+// On failure: remember the error for cpsd_gpu_strerror and clear the
+// runtime's last-error slot so that a caller's next CUDA call does not trip
+// over it.
 #define CK(call)                                                   \
     do {                                                           \
         cudaError_t e_ = (call);                                   \
         if (e_ != cudaSuccess) {                                   \
             last_cuda_error() = e_;                                \
+            (void)cudaGetLastError();                              \
             return CPSD_ERR_CUDA;                                  \
         }                                                          \
     } while (0)
@@ -171,7 +175,7 @@ struct FftOpsT final : FftOps {
         using L = Line<NF>;
         constexpr int P = L::P, CPB = kThreads / P;
         constexpr int TILE = (CPB * (NF + 1) > NF * (CPB + 1)) ? CPB * (NF + 1) : NF * (CPB + 1);
-        zsmem = sizeof(cx<T>) * ((size_t)TILE + (size_t)CPB * L::XB);
+        zsmem = sizeof(cx<T>) * ((size_t)TILE + (size_t)CPB * group_stride<T, NF>());
         int dev = 0, optin = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -181,14 +185,13 @@ struct FftOpsT final : FftOps {
         for (int m = 0; m < 4; ++m) psmem[m] = plane_smem_bytes<T, NF>(m, KX);
         for (int m = 0; m < 4; ++m)
             if ((int)psmem[m] > optin) psmem[m] = 0;  // mode unavailable for this sphere
-        if (psmem[PM_DENSITY])
-            CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem[PM_DENSITY]));
-        if (psmem[PM_APPLYV])
-            CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_APPLYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem[PM_APPLYV]));
-        if (psmem[PM_INVREAL])
-            CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_INVREAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem[PM_INVREAL]));
-        if (psmem[PM_FWDREAL])
-            CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_FWDREAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem[PM_FWDREAL]));
+        // The limit is a per-kernel (process-wide) attribute shared by every
+        // context on the device: set it to the device maximum, launch with
+        // what this sphere needs.
+        CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_APPLYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_INVREAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_FWDREAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
         return CPSD_OK;
     }
 
@@ -242,29 +245,43 @@ bool grid_supported(int n)
     return n == 16 || n == 24 || n == 32 || n == 48 || n == 64 || n == 128;
 }
 
-std::unique_ptr<FftOps> make_fft(int n)
+template <typename T>
+std::unique_ptr<FftOps> make_fft_t(int n)
 {
     switch (n) {
-    case 16: return std::unique_ptr<FftOps>(new FftOpsT<double, 16>());
-    case 24: return std::unique_ptr<FftOps>(new FftOpsT<double, 24>());
-    case 32: return std::unique_ptr<FftOps>(new FftOpsT<double, 32>());
-    case 48: return std::unique_ptr<FftOps>(new FftOpsT<double, 48>());
-    case 64: return std::unique_ptr<FftOps>(new FftOpsT<double, 64>());
-    case 128: return std::unique_ptr<FftOps>(new FftOpsT<double, 128>());
+    case 16: return std::unique_ptr<FftOps>(new FftOpsT<T, 16>());
+    case 24: return std::unique_ptr<FftOps>(new FftOpsT<T, 24>());
+    case 32: return std::unique_ptr<FftOps>(new FftOpsT<T, 32>());
+    case 48: return std::unique_ptr<FftOps>(new FftOpsT<T, 48>());
+    case 64: return std::unique_ptr<FftOps>(new FftOpsT<T, 64>());
+    case 128: return std::unique_ptr<FftOps>(new FftOpsT<T, 128>());
     default: return nullptr;
     }
 }
 
-size_t plane_need(int n, int mode, int KX)
+// FP64 transforms for the parity path; FP32 transforms for the mixed path
+// (orbitals, potentials, densities and every reduction stay FP64).
+std::unique_ptr<FftOps> make_fft(int n, int precision = CPSD_PREC_FP64)
+{
+    return precision == CPSD_PREC_MIXED ? make_fft_t<float>(n) : make_fft_t<double>(n);
+}
+
+template <typename T>
+size_t plane_need_t(int n, int mode, int KX)
 {
     switch (n) {
-    case 16: return plane_smem_bytes<double, 16>(mode, KX);
-    case 24: return plane_smem_bytes<double, 24>(mode, KX);
-    case 32: return plane_smem_bytes<double, 32>(mode, KX);
-    case 48: return plane_smem_bytes<double, 48>(mode, KX);
-    case 64: return plane_smem_bytes<double, 64>(mode, KX);
-    default: return plane_smem_bytes<double, 128>(mode, KX);
+    case 16: return plane_smem_bytes<T, 16>(mode, KX);
+    case 24: return plane_smem_bytes<T, 24>(mode, KX);
+    case 32: return plane_smem_bytes<T, 32>(mode, KX);
+    case 48: return plane_smem_bytes<T, 48>(mode, KX);
+    case 64: return plane_smem_bytes<T, 64>(mode, KX);
+    default: return plane_smem_bytes<T, 128>(mode, KX);
     }
+}
+
+size_t plane_need(int n, int mode, int KX, int precision = CPSD_PREC_FP64)
+{
+    return precision == CPSD_PREC_MIXED ? plane_need_t<float>(n, mode, KX) : plane_need_t<double>(n, mode, KX);
 }
 
 }  // namespace
@@ -279,7 +296,9 @@ struct cpsd_gpu_ctx {
     DevArena ar;
     HostGeom hg;
     Geom g{};
-    std::unique_ptr<FftOps> fft;
+    FftOps *fft = nullptr;                 // the active transform engine
+    std::unique_ptr<FftOps> fft64, fft32;  // FP64 (parity) and FP32 (mixed) engines
+    int precision = CPSD_PREC_FP64;
     int npw = 0, npw_pad = 0, nproj = 0;
     long ldc = 0;  // complex stride between bands
     int nchunk0 = 0, nchunk1 = 0;
@@ -291,6 +310,8 @@ struct cpsd_gpu_ctx {
     bool use_graph = true;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // one captured SD step per ping-pong parity
     int graph_launches = 0;
+    int lag_cluster = 8;  // CTAs per cluster of the Lagrange solver (16 where schedulable)
+    int lag_lb = 0;       // its row-tile width
     // optional phase timing: events recorded between the phases of a step
     // (captured into the step graphs), read back by cpsd_gpu_phase_times()
     bool phase_timing = false;
@@ -321,23 +342,40 @@ struct cpsd_gpu_ctx {
 
 namespace {
 
+// Batched weighted TN products C_q = alpha A_q' W B_q (+ beta C_q), q < nprod,
+// split along K so that about two CTAs per SM run, each split >= 64 reals.
+int gemm_tn_batch(cpsd_gpu_ctx *c, int M, int N, int K, int nprod, const double *const *A, long lda,
+                  const double *const *B, long ldb, const double *w, double alpha, double beta,
+                  double *const *C, long ldc)
+{
+    if (M <= 0 || N <= 0 || nprod <= 0) return CPSD_OK;
+    if (nprod > kTnMaxProd) return CPSD_ERR_ARG;
+    const long tiles = cdiv(M, GB) * cdiv(N, GB) * nprod;
+    long splits = std::max<long>(1, cdiv(2 * 148, tiles));
+    splits = std::min<long>(splits, std::max<long>(1, K / 64));
+    while ((size_t)splits * M * N * nprod > c->gemm_ws_elems && splits > 1) --splits;
+    const int kchunk = (int)(cdiv(cdiv(K, splits), GK) * GK);
+    splits = cdiv(K, kchunk);
+    TnBatch bt{};
+    for (int q = 0; q < nprod; ++q) {
+        bt.A[q] = A[q];
+        bt.B[q] = B[q];
+        bt.C[q] = C[q];
+    }
+    bt.nprod = nprod;
+    bt.splits = (int)splits;
+    dim3 grid((unsigned)cdiv(M, GB), (unsigned)cdiv(N, GB), (unsigned)(splits * nprod));
+    gemm_tn_w_kernel<<<grid, 256, 0, c->st>>>(M, N, K, lda, ldb, w, kchunk, bt, c->gws);
+    splitk_reduce_kernel<<<(unsigned)cdiv((long)M * N * nprod * 32, 256), 256, 0, c->st>>>(M, N, ldc, c->gws,
+                                                                                          alpha, beta, bt);
+    c->nlaunch += 2;
+    return CPSD_OK;
+}
+
 int gemm_tn(cpsd_gpu_ctx *c, int M, int N, int K, const double *A, long lda, const double *B, long ldb,
             const double *w, double alpha, double beta, double *C, long ldc)
 {
-    if (M <= 0 || N <= 0) return CPSD_OK;
-    const long tiles = cdiv(M, GB) * cdiv(N, GB);
-    long splits = std::max<long>(1, cdiv(2 * 148, tiles));
-    splits = std::min<long>(splits, cdiv(K, GK));
-    splits = std::min<long>(splits, c->gemm_splits_cap);
-    while ((size_t)splits * M * N > c->gemm_ws_elems && splits > 1) --splits;
-    const int kchunk = (int)(cdiv(cdiv(K, splits), GK) * GK);
-    splits = cdiv(K, kchunk);
-    dim3 grid((unsigned)cdiv(M, GB), (unsigned)cdiv(N, GB), (unsigned)splits);
-    gemm_tn_w_kernel<<<grid, 256, 0, c->st>>>(M, N, K, A, lda, B, ldb, w, kchunk, c->gws);
-    c->nlaunch += 2;
-    splitk_reduce_kernel<<<(unsigned)cdiv((long)M * N, 256), 256, 0, c->st>>>(M, N, (int)splits, c->gws,
-                                                                              alpha, beta, C, ldc);
-    return CPSD_OK;
+    return gemm_tn_batch(c, M, N, K, 1, &A, lda, &B, ldb, w, alpha, beta, &C, ldc);
 }
 
 void gemm_nn(cpsd_gpu_ctx *c, int NJ, int K, int L, double alpha, const double *Mat, long ldm,
@@ -363,7 +401,8 @@ constexpr int kNumPhases = (int)(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]));
 
 inline void mark(cpsd_gpu_ctx *c, int i)
 {
-    if (c->phase_timing) cudaEventRecord(c->pev[i], c->st);
+    // External: during stream capture the record becomes an event node of the graph
+    if (c->phase_timing) cudaEventRecordWithFlags(c->pev[i], c->st, cudaEventRecordExternal);
 }
 
 int one_step(cpsd_gpu_ctx *c)
@@ -475,9 +514,10 @@ int one_step(cpsd_gpu_ctx *c)
         const int m = ms ? c->ne1 : c->ne0;
         const long off = (long)(ms ? c->ne0 : 0) * ldr;
         const double *C1 = (const double *)c1 + off, *C2 = (const double *)c2 + off;
-        int rc = gemm_tn(c, m, m, K, C2, ldr, C2, ldr, c->w, 1.0, 0.0, (double *)Mblk(c, ms, 0), m);
-        if (!rc) rc = gemm_tn(c, m, m, K, C2, ldr, C1, ldr, c->w, 1.0, 0.0, (double *)Mblk(c, ms, 1), m);
-        if (!rc) rc = gemm_tn(c, m, m, K, C1, ldr, C1, ldr, c->w, 1.0, 0.0, (double *)Mblk(c, ms, 2), m);
+        // the three overlaps of this spin in one launch
+        const double *As[3] = {C2, C2, C1}, *Bs[3] = {C2, C1, C1};
+        double *Cs[3] = {(double *)Mblk(c, ms, 0), (double *)Mblk(c, ms, 1), (double *)Mblk(c, ms, 2)};
+        int rc = gemm_tn_batch(c, m, m, K, 3, As, ldr, Bs, ldr, c->w, 1.0, 0.0, Cs, m);
         if (rc) return rc;
         la.M22[ms] = Mblk(c, ms, 0);
         la.M21[ms] = Mblk(c, ms, 1);
@@ -494,7 +534,25 @@ int one_step(cpsd_gpu_ctx *c)
     la.lmd = c->lmd;
     la.red = c->red;
     la.fail = c->flags;
-    lagrange_kernel<<<kLagCluster, kLagThreads, 0, s>>>(la); c->nlaunch += 1;
+    la.lb = c->lag_lb;
+    if (c->ne0 <= kLagSmallMax)
+        lagrange_small_kernel<<<1, kLagThreads, sizeof(double) * 7 * ne02, s>>>(la);
+    else {
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = c->lag_cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(c->lag_cluster);
+        cfg.blockDim = dim3(kLagThreads);
+        cfg.dynamicSmemBytes = lagrange_cluster_smem(c->ne0, c->lag_cluster, c->lag_lb);
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, lagrange_kernel, la));
+    }
+    c->nlaunch += 1;
     mark(c, 11);
     // constraint correction c2 += dte C1 lmd, cpsd.c:482-488
     for (int ms = 0; ms < c->ispin; ++ms) {
@@ -596,7 +654,7 @@ int energies(cpsd_gpu_ctx *c, int inner)
     fa.dt = c->prm.dt;
     fa.dte = c->dte;
     fa.E = c->Edev;
-    final_energy_kernel<<<1, 32, 0, s>>>(fa); c->nlaunch += 1;
+    final_energy_kernel<<<1, kFinalThreads, 0, s>>>(fa); c->nlaunch += 1;
     CK(cudaGetLastError());
     return CPSD_OK;
 }
@@ -656,8 +714,160 @@ int cpsd_fft_run_full(int n, int dir, const Geom &g, double *grid, cx<double> *p
     return CPSD_OK;
 }
 
+// ------------------------------------------------------------ batches of cells
+// Many independent cells stepped together: one CUDA graph per SD step holds
+// one branch per cell (forked from and joined to the batch's stream), so the
+// small kernels of uneven cells run concurrently and the whole batch costs
+// one graph launch per step.
+struct cpsd_gpu_batch {
+    std::vector<cpsd_gpu_ctx *> cells;
+    cudaStream_t st = nullptr;
+    std::vector<cudaEvent_t> ev;  // fork + one join per cell
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int graph_launches = 0;
+    long long nlaunch = 0;
+};
+
+namespace {
+
+void batch_drop_graphs(cpsd_gpu_batch *b)
+{
+    for (auto &g : b->gexec)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+int batch_step(cpsd_gpu_batch *b)
+{
+    const int par = b->cells[0]->cur;
+    if (!b->gexec[par]) {
+        cudaGraph_t g = nullptr;
+        std::vector<long long> before;
+        for (auto *c : b->cells) before.push_back(c->nlaunch);
+        CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+        int rc = CPSD_OK;
+        cudaError_t e = cudaEventRecord(b->ev[0], b->st);
+        for (size_t i = 0; i < b->cells.size() && e == cudaSuccess && rc == CPSD_OK; ++i) {
+            cpsd_gpu_ctx *c = b->cells[i];
+            e = cudaStreamWaitEvent(c->st, b->ev[0], 0);
+            if (e == cudaSuccess) rc = one_step(c);
+            c->cur = par;  // capture launched nothing: undo the buffer flip
+            if (e == cudaSuccess) e = cudaEventRecord(b->ev[1 + i], c->st);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, b->ev[1 + i], 0);
+        }
+        cudaError_t e2 = cudaStreamEndCapture(b->st, &g);
+        long long captured = 0;
+        for (size_t i = 0; i < b->cells.size(); ++i) {  // capture launched nothing
+            captured += b->cells[i]->nlaunch - before[i];
+            b->cells[i]->nlaunch = before[i];
+        }
+        b->graph_launches = (int)captured;
+        if (rc || e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            (void)cudaGetLastError();
+            return rc ? rc : CPSD_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&b->gexec[par], g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+    }
+    CK(cudaGraphLaunch(b->gexec[par], b->st));
+    b->nlaunch += b->graph_launches;
+    for (auto *c : b->cells) c->cur ^= 1;
+    return CPSD_OK;
+}
+
+}  // namespace
+
 // ====================================================================== C ABI
 extern "C" {
+
+int cpsd_gpu_batch_create(cpsd_gpu_ctx **cells, int ncells, cpsd_gpu_batch **out)
+{
+    if (!cells || ncells < 1 || !out) return CPSD_ERR_ARG;
+    *out = nullptr;
+    const int dev = cells[0]->prm.device;
+    for (int i = 0; i < ncells; ++i)
+        if (!cells[i] || cells[i]->prm.device != dev || !cells[i]->tables_ok || !cells[i]->state_ok)
+            return CPSD_ERR_ARG;
+    std::unique_ptr<cpsd_gpu_batch> b(new cpsd_gpu_batch());
+    b->cells.assign(cells, cells + ncells);
+    CK(cudaSetDevice(dev));
+    CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+    b->ev.resize(ncells + 1);
+    for (auto &e : b->ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    // every cell must start from the same buffer parity
+    for (auto *c : b->cells)
+        if (c->cur != b->cells[0]->cur) return CPSD_ERR_ARG;
+    *out = b.release();
+    return CPSD_OK;
+}
+
+int cpsd_gpu_batch_run(cpsd_gpu_batch *b, int inner, double *E, double *deltae, double *deltac)
+{
+    if (!b || !E || inner < 1) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(b->cells[0]->prm.device));
+    const int n = (int)b->cells.size();
+    for (int i = 0; i < n; ++i) {
+        cpsd_gpu_ctx *c = b->cells[i];
+        CK(cudaMemsetAsync(c->flags, 0, sizeof(int), b->st));
+        CK(cudaMemcpyAsync(c->Edev, E + 10 * i, sizeof(double), cudaMemcpyHostToDevice, b->st));
+    }
+    for (int it = 0; it < inner; ++it) {
+        int rc = batch_step(b);
+        if (rc) return rc;
+    }
+    // energies per cell on its own stream after the batch's steps
+    CK(cudaEventRecord(b->ev[0], b->st));
+    int warn = 0;
+    std::vector<double> Eh(16 * n);
+    std::vector<int> fails(n, 0);
+    for (int i = 0; i < n; ++i) {
+        cpsd_gpu_ctx *c = b->cells[i];
+        CK(cudaStreamWaitEvent(c->st, b->ev[0], 0));
+        int rc = energies(c, inner);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(&Eh[16 * i], c->Edev, sizeof(double) * 12, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaMemcpyAsync(&fails[i], c->flags, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    }
+    for (int i = 0; i < n; ++i) {
+        cpsd_gpu_ctx *c = b->cells[i];
+        CK(cudaStreamSynchronize(c->st));
+        for (int k = 0; k < 10; ++k) E[10 * i + k] = Eh[16 * i + k];
+        if (deltae) deltae[i] = Eh[16 * i + 10];
+        if (deltac) deltac[i] = Eh[16 * i + 11];
+        c->lag_fail_total += fails[i];
+        c->ran = true;
+        warn |= fails[i];
+    }
+    return warn ? CPSD_WARN_LAGRANGE : CPSD_OK;
+}
+
+void cpsd_gpu_batch_counters(const cpsd_gpu_batch *b, long long *out)
+{
+    if (!out) return;
+    long long l = b ? b->nlaunch : 0;
+    if (b)
+        for (auto *c : b->cells) l += c->nlaunch;
+    out[0] = l;
+}
+
+void *cpsd_gpu_batch_stream(cpsd_gpu_batch *b) { return b ? (void *)b->st : nullptr; }
+
+void cpsd_gpu_batch_destroy(cpsd_gpu_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->cells[0]->prm.device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_drop_graphs(b);
+    for (auto e : b->ev)
+        if (e) cudaEventDestroy(e);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
 
 const char *cpsd_gpu_strerror(int status)
 {
@@ -715,13 +925,21 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     // the fused density plane must fit in shared memory
     int optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
+    if (p->precision != CPSD_PREC_FP64 && p->precision != CPSD_PREC_MIXED) return CPSD_ERR_ARG;
     for (int m = 0; m < 4; ++m)
-        if ((int)plane_need(c->n, m, h.KX) > optin) return CPSD_ERR_GRID;
-    c->fft = make_fft(c->n);
-    if (!c->fft) return CPSD_ERR_GRID;
+        if ((int)plane_need(c->n, m, h.KX, p->precision) > optin) return CPSD_ERR_GRID;
     DevArena &ar = c->ar;
-    int rc = c->fft->init(ar, h.KX);
+    c->fft64 = make_fft(c->n, CPSD_PREC_FP64);
+    if (!c->fft64) return CPSD_ERR_GRID;
+    int rc = c->fft64->init(ar, h.KX);
     if (rc) return rc;
+    if (p->precision == CPSD_PREC_MIXED) {
+        c->fft32 = make_fft(c->n, CPSD_PREC_MIXED);
+        rc = c->fft32->init(ar, h.KX);
+        if (rc) return rc;
+    }
+    c->precision = p->precision;
+    c->fft = (p->precision == CPSD_PREC_MIXED) ? c->fft32.get() : c->fft64.get();
     CK(upload(ar, &c->pt_i, h.pt_i));
     CK(upload(ar, &c->pt_j, h.pt_j));
     CK(upload(ar, &c->pt_k, h.pt_k));
@@ -763,7 +981,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->r1, 3 * std::max(nion, 1)));
     CK(ar.alloc(&c->r2, 3 * std::max(nion, 1)));
     CK(ar.alloc(&c->fion, 3 * std::max(nion, 1)));
-    const size_t tbytes = c->fft->elem() * (size_t)c->n * h.ncol;
+    const size_t tbytes = c->fft64->elem() * (size_t)c->n * h.ncol;  // widest element
     {
         unsigned char *t = nullptr;
         CK(ar.alloc(&t, tbytes * nb));
@@ -802,7 +1020,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->lag, (size_t)7 * ne02 + 1));
     CK(ar.alloc(&c->lmd, (size_t)2 * ne02));
     CK(ar.alloc(&c->hml, (size_t)2 * ne02));
-    CK(ar.alloc(&c->red, 2 * kLagCluster));
+    CK(ar.alloc(&c->red, 2 * kLagClusterMax));
     CK(ar.alloc(&c->Edev, 16));
     CK(ar.alloc(&c->flags, 4));
     c->gemm_splits_cap = 512;
@@ -815,6 +1033,39 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->bpart, (size_t)2 * nb * c->bblocks));
     CK(ar.alloc(&c->gpart, 2 * c->gblocks));
     CK(ar.alloc(&c->full, (size_t)std::max(nb, c->ispin) * c->n2ft3d));
+    if (c->ne0 <= kLagSmallMax)
+        CK(cudaFuncSetAttribute(lagrange_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(double) * 7 * kLagSmallMax * kLagSmallMax)));
+    else {
+        // 16-CTA clusters where the device can schedule them, else the portable 8
+        CK(cudaFuncSetAttribute(lagrange_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        CK(cudaFuncSetAttribute(lagrange_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        const size_t limit = (size_t)optin - 1024;
+        c->lag_cluster = kLagCluster;
+        c->lag_lb = lagrange_lb(c->ne0, kLagCluster, limit);
+        const int lb16 = lagrange_lb(c->ne0, kLagClusterMax, limit);
+        if (lb16) {
+            cudaLaunchConfig_t cfg{};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = kLagClusterMax;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(kLagClusterMax);
+            cfg.blockDim = dim3(kLagThreads);
+            cfg.dynamicSmemBytes = lagrange_cluster_smem(c->ne0, kLagClusterMax, lb16);
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, lagrange_kernel, &cfg) == cudaSuccess &&
+                nclusters >= 1) {
+                c->lag_cluster = kLagClusterMax;
+                c->lag_lb = lb16;
+            }
+            (void)cudaGetLastError();
+        }
+        if (!c->lag_lb) return CPSD_ERR_BANDS;
+    }
     CK(cudaDeviceSynchronize());  // allocation memsets run on the legacy stream
     *out = c.release();
     return CPSD_OK;
@@ -1046,10 +1297,16 @@ int cpsd_gpu_phase_timing(cpsd_gpu_ctx *c, int on)
 int cpsd_gpu_phase_times(cpsd_gpu_ctx *c, float *ms, int max)
 {
     if (!c || !c->phase_timing || !ms) return 0;
-    if (cudaEventSynchronize(c->pev[kNumPhases]) != cudaSuccess) return 0;
+    if (cudaEventSynchronize(c->pev[kNumPhases]) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
     int n = std::min(max, kNumPhases);
     for (int i = 0; i < n; ++i)
-        if (cudaEventElapsedTime(&ms[i], c->pev[i], c->pev[i + 1]) != cudaSuccess) ms[i] = -1.0f;
+        if (cudaEventElapsedTime(&ms[i], c->pev[i], c->pev[i + 1]) != cudaSuccess) {
+            (void)cudaGetLastError();
+            ms[i] = -1.0f;
+        }
     return n;
 }
 
@@ -1061,6 +1318,22 @@ void cpsd_gpu_counters(const cpsd_gpu_ctx *c, long long *out)
     out[0] = c ? c->nlaunch : 0;
     out[1] = c ? c->h2d : 0;
     out[2] = c ? c->d2h : 0;
+}
+
+int cpsd_gpu_set_precision(cpsd_gpu_ctx *c, int precision)
+{
+    if (!c) return CPSD_ERR_ARG;
+    if (precision == CPSD_PREC_FP64) {
+        c->fft = c->fft64.get();
+    } else if (precision == CPSD_PREC_MIXED) {
+        if (!c->fft32) return CPSD_ERR_ARG;  // the context was created FP64-only
+        c->fft = c->fft32.get();
+    } else {
+        return CPSD_ERR_ARG;
+    }
+    if (precision != c->precision) drop_graphs(c);
+    c->precision = precision;
+    return CPSD_OK;
 }
 
 int cpsd_gpu_use_graphs(cpsd_gpu_ctx *c, int on)

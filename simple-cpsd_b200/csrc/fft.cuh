@@ -50,6 +50,7 @@ inv_z_kernel(Geom g, const cx<double> *__restrict__ psi, long ldp, cx<T> *__rest
     constexpr int P = L::P, Q = L::Q, U = L::U, CPB = kThreads / P;
     constexpr int RS = NF + 1, CS = CPB + 1;  // row / column strides of the tile
     constexpr int TILE = (CPB * RS > NF * CS) ? CPB * RS : NF * CS;
+    constexpr int XS = group_stride<T, NF>();
     extern __shared__ unsigned char smem_raw[];
     cx<T> *tile = reinterpret_cast<cx<T> *>(smem_raw);
     cx<T> *xb = tile + TILE;
@@ -72,7 +73,7 @@ inv_z_kernel(Geom g, const cx<double> *__restrict__ psi, long ldp, cx<T> *__rest
     cx<T> v[Q];
 #pragma unroll
     for (int m = 0; m < Q; ++m) v[m] = row[L::in_index(t, m)];
-    line_fft<NF, +1, T>(v, t, xb + grp * L::XB, tw.n_inv);
+    line_fft<NF, +1, T>(v, t, xb + grp * XS, tw.n_inv);
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < U; ++u)
@@ -110,6 +111,7 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
     constexpr int P = L::P, Q = L::Q, U = L::U, CPB = kThreads / P;
     constexpr int RS = NF + 1, CS = CPB + 1;
     constexpr int TILE = (CPB * RS > NF * CS) ? CPB * RS : NF * CS;
+    constexpr int XS = group_stride<T, NF>();
     extern __shared__ unsigned char smem_raw[];
     cx<T> *tile = reinterpret_cast<cx<T> *>(smem_raw);
     cx<T> *xb = tile + TILE;
@@ -127,7 +129,7 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
     cx<T> v[Q];
 #pragma unroll
     for (int m = 0; m < Q; ++m) v[m] = tile[L::in_index(t, m) * CS + grp];
-    line_fft<NF, -1, T>(v, t, xb + grp * L::XB, tw.n_fwd);
+    line_fft<NF, -1, T>(v, t, xb + grp * XS, tw.n_fwd);
     __syncthreads();
     cx<T> *row = tile + grp * RS;
 #pragma unroll
@@ -165,63 +167,84 @@ struct PlaneArgs {
     const double *rin;    // FWDREAL: real input grid
 };
 
-template <int NF>
+template <typename T, int NF>
 struct PlaneShape {
     static constexpr int H = NF / 2;
     using LY = Line<NF>;
     using LX = Line<H>;
-    static constexpr int XBMAX = (LY::XB > LX::XB) ? LY::XB : LX::XB;
+    // exchange-buffer strides of the y-line groups and the x-row groups
+    static constexpr int SY = group_stride<T, NF>();
+    static constexpr int SX = group_stride<T, H>();
+    // y-line stride: lanes t of an x group read rows k = t + P m of one column
+    // and the 8/P groups of a phase read neighbouring columns
+    static constexpr int YS = (LX::P >= kSlots<T>) ? pad_to(NF + 1, kSlots<T>, 1)
+                                                   : pad_to(NF + 1, kSlots<T>, kSlots<T> / LX::P);
+    // density rows: one extra complex per row moves the next row's group
+    static constexpr int RS = NF + 2;
 };
 
 template <typename T, int NF>
 __host__ __device__ constexpr int plane_threads(int mode)
 {
-    // the density plane (n x n doubles) needs the room of a second CTA at n=128
-    return (mode == PM_DENSITY && NF >= 128) ? 128 : kThreads;
+    return kThreads;
 }
 
 template <typename T, int NF>
 size_t plane_smem_bytes(int mode, int KX)
 {
-    using S = PlaneShape<NF>;
-    int nt = plane_threads<T, NF>(mode);
-    int groups = nt / S::LX::P > nt / S::LY::P ? nt / S::LX::P : nt / S::LY::P;
-    size_t b = sizeof(cx<T>) * ((size_t)KX * (NF + 1) + (size_t)groups * S::XBMAX);
-    if (mode == PM_DENSITY) b += sizeof(double) * NF * NF;
-    return b;
+    using S = PlaneShape<T, NF>;
+    const int nt = plane_threads<T, NF>(mode);
+    const size_t ex_y = (size_t)(nt / S::LY::P) * S::SY, ex_x = (size_t)(nt / S::LX::P) * S::SX;
+    size_t b = sizeof(cx<T>) * ((size_t)KX * S::YS + (ex_y > ex_x ? ex_y : ex_x));
+    return (b + 15) / 16 * 16;
+}
+
+// Two CTAs per SM where the exchange buffers allow it (the density variant
+// keeps its per-lane sums in registers and takes the whole register file).
+template <int NF, int MODE>
+constexpr int plane_min_blocks()
+{
+    return (MODE == PM_DENSITY && NF >= 128) ? 1 : 2;
 }
 
 template <typename T, int NF, int MODE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, plane_min_blocks<NF, MODE>())
 plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
 {
-    using S = PlaneShape<NF>;
+    using S = PlaneShape<T, NF>;
     using LY = typename S::LY;
     using LX = typename S::LX;
     constexpr int H = S::H;
     constexpr int NT = plane_threads<T, NF>(MODE);
-    constexpr int YS = NF + 1;  // Ybuf row stride
+    constexpr int YS = S::YS;  // Ybuf row stride
     constexpr int PY = LY::P, QY = LY::Q, UY = LY::U, NGY = NT / PY;
     constexpr int PX = LX::P, QX = LX::Q, UX = LX::U, NGX = NT / PX;
-    constexpr int NGMAX = NGX > NGY ? NGX : NGY;
+    constexpr int EXB = (NGY * S::SY > NGX * S::SX) ? NGY * S::SY : NGX * S::SX;
     extern __shared__ unsigned char smem_raw[];
     const int KX = g.KX;
     cx<T> *Y = reinterpret_cast<cx<T> *>(smem_raw);  // [KX][YS]
-    cx<T> *xball = Y + KX * YS;                       // [NGMAX][XBMAX]
-    double *RHO = reinterpret_cast<double *>(xball + NGMAX * S::XBMAX);  // [NF][NF]
+    cx<T> *xball = Y + KX * YS;                       // group exchange buffers
+    // DENSITY: each lane owns the same (row, x) points for every band, so the
+    // sum of psi^2 over the band chunk stays in registers
+    constexpr int NIT = (NF + NGX - 1) / NGX;  // x-row iterations per lane
+    double rho[(MODE == PM_DENSITY) ? NIT : 1][(MODE == PM_DENSITY) ? 2 * QX : 1];
 
     const int z = blockIdx.x;
     const int b0 = (MODE == PM_DENSITY || MODE == PM_APPLYV) ? a.chunk_b0[blockIdx.y] : 0;
     const int b1 = (MODE == PM_DENSITY || MODE == PM_APPLYV) ? a.chunk_b0[blockIdx.y + 1] : 1;
     const long plane = (long)NF * NF;
 
-    if constexpr (MODE == PM_DENSITY)
-        for (int i = threadIdx.x; i < NF * NF; i += NT) RHO[i] = 0.0;
+    if constexpr (MODE == PM_DENSITY) {
+#pragma unroll
+        for (int it = 0; it < NIT; ++it)
+#pragma unroll
+            for (int q = 0; q < 2 * QX; ++q) rho[it][q] = 0.0;
+    }
 
     const int gy = threadIdx.x / PY, ty = threadIdx.x % PY;
     const int gx = threadIdx.x / PX, tx = threadIdx.x % PX;
-    cx<T> *xby = xball + gy * S::XBMAX;
-    cx<T> *xbx = xball + gx * S::XBMAX;
+    cx<T> *xby = xball + gy * S::SY;
+    cx<T> *xbx = xball + gx * S::SX;
 
     for (int b = b0; b < b1; ++b) {
         cx<T> *Tplane = Tb + ((long)b * NF + z) * g.ncol;
@@ -247,8 +270,9 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
             __syncthreads();
         }
         // ---- x rows --------------------------------------------------------
-        for (int base = 0; base < NF; base += NGX) {
-            const int j = base + gx;
+#pragma unroll
+        for (int it = 0; it < NIT; ++it) {
+            const int j = it * NGX + gx;
             const bool act = j < NF;
             const int jj = act ? j : 0;
             cx<T> v[QX];
@@ -271,17 +295,11 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
                 line_fft<H, +1, T>(v, tx, xbx, tw.h_inv);
                 // v[u*PX+s] = (psi(2m), psi(2m+1)), m = out_index
                 if constexpr (MODE == PM_DENSITY) {
-                    if (act) {
 #pragma unroll
-                        for (int u = 0; u < UX; ++u)
-#pragma unroll
-                            for (int s = 0; s < PX; ++s) {
-                                const int m = LX::out_index(tx, u, s);
-                                cx<T> w = v[u * PX + s];
-                                double *r = RHO + j * NF + 2 * m;
-                                r[0] += (double)w.x * (double)w.x;
-                                r[1] += (double)w.y * (double)w.y;
-                            }
+                    for (int q = 0; q < QX; ++q) {
+                        const cx<T> w = v[q];
+                        rho[it][2 * q] += (double)w.x * (double)w.x;
+                        rho[it][2 * q + 1] += (double)w.y * (double)w.y;
                     }
                 } else if constexpr (MODE == PM_INVREAL) {
                     if (act) {
@@ -305,21 +323,18 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
                                 }
                             }
                     }
-                } else {  // APPLYV: multiply, then redistribute for the forward
+                } else {  // APPLYV: multiply in place; the DIF forward takes this distribution
                     const double *V = a.V + ((b >= a.ne0) ? NF * plane : 0);
 #pragma unroll
                     for (int u = 0; u < UX; ++u)
 #pragma unroll
                         for (int s = 0; s < PX; ++s) {
                             const int m = LX::out_index(tx, u, s);
-                            cx<T> w = v[u * PX + s];
                             const long o = (long)z * plane + (long)jj * NF + 2 * m;
-                            xbx[m] = cx<T>{(T)((double)w.x * V[o]), (T)((double)w.y * V[o + 1])};
+                            const double2 vv = *reinterpret_cast<const double2 *>(V + o);
+                            cx<T> &w = v[u * PX + s];
+                            w = cx<T>{(T)((double)w.x * vv.x), (T)((double)w.y * vv.y)};
                         }
-                    __syncwarp();
-#pragma unroll
-                    for (int m = 0; m < QX; ++m) v[m] = xbx[LX::in_index(tx, m)];
-                    __syncwarp();
                 }
             } else {  // FWDREAL: load the real row directly in DIT order
                 const double *r = a.rin + (long)z * plane + (long)jj * NF;
@@ -329,13 +344,21 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
                     v[m] = cx<T>{(T)r[2 * mm], (T)r[2 * mm + 1]};
                 }
             }
-            if constexpr (MODE == PM_APPLYV || MODE == PM_FWDREAL) {
+            if constexpr (MODE == PM_APPLYV) {
+                line_fft_dif<H, -1, T>(v, tx, xbx, tw.h_fwd);
+#pragma unroll
+                for (int m = 0; m < QX; ++m) xbx[LX::in_index(tx, m)] = v[m];
+                __syncwarp();
+            }
+            if constexpr (MODE == PM_FWDREAL) {
                 line_fft<H, -1, T>(v, tx, xbx, tw.h_fwd);
 #pragma unroll
                 for (int u = 0; u < UX; ++u)
 #pragma unroll
                     for (int s = 0; s < PX; ++s) xbx[LX::out_index(tx, u, s)] = v[u * PX + s];
                 __syncwarp();
+            }
+            if constexpr (MODE == PM_APPLYV || MODE == PM_FWDREAL) {
                 // r2c post-processing for the kx < KX that are kept
                 for (int k = tx; k < KX; k += PX) {
                     cx<T> zk = xbx[k % H];
@@ -376,8 +399,20 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
     }
 
     if constexpr (MODE == PM_DENSITY) {
-        __syncthreads();
         double *dst = a.rho_part + ((long)blockIdx.y * NF + z) * plane;
-        for (int i = threadIdx.x; i < NF * NF; i += NT) dst[i] = RHO[i];
+#pragma unroll
+        for (int it = 0; it < NIT; ++it) {
+            const int j = it * NGX + gx;
+            if (j < NF) {
+#pragma unroll
+                for (int u = 0; u < UX; ++u)
+#pragma unroll
+                    for (int s = 0; s < PX; ++s) {
+                        const int m = LX::out_index(tx, u, s);
+                        double2 r2 = make_double2(rho[it][2 * (u * PX + s)], rho[it][2 * (u * PX + s) + 1]);
+                        *reinterpret_cast<double2 *>(dst + (long)j * NF + 2 * m) = r2;
+                    }
+            }
+        }
     }
 }

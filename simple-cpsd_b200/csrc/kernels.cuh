@@ -220,6 +220,13 @@ CPSD_D void dirac_vosko(int ispin, double nup_in, double ndn_in, double rho0, do
     const double ec_p = cp1 * log(rs / xxp) + cp2 * log((x + cp3) * (x + cp3) / xxp) + cp4 * atan(cp5 / (x + cp6));
     const double uc_p = ec_p - onesixth * x * (dp1 / x + dp2 / (x + cp3) + dp4 * dxxp / xxp +
                                                dp5 / ((x + dp6) * (x + dp6) + dp7));
+    if (ispin == 1) {
+        // closed shell: nup == ndown, so xi = 0 and f = df = 0 exactly; the
+        // reference's sums reduce to the paramagnetic terms bit for bit
+        ex += ec_p;
+        vx0 += uc_p;
+        return;
+    }
     const double xxf = rs + bf * x + cf;
     const double dxxf = 2.0 * x + bf;
     const double ec_f = cf1 * log(rs / xxf) + cf2 * log((x + cf3) * (x + cf3) / xxf) + cf4 * atan(cf5 / (x + cf6));
@@ -262,19 +269,29 @@ __global__ void density_xc_kernel(XcArgs a)
 }
 
 // ------------------------------------------------------------ FP64 GEMMs
-// part[split][i][j] = sum_{k in chunk} w(k) A[i*lda+k] B[j*ldb+k]; K counts
-// reals, the weight is per complex pair (w[k/2]); the Gamma-point dot of
-// ccpsdv3/gcdotc.c as a matrix product.
-constexpr int GB = 64, GK = 16;
+// part[prod][split][i][j] = sum_{k in chunk} w(k) A_prod[i*lda+k] B_prod[j*ldb+k];
+// K counts reals, the weight is per complex pair (w[k/2]): the Gamma-point
+// dot of ccpsdv3/gcdotc.c as a matrix product.  Up to kTnMaxProd products of
+// the same shape share one launch (blockIdx.z = prod * splits + split).
+constexpr int GB = 64, GK = 16, kTnMaxProd = 4;
+
+struct TnBatch {
+    const double *A[kTnMaxProd];
+    const double *B[kTnMaxProd];
+    double *C[kTnMaxProd];
+    int nprod, splits;
+};
 
 __global__ void __launch_bounds__(256)
-gemm_tn_w_kernel(int M, int N, int K, const double *__restrict__ A, long lda,
-                 const double *__restrict__ B, long ldb, const double *__restrict__ w, int kchunk,
-                 double *__restrict__ part)
+gemm_tn_w_kernel(int M, int N, int K, long lda, long ldb, const double *__restrict__ w, int kchunk,
+                 const __grid_constant__ TnBatch bt, double *__restrict__ part)
 {
     __shared__ double As[GK][GB + 1], Bs[GK][GB + 1];
+    const int prod = blockIdx.z / bt.splits, split = blockIdx.z % bt.splits;
+    const double *__restrict__ A = bt.A[prod];
+    const double *__restrict__ B = bt.B[prod];
     const int i0 = blockIdx.x * GB, j0 = blockIdx.y * GB;
-    const int k0 = blockIdx.z * kchunk;
+    const int k0 = split * kchunk;
     const int k1 = min(K, k0 + kchunk);
     const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
     double acc[4][4] = {};
@@ -307,7 +324,7 @@ gemm_tn_w_kernel(int M, int N, int K, const double *__restrict__ A, long lda,
         }
         __syncthreads();
     }
-    double *out = part + (long)blockIdx.z * M * N;
+    double *out = part + ((long)prod * bt.splits + split) * M * N;
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -317,17 +334,28 @@ gemm_tn_w_kernel(int M, int N, int K, const double *__restrict__ A, long lda,
         }
 }
 
-// C[i*ldc+j] = alpha * sum_s part[s][i][j] (+ beta C), summed in split order
-__global__ void splitk_reduce_kernel(int M, int N, int splits, const double *__restrict__ part,
-                                     double alpha, double beta, double *C, long ldc)
+// C_prod[i*ldc+j] = alpha * sum_s part[prod][s][i][j] (+ beta C): one warp
+// per output, lanes stride over the splits, then a fixed xor butterfly, so
+// the order of the additions (and the bits of the result) never changes.
+__global__ void splitk_reduce_kernel(int M, int N, long ldc, const double *__restrict__ part, double alpha,
+                                     double beta, const __grid_constant__ TnBatch bt)
 {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= M * N) return;
+    const long wid = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long MN = (long)M * N;
+    if (wid >= MN * bt.nprod) return;  // whole warps leave together
+    const int prod = (int)(wid / MN);
+    const long e = wid % MN;
+    const double *p = part + (long)prod * bt.splits * MN + e;
     double s = 0.0;
-    for (int q = 0; q < splits; ++q) s += part[(long)q * M * N + id];
-    const int i = id / N, j = id % N;
-    double *c = C + (long)i * ldc + j;
-    *c = alpha * s + (beta == 0.0 ? 0.0 : beta * *c);
+    for (int q = lane; q < bt.splits; q += 32) s += p[(long)q * MN];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        const int i = (int)(e / N), j = (int)(e % N);
+        double *c = bt.C[prod] + (long)i * ldc + j;
+        *c = alpha * s + (beta == 0.0 ? 0.0 : beta * *c);
+    }
 }
 
 // Out[j*ldo+k] = beta*Out + alpha * sum_l Mat[l + j*ldm] * B[l*ldb + k]
@@ -388,7 +416,6 @@ gemm_nn_kernel(int NJ, int K, int L, double alpha, const double *__restrict__ Ma
 // GEMMs: M22[i][j] = <c2_i|c2_j>, M21[i][j] = <c2_i|c1_j>, M11[i][j] = <c1_i|c1_j>.
 constexpr int kLagCluster = 8;
 constexpr int kLagThreads = 256;
-constexpr int kLagMaxPerThread = 32;  // m*ceil(m/8)/256 <= 32  ->  m <= 256
 
 struct LagArgs {
     int ispin, ne0, ne1;
@@ -396,16 +423,40 @@ struct LagArgs {
     const double *M22[2], *M21[2], *M11[2];
     double *s11, *s12, *s21, *s22, *st1, *X0, *X1;  // ne0^2 each, column-major
     double *lmd;                                     // [ms*ne0^2 + i + j*m]
-    double *red;                                     // [kLagCluster][2]
+    double *red;                                     // [cluster CTAs][2]
     int *fail;                                       // steps whose iteration did not converge
+    int lb;                                          // l-chunk of the cluster kernel's row tiles
 };
 
-__global__ void __cluster_dims__(kLagCluster, 1, 1) __launch_bounds__(kLagThreads)
-lagrange_kernel(LagArgs a)
+// Cluster of kLagClusterMax (or kLagCluster where 16 cannot be scheduled)
+// CTAs; CTA r owns a block of columns.  Thread layout: row i = tid % RT
+// (RT = min(m, 256)) and a block of this CTA's columns.  Per iteration the
+// rows of s21, s11 and X stream through shared memory in chunks of LB
+// columns l; the CTA's columns of X, s12 and st1 stay in shared memory.
+constexpr int kLagClusterMax = 16;
+constexpr int kLagCols = 16;
+
+CPSD_HD size_t lagrange_cluster_smem(int m, int cl, int lb)
+{
+    const int per = (m + cl - 1) / cl;
+    return sizeof(double) * (3 * (size_t)m * per + 3 * (size_t)m * lb);
+}
+
+// widest l-chunk (32, 16, 8 or 4) whose tiles fit in `limit` bytes; 0 if none
+inline int lagrange_lb(int m, int cl, size_t limit)
+{
+    for (int lb = 32; lb >= 4; lb /= 2)
+        if (lagrange_cluster_smem(m, cl, lb) <= limit) return lb;
+    return 0;
+}
+
+__global__ void __launch_bounds__(kLagThreads) lagrange_kernel(LagArgs a)
 {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
+    const int ncta = (int)cl.num_blocks();
     const int tid = threadIdx.x;
+    extern __shared__ double lsm[];
     __shared__ double shv[kLagThreads / 32];
     __shared__ int shi[kLagThreads / 32];
     const long ne02 = (long)a.ne0 * a.ne0;
@@ -416,7 +467,7 @@ lagrange_kernel(LagArgs a)
         const double *M22 = a.M22[ms], *M21 = a.M21[ms], *M11 = a.M11[ms];
         const double dte = a.dte;
         // s matrices, cpsd.c:420-437 (upper triangles mirrored as the reference does)
-        for (long e = (long)rank * kLagThreads + tid; e < kk; e += (long)kLagCluster * kLagThreads) {
+        for (long e = (long)rank * kLagThreads + tid; e < kk; e += (long)ncta * kLagThreads) {
             const int i = (int)(e % m), j = (int)(e / m);
             double v22, v21, v12, v11;
             if (i == j) {
@@ -438,55 +489,121 @@ lagrange_kernel(LagArgs a)
             a.X0[e] = v22;  // sa0 = s22, cpsd.c:441
         }
         cl.sync();
-        // my columns
-        const int per = (m + kLagCluster - 1) / kLagCluster;
+        const int per = (m + ncta - 1) / ncta;  // columns per CTA
         const int jb = rank * per, je = min(m, jb + per);
-        const int mine = (je > jb) ? (je - jb) * m : 0;
+        const int ncl = max(0, je - jb);
+        const int RT = min(m, kLagThreads);
+        const int nsub = kLagThreads / RT;
+        const int csub = (ncl + nsub - 1) / max(nsub, 1);  // columns per thread
+        const int i = tid % RT, sub = tid / RT;
+        const int j0 = sub * csub;
+        const bool active = (sub < nsub) && (i < m);
+        const int LB = a.lb;
+        double *Xs = lsm, *S12s = lsm + (long)m * per, *ST = lsm + 2L * m * per;
+        double *T21 = lsm + 3L * m * per, *T11 = T21 + (long)m * LB, *TX = T11 + (long)m * LB;
+        for (int e = tid; e < m * ncl; e += kLagThreads) {
+            const int l = e % m, jl = e / m;
+            S12s[jl * m + l] = a.s12[l + (long)(jb + jl) * m];
+        }
         double *cur = a.X0, *nxt = a.X1;
-        double keep[kLagMaxPerThread];
         bool done = false;
         int iter = 0;
         while (!done && iter < 30) {
             ++iter;
-            // sa1 = s22 + s21 sa0 + sa0 s12 ; st1 = s11 sa0   (cpsd.c:444-462)
-            int q = 0;
-            for (int e = tid; e < mine; e += kLagThreads, ++q) {
-                const int i = e % m, j = jb + e / m;
-                double t1 = 0.0, t2 = 0.0, t3 = 0.0;
-                for (int l = 0; l < m; ++l) {
-                    const double c_lj = cur[l + (long)j * m];
-                    t1 = fma(a.s21[i + (long)l * m], c_lj, t1);
-                    t2 = fma(cur[i + (long)l * m], a.s12[l + (long)j * m], t2);
-                    t3 = fma(a.s11[i + (long)l * m], c_lj, t3);
-                }
-                double sa1 = t1 + a.s22[i + (long)j * m];
-                sa1 = t2 + sa1;
-                keep[q] = sa1;
-                a.st1[i + (long)j * m] = t3;
+            for (int e = tid; e < m * ncl; e += kLagThreads) {
+                const int l = e % m, jl = e / m;
+                Xs[jl * m + l] = cur[l + (long)(jb + jl) * m];
             }
-            __syncthreads();
+            // sa1 = s22 + s21 sa0 + sa0 s12 ; st1 = s11 sa0   (cpsd.c:444-462);
+            // the partial sa1 waits in nxt for the second product
+            for (int cb = 0; cb < csub; cb += kLagCols) {
+                double t1[kLagCols], t2[kLagCols], t3[kLagCols];
+#pragma unroll
+                for (int q = 0; q < kLagCols; ++q) t1[q] = t2[q] = t3[q] = 0.0;
+                for (int l0 = 0; l0 < m; l0 += LB) {
+                    const int lw = min(LB, m - l0);
+                    __syncthreads();  // previous tile consumed (and Xs written)
+                    for (int e = tid; e < m * lw; e += kLagThreads) {
+                        const int ii = e % m, ll = e / m;
+                        const long g = ii + (long)(l0 + ll) * m;
+                        T21[ll * m + ii] = a.s21[g];
+                        T11[ll * m + ii] = a.s11[g];
+                        TX[ll * m + ii] = cur[g];
+                    }
+                    __syncthreads();
+                    if (active) {
+                        for (int ll = 0; ll < lw; ++ll) {
+                            const int l = l0 + ll;
+                            const double a21 = T21[ll * m + i], a11 = T11[ll * m + i], xil = TX[ll * m + i];
+#pragma unroll
+                            for (int q = 0; q < kLagCols; ++q) {
+                                const int jl = j0 + cb + q;
+                                if (cb + q < csub && jl < ncl) {
+                                    const double xlj = Xs[jl * m + l];
+                                    t1[q] = fma(a21, xlj, t1[q]);
+                                    t2[q] = fma(xil, S12s[jl * m + l], t2[q]);
+                                    t3[q] = fma(a11, xlj, t3[q]);
+                                }
+                            }
+                        }
+                    }
+                }
+                if (active) {
+#pragma unroll
+                    for (int q = 0; q < kLagCols; ++q) {
+                        const int jl = j0 + cb + q;
+                        if (cb + q < csub && jl < ncl) {
+                            const int j = jb + jl;
+                            nxt[i + (long)j * m] = t2[q] + (t1[q] + a.s22[i + (long)j * m]);
+                            ST[jl * m + i] = t3[q];
+                        }
+                    }
+                }
+            }
             // sa1 += sa0 st1 (cpsd.c:463-468); st1 = sa1 - sa0 (:469-470)
-            q = 0;
             double bestv = -1.0;
             int besti = 0x7fffffff;
-            for (int e = tid; e < mine; e += kLagThreads, ++q) {
-                const int i = e % m, j = jb + e / m;
-                double t4 = 0.0;
-                for (int l = 0; l < m; ++l) t4 = fma(cur[i + (long)l * m], a.st1[l + (long)j * m], t4);
-                keep[q] = t4 + keep[q];
-            }
-            __syncthreads();
-            q = 0;
-            for (int e = tid; e < mine; e += kLagThreads, ++q) {
-                const int i = e % m, j = jb + e / m;
-                const long f = i + (long)j * m;
-                nxt[f] = keep[q];
-                const double d = keep[q] - cur[f];
-                a.st1[f] = d;
-                const double ad = fabs(d);
-                if (ad > bestv || (ad == bestv && f < besti)) {
-                    bestv = ad;
-                    besti = (int)f;
+            for (int cb = 0; cb < csub; cb += kLagCols) {
+                double t4[kLagCols];
+#pragma unroll
+                for (int q = 0; q < kLagCols; ++q) t4[q] = 0.0;
+                for (int l0 = 0; l0 < m; l0 += LB) {
+                    const int lw = min(LB, m - l0);
+                    __syncthreads();
+                    for (int e = tid; e < m * lw; e += kLagThreads) {
+                        const int ii = e % m, ll = e / m;
+                        TX[ll * m + ii] = cur[ii + (long)(l0 + ll) * m];
+                    }
+                    __syncthreads();
+                    if (active) {
+                        for (int ll = 0; ll < lw; ++ll) {
+                            const int l = l0 + ll;
+                            const double xil = TX[ll * m + i];
+#pragma unroll
+                            for (int q = 0; q < kLagCols; ++q) {
+                                const int jl = j0 + cb + q;
+                                if (cb + q < csub && jl < ncl) t4[q] = fma(xil, ST[jl * m + l], t4[q]);
+                            }
+                        }
+                    }
+                }
+                if (active) {
+#pragma unroll
+                    for (int q = 0; q < kLagCols; ++q) {
+                        const int jl = j0 + cb + q;
+                        if (cb + q < csub && jl < ncl) {
+                            const long f = i + (long)(jb + jl) * m;
+                            const double sa1 = t4[q] + nxt[f];
+                            nxt[f] = sa1;
+                            const double d = sa1 - cur[f];
+                            a.st1[f] = d;
+                            const double ad = fabs(d);
+                            if (ad > bestv || (ad == bestv && f < besti)) {
+                                bestv = ad;
+                                besti = (int)f;
+                            }
+                        }
+                    }
                 }
             }
             // block argmax (first index of the largest |st1|, as idamax)
@@ -517,7 +634,7 @@ lagrange_kernel(LagArgs a)
             // every CTA reduces the cluster's candidates in the same order
             double gv = -1.0;
             long gi = 0x7fffffff;
-            for (int r = 0; r < kLagCluster; ++r) {
+            for (int r = 0; r < ncta; ++r) {
                 const double v = a.red[2 * r];
                 const long ix = (long)a.red[2 * r + 1];
                 if (v > gv || (v == gv && ix < gi)) {
@@ -538,12 +655,135 @@ lagrange_kernel(LagArgs a)
             }
         }
         if (!done && rank == 0 && tid == 0) atomicAdd(a.fail, 1);
-        // lmd = sa1, cpsd.c:478
-        for (int e = tid; e < mine; e += kLagThreads) {
-            const int i = e % m, j = jb + e / m;
-            a.lmd[ms * ne02 + i + (long)j * m] = nxt[i + (long)j * m];
+        // lmd = sa1, cpsd.c:478 (after 30 unconverged iterations sa1 was swapped into cur)
+        const double *fin = done ? nxt : cur;
+        for (int e = tid; e < m * ncl; e += kLagThreads) {
+            const int ii = e % m, j = jb + e / m;
+            a.lmd[ms * ne02 + ii + (long)j * m] = fin[ii + (long)j * m];
         }
         cl.sync();
+    }
+}
+
+// Small systems (ne0 <= kLagSmallMax): the same iteration in one CTA with
+// every matrix in shared memory; block barriers instead of cluster barriers.
+constexpr int kLagSmallMax = 32;
+
+__global__ void __launch_bounds__(kLagThreads) lagrange_small_kernel(LagArgs a)
+{
+    constexpr int MM = kLagSmallMax * kLagSmallMax;
+    extern __shared__ double lag_sm[];  // 7 * ne0^2 doubles (dynamic)
+    const int ld = a.ne0 * a.ne0;
+    double *s11 = lag_sm, *s12 = lag_sm + ld, *s21 = lag_sm + 2 * ld, *s22 = lag_sm + 3 * ld;
+    double *st1 = lag_sm + 4 * ld;
+    double *X[2] = {lag_sm + 5 * ld, lag_sm + 6 * ld};
+    __shared__ double shv[kLagThreads / 32];
+    __shared__ int shi[kLagThreads / 32];
+    __shared__ int s_done;
+    const int tid = threadIdx.x;
+    const long ne02 = (long)a.ne0 * a.ne0;
+    for (int ms = 0; ms < a.ispin; ++ms) {
+        const int m = ms ? a.ne1 : a.ne0;
+        const int kk = m * m;
+        if (m == 0) continue;
+        const double *M22 = a.M22[ms], *M21 = a.M21[ms], *M11 = a.M11[ms];
+        const double dte = a.dte;
+        for (int e = tid; e < kk; e += kLagThreads) {  // cpsd.c:420-437
+            const int i = e % m, j = e / m;
+            double v22, v21, v12, v11;
+            if (i == j) {
+                v22 = (1.0 - M22[i * m + i]) * 0.5 / dte;
+                v21 = (1.0 - M21[i * m + i]) * 0.5;
+                v12 = v21;
+                v11 = -M11[i * m + i] * 0.5 * dte;
+            } else {
+                const int lo = i < j ? i : j, hi = i < j ? j : i;
+                v22 = -M22[lo * m + hi] * 0.5 / dte;
+                v21 = -M21[lo * m + hi] * 0.5;
+                v12 = -M21[hi * m + lo] * 0.5;
+                v11 = -M11[lo * m + hi] * 0.5 * dte;
+            }
+            s22[e] = v22;
+            s21[e] = v21;
+            s12[e] = v12;
+            s11[e] = v11;
+            X[0][e] = v22;
+        }
+        __syncthreads();
+        int cur = 0, iter = 0;
+        bool done = false;
+        while (!done && iter < 30) {
+            ++iter;
+            double *c = X[cur], *nx = X[cur ^ 1];
+            for (int e = tid; e < kk; e += kLagThreads) {  // cpsd.c:444-462
+                const int i = e % m, j = e / m;
+                double t1 = 0.0, t2 = 0.0, t3 = 0.0;
+                for (int l = 0; l < m; ++l) {
+                    const double c_lj = c[l + j * m];
+                    t1 = fma(s21[i + l * m], c_lj, t1);
+                    t2 = fma(c[i + l * m], s12[l + j * m], t2);
+                    t3 = fma(s11[i + l * m], c_lj, t3);
+                }
+                nx[e] = t2 + (t1 + s22[e]);
+                st1[e] = t3;
+            }
+            __syncthreads();
+            double keep[(MM + kLagThreads - 1) / kLagThreads];
+            int q = 0;
+            for (int e = tid; e < kk; e += kLagThreads, ++q) {  // cpsd.c:463-468
+                const int i = e % m, j = e / m;
+                double t4 = 0.0;
+                for (int l = 0; l < m; ++l) t4 = fma(c[i + l * m], st1[l + j * m], t4);
+                keep[q] = t4 + nx[e];
+            }
+            __syncthreads();
+            double bestv = -1.0;
+            int besti = 0x7fffffff;
+            q = 0;
+            for (int e = tid; e < kk; e += kLagThreads, ++q) {  // cpsd.c:469-470
+                nx[e] = keep[q];
+                const double d = keep[q] - c[e];
+                st1[e] = d;
+                const double ad = fabs(d);
+                if (ad > bestv || (ad == bestv && e < besti)) {
+                    bestv = ad;
+                    besti = e;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                double ov = __shfl_xor_sync(0xffffffffu, bestv, o);
+                int oi = __shfl_xor_sync(0xffffffffu, besti, o);
+                if (ov > bestv || (ov == bestv && oi < besti)) {
+                    bestv = ov;
+                    besti = oi;
+                }
+            }
+            if ((tid & 31) == 0) {
+                shv[tid >> 5] = bestv;
+                shi[tid >> 5] = besti;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                for (int w = 1; w < kLagThreads / 32; ++w)
+                    if (shv[w] > bestv || (shv[w] == bestv && shi[w] < besti)) {
+                        bestv = shv[w];
+                        besti = shi[w];
+                    }
+                // idamax's 1-based index used as 0-based (cpsd.c:471); past st1 lies sa1
+                const long nxi = (long)besti + 1;
+                const double adiff = fabs(nxi < ne02 ? st1[nxi] : nx[nxi - ne02]);
+                s_done = adiff < 1e-15;
+            }
+            __syncthreads();
+            done = s_done != 0;
+            if (!done) cur ^= 1;
+        }
+        if (!done && tid == 0) atomicAdd(a.fail, 1);
+        // converged: sa1 is the buffer just written; stopped at 30: it was swapped into cur
+        const double *fin = done ? X[cur ^ 1] : X[cur];
+        for (int e = tid; e < kk; e += kLagThreads) a.lmd[ms * ne02 + e] = fin[e];
+        __syncthreads();
     }
 }
 
@@ -638,84 +878,121 @@ struct FinalArgs {
     double *E;  // in: E[0] previous energy; out: E[0..9], E[10] deltae, E[11] deltac
 };
 
-__global__ void final_energy_kernel(FinalArgs a)
+// One block of kFinalThreads: every sum is a fixed-order block reduction, so
+// the energies are bitwise reproducible run to run.
+constexpr int kFinalThreads = 256;
+
+__global__ void __launch_bounds__(kFinalThreads) final_energy_kernel(FinalArgs a)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double sh[32];
+    const int tid = threadIdx.x;
     const long ne02 = (long)a.ne0 * a.ne0;
-    // hml and eorbit
-    double eorbit = 0.0;
+    // hml (cpsd.c:497-513): the upper triangle is -<c1_i|cpsi_j>, mirrored; the
+    // mirror and eorbit read hml at the spin-0 offset for both spins
+    double eo = 0.0;
     for (int ms = 0; ms < a.ispin; ++ms) {
         const int m = ms ? a.ne1 : a.ne0;
         double *H = a.hml + ms * ne02;
         const double *M = a.Mh[ms];
-        for (int i = 0; i < m; ++i) {
-            H[i + i * m] = -M[(long)i * m + i];
-            eorbit += a.hml[i + i * m];
-            for (int j = i + 1; j < m; ++j) {
-                H[i + j * m] = -M[(long)i * m + j];
-                H[j + i * m] = a.hml[i + j * m];
-            }
+        for (int e = tid; e < m * m; e += kFinalThreads) {
+            const int i = e % m, j = e / m;
+            if (i <= j) H[i + j * m] = -M[(long)i * m + j];
         }
+        __syncthreads();
+        for (int e = tid; e < m * m; e += kFinalThreads) {
+            const int i = e % m, j = e / m;
+            if (i < j) H[j + i * m] = a.hml[i + j * m];
+        }
+        for (int i = tid; i < m; i += kFinalThreads) eo += a.hml[i + i * m];
+        __syncthreads();
     }
-    if (a.ispin == 1) eorbit *= 2;
+    double eorbit = block_sum<kFinalThreads>(eo, sh);
     // single-field packed terms
-    double t[3] = {0, 0, 0};
-    for (int q = 0; q < 3; ++q)
-        for (int k = 0; k < a.pblocks; ++k) t[q] += a.ppart[q * a.pblocks + k];
-    double eion = t[0] * 0.5 * a.scal2 + a.cewald;
-    // real-space Ewald, cpsd.c:527-545 (A&S 7.1.28 erfc, cpsd.c:11-17)
+    double t[3];
+    for (int q = 0; q < 3; ++q) {
+        double v = 0.0;
+        for (int k = tid; k < a.pblocks; k += kFinalThreads) v += a.ppart[q * a.pblocks + k];
+        t[q] = block_sum<kFinalThreads>(v, sh);
+    }
+    // real-space Ewald, cpsd.c:527-545 (A&S 7.1.28 erfc, cpsd.c:11-17), one
+    // (pair, image) term per thread
     const double B1 = 0.0705230784, B2 = 0.0422820123, B3 = 0.0092705272;
     const double B4 = 0.0001520143, B5 = 0.0002765672, B6 = 0.0000430638;
-    for (int ii = 0; ii < a.nion; ++ii)
-        for (int jj = ii + 1; jj < a.nion; ++jj) {
-            const double dx = a.r1[3 * ii] - a.r1[3 * jj];
-            const double dy = a.r1[1 + 3 * ii] - a.r1[1 + 3 * jj];
-            const double dz = a.r1[2 + 3 * ii] - a.r1[2 + 3 * jj];
-            const double zz = a.zv[a.katm[ii]] * a.zv[a.katm[jj]];
-            for (int l = 0; l < a.nsh; ++l) {
-                const double x = a.rcell[l] + dx, y = a.rcell[l + a.nsh] + dy, z = a.rcell[l + 2 * a.nsh] + dz;
-                const double r = sqrt(x * x + y * y + z * z);
-                const double w = r / a.rcut;
-                const double aa = (1.0 + w * (B1 + w * (B2 + w * (B3 + w * (B4 + w * (B5 + w * B6))))));
-                const double erfc = 1.0 / (aa * aa * aa * aa);
-                eion += zz * (erfc * erfc * erfc * erfc) / r;
-            }
+    const long npair = (long)a.nion * (a.nion - 1) / 2;
+    double ew = 0.0;
+    for (long e = tid; e < npair * a.nsh; e += kFinalThreads) {
+        const long pr = e / a.nsh;
+        const int l = (int)(e % a.nsh);
+        // pair index -> (ii < jj)
+        int ii = 0;
+        long rem = pr;
+        while (rem >= a.nion - 1 - ii) {
+            rem -= a.nion - 1 - ii;
+            ++ii;
         }
+        const int jj = ii + 1 + (int)rem;
+        const double dx = a.r1[3 * ii] - a.r1[3 * jj];
+        const double dy = a.r1[1 + 3 * ii] - a.r1[1 + 3 * jj];
+        const double dz = a.r1[2 + 3 * ii] - a.r1[2 + 3 * jj];
+        const double zz = a.zv[a.katm[ii]] * a.zv[a.katm[jj]];
+        const double x = a.rcell[l] + dx, y = a.rcell[l + a.nsh] + dy, z = a.rcell[l + 2 * a.nsh] + dz;
+        const double r = sqrt(x * x + y * y + z * z);
+        const double w = r / a.rcut;
+        const double aa = (1.0 + w * (B1 + w * (B2 + w * (B3 + w * (B4 + w * (B5 + w * B6))))));
+        const double erfc = 1.0 / (aa * aa * aa * aa);
+        ew += zz * (erfc * erfc * erfc * erfc) / r;
+    }
+    const double eion_real = block_sum<kFinalThreads>(ew, sh);
+    // xc
+    double ex = 0.0, px = 0.0;
+    for (int k = tid; k < a.gblocks; k += kFinalThreads) {
+        ex += a.gpart[k];
+        px += a.gpart[a.gblocks + k];
+    }
+    double exc = block_sum<kFinalThreads>(ex, sh);
+    double pxc = block_sum<kFinalThreads>(px, sh);
+    // kinetic and deltac per band
+    double ek = 0.0, dcmax = 0.0;
+    for (int b = tid; b < a.nb; b += kFinalThreads) {
+        double s1 = 0.0, s2 = 0.0;
+        for (int k = 0; k < a.bblocks; ++k) {
+            s1 += a.bpart[(long)b * a.bblocks + k];
+            s2 += a.bpart[((long)a.nb + b) * a.bblocks + k];
+        }
+        ek += s1;
+        dcmax = fmax(dcmax, s2);
+    }
+    double eke = block_sum<kFinalThreads>(ek, sh);
+    // max over threads (order-independent)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dcmax = fmax(dcmax, __shfl_xor_sync(0xffffffffu, dcmax, o));
+    __syncthreads();
+    if ((tid & 31) == 0) sh[tid >> 5] = dcmax;
+    __syncthreads();
+    double dc = 0.0;
+    if (tid == 0)
+        for (int i = 0; i < kFinalThreads / 32; ++i) dc = fmax(dc, sh[i]);
+    __syncthreads();
+    // nonlocal energy from the last step's projections, cpsd.c:593-634
+    double en = 0.0;
+    for (long e = tid; e < (long)a.nproj * a.nb; e += kFinalThreads) {
+        const double sw = a.beta[e];
+        en += sw * sw * a.scal2 / a.vnlnrm_p[e / a.nb];
+    }
+    double enl = block_sum<kFinalThreads>(en, sh);
+    if (tid != 0) return;
+    if (a.ispin == 1) eorbit *= 2;
+    const double eion = t[0] * 0.5 * a.scal2 + a.cewald + eion_real;
     const double ehartr = t[1] * a.omega * 0.5;
     const double elocal = t[2];
-    // xc
-    double exc = 0.0, pxc = 0.0;
-    for (int k = 0; k < a.gblocks; ++k) exc += a.gpart[k];
-    for (int k = 0; k < a.gblocks; ++k) pxc += a.gpart[a.gblocks + k];
     if (a.ispin == 1) {
         exc += exc;
         pxc += pxc;
     }
     exc *= a.dv;
     pxc *= a.dv;
-    // kinetic
-    double eke = 0.0;
-    for (int b = 0; b < a.nb; ++b) {
-        double s = 0.0;
-        for (int k = 0; k < a.bblocks; ++k) s += a.bpart[(long)b * a.bblocks + k];
-        eke += s;
-    }
     if (a.ispin == 1) eke = 2 * eke;
-    // nonlocal from the last step's projections, cpsd.c:593-634
-    double enl = 0.0;
-    for (int P = 0; P < a.nproj; ++P)
-        for (int b = 0; b < a.nb; ++b) {
-            const double sw = a.beta[(long)P * a.nb + b];
-            enl += sw * sw * a.scal2 / a.vnlnrm_p[P];
-        }
     if (a.ispin == 1) enl = 2 * enl;
-    // deltac
-    double dc = 0.0;
-    for (int b = 0; b < a.nb; ++b) {
-        double s = 0.0;
-        for (int k = 0; k < a.bblocks; ++k) s += a.bpart[((long)a.nb + b) * a.bblocks + k];
-        if (s > dc) dc = s;
-    }
     const double eold = a.E[0];
     a.E[0] = eorbit + eion + exc - ehartr - pxc;
     a.E[1] = eorbit;

@@ -244,3 +244,58 @@ def test_reference_main_linked_against_library(tmp_path):
     for r, w in zip(rows, g["rows"]):
         assert abs(r[1] - w[1]) <= 1e-9 * max(1.0, abs(w[1]))
     assert np.allclose([final[i] for i in range(10)], g["final"], rtol=1e-9, atol=1e-9)
+
+
+def test_batched_cells_equal_individual_runs():
+    """Config 4 style: uneven cells stepped in one graph per SD step give the
+    same bits as each cell run on its own."""
+    specs = [configs.small_diamond(24, 4, seed=21), configs.small_h2(16, seed=5),
+             configs.small_diamond(32, 5, ecut=25.0, seed=8), configs.small_diamond(48, 6, ecut=30.0, seed=9)]
+    inps = [inputs.build_inputs(s) for s in specs]
+    solo = []
+    for inp in inps:
+        cell = api.GpuCell(inp)
+        cell.set_state(inp.c2, inp.r2)
+        cell.run(3)
+        cell.run(2)
+        solo.append(cell.E.copy())
+        cell.close()
+    cells = []
+    for inp in inps:
+        cell = api.GpuCell(inp)
+        cell.set_state(inp.c2, inp.r2)
+        cells.append(cell)
+    batch = api.GpuBatch(cells)
+    batch.run(3)
+    E = batch.run(2)
+    for i in range(len(inps)):
+        assert np.array_equal(E[i], solo[i]), i
+    batch.close()
+    for c in cells:
+        c.close()
+
+
+def test_mixed_precision_tracks_fp64(restatement):
+    """FP32 transforms (orbitals, potentials and reductions FP64): the energy
+    follows the FP64 oracle to ~1e-7 relative; an FP64 refinement call on
+    the same state restores the parity bar on its energies' consistency."""
+    inp = inputs.build_inputs(configs.small_diamond(32, 5, ecut=25.0))
+    so = oracle.State(inp)
+    cell = api.GpuCell(inp, precision=lib.CPSD_PREC_MIXED)
+    cell.set_state(inp.c2, inp.r2)
+    for _ in range(3):
+        restatement.run(inp, 2, so)
+        cell.run(2)
+        assert abs(cell.E[0] - so.E[0]) < 1e-6 * abs(so.E[0]) + 1e-6
+    # switch to FP64 for a refinement call from the mixed state: its energy is
+    # that of an FP64 evaluation of the same state (checked against the oracle)
+    st = api.State(inp)
+    cell.get_state(st)
+    cell.set_precision(lib.CPSD_PREC_FP64)
+    cell.E[0] = 0.0
+    cell.run(1)
+    probe = oracle.State(inp)
+    probe.c2[:] = st.c2
+    restatement.run(inp, 1, probe)
+    assert abs(cell.E[0] - probe.E[0]) < E_TOL
+    cell.close()
