@@ -159,9 +159,11 @@ def cpu_reference(inp, budget_s, min_calls=3, inner=1):
 
 
 # ----------------------------------------------------------------- GPU arm
-def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True, precision=0):
+def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True, precision=0, gemm=0):
     from cpsd_b200 import api
     cell = api.GpuCell(inp, precision=precision)
+    if gemm:
+        cell.set_gemm(gemm)
     cell.set_state(inp.c2, inp.r2)
     if want_phases:
         cell.phase_timing(True)
@@ -272,7 +274,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="arithmetic of the timed workload (the default line is fp64)")
+    ap.add_argument("--gemm", default="fp64", choices=["fp64", "tf32x3", "tf32x3_overlaps"],
+                    help="TN-product engine of a mixed-precision run")
     args = ap.parse_args()
+    prec_code = {"fp64": 0, "mixed": 1}[args.precision]
+    gemm_code = {"fp64": 0, "tf32x3": 1, "tf32x3_overlaps": 3}[args.gemm] if prec_code else 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -284,7 +292,8 @@ def main():
     spec = configs.NAMED[args.workload]()
     inp = inputs.build_inputs(spec)
     config = {"workload": args.workload, "nfft": inp.nfft, "nbands": inp.nbands, "nion": inp.nion,
-              "npw": inp.npw, "ecut_ry": spec.ecut_ry, "inner": args.inner, "precision": "fp64",
+              "npw": inp.npw, "ecut_ry": spec.ecut_ry, "inner": args.inner, "precision": args.precision,
+              "gemm": args.gemm if prec_code else "fp64",
               "step": "one cpsd() call: %d SD steps + energies" % args.inner,
               "l2": "flushed (256 MB write) before every timed call", "parallelism": "replicas"}
 
@@ -333,7 +342,8 @@ def main():
 
     sampler = ClockSampler(local)
     sampler.start()
-    total_ms, launches, ph, geo, E = time_cell(inp, args.steps, args.warmup, args.inner, torch, dist)
+    total_ms, launches, ph, geo, E = time_cell(inp, args.steps, args.warmup, args.inner, torch, dist,
+                                               precision=prec_code, gemm=gemm_code)
     clocks = sampler.stop()
     total_ms = max_over_ranks(total_ms, dist, torch, "cuda")
     sd_steps = args.steps * args.inner * world
@@ -341,8 +351,8 @@ def main():
 
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": config, "gpu_launches": int(launches), "clocks": clocks,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if not prec_code else "f32+f64",
+            "data": "synthetic (seeded)", "config": config, "gpu_launches": int(launches), "clocks": clocks,
             "final_energy": float(E[0])}
     line["roofline"] = roofline_entry(ph, geo, inp.nbands, inp.nfft, inp.ispin, args.workload)
     line["phases_ms"] = {k: round(v, 5) for k, v in ph.items()}
@@ -376,6 +386,12 @@ def main():
         extra["mixed_diamond64_128"] = {"value": 3 * args.inner / (tmm * 1e-3), "unit": "steps/s",
                                         "ms_per_sd_step": tmm / (3 * args.inner),
                                         "phases_ms": {k: round(v, 4) for k, v in ph3m.items()}}
+        # the same with the TN products on the tensor cores (3xTF32, tcgen05)
+        for key, mode in (("mixed_tf32x3_diamond64_128", 1), ("mixed_tf32x3_overlaps_diamond64_128", 3)):
+            tmt, _, ph3t, _, _ = time_cell(big, 3, 1, args.inner, torch, None, precision=1, gemm=mode)
+            extra[key] = {"value": 3 * args.inner / (tmt * 1e-3), "unit": "steps/s",
+                          "ms_per_sd_step": tmt / (3 * args.inner),
+                          "phases_ms": {k: round(v, 4) for k, v in ph3t.items()}}
         line["extra"] = extra
         extra["diamond64_128"] = {
             "value": 3 * args.inner / (tms * 1e-3), "unit": "steps/s",

@@ -27,6 +27,7 @@ enum {
     CPSD_ERR_EMPTY_MASK = 5,    /* the cutoff mask selects no G vector */
     CPSD_ERR_UNMASKED_PSI = 6,  /* input orbitals have coefficients outside the mask */
     CPSD_ERR_MOVE = 7,          /* move=1 (ionic forces) requested but not built in */
+    CPSD_ERR_TIMEOUT = 8,       /* a bounded wait on the device ran out (tensor-core pipeline) */
     CPSD_WARN_LAGRANGE = 10     /* (positive warning) Lagrange iteration hit 30 steps; the
                                    reference prints "ierr=10" and continues (cpsd.c:477) */
 };
@@ -89,6 +90,15 @@ int cpsd_gpu_fft_status(void);
 typedef struct cpsd_gpu_ctx cpsd_gpu_ctx;
 
 enum { CPSD_PREC_FP64 = 0, CPSD_PREC_MIXED = 1 };
+/* Engine of the TN products of the mixed path: FP64 CUDA cores, or three
+ * TF32 tensor-core products (hi*hi + hi*lo + lo*hi, FP32 accumulate in tensor
+ * memory, FP64 split-K sums), about FP32 accuracy.  CPSD_GEMM_TF32X3 moves
+ * the projector coefficients (the KB contraction) to the tensor cores;
+ * CPSD_GEMM_TF32X3_OVERLAPS moves the three Lagrange overlaps as well.  The
+ * Lagrange solve divides (1 - <c2|c2>) by dte (about 1e-2), so FP32-level
+ * overlaps cost about 1e-6 relative in the energy per step: follow such a
+ * run with FP64 steps. */
+enum { CPSD_GEMM_FP64 = 0, CPSD_GEMM_TF32X3 = 1, CPSD_GEMM_TF32X3_OVERLAPS = 3 };
 
 typedef struct {
     int nfft;        /* grid edge */
@@ -173,6 +183,55 @@ void *cpsd_gpu_stream(cpsd_gpu_ctx *c);
 
 void cpsd_gpu_destroy(cpsd_gpu_ctx *c);
 
+/* ------------------------------------------------------ learned preconditioner */
+
+/*
+ * A 4 -> 64 -> 64 -> 64 -> 1 tanh network (BF16 weights, FP32 accumulate)
+ * that maps, per band and |G| shell, (shell kinetic energy / band kinetic
+ * energy, log band kinetic energy, log band residual, step feature) to the
+ * log of a scale of the SD step.  Training runs on the GPU (hand-written
+ * forward, backward and Adam kernels); inputs are host arrays of n x 4
+ * floats, targets n floats.
+ */
+typedef struct cpsd_mlp cpsd_mlp;
+int cpsd_mlp_nparams(void);
+int cpsd_mlp_create(unsigned long long seed, cpsd_mlp **out);
+int cpsd_mlp_forward(cpsd_mlp *m, const float *X, int n, float *y);
+/* mean-squared-error loss and its gradient with respect to the FP32 parameters */
+int cpsd_mlp_gradient(cpsd_mlp *m, const float *X, const float *T, int n, float *grad, float *loss);
+/* `steps` Adam steps over contiguous minibatches of the (pre-shuffled) data */
+int cpsd_mlp_train(cpsd_mlp *m, const float *X, const float *T, int n, int steps, int batch, float lr,
+                   float *losses);
+int cpsd_mlp_get_params(const cpsd_mlp *m, float *p);
+int cpsd_mlp_set_params(cpsd_mlp *m, const float *p);
+void cpsd_mlp_destroy(cpsd_mlp *m);
+
+/*
+ * Attach a network (or NULL for the reference's plain SD): each step then
+ * updates c2 = c1 + dte (cpsi + (K(band, shell) - 1) R) instead of
+ * c2 = c1 + dte cpsi, before the Lagrange correction, with
+ * R = cpsi - C1 (C1' W cpsi) the residual outside the occupied subspace.
+ * Where R = 0 the step is plain SD's, so the fixed point (H psi = psi Lambda)
+ * is unchanged; the caller keeps plain SD as the fallback when an energy
+ * rises.  No counterpart in the reference (its update is cpsd.c:398-400).
+ */
+int cpsd_gpu_set_preconditioner(cpsd_gpu_ctx *c, cpsd_mlp *m);
+/* Select the TN-product engine of the mixed-precision path (CPSD_GEMM_*).
+ * The hml product of the energies stays FP64.  The tensor-core modes need a
+ * context created with CPSD_PREC_MIXED and have no effect while it runs
+ * FP64. */
+int cpsd_gpu_set_gemm(cpsd_gpu_ctx *c, int mode);
+/* Trust-region bound on the learned log step scale, clamped to [-2, 4.5]
+ * (attaching a network opens it fully).  Read on the device at every step,
+ * so it takes effect without re-capturing the step graphs. */
+int cpsd_gpu_set_preconditioner_cap(cpsd_gpu_ctx *c, double max_log_k);
+
+/* Packed orbitals (ne0+ne1 bands x npw complex, sphere order) out and in. */
+int cpsd_gpu_get_packed(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi);
+int cpsd_gpu_set_packed(cpsd_gpu_ctx *c, const double *c2);
+/* The sphere: half-box index, Gamma-point weight and |G| shell of every point. */
+int cpsd_gpu_get_sphere(const cpsd_gpu_ctx *c, int *pt_idx, double *weights, int *shell);
+
 /* ------------------------------------------------------ batches of cells */
 
 typedef struct cpsd_gpu_batch cpsd_gpu_batch;
@@ -193,6 +252,20 @@ int cpsd_gpu_batch_run(cpsd_gpu_batch *b, int inner, double *E, double *deltae, 
 void cpsd_gpu_batch_counters(const cpsd_gpu_batch *b, long long *out);
 void *cpsd_gpu_batch_stream(cpsd_gpu_batch *b);
 void cpsd_gpu_batch_destroy(cpsd_gpu_batch *b);
+
+/*
+ * Weighted Gamma-point overlaps as one matrix product, on device memory:
+ *   C[i*ldc + j] = sum_{k<K} w[k/2] A[i*lda + k] B[j*ldb + k]   (i < M, j < N)
+ * with K reals per row (interleaved re/im of packed coefficients) and one
+ * weight per complex pair (w = NULL: all ones).  Each entry is the gcdotc()
+ * of ccpsdv3/gcdotc.c:15-28 between rows i and j; ccpsdv3/cpsd.c:420-431
+ * builds s22, s21, s12 and s11 from such products, one pair at a time.
+ * method: CPSD_GEMM_FP64 or CPSD_GEMM_TF32X3.  Runs on `stream` (NULL: the
+ * legacy stream) of the current device and returns after it finishes; the
+ * split-K workspace is allocated and freed inside the call.
+ */
+int cpsd_overlap_tn(int method, int M, int N, int K, const double *A, long lda, const double *B, long ldb,
+                    const double *w, double *C, long ldc, void *stream);
 
 #ifdef __cplusplus
 }

@@ -153,6 +153,41 @@ class GpuCell:
     def stream(self) -> int:
         return self._L.cpsd_gpu_stream(self.h) or 0
 
+    def set_preconditioner(self, mlp) -> None:
+        """Attach a trained Mlp (learned SD step scales) or None for plain SD."""
+        self._check(self._L.cpsd_gpu_set_preconditioner(self.h, mlp.h if mlp is not None else None),
+                    "cpsd_gpu_set_preconditioner")
+        self._mlp = mlp  # keep it alive while attached
+
+    def set_gemm(self, mode: int) -> None:
+        """TN-product engine of the mixed path: CPSD_GEMM_FP64 or CPSD_GEMM_TF32X3."""
+        self._check(self._L.cpsd_gpu_set_gemm(self.h, int(mode)), "cpsd_gpu_set_gemm")
+
+    def set_preconditioner_cap(self, max_log_k: float) -> None:
+        """Trust-region bound on the learned log step scale."""
+        self._check(self._L.cpsd_gpu_set_preconditioner_cap(self.h, float(max_log_k)),
+                    "cpsd_gpu_set_preconditioner_cap")
+
+    def get_packed(self):
+        """(c1, c2, cpsi) as complex (nbands, npw) arrays in sphere order."""
+        nb, npw = self.inp.nbands, self.npw
+        out = [np.zeros((nb, npw), dtype=np.complex128) for _ in range(3)]
+        self._check(self._L.cpsd_gpu_get_packed(self.h, *[_ptr(o) for o in out]), "cpsd_gpu_get_packed")
+        return out
+
+    def set_packed(self, c2: np.ndarray) -> None:
+        c2 = np.ascontiguousarray(c2, dtype=np.complex128)
+        self._check(self._L.cpsd_gpu_set_packed(self.h, _ptr(c2)), "cpsd_gpu_set_packed")
+
+    def sphere(self):
+        """(half-box index, Gamma weight, |G| shell) of every sphere point."""
+        npw = self.npw
+        idx = np.zeros(npw, dtype=np.int32)
+        w = np.zeros(npw)
+        sh = np.zeros(npw, dtype=np.int32)
+        self._check(self._L.cpsd_gpu_get_sphere(self.h, _ptr(idx), _ptr(w), _ptr(sh)), "cpsd_gpu_get_sphere")
+        return idx, w, sh
+
     def set_state(self, c2: np.ndarray, r2: np.ndarray) -> None:
         self._check(self._L.cpsd_gpu_set_state(self.h, _ptr(np.ascontiguousarray(c2)),
                                                _ptr(np.ascontiguousarray(r2))), "cpsd_gpu_set_state")
@@ -235,6 +270,71 @@ class GpuBatch:
             pass
 
 
+class Mlp:
+    """The preconditioner network on the GPU (forward, gradient, Adam training)."""
+
+    def __init__(self, seed: int = 0):
+        self._L = _l.load()
+        h = ctypes.c_void_p()
+        rc = self._L.cpsd_mlp_create(ctypes.c_ulonglong(seed), ctypes.byref(h))
+        if rc:
+            raise CpsdError(rc, "cpsd_mlp_create")
+        self.h = h
+        self.nparams = self._L.cpsd_mlp_nparams()
+
+    def forward(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.zeros(X.shape[0], dtype=np.float32)
+        rc = self._L.cpsd_mlp_forward(self.h, _ptr(X), X.shape[0], _ptr(y))
+        if rc:
+            raise CpsdError(rc, "cpsd_mlp_forward")
+        return y
+
+    def gradient(self, X: np.ndarray, T: np.ndarray):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = ctypes.c_float()
+        rc = self._L.cpsd_mlp_gradient(self.h, _ptr(X), _ptr(T), X.shape[0], _ptr(g), ctypes.byref(loss))
+        if rc:
+            raise CpsdError(rc, "cpsd_mlp_gradient")
+        return float(loss.value), g
+
+    def train(self, X: np.ndarray, T: np.ndarray, steps: int, batch: int, lr: float) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        losses = np.zeros(steps, dtype=np.float32)
+        rc = self._L.cpsd_mlp_train(self.h, _ptr(X), _ptr(T), X.shape[0], steps, batch, ctypes.c_float(lr),
+                                    _ptr(losses))
+        if rc:
+            raise CpsdError(rc, "cpsd_mlp_train")
+        return losses
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.nparams, dtype=np.float32)
+        self._L.cpsd_mlp_get_params(self.h, _ptr(p))
+        return p
+
+    @params.setter
+    def params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        rc = self._L.cpsd_mlp_set_params(self.h, _ptr(p))
+        if rc:
+            raise CpsdError(rc, "cpsd_mlp_set_params")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self._L.cpsd_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def dropin_counters():
     """Counters of the context the drop-in cpsd() keeps between calls."""
     L = _l.load()
@@ -264,3 +364,26 @@ def cr_fft3b(A: np.ndarray, nfft: int) -> None:
 def rc_fft3f(A: np.ndarray, nfft: int) -> None:
     """In place: real (padded x lines) -> half box (complex), unnormalised."""
     _fft(_l.load().rc_fft3f_, A, nfft)
+
+
+def overlap_tn(A, B, w=None, method: int = _l.CPSD_GEMM_FP64, out=None, stream=None):
+    """C = A^T W B on device tensors (torch float64 CUDA tensors, rows of K
+    reals with unit stride): C[i, j] = sum_k w[k // 2] A[i, k] B[j, k], the
+    Gamma-point gcdotc of every row pair.  Returns C (M x N)."""
+    import torch
+    M, K = A.shape
+    N = B.shape[0]
+    for t in (A, B):
+        if t.dtype != torch.float64 or not t.is_cuda or t.stride(1) != 1:
+            raise ValueError("A and B must be float64 CUDA tensors with unit stride along K")
+    if B.shape[1] != K:
+        raise ValueError("A and B must have the same K")
+    if out is None:
+        out = torch.empty((M, N), dtype=torch.float64, device=A.device)
+    s = stream if stream is not None else torch.cuda.current_stream(A.device).cuda_stream
+    wp = None if w is None else w.data_ptr()
+    rc = _l.load().cpsd_overlap_tn(int(method), M, N, K, A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0),
+                                   wp, out.data_ptr(), out.stride(0), s)
+    if rc != _l.CPSD_OK:
+        raise CpsdError(rc, "cpsd_overlap_tn")
+    return out

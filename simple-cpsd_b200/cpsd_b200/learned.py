@@ -1,0 +1,292 @@
+"""Learned preconditioner for the SD update: data, training, guarded use.
+
+The network (csrc/mlp.cuh, run and trained on the GPU) maps, per band b and
+|G| shell s, the features
+
+    x = (t_s / KE_b,  log KE_b,  log |r_b|^2,  log(1 + step) / 10)
+
+(t_s the shell's kinetic energy, KE_b the band's kinetic energy, r_b the part
+of -H psi_b orthogonal to psi_b) to log K, and each SD step becomes
+
+    c2 = c1 + dte (cpsi + (K(b, s) - 1) R),   R = cpsi - C1 (C1' W cpsi)
+
+before the reference's Lagrange correction: only the residual R (the part of
+-H psi outside the occupied subspace) is stepped by dte K, so wherever R = 0
+the step is plain SD's and the fixed point H psi = psi Lambda is unchanged.
+
+Training targets come from SD trajectories of the method itself: at a
+recorded step, with C the orbitals, G the occupied-subspace-projected
+gradient and C_h the orbitals `horizon` plain steps later (aligned to C by
+the orthogonal Procrustes rotation, since SD fixes only the subspace), the
+per-shell least-squares step that points G at C_h - C is
+
+    K*(b, s) = sum_{p in s} w_p Re(G_bp^* (C_h - C)_bp) / (dte sum_{p in s} w_p |G_bp|^2).
+
+For a mode of curvature lam plain SD contracts the error by (1 - dte lam) per
+step, so K* is about min(horizon, 1 / (dte lam)): one learned step stands in
+for up to `horizon` plain steps on slow modes and is critically damped on
+stiff ones.  Targets are clipped to the kernel's range [LOGK_MIN, LOGK_MAX].
+
+Use is guarded: energies are compared every `inner` steps and a block that
+raises the energy, or whose Lagrange iteration did not converge, is redone
+from its start with plain SD, so the converged answer is plain SD's (the fixed
+point H psi = psi Lambda does not depend on K).  A trust region bounds log K:
+it shrinks after a rejected block and grows back after accepted ones.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import time
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import api, inputs
+
+NSHELL = 64  # csrc/mlp.cuh kShells
+LOGK_MIN, LOGK_MAX = -2.0, 4.5  # csrc/mlp.cuh kLogKMin, kLogKMax
+
+
+@dataclasses.dataclass
+class Sphere:
+    w: np.ndarray      # Gamma-point weight per sphere point
+    tg: np.ndarray     # |G|^2 / 2 per sphere point
+    shell: np.ndarray  # shell index per point
+    tmax: float
+
+
+def sphere_of(cell: api.GpuCell) -> Sphere:
+    idx, w, sh = cell.sphere()
+    tg = cell.inp.tg[idx]
+    return Sphere(w=w, tg=tg, shell=sh, tmax=float(tg.max()))
+
+
+def features(sp: Sphere, c1: np.ndarray, cpsi: np.ndarray, step: int) -> np.ndarray:
+    """(nb*NSHELL, 4) float32 inputs, as prec_features_kernel builds them."""
+    w = sp.w
+    ke = np.maximum((w * sp.tg * (c1.real ** 2 + c1.imag ** 2)).sum(1), 1e-12)
+    h = (w * (c1.real * cpsi.real + c1.imag * cpsi.imag)).sum(1)
+    q = (w * (cpsi.real ** 2 + cpsi.imag ** 2)).sum(1)
+    res = np.maximum(q - h * h, 1e-30)
+    ts = (np.arange(NSHELL) + 0.5) * sp.tmax / NSHELL
+    nb = c1.shape[0]
+    X = np.zeros((nb, NSHELL, 4), dtype=np.float32)
+    X[:, :, 0] = ts[None, :] / ke[:, None]
+    X[:, :, 1] = np.log(ke)[:, None]
+    X[:, :, 2] = np.log(res)[:, None]
+    X[:, :, 3] = math.log1p(step) / 10.0
+    return X.reshape(-1, 4)
+
+
+def gamma_dot(w: np.ndarray, A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """Matrix of Gamma-point products <A_i|B_j> (real)."""
+    return (A.conj() * w) @ B.T
+
+
+def targets(sp: Sphere, c1: np.ndarray, cpsi: np.ndarray, cfin: np.ndarray, dte: float):
+    """(nb*NSHELL,) log K* and a validity mask (shells carrying gradient)."""
+    w = sp.w
+    # the residual: gradient projected out of the occupied subspace (the part
+    # the preconditioner steps)
+    G = cpsi - gamma_dot(w, c1, cpsi).real.T @ c1
+    # align the end point to C (orthogonal Procrustes on the real overlap)
+    M = gamma_dot(w, cfin, c1).real
+    Uo, _, Vt = np.linalg.svd(M)
+    D = (Uo @ Vt).T @ cfin - c1
+    # and keep only the displacement outside the occupied subspace
+    D = D - gamma_dot(w, c1, D).real.T @ c1
+    num = np.zeros((c1.shape[0], NSHELL))
+    den = np.zeros((c1.shape[0], NSHELL))
+    prod = w * (G.real * D.real + G.imag * D.imag)
+    pw = w * (G.real ** 2 + G.imag ** 2)
+    for s in range(NSHELL):
+        m = sp.shell == s
+        if m.any():
+            num[:, s] = prod[:, m].sum(1)
+            den[:, s] = pw[:, m].sum(1)
+    k = num / np.maximum(dte * den, 1e-300)
+    valid = (den > 1e-12 * max(den.max(), 1e-300)) & (k > 0)
+    logk = np.log(np.clip(k, math.exp(LOGK_MIN), math.exp(LOGK_MAX)))
+    return logk.reshape(-1).astype(np.float32), valid.reshape(-1)
+
+
+def record_trajectory(spec: inputs.CellSpec, nsteps: int, inner: int, every: int, horizon: int = 32):
+    """Plain SD; every `every` blocks of `inner` steps record (step, c1, cpsi,
+    C_h) with C_h the orbitals `horizon` steps later.  Returns (sphere,
+    records, dte, energies)."""
+    inp = inputs.build_inputs(spec)
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    sp = sphere_of(cell)
+    snaps, energies = [], []
+    step = 0
+    for k in range(nsteps // inner):
+        cell.run(inner)
+        step += inner
+        energies.append(float(cell.E[0]))
+        if k % every == 0:
+            # c1 is the input of the block's last step, taken after step - 1 steps
+            c1, _, cpsi = cell.get_packed()
+            cell.run(horizon)
+            step += horizon
+            snaps.append((step - horizon - 1, c1, cpsi, cell.get_packed()[1]))
+    dte = inp.dt / math.sqrt(inp.fmass)
+    cell.close()
+    return sp, snaps, dte, energies
+
+
+def dataset(trajs) -> Tuple[np.ndarray, np.ndarray]:
+    Xs, Ts = [], []
+    for sp, snaps, dte, _ in trajs:
+        for step, c1, cpsi, ch in snaps:
+            X = features(sp, c1, cpsi, step)
+            T, valid = targets(sp, c1, cpsi, ch, dte)
+            Xs.append(X[valid])
+            Ts.append(T[valid])
+    return np.concatenate(Xs), np.concatenate(Ts)
+
+
+def train(mlp: api.Mlp, X: np.ndarray, T: np.ndarray, steps: int = 3000, batch: int = 4096,
+          lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+    """Shuffle once (seeded) and run `steps` Adam steps on the GPU."""
+    perm = np.random.default_rng(seed).permutation(X.shape[0])
+    return mlp.train(X[perm], T[perm], steps, batch, lr)
+
+
+@dataclasses.dataclass
+class RunResult:
+    energies: List[float]
+    steps_to_tol: Optional[int]
+    seconds_to_tol: Optional[float]
+    rejected_blocks: int
+    steps: int
+
+
+def run(spec_or_inp, e_conv: Optional[float], tol_per_ion: float, max_steps: int, inner: int = 20,
+        mlp: Optional[api.Mlp] = None, precision: int = 0) -> RunResult:
+    """SD (plain or learned-preconditioned with fallback) until the energy is
+    within tol_per_ion * nion of e_conv (or max_steps)."""
+    inp = spec_or_inp if isinstance(spec_or_inp, inputs.CpsdInputs) else inputs.build_inputs(spec_or_inp)
+    cell = api.GpuCell(inp, precision=precision)
+    cell.set_state(inp.c2, inp.r2)
+    tol = tol_per_ion * inp.nion
+    energies, rejected, steps = [], 0, 0
+    hit_step, hit_time = None, None
+    prev = math.inf
+    cap = LOGK_MAX
+    min_bands = min(int(n) for n in inp.ne[:inp.ispin])
+    t0 = time.perf_counter()
+    if mlp is not None:
+        cell.set_preconditioner(mlp)
+    while steps < max_steps:
+        if mlp is not None:
+            start = cell.get_packed()[1]
+            warn0 = cell.lagrange_warnings
+            cell.set_preconditioner_cap(cap)
+            e = float(cell.run(inner)[0])
+            # (with one band per spin the reference's convergence test can never
+            # pass, so its warning says nothing there)
+            lag_failed = cell.lagrange_warnings > warn0 and min_bands > 1
+            if not math.isfinite(e) or e > prev or lag_failed:
+                # rejected: redo the block from its start with plain SD
+                rejected += 1
+                cap = max(LOGK_MIN, cap - 0.7)
+                cell.set_packed(start)
+                cell.set_preconditioner(None)
+                e = float(cell.run(inner)[0])
+                cell.set_preconditioner(mlp)
+            else:
+                cap = min(LOGK_MAX, cap + 0.35)
+        else:
+            e = float(cell.run(inner)[0])
+        steps += inner
+        energies.append(e)
+        prev = e
+        if e_conv is not None and hit_step is None and abs(e - e_conv) <= tol:
+            hit_step, hit_time = steps, time.perf_counter() - t0
+            break
+    cell.close()
+    return RunResult(energies, hit_step, hit_time, rejected, steps)
+
+
+def converged_energy(spec_or_inp, max_steps: int, inner: int = 200, tol: float = 1e-10) -> Tuple[float, int]:
+    """Plain FP64 SD until the energy changes by less than tol over each of
+    five consecutive blocks of `inner` steps (or max_steps).  Returns the
+    energy and the steps taken (== max_steps: not converged)."""
+    inp = spec_or_inp if isinstance(spec_or_inp, inputs.CpsdInputs) else inputs.build_inputs(spec_or_inp)
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    prev, steps, e, quiet = math.inf, 0, math.inf, 0
+    while steps < max_steps:
+        e = float(cell.run(inner)[0])
+        steps += inner
+        quiet = quiet + 1 if abs(e - prev) < tol else 0
+        if quiet >= 5:
+            break
+        prev = e
+    cell.close()
+    return e, steps
+
+
+def experiment(n_train: int = 12, n_eval: int = 4, traj_steps: int = 30000, inner: int = 100, every: int = 10,
+               train_steps: int = 3000, tol_per_ion: float = 1e-6, max_steps: int = 120000,
+               out: Optional[str] = None, weights: Optional[str] = None, horizon: int = 32) -> dict:
+    """Train on jittered 8-atom diamond cells, evaluate steps and time to
+    tol_per_ion on held-out cells against plain SD."""
+    import json
+    from . import configs
+    t0 = time.perf_counter()
+    trajs = [record_trajectory(configs.diamond8_64(seed=1000 + i), traj_steps, inner, every, horizon)
+             for i in range(n_train)]
+    t_traj = time.perf_counter() - t0
+    X, T = dataset(trajs)
+    mlp = api.Mlp(seed=0)
+    t0 = time.perf_counter()
+    losses = train(mlp, X, T, steps=train_steps)
+    t_train = time.perf_counter() - t0
+    if weights:
+        np.save(weights, mlp.params)
+    evals = []
+    for i in range(n_eval):
+        inp = inputs.build_inputs(configs.diamond8_64(seed=5000 + i))
+        e_conv, conv_steps = converged_energy(inp, max_steps=max_steps)
+        plain = run(inp, e_conv, tol_per_ion, max_steps, inner=inner)
+        lrn = run(inp, e_conv, tol_per_ion, max_steps, inner=inner, mlp=mlp)
+        evals.append({"seed": 5000 + i, "e_conv": e_conv, "conv_steps": conv_steps,
+                      "plain_steps": plain.steps_to_tol, "plain_s": plain.seconds_to_tol,
+                      "learned_steps": lrn.steps_to_tol, "learned_s": lrn.seconds_to_tol,
+                      "learned_rejected_blocks": lrn.rejected_blocks,
+                      "learned_final_abs_dE_per_ion": abs(lrn.energies[-1] - e_conv) / inp.nion})
+    res = {"train_cells": n_train, "samples": int(X.shape[0]), "trajectory_steps": traj_steps, "horizon": horizon,
+           "trajectory_seconds": t_traj, "train_steps": train_steps, "train_seconds": t_train,
+           "loss_first": float(losses[0]), "loss_last": float(np.mean(losses[-50:])),
+           "tol_per_ion": tol_per_ion, "eval": evals}
+    ok = [e for e in evals if e["plain_steps"] and e["learned_steps"]]
+    if ok:
+        res["mean_step_ratio_plain_over_learned"] = float(np.mean([e["plain_steps"] / e["learned_steps"] for e in ok]))
+        res["mean_time_ratio_plain_over_learned"] = float(np.mean([e["plain_s"] / e["learned_s"] for e in ok]))
+    if out:
+        with open(out, "w") as f:
+            json.dump(res, f, indent=1)
+    mlp.close()
+    return res
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=12)
+    ap.add_argument("--eval", type=int, default=4)
+    ap.add_argument("--traj-steps", type=int, default=30000)
+    ap.add_argument("--inner", type=int, default=100)
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--max-steps", type=int, default=120000)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--weights", default=None)
+    ap.add_argument("--horizon", type=int, default=32)
+    a = ap.parse_args()
+    r = experiment(a.train, a.eval, a.traj_steps, a.inner, 10, a.train_steps, 1e-6, a.max_steps, a.out, a.weights,
+                   a.horizon)
+    print(json.dumps(r, indent=1))

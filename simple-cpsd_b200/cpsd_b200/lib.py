@@ -21,10 +21,15 @@ CPSD_ERR_BANDS = 4
 CPSD_ERR_EMPTY_MASK = 5
 CPSD_ERR_UNMASKED_PSI = 6
 CPSD_ERR_MOVE = 7
+CPSD_ERR_TIMEOUT = 8
 CPSD_WARN_LAGRANGE = 10
 
 CPSD_PREC_FP64 = 0
 CPSD_PREC_MIXED = 1
+
+CPSD_GEMM_FP64 = 0
+CPSD_GEMM_TF32X3 = 1
+CPSD_GEMM_TF32X3_OVERLAPS = 3
 
 # every symbol include/cpsd_b200.h declares
 EXPORTS = [
@@ -37,6 +42,11 @@ EXPORTS = [
     "cpsd_gpu_dropin_context", "cpsd_gpu_phase_timing", "cpsd_gpu_phase_times",
     "cpsd_gpu_phase_name", "cpsd_gpu_stream", "cpsd_gpu_destroy", "cpsd_gpu_batch_create",
     "cpsd_gpu_batch_run", "cpsd_gpu_batch_counters", "cpsd_gpu_batch_stream", "cpsd_gpu_batch_destroy",
+    "cpsd_mlp_nparams", "cpsd_mlp_create", "cpsd_mlp_forward", "cpsd_mlp_gradient", "cpsd_mlp_train",
+    "cpsd_mlp_get_params", "cpsd_mlp_set_params", "cpsd_mlp_destroy", "cpsd_gpu_set_preconditioner",
+    "cpsd_gpu_set_preconditioner_cap",
+    "cpsd_gpu_get_packed", "cpsd_gpu_set_packed", "cpsd_gpu_get_sphere", "cpsd_gpu_set_gemm",
+    "cpsd_overlap_tn",
 ]
 
 
@@ -97,6 +107,22 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_gpu_batch_stream.restype = _P
     lib.cpsd_gpu_batch_destroy.argtypes = [_P]
     lib.cpsd_gpu_batch_destroy.restype = None
+    lib.cpsd_mlp_create.argtypes = [ctypes.c_ulonglong, ctypes.POINTER(_P)]
+    lib.cpsd_mlp_forward.argtypes = [_P, _P, _I, _P]
+    lib.cpsd_mlp_gradient.argtypes = [_P, _P, _P, _I, _P, _P]
+    lib.cpsd_mlp_train.argtypes = [_P, _P, _P, _I, _I, _I, ctypes.c_float, _P]
+    lib.cpsd_mlp_get_params.argtypes = [_P, _P]
+    lib.cpsd_mlp_set_params.argtypes = [_P, _P]
+    lib.cpsd_mlp_destroy.argtypes = [_P]
+    lib.cpsd_mlp_destroy.restype = None
+    lib.cpsd_gpu_set_preconditioner.argtypes = [_P, _P]
+    lib.cpsd_gpu_set_preconditioner_cap.argtypes = [_P, _D]
+    lib.cpsd_gpu_get_packed.argtypes = [_P, _P, _P, _P]
+    lib.cpsd_gpu_set_packed.argtypes = [_P, _P]
+    lib.cpsd_gpu_get_sphere.argtypes = [_P, _P, _P, _P]
+    lib.cpsd_gpu_set_gemm.argtypes = [_P, _I]
+    _L = ctypes.c_long
+    lib.cpsd_overlap_tn.argtypes = [_I, _I, _I, _I, _P, _L, _P, _L, _P, _P, _L, _P]
     lib.cpsd_gpu_destroy.argtypes = [_P]
     lib.cpsd_gpu_destroy.restype = None
     lib.cpsd_gpu_fft_status.restype = _I

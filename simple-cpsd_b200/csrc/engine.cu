@@ -15,6 +15,8 @@
 #include "cpsd_b200.h"
 #include "fft.cuh"
 #include "kernels.cuh"
+#include "mlp.cuh"
+#include "tc_gemm.cuh"
 
 namespace {
 
@@ -38,6 +40,17 @@ cudaError_t &last_cuda_error()
 }
 
 inline long cdiv(long a, long b) { return (a + b - 1) / b; }
+
+// Allow a kernel the device's opt-in shared memory minus its static part.
+template <typename K>
+cudaError_t allow_max_smem(K kernel, int optin)
+{
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - (int)fa.sharedSizeBytes);
+}
 
 // ------------------------------------------------------------ geometry
 struct HostGeom {
@@ -135,6 +148,7 @@ struct FftOpsT final : FftOps {
     int KX = 0;
     size_t zsmem = 0;
     size_t psmem[4] = {0, 0, 0, 0};
+    bool two_cta[4] = {false, false, false, false};  // launch the two-CTA build of a plane mode
 
     size_t elem() const override { return sizeof(cx<T>); }
 
@@ -188,11 +202,36 @@ struct FftOpsT final : FftOps {
         // The limit is a per-kernel (process-wide) attribute shared by every
         // context on the device: set it to the device maximum, launch with
         // what this sphere needs.
-        CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-        CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_APPLYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-        CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_INVREAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-        CK(cudaFuncSetAttribute(plane_kernel<T, NF, PM_FWDREAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(allow_plane<PM_DENSITY>(optin));
+        CK(allow_plane<PM_APPLYV>(optin));
+        CK(allow_plane<PM_INVREAL>(optin));
+        CK(allow_plane<PM_FWDREAL>(optin));
+        // two CTAs per SM when two planes (plus the per-CTA reserve) fit
+        int sm_bytes = 0, reserve = 0;
+        CK(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        CK(cudaDeviceGetAttribute(&reserve, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+        for (int m = 0; m < 4; ++m) two_cta[m] = 2 * (psmem[m] + (size_t)reserve) <= (size_t)sm_bytes;
         return CPSD_OK;
+    }
+
+    template <int MODE>
+    cudaError_t allow_plane(int optin)
+    {
+        cudaError_t e = allow_max_smem(plane_kernel<T, NF, MODE, 1>, optin);
+        if constexpr (plane_has_two_cta_build<NF, MODE>())
+            if (e == cudaSuccess) e = allow_max_smem(plane_kernel<T, NF, MODE, 2>, optin);
+        return e;
+    }
+
+    template <int MODE>
+    void launch_plane(dim3 grid, int nt, const Geom &g, void *Tb, const PlaneArgs &a, cudaStream_t s)
+    {
+        if constexpr (plane_has_two_cta_build<NF, MODE>())
+            if (two_cta[MODE]) {
+                plane_kernel<T, NF, MODE, 2><<<grid, nt, psmem[MODE], s>>>(g, (cx<T> *)Tb, a, tw);
+                return;
+            }
+        plane_kernel<T, NF, MODE, 1><<<grid, nt, psmem[MODE], s>>>(g, (cx<T> *)Tb, a, tw);
     }
 
     void inv_z(const Geom &g, const cx<double> *psi, long ldp, void *Tb, int nb, cudaStream_t s) override
@@ -223,18 +262,10 @@ struct FftOpsT final : FftOps {
         dim3 grid(NF, (unsigned)nchunks);
         const int nt = plane_threads<T, NF>(mode);
         switch (mode) {
-        case PM_DENSITY:
-            plane_kernel<T, NF, PM_DENSITY><<<grid, nt, psmem[mode], s>>>(g, (cx<T> *)Tb, a, tw);
-            break;
-        case PM_APPLYV:
-            plane_kernel<T, NF, PM_APPLYV><<<grid, nt, psmem[mode], s>>>(g, (cx<T> *)Tb, a, tw);
-            break;
-        case PM_INVREAL:
-            plane_kernel<T, NF, PM_INVREAL><<<grid, nt, psmem[mode], s>>>(g, (cx<T> *)Tb, a, tw);
-            break;
-        default:
-            plane_kernel<T, NF, PM_FWDREAL><<<grid, nt, psmem[mode], s>>>(g, (cx<T> *)Tb, a, tw);
-            break;
+        case PM_DENSITY: launch_plane<PM_DENSITY>(grid, nt, g, Tb, a, s); break;
+        case PM_APPLYV: launch_plane<PM_APPLYV>(grid, nt, g, Tb, a, s); break;
+        case PM_INVREAL: launch_plane<PM_INVREAL>(grid, nt, g, Tb, a, s); break;
+        default: launch_plane<PM_FWDREAL>(grid, nt, g, Tb, a, s); break;
         }
     }
     bool mode_ok(int mode) const { return psmem[mode] != 0; }
@@ -286,6 +317,19 @@ size_t plane_need(int n, int mode, int KX, int precision = CPSD_PREC_FP64)
 
 }  // namespace
 
+// ------------------------------------------------------------ network object
+struct cpsd_mlp {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    DevArena ar;
+    float *p = nullptr, *m1 = nullptr, *m2 = nullptr, *g = nullptr;
+    __nv_bfloat16 *wq = nullptr;
+    long adam_t = 0;
+    // training buffers, grown on demand
+    int cap = 0;
+    float *X = nullptr, *T = nullptr, *y = nullptr, *H = nullptr, *D = nullptr, *dy = nullptr, *lp = nullptr;
+};
+
 // ------------------------------------------------------------ context
 struct cpsd_gpu_ctx {
     cpsd_gpu_params prm{};
@@ -299,6 +343,7 @@ struct cpsd_gpu_ctx {
     FftOps *fft = nullptr;                 // the active transform engine
     std::unique_ptr<FftOps> fft64, fft32;  // FP64 (parity) and FP32 (mixed) engines
     int precision = CPSD_PREC_FP64;
+    int gemm_mode = CPSD_GEMM_FP64;  // TN products of the mixed path (CPSD_GEMM_*)
     int npw = 0, npw_pad = 0, nproj = 0;
     long ldc = 0;  // complex stride between bands
     int nchunk0 = 0, nchunk1 = 0;
@@ -312,6 +357,15 @@ struct cpsd_gpu_ctx {
     int graph_launches = 0;
     int lag_cluster = 8;  // CTAs per cluster of the Lagrange solver (16 where schedulable)
     int lag_lb = 0;       // its row-tile width
+    // learned preconditioner (optional): shells, stats, features, outputs
+    cpsd_mlp *mlp = nullptr;
+    int *shell = nullptr, *dstep = nullptr;
+    float *pcap = nullptr;  // trust-region bound on the learned log step scale
+    cx<double> *pR = nullptr;  // residual of -H psi outside the occupied subspace
+    double *pM = nullptr;      // <cpsi_b|c1_a> per spin
+    double *pstats = nullptr, tmax = 0.0;
+    long long steps_run = 0;  // SD steps taken by this context
+    float *pX = nullptr, *py = nullptr;
     // optional phase timing: events recorded between the phases of a step
     // (captured into the step graphs), read back by cpsd_gpu_phase_times()
     bool phase_timing = false;
@@ -342,20 +396,32 @@ struct cpsd_gpu_ctx {
 
 namespace {
 
-// Batched weighted TN products C_q = alpha A_q' W B_q (+ beta C_q), q < nprod,
-// split along K so that about two CTAs per SM run, each split >= 64 reals.
-int gemm_tn_batch(cpsd_gpu_ctx *c, int M, int N, int K, int nprod, const double *const *A, long lda,
-                  const double *const *B, long ldb, const double *w, double alpha, double beta,
-                  double *const *C, long ldc)
+// Split-K plan of a batch of weighted TN products: about two CTAs per SM,
+// each split at least 64 reals, partials within ws_elems.
+struct TnPlan {
+    long splits;
+    int kchunk;
+};
+
+TnPlan tn_plan(int M, int N, int K, int nprod, bool tc, size_t ws_elems)
 {
-    if (M <= 0 || N <= 0 || nprod <= 0) return CPSD_OK;
-    if (nprod > kTnMaxProd) return CPSD_ERR_ARG;
-    const long tiles = cdiv(M, GB) * cdiv(N, GB) * nprod;
+    const int tm = tc ? kTcM : GB, tn = tc ? kTcN : GB, bk = tc ? kTcBK : GK;
+    const long tiles = cdiv(M, tm) * cdiv(N, tn) * nprod;
     long splits = std::max<long>(1, cdiv(2 * 148, tiles));
     splits = std::min<long>(splits, std::max<long>(1, K / 64));
-    while ((size_t)splits * M * N * nprod > c->gemm_ws_elems && splits > 1) --splits;
-    const int kchunk = (int)(cdiv(cdiv(K, splits), GK) * GK);
-    splits = cdiv(K, kchunk);
+    while ((size_t)splits * M * N * nprod > ws_elems && splits > 1) --splits;
+    const int kchunk = (int)(cdiv(cdiv(K, splits), bk) * bk);
+    return TnPlan{cdiv(K, kchunk), kchunk};
+}
+
+// C_q = alpha A_q' W B_q (+ beta C_q), q < nprod: split-K partial products
+// (FP64 CUDA cores, or 3xTF32 on tcgen05 when tc) and a fixed-order FP64
+// reduction.  Returns the number of launches.
+int launch_tn(int M, int N, int K, int nprod, const double *const *A, long lda, const double *const *B, long ldb,
+              const double *w, double alpha, double beta, double *const *C, long ldc, bool tc, double *ws,
+              size_t ws_elems, int *err, cudaStream_t s)
+{
+    const TnPlan pl = tn_plan(M, N, K, nprod, tc, ws_elems);
     TnBatch bt{};
     for (int q = 0; q < nprod; ++q) {
         bt.A[q] = A[q];
@@ -363,19 +429,41 @@ int gemm_tn_batch(cpsd_gpu_ctx *c, int M, int N, int K, int nprod, const double 
         bt.C[q] = C[q];
     }
     bt.nprod = nprod;
-    bt.splits = (int)splits;
-    dim3 grid((unsigned)cdiv(M, GB), (unsigned)cdiv(N, GB), (unsigned)(splits * nprod));
-    gemm_tn_w_kernel<<<grid, 256, 0, c->st>>>(M, N, K, lda, ldb, w, kchunk, bt, c->gws);
-    splitk_reduce_kernel<<<(unsigned)cdiv((long)M * N * nprod * 32, 256), 256, 0, c->st>>>(M, N, ldc, c->gws,
-                                                                                          alpha, beta, bt);
-    c->nlaunch += 2;
+    bt.splits = (int)pl.splits;
+    if (tc) {
+        dim3 grid((unsigned)cdiv(M, kTcM), (unsigned)cdiv(N, kTcN), (unsigned)(pl.splits * nprod));
+        tc_gemm_tn_kernel<<<grid, kTcThreads, kTcSmem, s>>>(M, N, K, lda, ldb, w, pl.kchunk, bt, ws, err);
+    } else {
+        dim3 grid((unsigned)cdiv(M, GB), (unsigned)cdiv(N, GB), (unsigned)(pl.splits * nprod));
+        gemm_tn_w_kernel<<<grid, 256, 0, s>>>(M, N, K, lda, ldb, w, pl.kchunk, bt, ws);
+    }
+    splitk_reduce_kernel<<<(unsigned)cdiv((long)M * N * nprod * 32, 256), 256, 0, s>>>(M, N, ldc, ws, alpha, beta,
+                                                                                       bt);
+    return 2;
+}
+
+// Which TN products may run on the tensor cores (bits of CPSD_GEMM_*).
+enum { TN_PROJECTOR = 1, TN_OVERLAPS = 2 };
+
+// Batched weighted TN products of a context; `which` names the product so
+// that the tensor-core variant runs where the context runs mixed precision
+// and its GEMM mode includes that product.
+int gemm_tn_batch(cpsd_gpu_ctx *c, int M, int N, int K, int nprod, const double *const *A, long lda,
+                  const double *const *B, long ldb, const double *w, double alpha, double beta,
+                  double *const *C, long ldc, int which = 0)
+{
+    if (M <= 0 || N <= 0 || nprod <= 0) return CPSD_OK;
+    if (nprod > kTnMaxProd) return CPSD_ERR_ARG;
+    const bool tc = (c->gemm_mode & which) != 0 && c->precision == CPSD_PREC_MIXED;
+    c->nlaunch += launch_tn(M, N, K, nprod, A, lda, B, ldb, w, alpha, beta, C, ldc, tc, c->gws, c->gemm_ws_elems,
+                            c->flags + 2, c->st);
     return CPSD_OK;
 }
 
 int gemm_tn(cpsd_gpu_ctx *c, int M, int N, int K, const double *A, long lda, const double *B, long ldb,
-            const double *w, double alpha, double beta, double *C, long ldc)
+            const double *w, double alpha, double beta, double *C, long ldc, int which = 0)
 {
-    return gemm_tn_batch(c, M, N, K, 1, &A, lda, &B, ldb, w, alpha, beta, &C, ldc);
+    return gemm_tn_batch(c, M, N, K, 1, &A, lda, &B, ldb, w, alpha, beta, &C, ldc, which);
 }
 
 void gemm_nn(cpsd_gpu_ctx *c, int NJ, int K, int L, double alpha, const double *Mat, long ldm,
@@ -479,7 +567,7 @@ int one_step(cpsd_gpu_ctx *c)
                                                                                 c->tg, c1, c2); c->nlaunch += 1;
     if (c->nproj > 0) {
         int rc = gemm_tn(c, c->nproj, c->nb, K, (const double *)c->proj, ldr, (const double *)c1, ldr, c->w,
-                         1.0, 0.0, c->beta, c->nb);
+                         1.0, 0.0, c->beta, c->nb, TN_PROJECTOR);
         if (rc) return rc;
         kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, s>>>(
             c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT); c->nlaunch += 1;
@@ -502,6 +590,29 @@ int one_step(cpsd_gpu_ctx *c)
     e.scal1 = c->scal1;
     e.dte = c->dte;
     c->fft->fwd_z_sd(c->g, c->Tb, e, c->nb, s); c->nlaunch += 1;
+    if (c->mlp) {  // learned step scales per band and |G| shell
+        // The residual R = cpsi - C1 (C1' W cpsi) per spin: only R is
+        // preconditioned, so the update is plain SD wherever R = 0 and the
+        // fixed point H psi = psi Lambda is that of plain SD.
+        CK(cudaMemcpyAsync(c->pR, c->cpsi, sizeof(cx<double>) * c->nb * c->ldc, cudaMemcpyDeviceToDevice, s));
+        for (int ms = 0; ms < c->ispin; ++ms) {
+            const int m = ms ? c->ne1 : c->ne0;
+            const long off = (long)(ms ? c->ne0 : 0) * ldr;
+            double *Mt = c->pM + (long)ms * c->ne0 * c->ne0;  // Mt[b][a] = <cpsi_b|c1_a>
+            int rc = gemm_tn(c, m, m, K, (const double *)c->cpsi + off, ldr, (const double *)c1 + off, ldr, c->w,
+                             1.0, 0.0, Mt, m);
+            if (rc) return rc;
+            gemm_nn(c, m, K, m, -1.0, Mt, m, (const double *)c1 + off, ldr, 1.0, (double *)c->pR + off, ldr);
+        }
+        band_stats_kernel<<<c->nb, 256, 0, s>>>(c->npw, c->ldc, c->w, c->tg, c1, c->cpsi, c->pstats);
+        prec_features_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 256), 256, 0, s>>>(c->nb, c->tmax, c->pstats,
+                                                                                      c->dstep, c->pX);
+        mlp_forward_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 128), 128, 0, s>>>(
+            c->nb * kShells, c->pX, c->mlp->wq, c->mlp->p, c->py, nullptr);
+        prec_update_kernel<<<(unsigned)cdiv((long)c->nb * c->npw, 256), 256, 0, s>>>(
+            c->nb, c->npw, c->ldc, c->shell, c->py, c->pcap, c->dte, c->pR, c2, c->dstep);
+        c->nlaunch += 4;
+    }
     mark(c, 9);
     // overlaps and Lagrange multipliers, cpsd.c:415-479
     LagArgs la{};
@@ -517,7 +628,7 @@ int one_step(cpsd_gpu_ctx *c)
         // the three overlaps of this spin in one launch
         const double *As[3] = {C2, C2, C1}, *Bs[3] = {C2, C1, C1};
         double *Cs[3] = {(double *)Mblk(c, ms, 0), (double *)Mblk(c, ms, 1), (double *)Mblk(c, ms, 2)};
-        int rc = gemm_tn_batch(c, m, m, K, 3, As, ldr, Bs, ldr, c->w, 1.0, 0.0, Cs, m);
+        int rc = gemm_tn_batch(c, m, m, K, 3, As, ldr, Bs, ldr, c->w, 1.0, 0.0, Cs, m, TN_OVERLAPS);
         if (rc) return rc;
         la.M22[ms] = Mblk(c, ms, 0);
         la.M21[ms] = Mblk(c, ms, 1);
@@ -812,7 +923,7 @@ int cpsd_gpu_batch_run(cpsd_gpu_batch *b, int inner, double *E, double *deltae, 
     const int n = (int)b->cells.size();
     for (int i = 0; i < n; ++i) {
         cpsd_gpu_ctx *c = b->cells[i];
-        CK(cudaMemsetAsync(c->flags, 0, sizeof(int), b->st));
+        CK(cudaMemsetAsync(c->flags, 0, 3 * sizeof(int), b->st));
         CK(cudaMemcpyAsync(c->Edev, E + 10 * i, sizeof(double), cudaMemcpyHostToDevice, b->st));
     }
     for (int it = 0; it < inner; ++it) {
@@ -823,25 +934,29 @@ int cpsd_gpu_batch_run(cpsd_gpu_batch *b, int inner, double *E, double *deltae, 
     CK(cudaEventRecord(b->ev[0], b->st));
     int warn = 0;
     std::vector<double> Eh(16 * n);
-    std::vector<int> fails(n, 0);
+    std::vector<int> fails(3 * n, 0);
     for (int i = 0; i < n; ++i) {
         cpsd_gpu_ctx *c = b->cells[i];
         CK(cudaStreamWaitEvent(c->st, b->ev[0], 0));
         int rc = energies(c, inner);
         if (rc) return rc;
         CK(cudaMemcpyAsync(&Eh[16 * i], c->Edev, sizeof(double) * 12, cudaMemcpyDeviceToHost, c->st));
-        CK(cudaMemcpyAsync(&fails[i], c->flags, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaMemcpyAsync(&fails[3 * i], c->flags, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
     }
+    int timeout = 0;
     for (int i = 0; i < n; ++i) {
         cpsd_gpu_ctx *c = b->cells[i];
         CK(cudaStreamSynchronize(c->st));
         for (int k = 0; k < 10; ++k) E[10 * i + k] = Eh[16 * i + k];
         if (deltae) deltae[i] = Eh[16 * i + 10];
         if (deltac) deltac[i] = Eh[16 * i + 11];
-        c->lag_fail_total += fails[i];
+        c->lag_fail_total += fails[3 * i];
+        c->steps_run += inner;
         c->ran = true;
-        warn |= fails[i];
+        warn |= fails[3 * i];
+        timeout |= fails[3 * i + 2];
     }
+    if (timeout) return CPSD_ERR_TIMEOUT;
     return warn ? CPSD_WARN_LAGRANGE : CPSD_OK;
 }
 
@@ -875,6 +990,7 @@ const char *cpsd_gpu_strerror(int status)
     case CPSD_OK: return "ok";
     case CPSD_ERR_CUDA: return cudaGetErrorString(last_cuda_error());
     case CPSD_ERR_ARG: return "invalid argument";
+    case CPSD_ERR_TIMEOUT: return "a bounded wait on the device ran out (tensor-core pipeline)";
     case CPSD_ERR_GRID: return "unsupported FFT grid (nfft must be 16, 24, 32, 48, 64 or 128, and the sphere must fit the plane kernel)";
     case CPSD_ERR_BANDS: return "more than 256 bands in a spin channel";
     case CPSD_ERR_EMPTY_MASK: return "the cutoff mask selects no G vector";
@@ -937,6 +1053,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
         c->fft32 = make_fft(c->n, CPSD_PREC_MIXED);
         rc = c->fft32->init(ar, h.KX);
         if (rc) return rc;
+        CK(cudaFuncSetAttribute(tc_gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     }
     c->precision = p->precision;
     c->fft = (p->precision == CPSD_PREC_MIXED) ? c->fft32.get() : c->fft64.get();
@@ -1033,13 +1150,21 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->bpart, (size_t)2 * nb * c->bblocks));
     CK(ar.alloc(&c->gpart, 2 * c->gblocks));
     CK(ar.alloc(&c->full, (size_t)std::max(nb, c->ispin) * c->n2ft3d));
+    CK(ar.alloc(&c->shell, (size_t)c->npw_pad));
+    CK(ar.alloc(&c->dstep, 1));
+    CK(ar.alloc(&c->pcap, 1));
+    CK(ar.alloc(&c->pR, (size_t)nb * P));
+    CK(ar.alloc(&c->pM, (size_t)c->ispin * c->ne0 * c->ne0));
+    CK(ar.alloc(&c->pstats, (size_t)3 * nb));
+    CK(ar.alloc(&c->pX, (size_t)4 * nb * kShells));
+    CK(ar.alloc(&c->py, (size_t)nb * kShells));
     if (c->ne0 <= kLagSmallMax)
         CK(cudaFuncSetAttribute(lagrange_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(sizeof(double) * 7 * kLagSmallMax * kLagSmallMax)));
     else {
         // 16-CTA clusters where the device can schedule them, else the portable 8
         CK(cudaFuncSetAttribute(lagrange_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        CK(cudaFuncSetAttribute(lagrange_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(allow_max_smem(lagrange_kernel, optin));
         const size_t limit = (size_t)optin - 1024;
         c->lag_cluster = kLagCluster;
         c->lag_lb = lagrange_lb(c->ne0, kLagCluster, limit);
@@ -1136,6 +1261,15 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
         c->nproj = np;
     }
     CK(cudaMemcpy(c->tg, ptg.data(), sizeof(double) * c->npw_pad, cudaMemcpyHostToDevice));
+    {
+        double tmax = 0.0;
+        for (int p = 0; p < c->npw; ++p) tmax = std::max(tmax, ptg[p]);
+        c->tmax = tmax > 0 ? tmax : 1.0;
+        std::vector<int> sh(c->npw_pad, 0);
+        for (int p = 0; p < c->npw; ++p)
+            sh[p] = std::min(kShells - 1, (int)(ptg[p] / c->tmax * kShells));
+        CK(cudaMemcpy(c->shell, sh.data(), sizeof(int) * c->npw_pad, cudaMemcpyHostToDevice));
+    }
     CK(cudaMemcpy(c->vc, pvc.data(), sizeof(double) * c->npw_pad, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->vg, pvg.data(), sizeof(double) * c->npw_pad, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->vl, pvl.data(), sizeof(double) * pvl.size(), cudaMemcpyHostToDevice));
@@ -1186,7 +1320,7 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
     if (!c->tables_ok || !c->state_ok) return CPSD_ERR_ARG;
     CK(cudaSetDevice(c->prm.device));
     cudaStream_t s = c->st;
-    CK(cudaMemsetAsync(c->flags, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(c->flags, 0, 3 * sizeof(int), s));
     CK(cudaMemcpyAsync(c->Edev, E, sizeof(double), cudaMemcpyHostToDevice, s));
     for (int it = 0; it < inner; ++it) {
         int rc = run_step(c);
@@ -1195,9 +1329,9 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
     int rc = energies(c, inner);
     if (rc) return rc;
     double Eh[16];
-    int fails = 0;
+    int fl[3] = {0, 0, 0};
     CK(cudaMemcpyAsync(Eh, c->Edev, sizeof(double) * 12, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(&fails, c->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(fl, c->flags, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     c->h2d += sizeof(double);
     c->d2h += 12 * sizeof(double) + sizeof(int);
@@ -1205,8 +1339,11 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
     if (deltae) *deltae = Eh[10];
     if (deltac) *deltac = Eh[11];
     if (deltar) *deltar = 0.0;
+    const int fails = fl[0];
     c->lag_fail_total += fails;
+    c->steps_run += inner;
     c->ran = true;
+    if (fl[2]) return CPSD_ERR_TIMEOUT;
     return fails ? CPSD_WARN_LAGRANGE : CPSD_OK;
 }
 
@@ -1312,6 +1449,245 @@ int cpsd_gpu_phase_times(cpsd_gpu_ctx *c, float *ms, int max)
 
 const char *cpsd_gpu_phase_name(int i) { return (i >= 0 && i < kNumPhases) ? kPhaseNames[i] : ""; }
 
+int cpsd_gpu_set_preconditioner(cpsd_gpu_ctx *c, cpsd_mlp *m)
+{
+    if (!c) return CPSD_ERR_ARG;
+    if (m && m->device != c->prm.device) return CPSD_ERR_ARG;
+    if (m != c->mlp) drop_graphs(c);
+    c->mlp = m;
+    if (m) {
+        // the step feature counts every SD step of this context, and the
+        // trust region starts fully open
+        CK(cudaSetDevice(c->prm.device));
+        const int step = (int)std::min<long long>(c->steps_run, 1 << 30);
+        CK(cudaMemcpyAsync(c->dstep, &step, sizeof(int), cudaMemcpyHostToDevice, c->st));
+        const float cap = kLogKMax;
+        CK(cudaMemcpyAsync(c->pcap, &cap, sizeof(float), cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    }
+    return CPSD_OK;
+}
+
+int cpsd_gpu_set_preconditioner_cap(cpsd_gpu_ctx *c, double max_log_k)
+{
+    if (!c || !(max_log_k == max_log_k)) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    const float cap = (float)std::max<double>(kLogKMin, std::min<double>(kLogKMax, max_log_k));
+    CK(cudaMemcpyAsync(c->pcap, &cap, sizeof(float), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return CPSD_OK;
+}
+
+int cpsd_gpu_get_packed(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi)
+{
+    if (!c) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    const cx<double> *cc2 = c->cbuf[c->cur], *cc1 = c->ran ? c->cbuf[c->cur ^ 1] : c->cbuf[c->cur];
+    double *outs[3] = {c1, c2, cpsi};
+    const cx<double> *srcs[3] = {cc1, cc2, c->cpsi};
+    for (int k = 0; k < 3; ++k) {
+        if (!outs[k]) continue;
+        CK(cudaMemcpy2DAsync(outs[k], sizeof(cx<double>) * c->npw, srcs[k], sizeof(cx<double>) * c->ldc,
+                             sizeof(cx<double>) * c->npw, c->nb, cudaMemcpyDeviceToHost, c->st));
+        c->d2h += (long long)sizeof(cx<double>) * c->npw * c->nb;
+    }
+    CK(cudaStreamSynchronize(c->st));
+    return CPSD_OK;
+}
+
+int cpsd_gpu_set_packed(cpsd_gpu_ctx *c, const double *c2)
+{
+    if (!c || !c2) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    CK(cudaMemsetAsync(c->cbuf[c->cur], 0, sizeof(cx<double>) * c->nb * c->npw_pad, c->st));
+    CK(cudaMemcpy2DAsync(c->cbuf[c->cur], sizeof(cx<double>) * c->ldc, c2, sizeof(cx<double>) * c->npw,
+                         sizeof(cx<double>) * c->npw, c->nb, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->h2d += (long long)sizeof(cx<double>) * c->npw * c->nb;
+    c->state_ok = true;
+    return CPSD_OK;
+}
+
+int cpsd_gpu_get_sphere(const cpsd_gpu_ctx *c, int *pt_idx, double *weights, int *shell)
+{
+    if (!c) return CPSD_ERR_ARG;
+    for (int p = 0; p < c->npw; ++p) {
+        if (pt_idx) pt_idx[p] = c->hg.pt_idx[p];
+        if (weights) weights[p] = c->hg.w[p];
+    }
+    if (shell) CK(cudaMemcpy(shell, c->shell, sizeof(int) * c->npw, cudaMemcpyDeviceToHost));
+    return CPSD_OK;
+}
+
+// ---------------------------------------------------------------- network
+int cpsd_mlp_nparams(void) { return kMlpParams; }
+
+int cpsd_mlp_create(unsigned long long seed, cpsd_mlp **out)
+{
+    if (!out) return CPSD_ERR_ARG;
+    *out = nullptr;
+    std::unique_ptr<cpsd_mlp> m(new cpsd_mlp());
+    CK(cudaGetDevice(&m->device));
+    CK(cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking));
+    CK(m->ar.alloc(&m->p, kMlpParams));
+    CK(m->ar.alloc(&m->m1, kMlpParams));
+    CK(m->ar.alloc(&m->m2, kMlpParams));
+    CK(m->ar.alloc(&m->g, kMlpParams));
+    CK(m->ar.alloc(&m->wq, kMlpParams));
+    // Xavier-uniform weights from a splitmix64 stream, zero biases
+    std::vector<float> h(kMlpParams, 0.0f);
+    uint64_t st = seed;
+    auto next = [&]() {
+        uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto fill = [&](int ofs, int fan_out, int fan_in) {
+        const double a = sqrt(6.0 / (fan_in + fan_out));
+        for (int i = 0; i < fan_out * fan_in; ++i) h[ofs + i] = (float)((2.0 * next() - 1.0) * a);
+    };
+    fill(kW1, kMlpHid, kMlpIn);
+    fill(kW2, kMlpHid, kMlpHid);
+    fill(kW3, kMlpHid, kMlpHid);
+    fill(kW4, 1, kMlpHid);
+    CK(cudaMemcpy(m->p, h.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
+    mlp_quantize_kernel<<<(kMlpParams + 255) / 256, 256, 0, m->st>>>(kMlpParams, m->p, m->wq);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    *out = m.release();
+    return CPSD_OK;
+}
+
+namespace {
+int mlp_reserve(cpsd_mlp *m, int n)
+{
+    if (n <= m->cap) return CPSD_OK;
+    const int cap = std::max(n, 1024);
+    CK(m->ar.alloc(&m->X, (size_t)kMlpIn * cap));
+    CK(m->ar.alloc(&m->T, (size_t)cap));
+    CK(m->ar.alloc(&m->y, (size_t)cap));
+    CK(m->ar.alloc(&m->H, (size_t)3 * kMlpHid * cap));
+    CK(m->ar.alloc(&m->D, (size_t)3 * kMlpHid * cap));
+    CK(m->ar.alloc(&m->dy, (size_t)cap));
+    CK(m->ar.alloc(&m->lp, (size_t)cdiv(cap, 128)));
+    CK(cudaDeviceSynchronize());
+    m->cap = cap;
+    return CPSD_OK;
+}
+
+// forward + backward of one batch already in X/T (device); gradient into m->g
+int mlp_grad_batch(cpsd_mlp *m, const float *X, const float *T, int n)
+{
+    const unsigned b128 = (unsigned)cdiv(n, 128);
+    mlp_forward_kernel<<<b128, 128, 0, m->st>>>(n, X, m->wq, m->p, m->y, m->H);
+    mlp_backward_delta_kernel<<<b128, 128, 0, m->st>>>(n, m->y, T, m->wq, m->H, m->D, m->dy, m->lp);
+    mlp_wgrad_kernel<<<3 * kMlpHid + 1, kMlpGradThreads, 0, m->st>>>(n, X, m->H, m->D, m->dy, m->g);
+    CK(cudaGetLastError());
+    return CPSD_OK;
+}
+}  // namespace
+
+int cpsd_mlp_forward(cpsd_mlp *m, const float *X, int n, float *y)
+{
+    if (!m || !X || !y || n < 1) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(m->device));
+    int rc = mlp_reserve(m, n);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(m->X, X, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice, m->st));
+    mlp_forward_kernel<<<(unsigned)cdiv(n, 128), 128, 0, m->st>>>(n, m->X, m->wq, m->p, m->y, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(y, m->y, sizeof(float) * n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return CPSD_OK;
+}
+
+int cpsd_mlp_gradient(cpsd_mlp *m, const float *X, const float *T, int n, float *grad, float *loss)
+{
+    if (!m || !X || !T || n < 1) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(m->device));
+    int rc = mlp_reserve(m, n);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(m->X, X, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->T, T, sizeof(float) * n, cudaMemcpyHostToDevice, m->st));
+    rc = mlp_grad_batch(m, m->X, m->T, n);
+    if (rc) return rc;
+    if (grad) CK(cudaMemcpyAsync(grad, m->g, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, m->st));
+    std::vector<float> lp(cdiv(n, 128));
+    CK(cudaMemcpyAsync(lp.data(), m->lp, sizeof(float) * lp.size(), cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    if (loss) {
+        double t = 0;
+        for (float v : lp) t += v;
+        *loss = (float)(t / n);
+    }
+    return CPSD_OK;
+}
+
+int cpsd_mlp_train(cpsd_mlp *m, const float *X, const float *T, int n, int steps, int batch, float lr,
+                   float *losses)
+{
+    if (!m || !X || !T || n < 1 || steps < 1 || batch < 1) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(m->device));
+    batch = std::min(batch, n);
+    int rc = mlp_reserve(m, n);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(m->X, X, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->T, T, sizeof(float) * n, cudaMemcpyHostToDevice, m->st));
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    std::vector<float> lp(cdiv(batch, 128));
+    for (int it = 0; it < steps; ++it) {
+        const int start = (int)(((long)it * batch) % n);
+        const int len = std::min(batch, n - start);  // contiguous window of the (pre-shuffled) data
+        rc = mlp_grad_batch(m, m->X + (long)kMlpIn * start, m->T + start, len);
+        if (rc) return rc;
+        ++m->adam_t;
+        const float bc1 = 1.0f - powf(b1, (float)m->adam_t), bc2 = 1.0f - powf(b2, (float)m->adam_t);
+        mlp_adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, m->st>>>(kMlpParams, m->p, m->g, m->m1, m->m2, m->wq,
+                                                                      lr, b1, b2, eps, bc1, bc2);
+        CK(cudaGetLastError());
+        if (losses) {
+            const int nb = (int)cdiv(len, 128);
+            CK(cudaMemcpyAsync(lp.data(), m->lp, sizeof(float) * nb, cudaMemcpyDeviceToHost, m->st));
+            CK(cudaStreamSynchronize(m->st));
+            double t = 0;
+            for (int k = 0; k < nb; ++k) t += lp[k];
+            losses[it] = (float)(t / len);
+        }
+    }
+    CK(cudaStreamSynchronize(m->st));
+    return CPSD_OK;
+}
+
+int cpsd_mlp_get_params(const cpsd_mlp *m, float *p)
+{
+    if (!m || !p) return CPSD_ERR_ARG;
+    CK(cudaMemcpy(p, m->p, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost));
+    return CPSD_OK;
+}
+
+int cpsd_mlp_set_params(cpsd_mlp *m, const float *p)
+{
+    if (!m || !p) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(m->device));
+    CK(cudaMemcpy(m->p, p, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
+    mlp_quantize_kernel<<<(kMlpParams + 255) / 256, 256, 0, m->st>>>(kMlpParams, m->p, m->wq);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(m->st));
+    return CPSD_OK;
+}
+
+void cpsd_mlp_destroy(cpsd_mlp *m)
+{
+    if (!m) return;
+    cudaSetDevice(m->device);
+    if (m->st) cudaStreamSynchronize(m->st);
+    m->ar.release();
+    if (m->st) cudaStreamDestroy(m->st);
+    delete m;
+}
+
 void cpsd_gpu_counters(const cpsd_gpu_ctx *c, long long *out)
 {
     if (!out) return;
@@ -1336,6 +1712,17 @@ int cpsd_gpu_set_precision(cpsd_gpu_ctx *c, int precision)
     return CPSD_OK;
 }
 
+int cpsd_gpu_set_gemm(cpsd_gpu_ctx *c, int mode)
+{
+    if (!c) return CPSD_ERR_ARG;
+    if (mode != CPSD_GEMM_FP64 && mode != CPSD_GEMM_TF32X3 && mode != CPSD_GEMM_TF32X3_OVERLAPS)
+        return CPSD_ERR_ARG;
+    if (mode != CPSD_GEMM_FP64 && !c->fft32) return CPSD_ERR_ARG;  // FP64-only context
+    if (mode != c->gemm_mode) drop_graphs(c);
+    c->gemm_mode = mode;
+    return CPSD_OK;
+}
+
 int cpsd_gpu_use_graphs(cpsd_gpu_ctx *c, int on)
 {
     if (!c) return CPSD_ERR_ARG;
@@ -1357,6 +1744,39 @@ void cpsd_gpu_destroy(cpsd_gpu_ctx *c)
     c->ar.release();
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
+}
+
+int cpsd_overlap_tn(int method, int M, int N, int K, const double *A, long lda, const double *B, long ldb,
+                    const double *w, double *C, long ldc, void *stream)
+{
+    if (method != CPSD_GEMM_FP64 && method != CPSD_GEMM_TF32X3) return CPSD_ERR_ARG;
+    if (M < 0 || N < 0 || K < 0 || lda < K || ldb < K || ldc < N) return CPSD_ERR_ARG;
+    if (M == 0 || N == 0) return CPSD_OK;
+    if (!A || !B || !C) return CPSD_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool tc = method != CPSD_GEMM_FP64;
+    if (tc)
+        CK(cudaFuncSetAttribute(tc_gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    const size_t cap = std::max<size_t>((size_t)M * N, (size_t)4 << 20);
+    const TnPlan pl = tn_plan(M, N, K, 1, tc, cap);
+    struct Scratch {
+        double *ws = nullptr;
+        int *err = nullptr;
+        ~Scratch()
+        {
+            if (ws) cudaFree(ws);
+            if (err) cudaFree(err);
+        }
+    } sc;
+    CK(cudaMalloc(&sc.ws, sizeof(double) * (size_t)pl.splits * M * N));
+    CK(cudaMalloc(&sc.err, sizeof(int)));
+    CK(cudaMemsetAsync(sc.err, 0, sizeof(int), s));
+    (void)launch_tn(M, N, K, 1, &A, lda, &B, ldb, w, 1.0, 0.0, &C, ldc, tc, sc.ws, cap, sc.err, s);
+    CK(cudaGetLastError());
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, sc.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return herr ? CPSD_ERR_TIMEOUT : CPSD_OK;
 }
 
 }  // extern "C"

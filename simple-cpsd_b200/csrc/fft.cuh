@@ -199,16 +199,18 @@ size_t plane_smem_bytes(int mode, int KX)
     return (b + 15) / 16 * 16;
 }
 
-// Two CTAs per SM where the exchange buffers allow it (the density variant
-// keeps its per-lane sums in registers and takes the whole register file).
+// Every plane variant is built for one and for two CTAs per SM (MINB); the
+// host launches the two-CTA build where two planes' shared memory fits an SM
+// (it caps registers at 128 per thread).  The density variant at n >= 128
+// keeps its per-lane sums in registers and is built for one CTA only.
 template <int NF, int MODE>
-constexpr int plane_min_blocks()
+constexpr bool plane_has_two_cta_build()
 {
-    return (MODE == PM_DENSITY && NF >= 128) ? 1 : 2;
+    return !(MODE == PM_DENSITY && NF >= 128);
 }
 
-template <typename T, int NF, int MODE>
-__global__ void __launch_bounds__(kThreads, plane_min_blocks<NF, MODE>())
+template <typename T, int NF, int MODE, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
 {
     using S = PlaneShape<T, NF>;

@@ -642,6 +642,10 @@ __global__ void __launch_bounds__(kLagThreads) lagrange_kernel(LagArgs a)
                     gi = ix;
                 }
             }
+            // idamax returns an index in 1..kk even when every entry is NaN
+            // (then no comparison succeeds and it returns 1); the sentinel
+            // must never reach the read below
+            if (gi < 0 || gi >= kk) gi = 0;
             // the reference reads st1 at idamax's 1-based result (cpsd.c:471):
             // the element after the largest; past the end of st1 lies sa1
             const long nx = gi + 1;
@@ -770,6 +774,9 @@ __global__ void __launch_bounds__(kLagThreads) lagrange_small_kernel(LagArgs a)
                         bestv = shv[w];
                         besti = shi[w];
                     }
+                // idamax returns an index in 1..kk even when every entry is
+                // NaN: the sentinel must never reach the read below
+                if (besti < 0 || (long)besti >= kk) besti = 0;
                 // idamax's 1-based index used as 0-based (cpsd.c:471); past st1 lies sa1
                 const long nxi = (long)besti + 1;
                 const double adiff = fabs(nxi < ne02 ? st1[nxi] : nx[nxi - ne02]);

@@ -1,0 +1,299 @@
+// mlp.cuh -- the small network of the learned SD preconditioner.
+//
+// y = W4 h3 + b4,  h_k = tanh(W_k h_{k-1} + b_k),  h_0 = x  (4 -> 64 -> 64 -> 64 -> 1)
+//
+// Inference reads BF16 copies of the weights (FP32 biases) and accumulates
+// in FP32.  Training keeps FP32 master weights and Adam moments; the forward
+// pass stores the activations of the batch, the backward pass the deltas, and
+// each weight gradient is a fixed-order reduction over the batch (no
+// atomics), so a training step is bitwise reproducible.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+constexpr int kMlpIn = 4;
+constexpr int kMlpHid = 64;
+// flat parameter layout (FP32 master copy)
+constexpr int kW1 = 0;                            // [64][4]
+constexpr int kB1 = kW1 + kMlpHid * kMlpIn;       // [64]
+constexpr int kW2 = kB1 + kMlpHid;                // [64][64]
+constexpr int kB2 = kW2 + kMlpHid * kMlpHid;      // [64]
+constexpr int kW3 = kB2 + kMlpHid;                // [64][64]
+constexpr int kB3 = kW3 + kMlpHid * kMlpHid;      // [64]
+constexpr int kW4 = kB3 + kMlpHid;                // [64]
+constexpr int kB4 = kW4 + kMlpHid;                // [1]
+constexpr int kMlpParams = kB4 + 1;               // 8705
+constexpr int kMlpGradThreads = 128;
+
+struct MlpDev {
+    const __nv_bfloat16 *wq;  // BF16 weights (same layout; biases unused here)
+    const float *p;           // FP32 master parameters (biases read from here)
+};
+
+// one sample: x[4] -> y; optionally store activations h1,h2,h3 (each 64)
+template <bool STORE>
+CPSD_D float mlp_sample(const float *__restrict__ x, const __nv_bfloat16 *__restrict__ wq,
+                        const float *__restrict__ p, float *h1o, float *h2o, float *h3o)
+{
+    float a[kMlpHid], b[kMlpHid];
+#pragma unroll 4
+    for (int o = 0; o < kMlpHid; ++o) {
+        float s = p[kB1 + o];
+#pragma unroll
+        for (int i = 0; i < kMlpIn; ++i) s = fmaf(__bfloat162float(wq[kW1 + o * kMlpIn + i]), x[i], s);
+        a[o] = tanhf(s);
+    }
+    if (STORE)
+        for (int o = 0; o < kMlpHid; ++o) h1o[o] = a[o];
+#pragma unroll 2
+    for (int o = 0; o < kMlpHid; ++o) {
+        float s = p[kB2 + o];
+#pragma unroll 8
+        for (int i = 0; i < kMlpHid; ++i) s = fmaf(__bfloat162float(wq[kW2 + o * kMlpHid + i]), a[i], s);
+        b[o] = tanhf(s);
+    }
+    if (STORE)
+        for (int o = 0; o < kMlpHid; ++o) h2o[o] = b[o];
+#pragma unroll 2
+    for (int o = 0; o < kMlpHid; ++o) {
+        float s = p[kB3 + o];
+#pragma unroll 8
+        for (int i = 0; i < kMlpHid; ++i) s = fmaf(__bfloat162float(wq[kW3 + o * kMlpHid + i]), b[i], s);
+        a[o] = tanhf(s);
+    }
+    if (STORE)
+        for (int o = 0; o < kMlpHid; ++o) h3o[o] = a[o];
+    float y = p[kB4];
+#pragma unroll 8
+    for (int i = 0; i < kMlpHid; ++i) y = fmaf(__bfloat162float(wq[kW4 + i]), a[i], y);
+    return y;
+}
+
+// forward over a batch: y[s], and the activations when H is given ([3][n][64])
+__global__ void mlp_forward_kernel(int n, const float *__restrict__ X, const __nv_bfloat16 *__restrict__ wq,
+                                   const float *__restrict__ p, float *__restrict__ y, float *__restrict__ H)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    float x[kMlpIn];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; ++i) x[i] = X[(long)s * kMlpIn + i];
+    if (H) {
+        y[s] = mlp_sample<true>(x, wq, p, H + (long)s * kMlpHid, H + ((long)n + s) * kMlpHid,
+                                H + (2L * n + s) * kMlpHid);
+    } else {
+        y[s] = mlp_sample<false>(x, wq, p, nullptr, nullptr, nullptr);
+    }
+}
+
+// MSE loss on y - t: dy = 2 (y - t) / n; deltas dZ3, dZ2, dZ1 ([3][n][64]);
+// loss partials per block
+__global__ void mlp_backward_delta_kernel(int n, const float *__restrict__ y, const float *__restrict__ t,
+                                          const __nv_bfloat16 *__restrict__ wq, const float *__restrict__ H,
+                                          float *__restrict__ D, float *__restrict__ dy_out,
+                                          float *__restrict__ loss_part)
+{
+    __shared__ float sh[32];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (s < n) {
+        const float r = y[s] - t[s];
+        l = r * r;
+        const float dy = 2.0f * r / (float)n;
+        dy_out[s] = dy;
+        const float *h1 = H + (long)s * kMlpHid, *h2 = H + ((long)n + s) * kMlpHid, *h3 = H + (2L * n + s) * kMlpHid;
+        float *d3 = D + (2L * n + s) * kMlpHid, *d2 = D + ((long)n + s) * kMlpHid, *d1 = D + (long)s * kMlpHid;
+        float z3[kMlpHid], z2[kMlpHid];
+        for (int o = 0; o < kMlpHid; ++o) {
+            const float hv = h3[o];
+            z3[o] = dy * __bfloat162float(wq[kW4 + o]) * (1.0f - hv * hv);
+            d3[o] = z3[o];
+        }
+        for (int i = 0; i < kMlpHid; ++i) {
+            float acc = 0.0f;
+            for (int o = 0; o < kMlpHid; ++o) acc = fmaf(__bfloat162float(wq[kW3 + o * kMlpHid + i]), z3[o], acc);
+            const float hv = h2[i];
+            z2[i] = acc * (1.0f - hv * hv);
+            d2[i] = z2[i];
+        }
+        for (int i = 0; i < kMlpHid; ++i) {
+            float acc = 0.0f;
+            for (int o = 0; o < kMlpHid; ++o) acc = fmaf(__bfloat162float(wq[kW2 + o * kMlpHid + i]), z2[o], acc);
+            const float hv = h1[i];
+            d1[i] = acc * (1.0f - hv * hv);
+        }
+    }
+    // fixed-order block sum of the squared residuals
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float tot = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sh[w];
+        loss_part[blockIdx.x] = tot;
+    }
+}
+
+// gradient of one parameter row: blockIdx.x enumerates (layer, output unit);
+// each thread strides over the batch, then a fixed-order tree in shared memory.
+// grad[param] for W (row o, inputs i) and b[o].
+__global__ void __launch_bounds__(kMlpGradThreads) mlp_wgrad_kernel(int n, const float *__restrict__ X,
+                                                                    const float *__restrict__ H,
+                                                                    const float *__restrict__ D,
+                                                                    const float *__restrict__ dy,
+                                                                    float *__restrict__ grad)
+{
+    __shared__ float red[kMlpGradThreads][kMlpHid + 1];
+    const int row = blockIdx.x;  // 0..63: layer1, 64..127: layer2, 128..191: layer3, 192: layer4
+    int layer, o;
+    if (row < 3 * kMlpHid) {
+        layer = row / kMlpHid + 1;
+        o = row % kMlpHid;
+    } else {
+        layer = 4;
+        o = 0;
+    }
+    const int nin = (layer == 1) ? kMlpIn : kMlpHid;
+    float acc[kMlpHid + 1];
+    for (int i = 0; i <= kMlpHid; ++i) acc[i] = 0.0f;
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+        float delta;
+        const float *in;
+        if (layer == 4) {
+            delta = dy[s];
+            in = H + (2L * n + s) * kMlpHid;
+        } else {
+            delta = D[((long)(layer - 1) * n + s) * kMlpHid + o];
+            in = (layer == 1) ? X + (long)s * kMlpIn : H + ((long)(layer - 2) * n + s) * kMlpHid;
+        }
+        for (int i = 0; i < nin; ++i) acc[i] = fmaf(delta, in[i], acc[i]);
+        acc[kMlpHid] += delta;  // bias
+    }
+    for (int i = 0; i < nin; ++i) red[threadIdx.x][i] = acc[i];
+    red[threadIdx.x][kMlpHid] = acc[kMlpHid];
+    __syncthreads();
+    for (int stride = kMlpGradThreads / 2; stride > 0; stride >>= 1) {
+        if ((int)threadIdx.x < stride) {
+            for (int i = 0; i < nin; ++i) red[threadIdx.x][i] += red[threadIdx.x + stride][i];
+            red[threadIdx.x][kMlpHid] += red[threadIdx.x + stride][kMlpHid];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        int wofs, bofs;
+        switch (layer) {
+        case 1: wofs = kW1 + o * kMlpIn; bofs = kB1 + o; break;
+        case 2: wofs = kW2 + o * kMlpHid; bofs = kB2 + o; break;
+        case 3: wofs = kW3 + o * kMlpHid; bofs = kB3 + o; break;
+        default: wofs = kW4; bofs = kB4; break;
+        }
+        for (int i = 0; i < nin; ++i) grad[wofs + i] = red[0][i];
+        grad[bofs] = red[0][kMlpHid];
+    }
+}
+
+// Adam on the FP32 master parameters, then refresh the BF16 copy
+__global__ void mlp_adam_kernel(int np, float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m1,
+                                float *__restrict__ m2, __nv_bfloat16 *__restrict__ wq, float lr, float b1, float b2,
+                                float eps, float bc1, float bc2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.0f - b1) * gi;
+    const float v = b2 * m2[i] + (1.0f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = v;
+    const float pi = p[i] - lr * (a / bc1) / (sqrtf(v / bc2) + eps);
+    p[i] = pi;
+    wq[i] = __float2bfloat16(pi);
+}
+
+__global__ void mlp_quantize_kernel(int np, const float *__restrict__ p, __nv_bfloat16 *__restrict__ wq)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < np) wq[i] = __float2bfloat16(p[i]);
+}
+
+// ------------------------------------------------------------ preconditioned SD
+// |G| shells of the sphere (by kinetic energy tg = G^2/2) on which the
+// network's step scales are tabulated per band.
+constexpr int kShells = 64;
+// range of the learned log step scale (K from e^-2 to e^4.5, about 0.14 to 90)
+constexpr float kLogKMin = -2.0f, kLogKMax = 4.5f;
+
+// per band: KE_b = <c1|T|c1>, h_b = <c1|cpsi>, q_b = <cpsi|cpsi> (Gamma-point weights)
+__global__ void band_stats_kernel(int npw, long ldc, const double *__restrict__ w, const double *__restrict__ tg,
+                                  const cx<double> *__restrict__ c1, const cx<double> *__restrict__ cpsi,
+                                  double *__restrict__ stats)
+{
+    __shared__ double sh[3][32];
+    const int b = blockIdx.x;
+    const cx<double> *a = c1 + (long)b * ldc, *g = cpsi + (long)b * ldc;
+    double ke = 0, h = 0, q = 0;
+    for (int p = threadIdx.x; p < npw; p += blockDim.x) {
+        const double ww = w[p];
+        const cx<double> x = a[p], y = g[p];
+        ke += ww * tg[p] * (x.x * x.x + x.y * x.y);
+        h += ww * (x.x * y.x + x.y * y.y);
+        q += ww * (y.x * y.x + y.y * y.y);
+    }
+    double v[3] = {ke, h, q};
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 3; ++k) {
+            double t = 0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += sh[k][i];
+            stats[3 * b + k] = t;
+        }
+    }
+}
+
+// network inputs for (band, shell): tshell/KE, log KE, log |residual|^2, step
+// feature (the step counter advances in prec_update_kernel, a later launch)
+__global__ void prec_features_kernel(int nb, double tmax, const double *__restrict__ stats,
+                                     const int *__restrict__ step, float *__restrict__ X)
+{
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nb * kShells) return;
+    const int b = id / kShells, s = id % kShells;
+    const double ke = fmax(stats[3 * b], 1e-12);
+    const double hh = stats[3 * b + 1], qq = stats[3 * b + 2];
+    const double res = fmax(qq - hh * hh, 1e-30);  // |cpsi - <c1|cpsi> c1|^2
+    const double ts = (s + 0.5) * tmax / kShells;
+    X[4 * id + 0] = (float)(ts / ke);
+    X[4 * id + 1] = (float)log(ke);
+    X[4 * id + 2] = (float)log(res);
+    X[4 * id + 3] = (float)(log1p((double)*step) / 10.0);
+}
+
+// c2 (= c1 + dte cpsi, the plain SD update) += dte (K[b][shell(p)] - 1) R,
+// with R the residual of cpsi outside the occupied subspace: the residual is
+// stepped by dte K, the part inside the subspace exactly as plain SD.  log K
+// is the network output clamped to [kLogKMin, min(kLogKMax, *cap)]; *cap is
+// a trust-region bound the host lowers after a rejected block and raises
+// after an accepted one.
+__global__ void prec_update_kernel(int nb, int npw, long ldc, const int *__restrict__ shell,
+                                   const float *__restrict__ y, const float *__restrict__ cap, double dte,
+                                   const cx<double> *__restrict__ R, cx<double> *__restrict__ c2,
+                                   int *__restrict__ step)
+{
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id == 0) atomicAdd(step, 1);
+    if (id >= (long)nb * npw) return;
+    const int b = (int)(id / npw), p = (int)(id % npw);
+    const float hi = fmaxf(kLogKMin, fminf(kLogKMax, *cap));
+    const float lk = fminf(fmaxf(y[b * kShells + shell[p]], kLogKMin), hi);
+    const double f = dte * (exp((double)lk) - 1.0);
+    const long o = (long)b * ldc + p;
+    const cx<double> r = R[o], u = c2[o];
+    c2[o] = cx<double>{u.x + f * r.x, u.y + f * r.y};
+}

@@ -1,0 +1,225 @@
+// tc_gemm.cuh -- weighted TN products on the 5th-generation tensor cores
+// (tcgen05, sm_100a) for the mixed-precision path.
+//
+//   part[prod][split][i][j] = sum_{k in chunk} (w_k A[i][k]) B[j][k]
+//
+// the same contract as gemm_tn_w_kernel (kernels.cuh): A and B FP64 in HBM,
+// rows K-contiguous, weight per complex pair.  Each stage converts a 128 x 32
+// slab of each operand to a TF32 pair x = hi + lo and one elected thread
+// issues the three products hi*hi + hi*lo + lo*hi (tcgen05.mma kind::tf32,
+// FP32 accumulation in tensor memory): close to FP32 accuracy from TF32
+// tensor cores.  Split-K partials are summed in FP64 by splitk_reduce_kernel.
+//
+// Shared-memory operand layout: K-major, no swizzle.  The canonical layout
+// is built from core matrices of 8 rows x 16 bytes (4 TF32 values); a
+// 128 x 32 slab holds 16 row groups x 8 K-chunks of them, core matrix
+// (group g, chunk c) at byte (c * 16 + g) * 128.  One MMA consumes K = 8
+// (two chunks): descriptor start at chunk 2s, leading-byte offset 2048
+// (chunk to chunk), stride-byte offset 128 (row group to row group).
+//
+// Two slab sets alternate: while the tensor cores work on one, the threads
+// load and split the next.  Every wait on an mbarrier is bounded; a wait
+// that runs out sets *err, the block stops issuing work, waits (bounded)
+// for what it issued, frees its tensor memory and returns.
+#pragma once
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+constexpr int kTcM = 128, kTcN = 128, kTcBK = 32, kTcThreads = 256;
+constexpr int kTcSlabWords = kTcM * kTcBK;               // 4096 words = 16 KB per operand slab
+constexpr int kTcStageWords = 4 * kTcSlabWords;          // Ah, Al, Bh, Bl
+constexpr size_t kTcSmem = 2 * kTcStageWords * 4 + 128;  // two stages (+ alignment slack)
+constexpr long kTcSpinLimit = 1L << 22;                  // polls per mbarrier wait
+
+CPSD_D uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// SWIZZLE_NONE K-major shared-memory matrix descriptor (sm_100 format,
+// version 1 at bits 46-47, layout type 0 at bits 61-63)
+CPSD_D uint64_t tc_desc(uint32_t saddr)
+{
+    const uint64_t lbo = 2048 >> 4, sbo = 128 >> 4;
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+// instruction descriptor: D f32 (bits 4-5 = 1), A and B tf32 (bits 7-9,
+// 10-12 = 2), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
+                              ((uint32_t)(kTcM >> 4) << 24);
+
+CPSD_D void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+        "l"(da), "l"(db), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+CPSD_D void tc_commit(uint32_t mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+CPSD_D uint32_t tf32_bits(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// true once the mbarrier has completed the phase with this parity; false if
+// the poll limit ran out first
+CPSD_D bool mbar_wait(uint32_t addr, uint32_t parity)
+{
+    for (long it = 0; it < kTcSpinLimit; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(kTcThreads)
+tc_gemm_tn_kernel(int M, int N, int K, long lda, long ldb, const double *__restrict__ w, int kchunk,
+                  const __grid_constant__ TnBatch bt, double *__restrict__ part, int *__restrict__ err)
+{
+    extern __shared__ unsigned char tc_raw[];
+    uint32_t *sm = reinterpret_cast<uint32_t *>(((uintptr_t)tc_raw + 127) & ~(uintptr_t)127);
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int prod = blockIdx.z / bt.splits, split = blockIdx.z % bt.splits;
+    const double *__restrict__ A = bt.A[prod];
+    const double *__restrict__ B = bt.B[prod];
+    const int i0 = blockIdx.x * kTcM, j0 = blockIdx.y * kTcN;
+    const int k0 = split * kchunk, k1 = min(K, k0 + kchunk);
+    const int nst = k1 > k0 ? (k1 - k0 + kTcBK - 1) / kTcBK : 0;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"((uint32_t)kTcN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+
+    // staging map: a warp covers 8 rows x 4 consecutive k (one 32-byte
+    // sector per row in HBM, 32 consecutive words in shared memory)
+    const int kq = tid & 3, rlo = (tid >> 2) & 7, chunk = tid >> 5;  // chunk 0..7 of the 32-wide slab
+    bool fail = false;
+    int issued = 0;  // stages whose MMAs were committed
+    for (int it = 0; it < nst; ++it) {
+        const int b = it & 1;
+        uint32_t *Ah = sm + b * kTcStageWords, *Al = Ah + kTcSlabWords, *Bh = Al + kTcSlabWords,
+                 *Bl = Bh + kTcSlabWords;
+        // the MMAs of stage it-2 read this slab set: wait for them
+        if (it >= 2 && !mbar_wait(smem_u32(&mbar[b]), (uint32_t)(((it >> 1) + 1) & 1))) fail = true;
+        if (__syncthreads_or(fail)) {
+            fail = true;
+            break;
+        }
+        const int k = k0 + it * kTcBK + chunk * 4 + kq;
+        const double wk = (w && k < k1) ? w[k >> 1] : 1.0;
+        // all 32 loads of this thread first (memory-level parallelism), then split
+        double ra[16], rb[16];
+#pragma unroll
+        for (int rhi = 0; rhi < 16; ++rhi) {
+            const int r = rhi * 8 + rlo;
+            ra[rhi] = (k < k1 && i0 + r < M) ? A[(long)(i0 + r) * lda + k] : 0.0;
+            rb[rhi] = (k < k1 && j0 + r < N) ? B[(long)(j0 + r) * ldb + k] : 0.0;
+        }
+#pragma unroll
+        for (int rhi = 0; rhi < 16; ++rhi) {
+            const float a = (float)(ra[rhi] * wk), bv = (float)rb[rhi];
+            const uint32_t ah = tf32_bits(a), bh = tf32_bits(bv);
+            const int o = ((chunk * 16 + rhi) << 5) + lane;  // = (chunk*16 + rhi)*32 + rlo*4 + kq
+            Ah[o] = ah;
+            Al[o] = tf32_bits(a - __uint_as_float(ah));
+            Bh[o] = bh;
+            Bl[o] = tf32_bits(bv - __uint_as_float(bh));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t ah = smem_u32(Ah), al = smem_u32(Al), bh = smem_u32(Bh), bl = smem_u32(Bl);
+#pragma unroll
+            for (int s = 0; s < kTcBK / 8; ++s) {
+                const uint32_t o = (uint32_t)s * 4096;  // K-chunk 2s
+                tc_mma(tmem, tc_desc(ah + o), tc_desc(bh + o), (it > 0 || s > 0) ? 1u : 0u);
+                tc_mma(tmem, tc_desc(ah + o), tc_desc(bl + o), 1u);
+                tc_mma(tmem, tc_desc(al + o), tc_desc(bh + o), 1u);
+            }
+            tc_commit(smem_u32(&mbar[b]));
+        }
+        issued = it + 1;
+    }
+    // the last commit tracks every MMA this block issued
+    bool done = true;
+    if (issued > 0) {
+        const int last = issued - 1;
+        done = mbar_wait(smem_u32(&mbar[last & 1]), (uint32_t)((last >> 1) & 1));
+    }
+    if (__syncthreads_or(!done)) fail = true;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (!fail) {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows), columns
+        // 64 (w / 4) .. +63, and writes rows through shared memory
+        double *out = part + ((long)prod * bt.splits + split) * M * N;
+        double *E = reinterpret_cast<double *>(sm) + warp * 32 * 33;
+        const int rbase = 32 * (warp & 3), cbase = 64 * (warp >> 2);
+#pragma unroll 1
+        for (int cc = 0; cc < 2; ++cc) {
+            uint32_t v[32];
+            if (issued > 0) {
+                const uint32_t ta = tmem + ((uint32_t)rbase << 16) + (uint32_t)(cbase + 32 * cc);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                    "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+                    "%30, %31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(ta));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            } else {
+#pragma unroll
+                for (int q = 0; q < 32; ++q) v[q] = 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 32; ++q) E[lane * 33 + q] = (double)__uint_as_float(v[q]);
+            __syncwarp();
+            const int col = j0 + cbase + 32 * cc + lane;
+            for (int rr = 0; rr < 32; ++rr) {
+                const int row = i0 + rbase + rr;
+                if (row < M && col < N) out[(long)row * N + col] = E[rr * 33 + lane];
+            }
+            __syncwarp();
+        }
+    } else if (tid == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcN));
+}

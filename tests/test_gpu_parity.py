@@ -212,6 +212,27 @@ def test_error_paths():
         api.rc_fft3f(A, 20)
 
 
+@pytest.mark.parametrize("nb", [4, 40])
+def test_non_finite_orbitals_warn_without_fault(nb):
+    """NaN orbitals (a diverged step) reach the Lagrange solver's convergence
+    test, whose idamax must still return an index inside st1: the call warns
+    (no convergence) and the context stays usable.  nb = 4 runs the
+    single-CTA solver, nb = 40 the cluster solver."""
+    inp = inputs.build_inputs(configs.small_diamond(32, nb, ecut=25.0))
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    _, c2, _ = cell.get_packed()
+    c2[:] = np.nan
+    cell.set_packed(c2)
+    cell.run(1)
+    assert cell.lagrange_warnings == 1
+    assert not np.isfinite(cell.E[0])
+    cell.set_state(inp.c2, inp.r2)
+    cell.run(1)
+    assert np.isfinite(cell.E[0])
+    cell.close()
+
+
 def test_graphs_and_direct_launches_agree():
     inp = inputs.build_inputs(configs.small_diamond(32, 5, ecut=25.0))
     out = []
