@@ -28,6 +28,7 @@ enum {
     CPSD_ERR_UNMASKED_PSI = 6,  /* input orbitals have coefficients outside the mask */
     CPSD_ERR_MOVE = 7,          /* move=1 (ionic forces) requested but not built in */
     CPSD_ERR_TIMEOUT = 8,       /* a bounded wait on the device ran out (tensor-core pipeline) */
+    CPSD_ERR_SCRATCH = 9,       /* a problem larger than cpsd_overlap_tn_noalloc's static scratch */
     CPSD_WARN_LAGRANGE = 10     /* (positive warning) Lagrange iteration hit 30 steps; the
                                    reference prints "ierr=10" and continues (cpsd.c:477) */
 };
@@ -266,6 +267,38 @@ void cpsd_gpu_batch_destroy(cpsd_gpu_batch *b);
  */
 int cpsd_overlap_tn(int method, int M, int N, int K, const double *A, long lda, const double *B, long ldb,
                     const double *w, double *C, long ldc, void *stream);
+
+/* Largest M*N that cpsd_overlap_tn_noalloc accepts (its split-K workspace,
+ * in doubles: 8 MiB less a 256-byte status word). */
+#define CPSD_NOALLOC_MAX_DOUBLES 1048544
+
+/*
+ * cpsd_overlap_tn without any device allocation.  No counterpart in the
+ * reference: an addition for callers that cannot allocate device memory at
+ * this point, such as a host code that hands all of the GPU's memory to its
+ * own pool at start-up (plane-wave codes sized to the 180 GB of a B200 do),
+ * or a caller that must not let cudaMalloc/cudaFree synchronise the device
+ * while its other streams are working.
+ *
+ * Same arguments, method and result as cpsd_overlap_tn (device pointers;
+ * returns after `stream` finishes).  The split-K workspace is a file-scope
+ * device array of CPSD_NOALLOC_MAX_DOUBLES doubles plus a 256-byte status
+ * word, 8 MiB that every GPU which loads this library holds until the
+ * process exits; the call makes no cudaMalloc, cudaFree or other allocating
+ * call.  Limit: M*N <= CPSD_NOALLOC_MAX_DOUBLES, else CPSD_ERR_SCRATCH and
+ * nothing is launched.
+ *
+ * The first call on each device does a set-up: with that device current it
+ * looks up the array's device address (cudaGetSymbolAddress) and sets the
+ * tensor-core kernel's shared-memory limit.  A caller that captures streams
+ * into CUDA graphs should make that first call before any capture begins.
+ * Every call on a device shares the one array, which keeps the last call's
+ * contents: each call clears the status word, and every partial is written
+ * before it is read.  Calls whose GPU work overlaps (on concurrent streams,
+ * or from several host threads) race on the array: serialise them.
+ */
+int cpsd_overlap_tn_noalloc(int method, int M, int N, int K, const double *A, long lda, const double *B,
+                            long ldb, const double *w, double *C, long ldc, void *stream);
 
 #ifdef __cplusplus
 }

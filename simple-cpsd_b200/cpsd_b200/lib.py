@@ -22,6 +22,7 @@ CPSD_ERR_EMPTY_MASK = 5
 CPSD_ERR_UNMASKED_PSI = 6
 CPSD_ERR_MOVE = 7
 CPSD_ERR_TIMEOUT = 8
+CPSD_ERR_SCRATCH = 9
 CPSD_WARN_LAGRANGE = 10
 
 CPSD_PREC_FP64 = 0
@@ -46,7 +47,7 @@ EXPORTS = [
     "cpsd_mlp_get_params", "cpsd_mlp_set_params", "cpsd_mlp_destroy", "cpsd_gpu_set_preconditioner",
     "cpsd_gpu_set_preconditioner_cap",
     "cpsd_gpu_get_packed", "cpsd_gpu_set_packed", "cpsd_gpu_get_sphere", "cpsd_gpu_set_gemm",
-    "cpsd_overlap_tn",
+    "cpsd_overlap_tn", "cpsd_overlap_tn_noalloc",
 ]
 
 
@@ -123,6 +124,7 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_gpu_set_gemm.argtypes = [_P, _I]
     _L = ctypes.c_long
     lib.cpsd_overlap_tn.argtypes = [_I, _I, _I, _I, _P, _L, _P, _L, _P, _P, _L, _P]
+    lib.cpsd_overlap_tn_noalloc.argtypes = [_I, _I, _I, _I, _P, _L, _P, _L, _P, _P, _L, _P]
     lib.cpsd_gpu_destroy.argtypes = [_P]
     lib.cpsd_gpu_destroy.restype = None
     lib.cpsd_gpu_fft_status.restype = _I

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -991,6 +992,7 @@ const char *cpsd_gpu_strerror(int status)
     case CPSD_ERR_CUDA: return cudaGetErrorString(last_cuda_error());
     case CPSD_ERR_ARG: return "invalid argument";
     case CPSD_ERR_TIMEOUT: return "a bounded wait on the device ran out (tensor-core pipeline)";
+    case CPSD_ERR_SCRATCH: return "M*N exceeds the static scratch of the no-alloc entry point (CPSD_NOALLOC_MAX_DOUBLES)";
     case CPSD_ERR_GRID: return "unsupported FFT grid (nfft must be 16, 24, 32, 48, 64 or 128, and the sphere must fit the plane kernel)";
     case CPSD_ERR_BANDS: return "more than 256 bands in a spin channel";
     case CPSD_ERR_EMPTY_MASK: return "the cutoff mask selects no G vector";
@@ -1746,6 +1748,46 @@ void cpsd_gpu_destroy(cpsd_gpu_ctx *c)
     delete c;
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------- no-alloc overlaps
+// Split-K workspace of cpsd_overlap_tn_noalloc: a file-scope device array,
+// so that entry point never allocates.  Its first 256 bytes hold the
+// timeout word, the rest (CPSD_NOALLOC_MAX_DOUBLES doubles) the partials.
+// Every GPU that loads this library holds the array until the process exits.
+constexpr size_t kNoAllocHeadDoubles = 32;
+constexpr size_t kNoAllocScratchDoubles = kNoAllocHeadDoubles + CPSD_NOALLOC_MAX_DOUBLES;  // 8 MiB
+static __device__ __align__(256) double g_overlap_scratch[kNoAllocScratchDoubles];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Device address of g_overlap_scratch on the current device: looked up once
+// per device, with that device current, then cached (with the tensor-core
+// kernel's shared-memory limit set at the same time).
+int noalloc_scratch(double **out)
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return CPSD_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+        double *p = nullptr;
+        CK(cudaGetSymbolAddress((void **)&p, g_overlap_scratch));
+        CK(cudaFuncSetAttribute(tc_gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+        g_noalloc_base[dev] = p;
+    }
+    *out = g_noalloc_base[dev];
+    return CPSD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int cpsd_overlap_tn(int method, int M, int N, int K, const double *A, long lda, const double *B, long ldb,
                     const double *w, double *C, long ldc, void *stream)
 {
@@ -1775,6 +1817,30 @@ int cpsd_overlap_tn(int method, int M, int N, int K, const double *A, long lda, 
     CK(cudaGetLastError());
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, sc.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return herr ? CPSD_ERR_TIMEOUT : CPSD_OK;
+}
+
+int cpsd_overlap_tn_noalloc(int method, int M, int N, int K, const double *A, long lda, const double *B, long ldb,
+                            const double *w, double *C, long ldc, void *stream)
+{
+    if (method != CPSD_GEMM_FP64 && method != CPSD_GEMM_TF32X3) return CPSD_ERR_ARG;
+    if (M < 0 || N < 0 || K < 0 || lda < K || ldb < K || ldc < N) return CPSD_ERR_ARG;
+    if (M == 0 || N == 0) return CPSD_OK;
+    if (!A || !B || !C) return CPSD_ERR_ARG;
+    if ((size_t)M * (size_t)N > (size_t)CPSD_NOALLOC_MAX_DOUBLES) return CPSD_ERR_SCRATCH;
+    double *base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    int *err = reinterpret_cast<int *>(base);  // the timeout word: must start at zero
+    double *ws = base + kNoAllocHeadDoubles;   // partials: every one is written before it is read
+    CK(cudaMemsetAsync(err, 0, sizeof(int), s));
+    (void)launch_tn(M, N, K, 1, &A, lda, &B, ldb, w, 1.0, 0.0, &C, ldc, method != CPSD_GEMM_FP64, ws,
+                    (size_t)CPSD_NOALLOC_MAX_DOUBLES, err, s);
+    CK(cudaGetLastError());
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return herr ? CPSD_ERR_TIMEOUT : CPSD_OK;
 }
