@@ -175,6 +175,12 @@ class GpuCell:
         self._check(self._L.cpsd_gpu_get_packed(self.h, *[_ptr(o) for o in out]), "cpsd_gpu_get_packed")
         return out
 
+    def get_c2(self) -> np.ndarray:
+        """The current orbitals only, complex (nbands, npw) in sphere order."""
+        out = np.zeros((self.inp.nbands, self.npw), dtype=np.complex128)
+        self._check(self._L.cpsd_gpu_get_packed(self.h, None, _ptr(out), None), "cpsd_gpu_get_packed")
+        return out
+
     def set_packed(self, c2: np.ndarray) -> None:
         c2 = np.ascontiguousarray(c2, dtype=np.complex128)
         self._check(self._L.cpsd_gpu_set_packed(self.h, _ptr(c2)), "cpsd_gpu_set_packed")

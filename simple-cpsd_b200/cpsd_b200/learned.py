@@ -156,23 +156,36 @@ def train(mlp: api.Mlp, X: np.ndarray, T: np.ndarray, steps: int = 3000, batch: 
 
 @dataclasses.dataclass
 class RunResult:
-    energies: List[float]
+    energies: List[float]          # E[0] after every block
+    seconds: List[float]           # wall time since the start after every block
     steps_to_tol: Optional[int]
     seconds_to_tol: Optional[float]
     rejected_blocks: int
     steps: int
+    refine_step: Optional[int] = None     # step at which a mixed run switched to FP64
+    final_c2: Optional[np.ndarray] = None
 
 
 def run(spec_or_inp, e_conv: Optional[float], tol_per_ion: float, max_steps: int, inner: int = 20,
-        mlp: Optional[api.Mlp] = None, precision: int = 0) -> RunResult:
-    """SD (plain or learned-preconditioned with fallback) until the energy is
-    within tol_per_ion * nion of e_conv (or max_steps)."""
+        mlp: Optional[api.Mlp] = None, precision: int = 0, gemm: int = 0,
+        refine_per_ion: Optional[float] = None, start_c2: Optional[np.ndarray] = None,
+        keep_state: bool = False) -> RunResult:
+    """SD (plain, or learned-preconditioned with plain SD as the fallback)
+    until the energy is within tol_per_ion * nion of e_conv, or max_steps.
+
+    precision/gemm select the mixed path; with refine_per_ion set, a mixed
+    run switches the same context to FP64 once an accepted block changes the
+    energy by less than refine_per_ion * nion (the final FP64 refinement)."""
     inp = spec_or_inp if isinstance(spec_or_inp, inputs.CpsdInputs) else inputs.build_inputs(spec_or_inp)
     cell = api.GpuCell(inp, precision=precision)
+    if gemm:
+        cell.set_gemm(gemm)
     cell.set_state(inp.c2, inp.r2)
+    if start_c2 is not None:
+        cell.set_packed(start_c2)
     tol = tol_per_ion * inp.nion
-    energies, rejected, steps = [], 0, 0
-    hit_step, hit_time = None, None
+    energies, seconds, rejected, steps = [], [], 0, 0
+    hit_step, hit_time, refine_step = None, None, None
     prev = math.inf
     cap = LOGK_MAX
     min_bands = min(int(n) for n in inp.ne[:inp.ispin])
@@ -181,7 +194,7 @@ def run(spec_or_inp, e_conv: Optional[float], tol_per_ion: float, max_steps: int
         cell.set_preconditioner(mlp)
     while steps < max_steps:
         if mlp is not None:
-            start = cell.get_packed()[1]
+            start = cell.get_c2()
             warn0 = cell.lagrange_warnings
             cell.set_preconditioner_cap(cap)
             e = float(cell.run(inner)[0])
@@ -202,12 +215,27 @@ def run(spec_or_inp, e_conv: Optional[float], tol_per_ion: float, max_steps: int
             e = float(cell.run(inner)[0])
         steps += inner
         energies.append(e)
+        seconds.append(time.perf_counter() - t0)
+        if (refine_per_ion is not None and refine_step is None and precision != 0
+                and abs(e - prev) < refine_per_ion * inp.nion):
+            cell.set_precision(0)  # FP64 refinement from here on
+            refine_step = steps
+            e = math.inf  # FP64 energies are compared among themselves only
         prev = e
         if e_conv is not None and hit_step is None and abs(e - e_conv) <= tol:
-            hit_step, hit_time = steps, time.perf_counter() - t0
+            hit_step, hit_time = steps, seconds[-1]
             break
+    final = cell.get_c2() if keep_state else None
     cell.close()
-    return RunResult(energies, hit_step, hit_time, rejected, steps)
+    return RunResult(energies, seconds, hit_step, hit_time, rejected, steps, refine_step, final)
+
+
+def first_within(res: RunResult, e_conv: float, tol: float, inner: int):
+    """(steps, seconds) of the first block within tol of e_conv, or (None, None)."""
+    for k, e in enumerate(res.energies):
+        if abs(e - e_conv) <= tol:
+            return (k + 1) * inner, res.seconds[k]
+    return None, None
 
 
 def converged_energy(spec_or_inp, max_steps: int, inner: int = 200, tol: float = 1e-10) -> Tuple[float, int]:
@@ -273,6 +301,89 @@ def experiment(n_train: int = 12, n_eval: int = 4, traj_steps: int = 30000, inne
     return res
 
 
+def evaluate(inp, mlp: api.Mlp, inner: int, tol_per_ion: float, learned_steps: int, plain_steps: int,
+             verify_steps: int, precision: int = 1, gemm: int = 1, refine_per_ion: float = 1e-7) -> dict:
+    """Time to tol_per_ion (Ha per ion) of the learned mixed-precision path and
+    of plain FP64 SD on one cell.
+
+    The converged energy is taken without trusting either run to finish:
+    plain FP64 SD is continued for verify_steps from the learned run's end
+    state, and its final energy is e_conv (the continuation's drift is
+    reported: a learned end state that is not stationary under plain SD
+    shows up there).  Plain SD then runs from the initial state until it is
+    within tolerance of e_conv or plain_steps."""
+    nion = inp.nion
+    tol = tol_per_ion * nion
+    lrn = run(inp, None, tol_per_ion, learned_steps, inner, mlp=mlp, precision=precision, gemm=gemm,
+              refine_per_ion=refine_per_ion, keep_state=True)
+    ver = run(inp, None, tol_per_ion, verify_steps, inner, start_c2=lrn.final_c2)
+    e_conv = ver.energies[-1]
+    plain = run(inp, e_conv, tol_per_ion, plain_steps, inner)
+    ls, lt = first_within(lrn, e_conv, tol, inner)
+    ps, pt = first_within(plain, e_conv, tol, inner)
+    out = {"nion": nion, "nbands": int(inp.nbands), "npw": int(inp.npw), "nfft": int(inp.nfft),
+           "tol_per_ion": tol_per_ion, "e_conv": e_conv,
+           "verify_drift_per_ion": abs(ver.energies[-1] - lrn.energies[-1]) / nion,
+           "verify_steps": verify_steps,
+           "learned": {"steps_to_tol": ls, "seconds_to_tol": lt, "steps_run": lrn.steps,
+                       "seconds_run": lrn.seconds[-1], "rejected_blocks": lrn.rejected_blocks,
+                       "fp64_refinement_from_step": lrn.refine_step, "final_energy": lrn.energies[-1],
+                       "precision": "mixed" if precision else "fp64", "gemm": gemm},
+           "plain_fp64": {"steps_to_tol": ps, "seconds_to_tol": pt, "steps_run": plain.steps,
+                          "seconds_run": plain.seconds[-1], "final_energy": plain.energies[-1]},
+           "plain_final_minus_e_conv_per_ion": (plain.energies[-1] - e_conv) / nion}
+    if ps and ls:
+        out["speedup_time"] = pt / lt
+        out["speedup_steps"] = ps / ls
+    elif ls:
+        # plain SD did not get there within its budget: a lower bound
+        out["speedup_time_lower_bound"] = plain.seconds[-1] / lt
+        out["speedup_steps_lower_bound"] = plain.steps / ls
+    return out
+
+
+def headline(n8: int = 6, n64: int = 1, traj8: int = 12000, traj64: int = 3000, inner: int = 100,
+             train_steps: int = 3000, eval8: int = 2, eval64: int = 1, tol_per_ion: float = 1e-6,
+             learned_steps8: int = 40000, plain_steps8: int = 250000, learned_steps64: int = 20000,
+             plain_steps64: int = 40000, verify_steps: int = 3000, out: Optional[str] = None,
+             weights: Optional[str] = None) -> dict:
+    """Train on trajectories of jittered 8- and 64-atom cells, then time the
+    learned mixed-precision path against plain FP64 SD on held-out cells."""
+    import json
+    from . import configs
+    t0 = time.perf_counter()
+    trajs = [record_trajectory(configs.diamond8_64(seed=1000 + i), traj8, inner, 10) for i in range(n8)]
+    trajs += [record_trajectory(configs.diamond64_128(seed=2000 + i), traj64, inner, 5) for i in range(n64)]
+    t_traj = time.perf_counter() - t0
+    X, T = dataset(trajs)
+    mlp = api.Mlp(seed=0)
+    t0 = time.perf_counter()
+    losses = train(mlp, X, T, steps=train_steps)
+    t_train = time.perf_counter() - t0
+    if weights:
+        np.save(weights, mlp.params)
+    res = {"train": {"cells_8atom": n8, "cells_64atom": n64, "trajectory_steps": [traj8, traj64],
+                     "samples": int(X.shape[0]), "trajectory_seconds": t_traj, "train_steps": train_steps,
+                     "train_seconds": t_train, "loss_first": float(losses[0]),
+                     "loss_last": float(np.mean(losses[-50:]))},
+           "eval": []}
+    for i in range(eval8):
+        inp = inputs.build_inputs(configs.diamond8_64(seed=5000 + i))
+        r = evaluate(inp, mlp, inner, tol_per_ion, learned_steps8, plain_steps8, verify_steps)
+        r["cell"] = "diamond8_64 seed %d" % (5000 + i)
+        res["eval"].append(r)
+    for i in range(eval64):
+        inp = inputs.build_inputs(configs.diamond64_128(seed=6000 + i))
+        r = evaluate(inp, mlp, inner, tol_per_ion, learned_steps64, plain_steps64, verify_steps)
+        r["cell"] = "diamond64_128 seed %d" % (6000 + i)
+        res["eval"].append(r)
+    if out:
+        with open(out, "w") as f:
+            json.dump(res, f, indent=1)
+    mlp.close()
+    return res
+
+
 if __name__ == "__main__":
     import argparse
     import json
@@ -286,7 +397,12 @@ if __name__ == "__main__":
     ap.add_argument("--out", default=None)
     ap.add_argument("--weights", default=None)
     ap.add_argument("--horizon", type=int, default=32)
+    ap.add_argument("--headline", action="store_true",
+                    help="8- and 64-atom training, timed learned mixed path vs plain FP64")
     a = ap.parse_args()
+    if a.headline:
+        print(json.dumps(headline(out=a.out, weights=a.weights), indent=1))
+        raise SystemExit(0)
     r = experiment(a.train, a.eval, a.traj_steps, a.inner, 10, a.train_steps, 1e-6, a.max_steps, a.out, a.weights,
                    a.horizon)
     print(json.dumps(r, indent=1))
