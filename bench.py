@@ -274,6 +274,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain extra (about a minute)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="arithmetic of the timed workload (the default line is fp64)")
     ap.add_argument("--gemm", default="fp64", choices=["fp64", "tf32x3", "tf32x3_overlaps"],
@@ -379,6 +380,17 @@ def main():
             "phases_ms": {k: round(v, 5) for k, v in phm.items()}}
         # config 4: 48 uneven cells, one graph launch per SD step for all of them
         extra["batched_cells"] = time_batched(C.batched_cells(0), args.inner, 3)
+        # the learned path (committed network, mixed precision with a final FP64
+        # refinement) against plain FP64 SD: steps and wall time to 1e-6 Ha/atom
+        # on a held-out 8-atom cell
+        from cpsd_b200 import learned
+        if os.path.exists(learned.PRETRAINED) and not args.no_learned:
+            mlp = learned.load_pretrained()
+            ev = learned.evaluate(inputs.build_inputs(C.diamond8_64(seed=5001)), mlp, 100, 1e-6,
+                                  learned_steps=40000, plain_steps=250000, verify_steps=3000)
+            mlp.close()
+            ev["cell"] = "diamond8_64 seed 5001 (held out)"
+            extra["learned_vs_plain_diamond8_64"] = ev
         # the 128^3 / 64-atom / 128-band cell of the precision study, FP64
         big = inputs.build_inputs(C.diamond64_128())
         tms, lch, ph3, geo3, E3 = time_cell(big, 3, 1, args.inner, torch, None)

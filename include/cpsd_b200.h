@@ -222,10 +222,17 @@ int cpsd_gpu_set_preconditioner(cpsd_gpu_ctx *c, cpsd_mlp *m);
  * context created with CPSD_PREC_MIXED and have no effect while it runs
  * FP64. */
 int cpsd_gpu_set_gemm(cpsd_gpu_ctx *c, int mode);
-/* Trust-region bound on the learned log step scale, clamped to [-2, 4.5]
- * (attaching a network opens it fully).  Read on the device at every step,
- * so it takes effect without re-capturing the step graphs. */
-int cpsd_gpu_set_preconditioner_cap(cpsd_gpu_ctx *c, double max_log_k);
+/* Range [min_log_k, max_log_k] of the learned log step scale, inside
+ * [-2, 4.5] (attaching a network opens it fully).  A caller narrows the upper
+ * end as a trust region and sets [0, 0] for plain SD steps (K = 1).  Read on
+ * the device at every step, so it takes effect without re-capturing the
+ * step graphs. */
+int cpsd_gpu_set_preconditioner_range(cpsd_gpu_ctx *c, double min_log_k, double max_log_k);
+/* Keep a device copy of the current orbitals and step count / go back to it
+ * (the rollback point of a guarded block, without a round trip through the
+ * host). */
+int cpsd_gpu_save_orbitals(cpsd_gpu_ctx *c);
+int cpsd_gpu_restore_orbitals(cpsd_gpu_ctx *c);
 
 /* Packed orbitals (ne0+ne1 bands x npw complex, sphere order) out and in. */
 int cpsd_gpu_get_packed(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi);

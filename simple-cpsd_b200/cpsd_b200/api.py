@@ -163,10 +163,16 @@ class GpuCell:
         """TN-product engine of the mixed path: CPSD_GEMM_FP64 or CPSD_GEMM_TF32X3."""
         self._check(self._L.cpsd_gpu_set_gemm(self.h, int(mode)), "cpsd_gpu_set_gemm")
 
-    def set_preconditioner_cap(self, max_log_k: float) -> None:
-        """Trust-region bound on the learned log step scale."""
-        self._check(self._L.cpsd_gpu_set_preconditioner_cap(self.h, float(max_log_k)),
-                    "cpsd_gpu_set_preconditioner_cap")
+    def set_preconditioner_range(self, min_log_k: float, max_log_k: float) -> None:
+        """Range of the learned log step scale ([0, 0]: plain SD steps)."""
+        self._check(self._L.cpsd_gpu_set_preconditioner_range(self.h, float(min_log_k), float(max_log_k)),
+                    "cpsd_gpu_set_preconditioner_range")
+
+    def save_orbitals(self) -> None:
+        self._check(self._L.cpsd_gpu_save_orbitals(self.h), "cpsd_gpu_save_orbitals")
+
+    def restore_orbitals(self) -> None:
+        self._check(self._L.cpsd_gpu_restore_orbitals(self.h), "cpsd_gpu_restore_orbitals")
 
     def get_packed(self):
         """(c1, c2, cpsi) as complex (nbands, npw) arrays in sphere order."""

@@ -37,6 +37,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import os
 import time
 from typing import List, Optional, Sequence, Tuple
 
@@ -45,7 +46,13 @@ import numpy as np
 from . import api, inputs
 
 NSHELL = 64  # csrc/mlp.cuh kShells
+# network trained by `python -m cpsd_b200.learned --headline` (8- and 64-atom
+# jittered diamond cells); loaded by load_pretrained()
+PRETRAINED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "preconditioner_diamond.npy")
 LOGK_MIN, LOGK_MAX = -2.0, 4.5  # csrc/mlp.cuh kLogKMin, kLogKMax
+# trust region on log K: steady state near CAP_GROW / (CAP_GROW + CAP_SHRINK)
+# rejected blocks (about one in eight)
+CAP_SHRINK, CAP_GROW = 0.7, 0.1
 
 
 @dataclasses.dataclass
@@ -194,23 +201,23 @@ def run(spec_or_inp, e_conv: Optional[float], tol_per_ion: float, max_steps: int
         cell.set_preconditioner(mlp)
     while steps < max_steps:
         if mlp is not None:
-            start = cell.get_c2()
+            cell.save_orbitals()
             warn0 = cell.lagrange_warnings
-            cell.set_preconditioner_cap(cap)
+            cell.set_preconditioner_range(LOGK_MIN, cap)
             e = float(cell.run(inner)[0])
             # (with one band per spin the reference's convergence test can never
             # pass, so its warning says nothing there)
             lag_failed = cell.lagrange_warnings > warn0 and min_bands > 1
             if not math.isfinite(e) or e > prev or lag_failed:
-                # rejected: redo the block from its start with plain SD
+                # rejected: redo the block from its start with plain SD steps
+                # (K = 1 exactly: the update reduces to the reference's)
                 rejected += 1
-                cap = max(LOGK_MIN, cap - 0.7)
-                cell.set_packed(start)
-                cell.set_preconditioner(None)
+                cap = max(LOGK_MIN, cap - CAP_SHRINK)
+                cell.restore_orbitals()
+                cell.set_preconditioner_range(0.0, 0.0)
                 e = float(cell.run(inner)[0])
-                cell.set_preconditioner(mlp)
             else:
-                cap = min(LOGK_MAX, cap + 0.35)
+                cap = min(LOGK_MAX, cap + CAP_GROW)
         else:
             e = float(cell.run(inner)[0])
         steps += inner
@@ -299,6 +306,13 @@ def experiment(n_train: int = 12, n_eval: int = 4, traj_steps: int = 30000, inne
             json.dump(res, f, indent=1)
     mlp.close()
     return res
+
+
+def load_pretrained(path: str = PRETRAINED) -> api.Mlp:
+    """The committed network (FP32 master parameters of csrc/mlp.cuh)."""
+    mlp = api.Mlp(seed=0)
+    mlp.params = np.load(path)
+    return mlp
 
 
 def evaluate(inp, mlp: api.Mlp, inner: int, tol_per_ion: float, learned_steps: int, plain_steps: int,

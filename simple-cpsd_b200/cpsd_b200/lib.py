@@ -45,7 +45,7 @@ EXPORTS = [
     "cpsd_gpu_batch_run", "cpsd_gpu_batch_counters", "cpsd_gpu_batch_stream", "cpsd_gpu_batch_destroy",
     "cpsd_mlp_nparams", "cpsd_mlp_create", "cpsd_mlp_forward", "cpsd_mlp_gradient", "cpsd_mlp_train",
     "cpsd_mlp_get_params", "cpsd_mlp_set_params", "cpsd_mlp_destroy", "cpsd_gpu_set_preconditioner",
-    "cpsd_gpu_set_preconditioner_cap",
+    "cpsd_gpu_set_preconditioner_range", "cpsd_gpu_save_orbitals", "cpsd_gpu_restore_orbitals",
     "cpsd_gpu_get_packed", "cpsd_gpu_set_packed", "cpsd_gpu_get_sphere", "cpsd_gpu_set_gemm",
     "cpsd_overlap_tn", "cpsd_overlap_tn_noalloc",
 ]
@@ -117,7 +117,9 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_mlp_destroy.argtypes = [_P]
     lib.cpsd_mlp_destroy.restype = None
     lib.cpsd_gpu_set_preconditioner.argtypes = [_P, _P]
-    lib.cpsd_gpu_set_preconditioner_cap.argtypes = [_P, _D]
+    lib.cpsd_gpu_set_preconditioner_range.argtypes = [_P, _D, _D]
+    lib.cpsd_gpu_save_orbitals.argtypes = [_P]
+    lib.cpsd_gpu_restore_orbitals.argtypes = [_P]
     lib.cpsd_gpu_get_packed.argtypes = [_P, _P, _P, _P]
     lib.cpsd_gpu_set_packed.argtypes = [_P, _P]
     lib.cpsd_gpu_get_sphere.argtypes = [_P, _P, _P, _P]

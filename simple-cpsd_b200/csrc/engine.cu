@@ -356,12 +356,17 @@ struct cpsd_gpu_ctx {
     bool use_graph = true;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // one captured SD step per ping-pong parity
     int graph_launches = 0;
+    bool lag_tile = false;  // 4 x 4 tiled solver (<= 128 bands, 16-CTA clusters schedulable)
     int lag_cluster = 8;  // CTAs per cluster of the Lagrange solver (16 where schedulable)
     int lag_lb = 0;       // its row-tile width
     // learned preconditioner (optional): shells, stats, features, outputs
     cpsd_mlp *mlp = nullptr;
     int *shell = nullptr, *dstep = nullptr;
-    float *pcap = nullptr;  // trust-region bound on the learned log step scale
+    float *pcap = nullptr;  // [lo, hi] range of the learned log step scale
+    cx<double> *saved = nullptr;  // cpsd_gpu_save_orbitals copy (with the step counters)
+    int *saved_step = nullptr;
+    long long saved_steps_run = 0;
+    double *epart = nullptr;  // real-space Ewald sum per ion
     cx<double> *pR = nullptr;  // residual of -H psi outside the occupied subspace
     double *pM = nullptr;      // <cpsi_b|c1_a> per spin
     double *pstats = nullptr, tmax = 0.0;
@@ -443,7 +448,10 @@ int launch_tn(int M, int N, int K, int nprod, const double *const *A, long lda, 
     return 2;
 }
 
-// Which TN products may run on the tensor cores (bits of CPSD_GEMM_*).
+// Which TN products may run on the tensor cores (bits of CPSD_GEMM_*):
+// the projector coefficients and the learned step's residual (errors there
+// stay inside the occupied subspace, which the constraint rotates away), and
+// the Lagrange overlaps.
 enum { TN_PROJECTOR = 1, TN_OVERLAPS = 2 };
 
 // Batched weighted TN products of a context; `which` names the product so
@@ -465,6 +473,37 @@ int gemm_tn(cpsd_gpu_ctx *c, int M, int N, int K, const double *A, long lda, con
             const double *w, double alpha, double beta, double *C, long ldc, int which = 0)
 {
     return gemm_tn_batch(c, M, N, K, 1, &A, lda, &B, ldb, w, alpha, beta, &C, ldc, which);
+}
+
+// The three overlaps C2'WC2, C2'WC1, C1'WC1 of one spin: one fused
+// tensor-core pass (tc_overlaps3_kernel) where the context runs its overlaps
+// on the tensor cores, the spin has at most 128 bands and the operands are
+// 16-byte aligned for cp.async; otherwise the batched TN products.
+int overlaps3(cpsd_gpu_ctx *c, int m, int K, long ld, const double *C2, const double *C1, double *const *Cs)
+{
+    const double *As[3] = {C2, C2, C1}, *Bs[3] = {C2, C1, C1};
+    const bool tc = (c->gemm_mode & TN_OVERLAPS) != 0 && c->precision == CPSD_PREC_MIXED;
+    const bool fits = m > 0 && m <= kTcM && (ld % 2) == 0 && K % 2 == 0 && ((uintptr_t)C1 % 16) == 0 &&
+                      ((uintptr_t)C2 % 16) == 0;
+    if (!tc || !fits) return gemm_tn_batch(c, m, m, K, 3, As, ld, Bs, ld, c->w, 1.0, 0.0, Cs, m, TN_OVERLAPS);
+    const long mm = (long)m * m;
+    long splits = std::min<long>(148, std::max<long>(1, K / 64));
+    while ((size_t)splits * 3 * mm > c->gemm_ws_elems && splits > 1) --splits;
+    const int kchunk = (int)(cdiv(cdiv(K, splits), kOvBK) * kOvBK);
+    splits = cdiv(K, kchunk);
+    tc_overlaps3_kernel<<<(unsigned)splits, kTcThreads, kOvSmem, c->st>>>(m, K, ld, C2, C1, c->w, kchunk,
+                                                                         (int)splits, c->gws, c->flags + 2);
+    TnBatch bt{};
+    for (int q = 0; q < 3; ++q) {
+        bt.A[q] = As[q];
+        bt.B[q] = Bs[q];
+        bt.C[q] = Cs[q];
+    }
+    bt.nprod = 3;
+    bt.splits = (int)splits;
+    splitk_reduce_kernel<<<(unsigned)cdiv(mm * 3 * 32, 256), 256, 0, c->st>>>(m, m, m, c->gws, 1.0, 0.0, bt);
+    c->nlaunch += 2;
+    return CPSD_OK;
 }
 
 void gemm_nn(cpsd_gpu_ctx *c, int NJ, int K, int L, double alpha, const double *Mat, long ldm,
@@ -601,7 +640,7 @@ int one_step(cpsd_gpu_ctx *c)
             const long off = (long)(ms ? c->ne0 : 0) * ldr;
             double *Mt = c->pM + (long)ms * c->ne0 * c->ne0;  // Mt[b][a] = <cpsi_b|c1_a>
             int rc = gemm_tn(c, m, m, K, (const double *)c->cpsi + off, ldr, (const double *)c1 + off, ldr, c->w,
-                             1.0, 0.0, Mt, m);
+                             1.0, 0.0, Mt, m, TN_PROJECTOR);
             if (rc) return rc;
             gemm_nn(c, m, K, m, -1.0, Mt, m, (const double *)c1 + off, ldr, 1.0, (double *)c->pR + off, ldr);
         }
@@ -629,7 +668,7 @@ int one_step(cpsd_gpu_ctx *c)
         // the three overlaps of this spin in one launch
         const double *As[3] = {C2, C2, C1}, *Bs[3] = {C2, C1, C1};
         double *Cs[3] = {(double *)Mblk(c, ms, 0), (double *)Mblk(c, ms, 1), (double *)Mblk(c, ms, 2)};
-        int rc = gemm_tn_batch(c, m, m, K, 3, As, ldr, Bs, ldr, c->w, 1.0, 0.0, Cs, m, TN_OVERLAPS);
+        int rc = overlaps3(c, m, K, ldr, C2, C1, Cs);
         if (rc) return rc;
         la.M22[ms] = Mblk(c, ms, 0);
         la.M21[ms] = Mblk(c, ms, 1);
@@ -649,7 +688,21 @@ int one_step(cpsd_gpu_ctx *c)
     la.lb = c->lag_lb;
     if (c->ne0 <= kLagSmallMax)
         lagrange_small_kernel<<<1, kLagThreads, sizeof(double) * 7 * ne02, s>>>(la);
-    else {
+    else if (c->lag_tile) {
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kLagTileGrid * kLagTileGrid;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(kLagTileGrid * kLagTileGrid);
+        cfg.blockDim = dim3(kLagThreads);
+        cfg.dynamicSmemBytes = lagrange_tile_smem(c->ne0);
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, lagrange_tile_kernel, la));
+    } else {
         cudaLaunchConfig_t cfg{};
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -754,10 +807,12 @@ int energies(cpsd_gpu_ctx *c, int inner)
     fa.hml = c->hml;
     fa.beta = c->beta;
     fa.vnlnrm_p = c->vnlnrm_p;
-    fa.r1 = c->r1;
-    fa.rcell = c->rcell;
-    fa.zv = c->zv;
-    fa.katm = c->katm;
+    if (c->nion > 1) {
+        ewald_real_kernel<<<c->nion - 1, 256, 0, s>>>(c->nion, c->nsh, c->r1, c->rcell, c->zv, c->katm,
+                                                      c->prm.rcut, c->epart);
+        c->nlaunch += 1;
+    }
+    fa.ewald_part = c->epart;
     fa.scal2 = c->scal2;
     fa.omega = c->prm.omega;
     fa.dv = c->dv;
@@ -1056,6 +1111,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
         rc = c->fft32->init(ar, h.KX);
         if (rc) return rc;
         CK(cudaFuncSetAttribute(tc_gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+        CK(cudaFuncSetAttribute(tc_overlaps3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOvSmem));
     }
     c->precision = p->precision;
     c->fft = (p->precision == CPSD_PREC_MIXED) ? c->fft32.get() : c->fft64.get();
@@ -1143,7 +1199,9 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->Edev, 16));
     CK(ar.alloc(&c->flags, 4));
     c->gemm_splits_cap = 512;
-    c->gemm_ws_elems = (size_t)4 << 20;  // 32 MB of split-K partials
+    // split-K partials: at least 32 MB, and room for 148 splits of the three
+    // overlaps of the largest spin
+    c->gemm_ws_elems = std::max<size_t>((size_t)4 << 20, (size_t)3 * c->ne0 * c->ne0 * 148);
     CK(ar.alloc(&c->gws, c->gemm_ws_elems));
     c->pblocks = 148;
     c->bblocks = (int)std::max<long>(1, std::min<long>(64, cdiv(c->npw, 256 * 8)));
@@ -1154,7 +1212,8 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->full, (size_t)std::max(nb, c->ispin) * c->n2ft3d));
     CK(ar.alloc(&c->shell, (size_t)c->npw_pad));
     CK(ar.alloc(&c->dstep, 1));
-    CK(ar.alloc(&c->pcap, 1));
+    CK(ar.alloc(&c->pcap, 2));
+    CK(ar.alloc(&c->epart, std::max(nion, 1)));  // zero: the last ion has no pair of its own
     CK(ar.alloc(&c->pR, (size_t)nb * P));
     CK(ar.alloc(&c->pM, (size_t)c->ispin * c->ne0 * c->ne0));
     CK(ar.alloc(&c->pstats, (size_t)3 * nb));
@@ -1192,6 +1251,30 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
             (void)cudaGetLastError();
         }
         if (!c->lag_lb) return CPSD_ERR_BANDS;
+        // the tiled solver where its 16-CTA clusters fit (CPSD_B200_LAGRANGE=cluster
+        // keeps the column solver, for comparisons)
+        const char *lag_env = getenv("CPSD_B200_LAGRANGE");
+        const size_t tsm = lagrange_tile_smem(c->ne0);
+        if (c->ne0 <= kLagTileMax && tsm <= limit && !(lag_env && !strcmp(lag_env, "cluster"))) {
+            CK(cudaFuncSetAttribute(lagrange_tile_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            CK(allow_max_smem(lagrange_tile_kernel, optin));
+            cudaLaunchConfig_t cfg{};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = kLagTileGrid * kLagTileGrid;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(kLagTileGrid * kLagTileGrid);
+            cfg.blockDim = dim3(kLagThreads);
+            cfg.dynamicSmemBytes = tsm;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, lagrange_tile_kernel, &cfg) == cudaSuccess &&
+                nclusters >= 1)
+                c->lag_tile = true;
+            (void)cudaGetLastError();
+        }
     }
     CK(cudaDeviceSynchronize());  // allocation memsets run on the legacy stream
     *out = c.release();
@@ -1463,20 +1546,50 @@ int cpsd_gpu_set_preconditioner(cpsd_gpu_ctx *c, cpsd_mlp *m)
         CK(cudaSetDevice(c->prm.device));
         const int step = (int)std::min<long long>(c->steps_run, 1 << 30);
         CK(cudaMemcpyAsync(c->dstep, &step, sizeof(int), cudaMemcpyHostToDevice, c->st));
-        const float cap = kLogKMax;
-        CK(cudaMemcpyAsync(c->pcap, &cap, sizeof(float), cudaMemcpyHostToDevice, c->st));
+        const float range[2] = {kLogKMin, kLogKMax};
+        CK(cudaMemcpyAsync(c->pcap, range, sizeof(range), cudaMemcpyHostToDevice, c->st));
         CK(cudaStreamSynchronize(c->st));
     }
     return CPSD_OK;
 }
 
-int cpsd_gpu_set_preconditioner_cap(cpsd_gpu_ctx *c, double max_log_k)
+int cpsd_gpu_set_preconditioner_range(cpsd_gpu_ctx *c, double min_log_k, double max_log_k)
 {
-    if (!c || !(max_log_k == max_log_k)) return CPSD_ERR_ARG;
+    if (!c || !(min_log_k == min_log_k) || !(max_log_k == max_log_k) || min_log_k > max_log_k)
+        return CPSD_ERR_ARG;
     CK(cudaSetDevice(c->prm.device));
-    const float cap = (float)std::max<double>(kLogKMin, std::min<double>(kLogKMax, max_log_k));
-    CK(cudaMemcpyAsync(c->pcap, &cap, sizeof(float), cudaMemcpyHostToDevice, c->st));
+    auto clamp = [](double v) { return (float)std::max<double>(kLogKMin, std::min<double>(kLogKMax, v)); };
+    const float range[2] = {clamp(min_log_k), clamp(max_log_k)};
+    CK(cudaMemcpyAsync(c->pcap, range, sizeof(range), cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
+    return CPSD_OK;
+}
+
+int cpsd_gpu_save_orbitals(cpsd_gpu_ctx *c)
+{
+    if (!c || !c->state_ok) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    if (!c->saved) {
+        CK(c->ar.alloc(&c->saved, (size_t)c->nb * c->npw_pad));
+        CK(c->ar.alloc(&c->saved_step, 1));
+    }
+    CK(cudaMemcpyAsync(c->saved, c->cbuf[c->cur], sizeof(cx<double>) * c->nb * c->npw_pad,
+                       cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(c->saved_step, c->dstep, sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->saved_steps_run = c->steps_run;
+    return CPSD_OK;
+}
+
+int cpsd_gpu_restore_orbitals(cpsd_gpu_ctx *c)
+{
+    if (!c || !c->saved) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    CK(cudaMemcpyAsync(c->cbuf[c->cur], c->saved, sizeof(cx<double>) * c->nb * c->npw_pad,
+                       cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(c->dstep, c->saved_step, sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->steps_run = c->saved_steps_run;
     return CPSD_OK;
 }
 

@@ -794,6 +794,232 @@ __global__ void __launch_bounds__(kLagThreads) lagrange_small_kernel(LagArgs a)
     }
 }
 
+// ------------------------------------------------- Lagrange, 2-D tiles
+// lagrange_tile_kernel: the same fixed point as lagrange_kernel (cpsd.c:
+// 439-478, including the idamax read and the 30-iteration limit) for up to
+// 128 bands per spin, on a cluster of 4 x 4 CTAs.  CTA (p, q) owns the tile
+// rows I_p x columns J_q (T = ceil(m / 4) of each) of sa0, sa1 and st1, and
+// keeps its constant panels s21[I_p, :], s11[I_p, :], s12[:, J_q] and
+// s22[I_p, J_q] in shared memory for all iterations.  Per iteration:
+//   phase 1: gather sa0[I_p, :] and sa0[:, J_q] from the tiles of its row and
+//            column (distributed shared memory), t = s22 + s21 sa0 + sa0 s12,
+//            st1 = s11 sa0 on its tile;               cluster barrier;
+//   phase 2: gather st1[:, J_q], sa1 = t + sa0 st1, st1 = sa1 - sa0, the
+//            tile's argmax of |st1|;                  cluster barrier;
+// then every CTA reduces the 16 candidates in rank order and reads the
+// element after the maximum, as the reference does.  sa1 goes into the
+// other half of a double-buffered tile, so the two barriers are all an
+// iteration needs.
+constexpr int kLagTileGrid = 4;  // 4 x 4 CTAs
+constexpr int kLagTileMax = 128;
+
+CPSD_HD size_t lagrange_tile_smem(int m)
+{
+    const size_t T = (size_t)(m + kLagTileGrid - 1) / kLagTileGrid;
+    // S21r, S11r, S12c, Xr, Xc, STc: m*T each; S22t, STt: T*T; Xt: 2*T*T; slots
+    return sizeof(double) * (6 * (size_t)m * T + 4 * T * T + 2 * kLagTileGrid * kLagTileGrid);
+}
+
+__global__ void __launch_bounds__(kLagThreads) lagrange_tile_kernel(LagArgs a)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int p = rank / kLagTileGrid, q = rank % kLagTileGrid;
+    const int tid = threadIdx.x;
+    extern __shared__ double tsm[];
+    const long ne02 = (long)a.ne0 * a.ne0;
+    const int T = (a.ne0 + kLagTileGrid - 1) / kLagTileGrid;  // tile edge (sized for the larger spin)
+    double *S21r = tsm, *S11r = S21r + (long)a.ne0 * T, *S12c = S11r + (long)a.ne0 * T;
+    double *Xr = S12c + (long)a.ne0 * T, *Xc = Xr + (long)a.ne0 * T, *STc = Xc + (long)a.ne0 * T;
+    double *S22t = STc + (long)a.ne0 * T, *STt = S22t + T * T, *Xt = STt + T * T;  // Xt: two halves
+    double *slot = Xt + 2 * T * T;                                                 // [rank][2]
+    for (int ms = 0; ms < a.ispin; ++ms) {
+        const int m = ms ? a.ne1 : a.ne0;
+        const long kk = (long)m * m;
+        if (m == 0) continue;
+        const int t = (m + kLagTileGrid - 1) / kLagTileGrid;  // this spin's tile edge
+        const int i0 = p * t, j0 = q * t;
+        const int nr = max(0, min(m, i0 + t) - i0), nc = max(0, min(m, j0 + t) - j0);
+        const double *M22 = a.M22[ms], *M21 = a.M21[ms], *M11 = a.M11[ms];
+        const double dte = a.dte;
+        // s matrices, cpsd.c:420-437 (upper triangles mirrored as the reference does)
+        for (long e = (long)rank * kLagThreads + tid; e < kk; e += (long)kLagTileGrid * kLagTileGrid * kLagThreads) {
+            const int i = (int)(e % m), j = (int)(e / m);
+            double v22, v21, v12, v11;
+            if (i == j) {
+                v22 = (1.0 - M22[(long)i * m + i]) * 0.5 / dte;
+                v21 = (1.0 - M21[(long)i * m + i]) * 0.5;
+                v12 = v21;
+                v11 = -M11[(long)i * m + i] * 0.5 * dte;
+            } else {
+                const int lo = i < j ? i : j, hi = i < j ? j : i;
+                v22 = -M22[(long)lo * m + hi] * 0.5 / dte;
+                v21 = -M21[(long)lo * m + hi] * 0.5;   // <c2_lo|c1_hi>
+                v12 = -M21[(long)hi * m + lo] * 0.5;   // <c1_lo|c2_hi>
+                v11 = -M11[(long)lo * m + hi] * 0.5 * dte;
+            }
+            a.s22[e] = v22;
+            a.s21[e] = v21;
+            a.s12[e] = v12;
+            a.s11[e] = v11;
+        }
+        cl.sync();
+        // constant panels; sa0 = s22 (cpsd.c:441) into the first half of Xt
+        for (int e = tid; e < m * t; e += kLagThreads) {
+            const int l = e / t, ii = e % t;
+            S21r[l * t + ii] = ii < nr ? a.s21[(i0 + ii) + (long)l * m] : 0.0;
+            S11r[l * t + ii] = ii < nr ? a.s11[(i0 + ii) + (long)l * m] : 0.0;
+            const int jj = e % t;
+            S12c[l * t + jj] = jj < nc ? a.s12[l + (long)(j0 + jj) * m] : 0.0;
+        }
+        for (int e = tid; e < t * t; e += kLagThreads) {
+            const int jj = e / t, ii = e % t;
+            const double v = (ii < nr && jj < nc) ? a.s22[(i0 + ii) + (long)(j0 + jj) * m] : 0.0;
+            S22t[jj * t + ii] = v;
+            Xt[jj * t + ii] = v;
+        }
+        // thread -> one row ii of the tile and 4 of its columns
+        const int ii = tid % 32, jq = (tid / 32) * 4;
+        const bool rowok = ii < nr;
+        int half = 0;  // which half of Xt holds sa0
+        bool done = false;
+        int iter = 0;
+        cl.sync();  // every tile's sa0 is in place (later: ordered by the candidates' barrier)
+        while (!done && iter < 30) {
+            ++iter;
+            // gather sa0[I_p, :] (Xr, [l][ii]) and sa0[:, J_q] (Xc, [l][jj])
+            for (int g = 0; g < kLagTileGrid; ++g) {
+                const double *rowt = cl.map_shared_rank(Xt + half * t * t, p * kLagTileGrid + g);
+                const double *colt = cl.map_shared_rank(Xt + half * t * t, g * kLagTileGrid + q);
+                for (int e = tid; e < t * t; e += kLagThreads) {
+                    const int c = e / t, r = e % t;  // tile element (r, c), stored [c][r]
+                    const int lr = g * t + c, lc = g * t + r;
+                    if (lr < m) Xr[lr * t + r] = rowt[e];
+                    if (lc < m) Xc[lc * t + c] = colt[e];
+                }
+            }
+            __syncthreads();
+            // t = s22 + s21 sa0 + sa0 s12 ; st1 = s11 sa0   (cpsd.c:444-462)
+            double t1[4], t2[4], st[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) t1[k] = t2[k] = st[k] = 0.0;
+            if (rowok)
+                for (int l = 0; l < m; ++l) {
+                    const double a21 = S21r[l * t + ii], a11 = S11r[l * t + ii], xil = Xr[l * t + ii];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const double xlj = Xc[l * t + jq + k];
+                        t1[k] = fma(a21, xlj, t1[k]);
+                        t2[k] = fma(xil, S12c[l * t + jq + k], t2[k]);
+                        st[k] = fma(a11, xlj, st[k]);
+                    }
+                }
+            // (rows ii >= t are not in the tile: their slots belong to the next column)
+            if (ii < t) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (jq + k < t) STt[(jq + k) * t + ii] = st[k];
+            }
+            cl.sync();  // every tile's st1 = s11 sa0 is in place
+            for (int g = 0; g < kLagTileGrid; ++g) {
+                const double *stt = cl.map_shared_rank(STt, g * kLagTileGrid + q);
+                for (int e = tid; e < t * t; e += kLagThreads) {
+                    const int c = e / t, r = e % t;
+                    const int lc = g * t + r;
+                    if (lc < m) STc[lc * t + c] = stt[e];
+                }
+            }
+            __syncthreads();
+            // sa1 += sa0 st1 (cpsd.c:463-468); st1 = sa1 - sa0 (:469-470)
+            double s2[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) s2[k] = 0.0;
+            if (rowok)
+                for (int l = 0; l < m; ++l) {
+                    const double xil = Xr[l * t + ii];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) s2[k] = fma(xil, STc[l * t + jq + k], s2[k]);
+                }
+            double bestv = -1.0;
+            long besti = 0x7fffffff;
+            double *nxt = Xt + (half ^ 1) * t * t;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int jj = jq + k;
+                if (rowok && jj < nc) {
+                    // sa1 = s22, += s21 sa0, += sa0 s12, += sa0 st1: the
+                    // order of lagrange_kernel
+                    const double sa1 = s2[k] + (t2[k] + (t1[k] + S22t[jj * t + ii]));
+                    const long f = (i0 + ii) + (long)(j0 + jj) * m;
+                    nxt[jj * t + ii] = sa1;
+                    a.X1[f] = sa1;
+                    const double d = sa1 - Xt[half * t * t + jj * t + ii];
+                    a.st1[f] = d;
+                    const double ad = fabs(d);
+                    if (ad > bestv || (ad == bestv && f < besti)) {
+                        bestv = ad;
+                        besti = f;
+                    }
+                }
+            }
+            // tile argmax (first column-major index of the largest |st1|, as idamax)
+            __shared__ double shv[kLagThreads / 32];
+            __shared__ long shi[kLagThreads / 32];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bestv, o);
+                const long oi = __shfl_xor_sync(0xffffffffu, besti, o);
+                if (ov > bestv || (ov == bestv && oi < besti)) {
+                    bestv = ov;
+                    besti = oi;
+                }
+            }
+            if ((tid & 31) == 0) {
+                shv[tid >> 5] = bestv;
+                shi[tid >> 5] = besti;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                for (int w = 1; w < kLagThreads / 32; ++w)
+                    if (shv[w] > bestv || (shv[w] == bestv && shi[w] < besti)) {
+                        bestv = shv[w];
+                        besti = shi[w];
+                    }
+                slot[2 * rank] = bestv;
+                slot[2 * rank + 1] = (double)besti;
+            }
+            cl.sync();  // every tile's candidate, st1 and sa1 are in place
+            double gv = -1.0;
+            long gi = 0x7fffffff;
+            for (int r = 0; r < kLagTileGrid * kLagTileGrid; ++r) {
+                const double *sl = cl.map_shared_rank(slot, r);
+                const double v = sl[0];
+                const long ix = (long)sl[1];
+                if (v > gv || (v == gv && ix < gi)) {
+                    gv = v;
+                    gi = ix;
+                }
+            }
+            // idamax returns an index in 1..kk even when every entry is NaN
+            if (gi < 0 || gi >= kk) gi = 0;
+            // the reference reads st1 at idamax's 1-based result (cpsd.c:471):
+            // the element after the largest; past the end of st1 lies sa1
+            const long nx = gi + 1;
+            const double adiff = fabs(nx < ne02 ? a.st1[nx] : a.X1[nx - ne02]);
+            done = adiff < 1e-15;
+            half ^= 1;  // sa1 becomes sa0 (when done, it is the result)
+        }
+        if (!done && rank == 0 && tid == 0) atomicAdd(a.fail, 1);
+        // lmd = the last sa1 (cpsd.c:478)
+        const double *fin = Xt + half * t * t;
+        for (int e = tid; e < t * t; e += kLagThreads) {
+            const int jj = e / t, r = e % t;
+            if (r < nr && jj < nc) a.lmd[ms * ne02 + (i0 + r) + (long)(j0 + jj) * m] = fin[e];
+        }
+        cl.sync();  // the slots and tiles are reused by the next spin
+    }
+}
+
 // ------------------------------------------------------------ energies
 // per-block partial sums over packed points of the three single-field terms
 // (cpsd.c:520-526 k-space Ewald, :548-554 Hartree, :590 local)
@@ -879,11 +1105,43 @@ struct FinalArgs {
     const double *Mh[2];
     double *hml;
     const double *beta, *vnlnrm_p;
-    const double *r1, *rcell, *zv;
-    const int *katm;
+    const double *ewald_part;  // real-space Ewald sum per ion (ewald_real_kernel)
     double scal2, omega, dv, cewald, rcut, dt, dte;
     double *E;  // in: E[0] previous energy; out: E[0..9], E[10] deltae, E[11] deltac
 };
+
+// Real-space Ewald sum, cpsd.c:527-545 (A&S 7.1.28 erfc, cpsd.c:11-17): block
+// ii sums the pairs (ii, jj > ii) over the nsh image cells, one (pair, image)
+// term per thread, and writes a fixed-order block sum to part[ii].
+__global__ void __launch_bounds__(256) ewald_real_kernel(int nion, int nsh, const double *__restrict__ r1,
+                                                         const double *__restrict__ rcell,
+                                                         const double *__restrict__ zv,
+                                                         const int *__restrict__ katm, double rcut,
+                                                         double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    const double B1 = 0.0705230784, B2 = 0.0422820123, B3 = 0.0092705272;
+    const double B4 = 0.0001520143, B5 = 0.0002765672, B6 = 0.0000430638;
+    const int ii = blockIdx.x;
+    const long cnt = (long)(nion - 1 - ii) * nsh;
+    double ew = 0.0;
+    for (long e = threadIdx.x; e < cnt; e += 256) {
+        const int jj = ii + 1 + (int)(e / nsh);
+        const int l = (int)(e % nsh);
+        const double dx = r1[3 * ii] - r1[3 * jj];
+        const double dy = r1[1 + 3 * ii] - r1[1 + 3 * jj];
+        const double dz = r1[2 + 3 * ii] - r1[2 + 3 * jj];
+        const double zz = zv[katm[ii]] * zv[katm[jj]];
+        const double x = rcell[l] + dx, y = rcell[l + nsh] + dy, z = rcell[l + 2 * nsh] + dz;
+        const double r = sqrt(x * x + y * y + z * z);
+        const double w = r / rcut;
+        const double aa = (1.0 + w * (B1 + w * (B2 + w * (B3 + w * (B4 + w * (B5 + w * B6))))));
+        const double erfc = 1.0 / (aa * aa * aa * aa);
+        ew += zz * (erfc * erfc * erfc * erfc) / r;
+    }
+    const double t = block_sum<256>(ew, sh);
+    if (threadIdx.x == 0) part[ii] = t;
+}
 
 // One block of kFinalThreads: every sum is a fixed-order block reduction, so
 // the energies are bitwise reproducible run to run.
@@ -921,35 +1179,10 @@ __global__ void __launch_bounds__(kFinalThreads) final_energy_kernel(FinalArgs a
         for (int k = tid; k < a.pblocks; k += kFinalThreads) v += a.ppart[q * a.pblocks + k];
         t[q] = block_sum<kFinalThreads>(v, sh);
     }
-    // real-space Ewald, cpsd.c:527-545 (A&S 7.1.28 erfc, cpsd.c:11-17), one
-    // (pair, image) term per thread
-    const double B1 = 0.0705230784, B2 = 0.0422820123, B3 = 0.0092705272;
-    const double B4 = 0.0001520143, B5 = 0.0002765672, B6 = 0.0000430638;
-    const long npair = (long)a.nion * (a.nion - 1) / 2;
-    double ew = 0.0;
-    for (long e = tid; e < npair * a.nsh; e += kFinalThreads) {
-        const long pr = e / a.nsh;
-        const int l = (int)(e % a.nsh);
-        // pair index -> (ii < jj)
-        int ii = 0;
-        long rem = pr;
-        while (rem >= a.nion - 1 - ii) {
-            rem -= a.nion - 1 - ii;
-            ++ii;
-        }
-        const int jj = ii + 1 + (int)rem;
-        const double dx = a.r1[3 * ii] - a.r1[3 * jj];
-        const double dy = a.r1[1 + 3 * ii] - a.r1[1 + 3 * jj];
-        const double dz = a.r1[2 + 3 * ii] - a.r1[2 + 3 * jj];
-        const double zz = a.zv[a.katm[ii]] * a.zv[a.katm[jj]];
-        const double x = a.rcell[l] + dx, y = a.rcell[l + a.nsh] + dy, z = a.rcell[l + 2 * a.nsh] + dz;
-        const double r = sqrt(x * x + y * y + z * z);
-        const double w = r / a.rcut;
-        const double aa = (1.0 + w * (B1 + w * (B2 + w * (B3 + w * (B4 + w * (B5 + w * B6))))));
-        const double erfc = 1.0 / (aa * aa * aa * aa);
-        ew += zz * (erfc * erfc * erfc * erfc) / r;
-    }
-    const double eion_real = block_sum<kFinalThreads>(ew, sh);
+    // real-space Ewald: per-ion partials of ewald_real_kernel, summed in ion order
+    double eion_real = 0.0;
+    if (tid == 0)
+        for (int ii = 0; ii < a.nion; ++ii) eion_real += a.ewald_part[ii];
     // xc
     double ex = 0.0, px = 0.0;
     for (int k = tid; k < a.gblocks; k += kFinalThreads) {

@@ -278,11 +278,11 @@ __global__ void prec_features_kernel(int nb, double tmax, const double *__restri
 // c2 (= c1 + dte cpsi, the plain SD update) += dte (K[b][shell(p)] - 1) R,
 // with R the residual of cpsi outside the occupied subspace: the residual is
 // stepped by dte K, the part inside the subspace exactly as plain SD.  log K
-// is the network output clamped to [kLogKMin, min(kLogKMax, *cap)]; *cap is
-// a trust-region bound the host lowers after a rejected block and raises
-// after an accepted one.
+// is the network output clamped to [range[0], range[1]] (inside [kLogKMin,
+// kLogKMax]): the host narrows the upper end after a rejected block (a trust
+// region) and sets [0, 0] for plain SD steps (K = 1, c2 unchanged here).
 __global__ void prec_update_kernel(int nb, int npw, long ldc, const int *__restrict__ shell,
-                                   const float *__restrict__ y, const float *__restrict__ cap, double dte,
+                                   const float *__restrict__ y, const float *__restrict__ range, double dte,
                                    const cx<double> *__restrict__ R, cx<double> *__restrict__ c2,
                                    int *__restrict__ step)
 {
@@ -290,8 +290,8 @@ __global__ void prec_update_kernel(int nb, int npw, long ldc, const int *__restr
     if (id == 0) atomicAdd(step, 1);
     if (id >= (long)nb * npw) return;
     const int b = (int)(id / npw), p = (int)(id % npw);
-    const float hi = fmaxf(kLogKMin, fminf(kLogKMax, *cap));
-    const float lk = fminf(fmaxf(y[b * kShells + shell[p]], kLogKMin), hi);
+    const float lo = fmaxf(kLogKMin, range[0]), hi = fminf(kLogKMax, range[1]);
+    const float lk = fminf(fmaxf(y[b * kShells + shell[p]], lo), hi);
     const double f = dte * (exp((double)lk) - 1.0);
     const long o = (long)b * ldc + p;
     const cx<double> r = R[o], u = c2[o];

@@ -223,3 +223,200 @@ tc_gemm_tn_kernel(int M, int N, int K, long lda, long ldb, const double *__restr
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcN));
 }
+
+// ------------------------------------------------------ the three overlaps
+// tc_overlaps3_kernel: the three overlaps of the Lagrange step in one pass
+// over the orbitals (m <= 128 bands of a spin):
+//
+//   part[0][split] = X' W X,  part[1][split] = X' W Y,  part[2][split] = Y' W Y
+//
+// with X = C2 and Y = C1 (rows K-contiguous).  Both operands are scaled by
+// sqrt(w) so one TF32 hi/lo pair of each serves all three products, and the
+// three FP32 accumulators (3 x 128 columns) share one 512-column tensor-
+// memory allocation.  Raw FP64 slabs arrive by cp.async, kOvRaw stages ahead,
+// so the loads are in flight while earlier stages are split and multiplied;
+// every operand byte is read once, against three times for three separate
+// products.  Same partial layout as tc_gemm_tn_kernel (prod = 0, 1, 2), summed
+// by splitk_reduce_kernel.
+constexpr int kOvBK = 16;                               // K per stage
+constexpr int kOvRaw = 4;                               // raw FP64 stages in flight
+constexpr int kOvRow = 20;                              // raw row stride in doubles (160 B: no bank conflicts)
+constexpr int kOvSlabWords = kTcM * kOvBK;              // 2048 words = 8 KB per TF32 slab
+constexpr int kOvRawDoubles = 2 * kTcM * kOvRow;        // X and Y, [row][k]: 40 KB per stage
+constexpr size_t kOvSmem = (size_t)kOvRaw * kOvRawDoubles * 8 + 2 * 4 * kOvSlabWords * 4 + 128;
+constexpr uint32_t kOvTmemCols = 512;
+
+CPSD_D void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+CPSD_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+CPSD_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__global__ void __launch_bounds__(kTcThreads)
+tc_overlaps3_kernel(int m, int K, long ld, const double *__restrict__ X, const double *__restrict__ Y,
+                    const double *__restrict__ w, int kchunk, int splits, double *__restrict__ part,
+                    int *__restrict__ err)
+{
+    extern __shared__ unsigned char ov_raw[];
+    double *raw = reinterpret_cast<double *>(((uintptr_t)ov_raw + 127) & ~(uintptr_t)127);
+    uint32_t *slab = reinterpret_cast<uint32_t *>(raw + (size_t)kOvRaw * kOvRawDoubles);
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int split = blockIdx.x;
+    const int k0 = split * kchunk, k1 = min(K, k0 + kchunk);
+    const int nst = k1 > k0 ? (k1 - k0 + kOvBK - 1) / kOvBK : 0;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(kOvTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+
+    // cp.async map: 2 operands x 128 rows x 8 16-byte chunks = 2048 chunks,
+    // 8 per thread; rows past m and K past k1 are zero-filled (src bytes 0,
+    // source address kept inside the operand)
+    auto issue = [&](int st) {
+        double *dst = raw + (size_t)(st % kOvRaw) * kOvRawDoubles;
+        const int kb = k0 + st * kOvBK;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int c = tid + q * kTcThreads;  // 0..2047
+            const int op = c >> 10, r = (c >> 3) & 127, kc = (c & 7) * 2;
+            const double *src = op ? Y : X;
+            const int k = kb + kc;
+            const bool ok = (r < m) && (k < k1);
+            const double *g = ok ? src + (long)r * ld + k : src;
+            cp_async16(smem_u32(dst + (size_t)op * kTcM * kOvRow + r * kOvRow + kc), g, ok ? 16u : 0u);
+        }
+    };
+#pragma unroll
+    for (int st = 0; st < kOvRaw - 1; ++st) {
+        if (st < nst) issue(st);
+        cp_async_commit();
+    }
+
+    // conversion map: thread -> (chunk c of 4 K values, row group, lane in core matrix)
+    const int kq = tid & 3, rlo = (tid >> 2) & 7, chunk = (tid >> 5) & 3, rhalf = tid >> 7;
+    bool fail = false;
+    int issued = 0;
+    for (int it = 0; it < nst; ++it) {
+        const int b = it & 1;
+        cp_async_wait<kOvRaw - 2>();  // this thread's copies of stage it have landed
+        // the MMAs of stage it-2 read slab set b: wait for them
+        if (it >= 2 && !mbar_wait(smem_u32(&mbar[b]), (uint32_t)(((it >> 1) + 1) & 1))) fail = true;
+        if (__syncthreads_or(fail)) {  // every thread's stage-it copies are visible too
+            fail = true;
+            break;
+        }
+        if (it + kOvRaw - 1 < nst) issue(it + kOvRaw - 1);  // into the slot stage it-1 used
+        cp_async_commit();
+        const double *rs = raw + (size_t)(it % kOvRaw) * kOvRawDoubles;
+        uint32_t *Xh = slab + b * 4 * kOvSlabWords, *Xl = Xh + kOvSlabWords, *Yh = Xl + kOvSlabWords,
+                 *Yl = Yh + kOvSlabWords;
+        const int k = k0 + it * kOvBK + chunk * 4 + kq;
+        const double sw = (w && k < k1) ? sqrt(fmax(w[k >> 1], 0.0)) : 1.0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int rhi = rhalf * 8 + j, r = rhi * 8 + rlo;
+            const int kl = chunk * 4 + kq;
+            const float xv = (float)(rs[r * kOvRow + kl] * sw);
+            const float yv = (float)(rs[kTcM * kOvRow + r * kOvRow + kl] * sw);
+            const uint32_t xh = tf32_bits(xv), yh = tf32_bits(yv);
+            const int o = ((chunk * 16 + rhi) << 5) + lane;  // (chunk*16 + rhi)*32 + rlo*4 + kq
+            Xh[o] = xh;
+            Xl[o] = tf32_bits(xv - __uint_as_float(xh));
+            Yh[o] = yh;
+            Yl[o] = tf32_bits(yv - __uint_as_float(yh));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t xh = smem_u32(Xh), xl = smem_u32(Xl), yh = smem_u32(Yh), yl = smem_u32(Yl);
+            const uint32_t d0 = tmem, d1 = tmem + kTcN, d2 = tmem + 2 * kTcN;
+#pragma unroll
+            for (int s = 0; s < kOvBK / 8; ++s) {
+                const uint32_t o = (uint32_t)s * 4096;  // K-chunk 2s
+                const uint32_t acc0 = (it > 0 || s > 0) ? 1u : 0u;
+                tc_mma(d0, tc_desc(xh + o), tc_desc(xh + o), acc0);  // X'X
+                tc_mma(d0, tc_desc(xh + o), tc_desc(xl + o), 1u);
+                tc_mma(d0, tc_desc(xl + o), tc_desc(xh + o), 1u);
+                tc_mma(d1, tc_desc(xh + o), tc_desc(yh + o), acc0);  // X'Y
+                tc_mma(d1, tc_desc(xh + o), tc_desc(yl + o), 1u);
+                tc_mma(d1, tc_desc(xl + o), tc_desc(yh + o), 1u);
+                tc_mma(d2, tc_desc(yh + o), tc_desc(yh + o), acc0);  // Y'Y
+                tc_mma(d2, tc_desc(yh + o), tc_desc(yl + o), 1u);
+                tc_mma(d2, tc_desc(yl + o), tc_desc(yh + o), 1u);
+            }
+            tc_commit(smem_u32(&mbar[b]));
+        }
+        issued = it + 1;
+    }
+    cp_async_wait<0>();
+    bool done = true;
+    if (issued > 0) {
+        const int last = issued - 1;
+        done = mbar_wait(smem_u32(&mbar[last & 1]), (uint32_t)((last >> 1) & 1));
+    }
+    if (__syncthreads_or(!done)) fail = true;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (!fail) {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows) and 6 of
+        // the 12 32-column chunks (3 products x 128 columns)
+        const long MN = (long)m * m;
+        double *E = raw + warp * 32 * 33;
+        const int rbase = 32 * (warp & 3);
+#pragma unroll 1
+        for (int cc = (warp >> 2) * 6; cc < (warp >> 2) * 6 + 6; ++cc) {
+            const int prod = cc >> 2, c0 = (cc & 3) * 32;
+            uint32_t v[32];
+            if (issued > 0) {
+                const uint32_t ta = tmem + ((uint32_t)rbase << 16) + (uint32_t)(prod * kTcN + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                    "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+                    "%30, %31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(ta));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            } else {
+#pragma unroll
+                for (int q = 0; q < 32; ++q) v[q] = 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 32; ++q) E[lane * 33 + q] = (double)__uint_as_float(v[q]);
+            __syncwarp();
+            double *out = part + ((long)prod * splits + split) * MN;
+            const int col = c0 + lane;
+            for (int rr = 0; rr < 32; ++rr) {
+                const int row = rbase + rr;
+                if (row < m && col < m) out[(long)row * m + col] = E[rr * 33 + lane];
+            }
+            __syncwarp();
+        }
+    } else if (tid == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kOvTmemCols));
+}

@@ -112,3 +112,40 @@ def test_trained_network_needs_fewer_steps_than_plain_sd():
     assert lrn.steps_to_tol < plain.steps_to_tol, (plain.steps_to_tol, lrn.steps_to_tol, lrn.rejected_blocks)
     assert abs(lrn.energies[-1] - e_conv) <= 1e-8 * inp.nion
     m.close()
+
+
+def test_unit_step_scale_is_plain_sd_bitwise():
+    """With the log-K range set to [0, 0] the learned step graph takes plain
+    SD steps: same energies, bit for bit, as a cell without a network."""
+    inp = inputs.build_inputs(configs.small_diamond(24, 4, ecut=16.0, seed=7))
+    plain = api.GpuCell(inp)
+    plain.set_state(inp.c2, inp.r2)
+    e_plain = [plain.run(10)[0] for _ in range(3)]
+    m = api.Mlp(seed=2)
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    cell.set_preconditioner(m)
+    cell.set_preconditioner_range(0.0, 0.0)
+    e_unit = [cell.run(10)[0] for _ in range(3)]
+    assert e_unit == e_plain
+    plain.close()
+    cell.close()
+    m.close()
+
+
+def test_save_and_restore_orbitals_repeat_a_block():
+    inp = inputs.build_inputs(configs.small_diamond(24, 4, ecut=16.0, seed=8))
+    m = api.Mlp(seed=3)
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    cell.set_preconditioner(m)
+    cell.run(5)
+    cell.save_orbitals()
+    e1 = cell.run(10).copy()
+    c_after = cell.get_c2()
+    cell.restore_orbitals()
+    e2 = cell.run(10).copy()
+    assert np.array_equal(c_after, cell.get_c2())
+    assert e1[0] == e2[0]
+    cell.close()
+    m.close()

@@ -113,6 +113,33 @@ def test_intermediates_match_restatement(restatement):
     assert np.abs(S - np.eye(inp.nbands)).max() < 1e-4
 
 
+@pytest.mark.parametrize("solver", ["tile", "cluster"])
+@pytest.mark.parametrize("nb", [40, 128])
+def test_many_band_lagrange_solvers_match_restatement(restatement, monkeypatch, solver, nb):
+    """More than 32 bands run the cluster Lagrange solvers (the 4 x 4 tiled
+    one by default, the column one with CPSD_B200_LAGRANGE=cluster): lmd, hml
+    and the energies of three SD steps against the restatement (40 bands:
+    ragged 10 x 10 tiles; 128: full 32 x 32 tiles)."""
+    if solver == "cluster":
+        monkeypatch.setenv("CPSD_B200_LAGRANGE", "cluster")
+    else:
+        monkeypatch.delenv("CPSD_B200_LAGRANGE", raising=False)
+    inp = inputs.build_inputs(configs.small_diamond(32, nb, ecut=25.0, seed=12))
+    so = oracle.State(inp)
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    for _ in range(3):
+        restatement.run(inp, 1, so)
+        cell.run(1)
+        assert abs(cell.E[0] - so.E[0]) < E_TOL
+    sg = api.State(inp)
+    cell.get_state(sg)
+    assert np.abs(so.lmd - sg.lmd).max() < 1e-10
+    assert np.abs(so.hml - sg.hml).max() < 1e-10
+    assert cell.lagrange_warnings == so.lagrange_fail  # same converged / not-converged steps
+    cell.close()
+
+
 @pytest.mark.parametrize("n", [16, 24, 32, 48, 64, 128])
 def test_fft_dropins_match_oracle(restatement, n):
     """cr_fft3b_/rc_fft3f_ drop-ins (whole box) == the fftpack3d restatement."""

@@ -107,3 +107,18 @@ def test_tf32x3_needs_a_mixed_context():
     with pytest.raises(lib.CpsdError):
         cell.set_gemm(lib.CPSD_GEMM_TF32X3)
     cell.close()
+
+
+def test_fused_overlaps_at_128_bands():
+    """The fused three-overlap tcgen05 pass (128 bands, 128^3) against the
+    same mixed-precision steps with FP64 overlaps."""
+    inp = inputs.build_inputs(configs.diamond64_128())
+    E = []
+    for mode in (lib.CPSD_GEMM_TF32X3, lib.CPSD_GEMM_TF32X3_OVERLAPS):
+        cell = api.GpuCell(inp, precision=lib.CPSD_PREC_MIXED)
+        cell.set_gemm(mode)
+        cell.set_state(inp.c2, inp.r2)
+        E.append([float(cell.run(2)[0]) for _ in range(2)])
+        cell.close()
+    for a, b in zip(*E):
+        assert abs(a - b) < 1e-5 * abs(a), (a, b)
