@@ -94,8 +94,9 @@ enum { CPSD_PREC_FP64 = 0, CPSD_PREC_MIXED = 1 };
 /* Engine of the TN products of the mixed path: FP64 CUDA cores, or three
  * TF32 tensor-core products (hi*hi + hi*lo + lo*hi, FP32 accumulate in tensor
  * memory, FP64 split-K sums), about FP32 accuracy.  CPSD_GEMM_TF32X3 moves
- * the projector coefficients (the KB contraction) to the tensor cores;
- * CPSD_GEMM_TF32X3_OVERLAPS moves the three Lagrange overlaps as well.  The
+ * the KB projector contraction and back-projection (and the learned step's
+ * residual) to the tensor cores; CPSD_GEMM_TF32X3_OVERLAPS moves the three
+ * Lagrange overlaps and the constraint correction as well.  The
  * Lagrange solve divides (1 - <c2|c2>) by dte (about 1e-2), so FP32-level
  * overlaps cost about 1e-6 relative in the energy per step: follow such a
  * run with FP64 steps. */

@@ -448,10 +448,11 @@ int launch_tn(int M, int N, int K, int nprod, const double *const *A, long lda, 
     return 2;
 }
 
-// Which TN products may run on the tensor cores (bits of CPSD_GEMM_*):
-// the projector coefficients and the learned step's residual (errors there
-// stay inside the occupied subspace, which the constraint rotates away), and
-// the Lagrange overlaps.
+// Which products may run on the tensor cores (bits of CPSD_GEMM_*):
+// TN_PROJECTOR: the KB projector coefficients and back-projection, and the
+// learned step's residual (errors there stay inside the occupied subspace,
+// which the constraint rotates away); TN_OVERLAPS: the Lagrange overlaps and
+// the constraint correction c2 += dte C1 lmd.
 enum { TN_PROJECTOR = 1, TN_OVERLAPS = 2 };
 
 // Batched weighted TN products of a context; `which` names the product so
@@ -506,12 +507,21 @@ int overlaps3(cpsd_gpu_ctx *c, int m, int K, long ld, const double *C2, const do
     return CPSD_OK;
 }
 
+// Out = beta Out + alpha Mat B (K the long grid dimension); `which` names the
+// product as for gemm_tn_batch, so the tensor-core variant runs where the
+// context runs mixed precision and its GEMM mode includes it.
 void gemm_nn(cpsd_gpu_ctx *c, int NJ, int K, int L, double alpha, const double *Mat, long ldm,
-             const double *B, long ldb, double beta, double *Out, long ldo)
+             const double *B, long ldb, double beta, double *Out, long ldo, int which = 0)
 {
     if (NJ <= 0 || L <= 0) return;
-    dim3 grid((unsigned)cdiv(K, GB), (unsigned)cdiv(NJ, GB));
-    gemm_nn_kernel<<<grid, 256, 0, c->st>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo);
+    if ((c->gemm_mode & which) != 0 && c->precision == CPSD_PREC_MIXED) {
+        dim3 grid((unsigned)cdiv(K, kTcN), (unsigned)cdiv(NJ, kTcM));
+        tc_gemm_nn_kernel<<<grid, kTcThreads, kTcSmem, c->st>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo,
+                                                                c->flags + 2);
+    } else {
+        dim3 grid((unsigned)cdiv(K, GB), (unsigned)cdiv(NJ, GB));
+        gemm_nn_kernel<<<grid, 256, 0, c->st>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo);
+    }
     c->nlaunch += 1;
 }
 
@@ -612,7 +622,7 @@ int one_step(cpsd_gpu_ctx *c)
         kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, s>>>(
             c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT); c->nlaunch += 1;
         gemm_nn(c, c->nb, K, c->nproj, 1.0, c->coefT, c->nproj, (const double *)c->proj, ldr, 1.0,
-                (double *)c2, ldr);
+                (double *)c2, ldr, TN_PROJECTOR);
     }
     mark(c, 7);
     // (V + xc) psi back to G, -H psi and the SD step, cpsd.c:384-400
@@ -642,7 +652,8 @@ int one_step(cpsd_gpu_ctx *c)
             int rc = gemm_tn(c, m, m, K, (const double *)c->cpsi + off, ldr, (const double *)c1 + off, ldr, c->w,
                              1.0, 0.0, Mt, m, TN_PROJECTOR);
             if (rc) return rc;
-            gemm_nn(c, m, K, m, -1.0, Mt, m, (const double *)c1 + off, ldr, 1.0, (double *)c->pR + off, ldr);
+            gemm_nn(c, m, K, m, -1.0, Mt, m, (const double *)c1 + off, ldr, 1.0, (double *)c->pR + off, ldr,
+                    TN_PROJECTOR);
         }
         band_stats_kernel<<<c->nb, 256, 0, s>>>(c->npw, c->ldc, c->w, c->tg, c1, c->cpsi, c->pstats);
         prec_features_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 256), 256, 0, s>>>(c->nb, c->tmax, c->pstats,
@@ -724,7 +735,7 @@ int one_step(cpsd_gpu_ctx *c)
         const int m = ms ? c->ne1 : c->ne0;
         const long off = (long)(ms ? c->ne0 : 0) * ldr;
         gemm_nn(c, m, K, m, c->dte, c->lmd + ms * ne02, m, (const double *)c1 + off, ldr, 1.0,
-                (double *)c2 + off, ldr);
+                (double *)c2 + off, ldr, TN_OVERLAPS);
     }
     mark(c, 12);
     CK(cudaGetLastError());
@@ -1112,6 +1123,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
         if (rc) return rc;
         CK(cudaFuncSetAttribute(tc_gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
         CK(cudaFuncSetAttribute(tc_overlaps3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOvSmem));
+        CK(cudaFuncSetAttribute(tc_gemm_nn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     }
     c->precision = p->precision;
     c->fft = (p->precision == CPSD_PREC_MIXED) ? c->fft32.get() : c->fft64.get();

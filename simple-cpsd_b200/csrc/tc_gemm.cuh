@@ -420,3 +420,162 @@ tc_overlaps3_kernel(int m, int K, long ld, const double *__restrict__ X, const d
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kOvTmemCols));
 }
+
+// ------------------------------------------------------------- NN products
+// tc_gemm_nn_kernel: Out[j][k] = beta Out[j][k] + alpha sum_l Mat[j][l] B[l][k]
+// (the contract of gemm_nn_kernel: back-projection, residual and constraint
+// products with K the long grid dimension) in 3xTF32 on tcgen05.  CTA tile:
+// 128 rows j x 128 columns k, the reduction over l in slabs of 32.  Mat
+// rows are l-contiguous (K-major as loaded); B rows are k-contiguous, so B is
+// read along k (coalesced) and transposed into the K-major slab while it is
+// split into TF32 hi/lo.  Same pipeline, waits and error handling as
+// tc_gemm_tn_kernel; the epilogue stages rows through shared memory.
+__global__ void __launch_bounds__(kTcThreads)
+tc_gemm_nn_kernel(int NJ, int K, int L, double alpha, const double *__restrict__ Mat, long ldm,
+                  const double *__restrict__ B, long ldb, double beta, double *__restrict__ Out, long ldo,
+                  int *__restrict__ err)
+{
+    extern __shared__ unsigned char nn_raw[];
+    uint32_t *sm = reinterpret_cast<uint32_t *>(((uintptr_t)nn_raw + 127) & ~(uintptr_t)127);
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int k0 = blockIdx.x * kTcN, j0 = blockIdx.y * kTcM;
+    const int nst = (L + kTcBK - 1) / kTcBK;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"((uint32_t)kTcN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+
+    // Mat slab map (as the A operand of the TN kernel): 8 rows x 4 l per warp
+    const int kq = tid & 3, rlo = (tid >> 2) & 7, chunk = tid >> 5;
+    // B slab map: thread -> column kk of the tile and 16 consecutive l
+    const int kk = tid & 127, lq = tid >> 7;
+    bool fail = false;
+    int issued = 0;
+    for (int it = 0; it < nst; ++it) {
+        const int b = it & 1;
+        uint32_t *Ah = sm + b * kTcStageWords, *Al = Ah + kTcSlabWords, *Bh = Al + kTcSlabWords,
+                 *Bl = Bh + kTcSlabWords;
+        if (it >= 2 && !mbar_wait(smem_u32(&mbar[b]), (uint32_t)(((it >> 1) + 1) & 1))) fail = true;
+        if (__syncthreads_or(fail)) {
+            fail = true;
+            break;
+        }
+        const int l0 = it * kTcBK;
+        double ra[16], rb[16];
+        {
+            const int l = l0 + chunk * 4 + kq;
+#pragma unroll
+            for (int rhi = 0; rhi < 16; ++rhi) {
+                const int r = rhi * 8 + rlo;
+                ra[rhi] = (l < L && j0 + r < NJ) ? Mat[(long)(j0 + r) * ldm + l] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int l = l0 + lq * 16 + q;
+            rb[q] = (l < L && k0 + kk < K) ? B[(long)l * ldb + k0 + kk] : 0.0;
+        }
+#pragma unroll
+        for (int rhi = 0; rhi < 16; ++rhi) {
+            const float a = (float)ra[rhi];
+            const uint32_t ah = tf32_bits(a);
+            const int o = ((chunk * 16 + rhi) << 5) + lane;  // row rhi*8+rlo, l = chunk*4+kq
+            Ah[o] = ah;
+            Al[o] = tf32_bits(a - __uint_as_float(ah));
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int ll = lq * 16 + q;  // l within the slab
+            const float v = (float)rb[q];
+            const uint32_t vh = tf32_bits(v);
+            const int o = (((ll >> 2) * 16 + (kk >> 3)) << 5) + ((kk & 7) << 2) + (ll & 3);
+            Bh[o] = vh;
+            Bl[o] = tf32_bits(v - __uint_as_float(vh));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t ah = smem_u32(Ah), al = smem_u32(Al), bh = smem_u32(Bh), bl = smem_u32(Bl);
+#pragma unroll
+            for (int s = 0; s < kTcBK / 8; ++s) {
+                const uint32_t o = (uint32_t)s * 4096;
+                tc_mma(tmem, tc_desc(ah + o), tc_desc(bh + o), (it > 0 || s > 0) ? 1u : 0u);
+                tc_mma(tmem, tc_desc(ah + o), tc_desc(bl + o), 1u);
+                tc_mma(tmem, tc_desc(al + o), tc_desc(bh + o), 1u);
+            }
+            tc_commit(smem_u32(&mbar[b]));
+        }
+        issued = it + 1;
+    }
+    bool done = true;
+    if (issued > 0) {
+        const int last = issued - 1;
+        done = mbar_wait(smem_u32(&mbar[last & 1]), (uint32_t)((last >> 1) & 1));
+    }
+    if (__syncthreads_or(!done)) fail = true;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (!fail) {
+        double *E = reinterpret_cast<double *>(sm) + warp * 32 * 33;
+        const int rbase = 32 * (warp & 3), cbase = 64 * (warp >> 2);
+#pragma unroll 1
+        for (int cc = 0; cc < 2; ++cc) {
+            uint32_t v[32];
+            if (issued > 0) {
+                const uint32_t ta = tmem + ((uint32_t)rbase << 16) + (uint32_t)(cbase + 32 * cc);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                    "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+                    "%30, %31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(ta));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            } else {
+#pragma unroll
+                for (int q = 0; q < 32; ++q) v[q] = 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 32; ++q) E[lane * 33 + q] = (double)__uint_as_float(v[q]);
+            __syncwarp();
+            const int col = k0 + cbase + 32 * cc + lane;
+            // the 32 rows' old values first (all loads in flight), then the stores
+            double ov[32];
+#pragma unroll
+            for (int rr = 0; rr < 32; ++rr) {
+                const int row = j0 + rbase + rr;
+                ov[rr] = (beta != 0.0 && row < NJ && col < K) ? Out[(long)row * ldo + col] : 0.0;
+            }
+#pragma unroll
+            for (int rr = 0; rr < 32; ++rr) {
+                const int row = j0 + rbase + rr;
+                if (row < NJ && col < K) Out[(long)row * ldo + col] = alpha * E[rr * 33 + lane] + beta * ov[rr];
+            }
+            __syncwarp();
+        }
+    } else if (tid == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcN));
+}
