@@ -26,7 +26,7 @@ enum {
     CPSD_ERR_BANDS = 4,         /* more than 256 bands in a spin channel */
     CPSD_ERR_EMPTY_MASK = 5,    /* the cutoff mask selects no G vector */
     CPSD_ERR_UNMASKED_PSI = 6,  /* input orbitals have coefficients outside the mask */
-    CPSD_ERR_MOVE = 7,          /* move=1 (ionic forces) requested but not built in */
+    CPSD_ERR_MOVE = 7,          /* move=1 requested but no G vectors / masses were given */
     CPSD_ERR_TIMEOUT = 8,       /* a bounded wait on the device ran out (tensor-core pipeline) */
     CPSD_ERR_SCRATCH = 9,       /* a problem larger than cpsd_overlap_tn_noalloc's static scratch */
     CPSD_WARN_LAGRANGE = 10     /* (positive warning) Lagrange iteration hit 30 steps; the
@@ -127,7 +127,9 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
 int cpsd_gpu_set_scalars(cpsd_gpu_ctx *c, const double *unitg, double omega, double dt, double fmass,
                          double cewald, double rcut);
 
-/* Upload the per-cell tables in the layouts cpsd() takes. */
+/* Upload the per-cell tables in the layouts cpsd() takes.  G (3 x nfft3d,
+ * ccpsdv3/get_g.c) and amass (per kind) are needed only for move = 1 and may
+ * be NULL otherwise. */
 int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, const double *zv,
                         const double *rcell, const double *G, const double *tg, const double *vc,
                         const double *vg, const int *lmmax, const double *vnlnrm, const double *vl,
@@ -139,6 +141,9 @@ int cpsd_gpu_set_state(cpsd_gpu_ctx *c, const double *c2, const double *r2);
 /*
  * Run `inner` SD steps and the energy evaluation, the body of cpsd().
  * E[0] must hold the previous total energy (for deltae), as in cpsd().
+ * move = 1 also computes the ion forces (local, nonlocal, k- and real-space
+ * Ewald, cpsd.c:246-364) and takes the ion step r2 = r1 + dt/sqrt(M) fion
+ * (cpsd.c:401-411); deltar is then the largest |fion| of the last step.
  */
 int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae, double *deltac,
                  double *deltar);

@@ -316,7 +316,7 @@ def load_pretrained(path: str = PRETRAINED) -> api.Mlp:
 
 
 def evaluate(inp, mlp: api.Mlp, inner: int, tol_per_ion: float, learned_steps: int, plain_steps: int,
-             verify_steps: int, precision: int = 1, gemm: int = 1, refine_per_ion: float = 1e-7) -> dict:
+             verify_steps: int, precision: int = 1, gemm: int = 3, refine_per_ion: float = 1e-7) -> dict:
     """Time to tol_per_ion (Ha per ion) of the learned mixed-precision path and
     of plain FP64 SD on one cell.
 
@@ -356,10 +356,10 @@ def evaluate(inp, mlp: api.Mlp, inner: int, tol_per_ion: float, learned_steps: i
     return out
 
 
-def headline(n8: int = 6, n64: int = 1, traj8: int = 12000, traj64: int = 3000, inner: int = 100,
+def headline(n8: int = 6, n64: int = 2, traj8: int = 12000, traj64: int = 4000, inner: int = 100,
              train_steps: int = 3000, eval8: int = 2, eval64: int = 1, tol_per_ion: float = 1e-6,
-             learned_steps8: int = 40000, plain_steps8: int = 250000, learned_steps64: int = 20000,
-             plain_steps64: int = 40000, verify_steps: int = 3000, out: Optional[str] = None,
+             learned_steps8: int = 40000, plain_steps8: int = 250000, learned_steps64: int = 30000,
+             plain_steps64: int = 80000, verify_steps: int = 5000, out: Optional[str] = None,
              weights: Optional[str] = None) -> dict:
     """Train on trajectories of jittered 8- and 64-atom cells, then time the
     learned mixed-precision path against plain FP64 SD on held-out cells."""

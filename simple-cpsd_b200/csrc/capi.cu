@@ -43,7 +43,6 @@ extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, co
     if (!ne || !unitg || !masker || !c2 || !E) return CPSD_ERR_ARG;
     const int nh = nfft / 2 + 1;
     if (nfft <= 0 || nfft3d != nh * nfft * nfft || n2ft3d != (nfft + 2) * nfft * nfft) return CPSD_ERR_ARG;
-    if (move) return CPSD_ERR_MOVE;
     int nkatm = 1;
     for (int ii = 0; ii < nion; ++ii) nkatm = std::max(nkatm, katm[ii] + 1);
     Signature sig;

@@ -368,6 +368,12 @@ struct cpsd_gpu_ctx {
     long long saved_steps_run = 0;
     double *epart = nullptr;  // real-space Ewald sum per ion
     cx<double> *pR = nullptr;  // residual of -H psi outside the occupied subspace
+    // ion motion (move = 1)
+    bool motion_ok = false;  // G vectors and masses given by cpsd_gpu_set_tables
+    int move = 0;            // the step graphs hold the force kernels
+    std::vector<double> amass_h;
+    double *Gv = nullptr, *dti = nullptr, *fpart = nullptr, *fnl = nullptr, *ewp = nullptr, *coefP = nullptr;
+    cx<double> *Ynl = nullptr;
     double *pM = nullptr;      // <cpsi_b|c1_a> per spin
     double *pstats = nullptr, tmax = 0.0;
     long long steps_run = 0;  // SD steps taken by this context
@@ -603,6 +609,35 @@ int one_step(cpsd_gpu_ctx *c)
     va.Vg = c->Vg;
     va.proj = c->proj;
     vloc_proj_kernel<<<(unsigned)cdiv(c->npw_pad, 128), 128, 0, s>>>(va); c->nlaunch += 1;
+    if (c->move && c->nion > 0) {  // local, k-space and real-space Ewald forces
+        ForceArgs fa{};
+        fa.npw = c->npw;
+        fa.n = c->n;
+        fa.nh = c->nh;
+        fa.nion = c->nion;
+        fa.pt_i = c->pt_i;
+        fa.pt_j = c->pt_j;
+        fa.pt_k = c->pt_k;
+        fa.katm = c->katm;
+        fa.ex1 = c->ex1;
+        fa.ex2 = c->ex2;
+        fa.ex3 = c->ex3;
+        fa.w = c->w;
+        fa.G = c->Gv;
+        fa.vl = c->vl;
+        fa.vg = c->vg;
+        fa.zv = c->zv;
+        fa.dng = c->dng;
+        fa.s = c->sfac;
+        fa.scal2 = c->scal2;
+        fa.fpart = c->fpart;
+        force_local_ewald_kernel<<<dim3(kForceChunks, c->nion), 256, 0, s>>>(fa); c->nlaunch += 1;
+        if (c->nion > 1) {
+            force_ewald_pairs_kernel<<<c->nion, 256, 0, s>>>(c->nion, c->nsh, c->r1, c->rcell, c->zv, c->katm,
+                                                             c->prm.rcut, c->ewp);
+            c->nlaunch += 1;
+        }
+    }
     mark(c, 5);
     // V_loc + V_H to real space, plus xc per spin (cpsd.c:380-388)
     c->fft->inv_z(c->g, c->Vg, c->ldc, c->Taux, 1, s); c->nlaunch += 1;
@@ -620,9 +655,22 @@ int one_step(cpsd_gpu_ctx *c)
                          1.0, 0.0, c->beta, c->nb, TN_PROJECTOR);
         if (rc) return rc;
         kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, s>>>(
-            c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT); c->nlaunch += 1;
+            c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT, c->move ? c->coefP : nullptr);
+        c->nlaunch += 1;
         gemm_nn(c, c->nb, K, c->nproj, 1.0, c->coefT, c->nproj, (const double *)c->proj, ldr, 1.0,
                 (double *)c2, ldr, TN_PROJECTOR);
+        if (c->move) {  // nonlocal force: Y_P = sum_b sw1(P, b) c1_b, then sum_G G Im(conj(chi_P) Y_P)
+            gemm_nn(c, c->nproj, K, c->nb, 1.0, c->coefP, c->nb, (const double *)c1, ldr, 0.0, (double *)c->Ynl,
+                    ldr);
+            force_nonlocal_kernel<<<c->nproj, 256, 0, s>>>(c->npw, c->ldc, c->w, c->Gv, c->proj, c->Ynl, c->fnl);
+            c->nlaunch += 1;
+        }
+    }
+    if (c->move && c->nion > 0) {  // total force and the ion step r2 = r1 + dti fion
+        force_total_kernel<<<(unsigned)cdiv(c->nion, 128), 128, 0, s>>>(
+            c->nion, 2.0 * (c->ispin == 1 ? 2.0 : 1.0), c->proj_off, c->lmmax, c->katm, c->fpart, c->fnl, c->ewp,
+            c->dti, c->r1, c->fion, c->r2);
+        c->nlaunch += 1;
     }
     mark(c, 7);
     // (V + xc) psi back to G, -H psi and the SD step, cpsd.c:384-400
@@ -676,8 +724,7 @@ int one_step(cpsd_gpu_ctx *c)
         const int m = ms ? c->ne1 : c->ne0;
         const long off = (long)(ms ? c->ne0 : 0) * ldr;
         const double *C1 = (const double *)c1 + off, *C2 = (const double *)c2 + off;
-        // the three overlaps of this spin in one launch
-        const double *As[3] = {C2, C2, C1}, *Bs[3] = {C2, C1, C1};
+        // the three overlaps of this spin: C2'WC2, C2'WC1, C1'WC1
         double *Cs[3] = {(double *)Mblk(c, ms, 0), (double *)Mblk(c, ms, 1), (double *)Mblk(c, ms, 2)};
         int rc = overlaps3(c, m, K, ldr, C2, C1, Cs);
         if (rc) return rc;
@@ -990,6 +1037,11 @@ int cpsd_gpu_batch_run(cpsd_gpu_batch *b, int inner, double *E, double *deltae, 
     const int n = (int)b->cells.size();
     for (int i = 0; i < n; ++i) {
         cpsd_gpu_ctx *c = b->cells[i];
+        if (c->move) {  // batched cells take fixed-ion steps
+            drop_graphs(c);
+            batch_drop_graphs(b);
+            c->move = 0;
+        }
         CK(cudaMemsetAsync(c->flags, 0, 3 * sizeof(int), b->st));
         CK(cudaMemcpyAsync(c->Edev, E + 10 * i, sizeof(double), cudaMemcpyHostToDevice, b->st));
     }
@@ -1226,6 +1278,11 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->dstep, 1));
     CK(ar.alloc(&c->pcap, 2));
     CK(ar.alloc(&c->epart, std::max(nion, 1)));  // zero: the last ion has no pair of its own
+    CK(ar.alloc(&c->Gv, (size_t)3 * c->npw));
+    CK(ar.alloc(&c->dti, std::max(nion, 1)));
+    CK(ar.alloc(&c->fpart, (size_t)kForceChunks * std::max(nion, 1) * 3));
+    CK(ar.alloc(&c->fnl, (size_t)27 * std::max(nion, 1)));  // at most 9 projectors per ion
+    CK(ar.alloc(&c->ewp, (size_t)3 * std::max<long>(1, (long)nion * (nion - 1) / 2)));
     CK(ar.alloc(&c->pR, (size_t)nb * P));
     CK(ar.alloc(&c->pM, (size_t)c->ispin * c->ne0 * c->ne0));
     CK(ar.alloc(&c->pstats, (size_t)3 * nb));
@@ -1315,8 +1372,6 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
                         const double *vg, const int *lmmax, const double *vnlnrm, const double *vl,
                         const double *vnl)
 {
-    (void)amass;
-    (void)G;
     if (!c || !zv || !tg || !vc || !vg || !lmmax || !vnlnrm || !vl || !vnl) return CPSD_ERR_ARG;
     if (c->nion > 0 && (!katm || !rcell)) return CPSD_ERR_ARG;
     CK(cudaSetDevice(c->prm.device));
@@ -1380,6 +1435,18 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
     }
     if (c->nsh > 0) CK(cudaMemcpy(c->rcell, rcell, sizeof(double) * 3 * c->nsh, cudaMemcpyHostToDevice));
     if (np > 0) CK(cudaMemcpy(c->vnlnrm_p, pn.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
+    // ion motion needs the G vectors (packed like tg) and the masses
+    c->motion_ok = false;
+    if (G && amass && c->nion > 0) {
+        std::vector<double> pg((size_t)3 * c->npw);
+        for (int d = 0; d < 3; ++d)
+            for (int p = 0; p < c->npw; ++p) pg[(size_t)d * c->npw + p] = G[(size_t)d * c->nfft3d + h.pt_idx[p]];
+        CK(cudaMemcpy(c->Gv, pg.data(), sizeof(double) * pg.size(), cudaMemcpyHostToDevice));
+        c->amass_h.assign(amass, amass + nkatm);
+        for (double m : c->amass_h)
+            if (!(m > 0)) return CPSD_ERR_ARG;
+        c->motion_ok = true;
+    }
     CK(cudaDeviceSynchronize());
     c->h2d += (long long)sizeof(double) * (3 * c->npw_pad + (long)pvl.size() + (long)pvnl.size() + nkatm + 9 + np +
                                           3 * c->nsh) + (long long)sizeof(int) * (nkatm + 2 * c->nion);
@@ -1413,9 +1480,24 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
                  double *deltar)
 {
     if (!c || !E || inner < 1) return CPSD_ERR_ARG;
-    if (move) return CPSD_ERR_MOVE;
     if (!c->tables_ok || !c->state_ok) return CPSD_ERR_ARG;
+    if (move && !c->motion_ok) return CPSD_ERR_MOVE;  // no G vectors or masses were given
     CK(cudaSetDevice(c->prm.device));
+    if ((move != 0) != (c->move != 0)) {
+        drop_graphs(c);
+        c->move = move ? 1 : 0;
+    }
+    if (c->move) {
+        if (c->nproj > 0 && !c->Ynl) {
+            CK(c->ar.alloc(&c->Ynl, (size_t)c->nproj * c->npw_pad));
+            CK(c->ar.alloc(&c->coefP, (size_t)c->nproj * c->nb));
+        }
+        std::vector<double> dti(c->nion);  // cpsd.c:116-122
+        std::vector<int> katm(c->nion);
+        CK(cudaMemcpy(katm.data(), c->katm, sizeof(int) * c->nion, cudaMemcpyDeviceToHost));
+        for (int ii = 0; ii < c->nion; ++ii) dti[ii] = c->prm.dt / sqrt(c->amass_h[katm[ii]]);
+        CK(cudaMemcpy(c->dti, dti.data(), sizeof(double) * c->nion, cudaMemcpyHostToDevice));
+    }
     cudaStream_t s = c->st;
     CK(cudaMemsetAsync(c->flags, 0, 3 * sizeof(int), s));
     CK(cudaMemcpyAsync(c->Edev, E, sizeof(double), cudaMemcpyHostToDevice, s));
@@ -1435,7 +1517,17 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
     for (int i = 0; i < 10; ++i) E[i] = Eh[i];
     if (deltae) *deltae = Eh[10];
     if (deltac) *deltac = Eh[11];
-    if (deltar) *deltar = 0.0;
+    double dr = 0.0;  // the largest force of the last step, cpsd.c:662-672
+    if (c->move && c->nion > 0) {
+        std::vector<double> f((size_t)3 * c->nion);
+        CK(cudaMemcpy(f.data(), c->fion, sizeof(double) * f.size(), cudaMemcpyDeviceToHost));
+        c->d2h += (long long)sizeof(double) * f.size();
+        for (int ii = 0; ii < c->nion; ++ii) {
+            const double a = sqrt(f[3 * ii] * f[3 * ii] + f[3 * ii + 1] * f[3 * ii + 1] + f[3 * ii + 2] * f[3 * ii + 2]);
+            if (a > dr) dr = a;
+        }
+    }
+    if (deltar) *deltar = dr;
     const int fails = fl[0];
     c->lag_fail_total += fails;
     c->steps_run += inner;
@@ -1483,8 +1575,13 @@ int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, do
     if (c->nion > 0) {
         if (r1) CK(cudaMemcpyAsync(r1, c->r1, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
         if (r2) CK(cudaMemcpyAsync(r2, c->r2, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
+        // the forces exist only after a move = 1 run (cpsd.c:246-364); as in
+        // the reference, fion is left untouched otherwise
+        if (fion && c->move) {
+            CK(cudaMemcpyAsync(fion, c->fion, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
+            c->d2h += (long long)sizeof(double) * 3 * c->nion;
+        }
     }
-    (void)fion;  // written only with move=1 (ccpsdv3/cpsd.c:246-364)
     CK(cudaStreamSynchronize(s));
     return CPSD_OK;
 }

@@ -120,6 +120,142 @@ __global__ void vloc_proj_kernel(VlocArgs a)
     a.Vg[p] = cx<double>{vall.x * a.scal2 + d.x * vc, vall.y * a.scal2 + d.y * vc};
 }
 
+// ------------------------------------------------------------ ion forces
+// move = 1 (cpsd.c:246-257, 291-304, 310-364).  All Gamma-point sums use the
+// weight w (1 on kx = 0, 2 elsewhere: gsdot of ccpsdv3/gsdot.c) over the
+// sphere; G_d is the d-th Cartesian component of G per sphere point.
+constexpr int kForceChunks = 16;  // point chunks of the local + k-space Ewald sums
+
+struct ForceArgs {
+    int npw, n, nh, nion;
+    const int *pt_i, *pt_j, *pt_k, *katm;
+    const cx<double> *ex1, *ex2, *ex3;  // phase tables of r1
+    const double *w, *G;                // G: [3][npw]
+    const double *vl, *vg, *zv;
+    const cx<double> *dng, *s;
+    double scal2;
+    double *fpart;  // [chunk][ion][3]
+};
+
+// Local force (cpsd.c:246-257: sum_G G_d (Im dng Re exi - Re dng Im exi) vl)
+// and k-space Ewald force (cpsd.c:318-328: sum_G G_d (exi x s) vg zv scal2)
+// of ion blockIdx.y over point chunk blockIdx.x, fixed-order block sums.
+__global__ void __launch_bounds__(256) force_local_ewald_kernel(ForceArgs a)
+{
+    __shared__ double sh[32];
+    const int ii = blockIdx.y, ch = blockIdx.x;
+    const int per = (a.npw + kForceChunks - 1) / kForceChunks;
+    const int p0 = ch * per, p1 = min(a.npw, p0 + per);
+    const int ia = a.katm[ii];
+    const double zs = a.zv[ia] * a.scal2;
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int p = p0 + threadIdx.x; p < p1; p += 256) {
+        const cx<double> e = strfac_point(a.ex1[(long)ii * a.nh + a.pt_i[p]], a.ex2[(long)ii * a.n + a.pt_j[p]],
+                                          a.ex3[(long)ii * a.n + a.pt_k[p]]);
+        const cx<double> d = a.dng[p], sp = a.s[p];
+        const double vl = a.vl[(long)ia * a.npw + p];
+        const double loc = vl * (d.y * e.x - d.x * e.y);
+        const double ewk = (e.x * sp.y - e.y * sp.x) * a.vg[p] * zs;
+        const double t = a.w[p] * (loc + ewk);
+        for (int k = 0; k < 3; ++k) f[k] += t * a.G[(long)k * a.npw + p];
+    }
+    for (int k = 0; k < 3; ++k) {
+        const double v = block_sum<256>(f[k], sh);
+        if (threadIdx.x == 0) a.fpart[((long)ch * a.nion + ii) * 3 + k] = v;
+    }
+}
+
+// Nonlocal force per projector P (cpsd.c:291-304): with Y_P = sum_b sw1(P, b)
+// c1_b, fnl[P][d] = sum_G w G_d Im(conj(chi_P) Y_P).
+__global__ void __launch_bounds__(256) force_nonlocal_kernel(int npw, long ld, const double *__restrict__ w,
+                                                             const double *__restrict__ G,
+                                                             const cx<double> *__restrict__ proj,
+                                                             const cx<double> *__restrict__ Y,
+                                                             double *__restrict__ fnl)
+{
+    __shared__ double sh[32];
+    const int P = blockIdx.x;
+    const cx<double> *chi = proj + (long)P * ld, *y = Y + (long)P * ld;
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int p = threadIdx.x; p < npw; p += 256) {
+        const cx<double> c = chi[p], v = y[p];
+        const double t = w[p] * (c.x * v.y - c.y * v.x);
+        for (int k = 0; k < 3; ++k) f[k] += t * G[(long)k * npw + p];
+    }
+    for (int k = 0; k < 3; ++k) {
+        const double v = block_sum<256>(f[k], sh);
+        if (threadIdx.x == 0) fnl[3 * P + k] = v;
+    }
+}
+
+// Real-space Ewald force of each pair ii < jj (cpsd.c:331-362), summed over
+// the image cells: ewp[pair][3], pair = ii (2 nion - ii - 1) / 2 + jj - ii - 1.
+__global__ void __launch_bounds__(256) force_ewald_pairs_kernel(int nion, int nsh, const double *__restrict__ r1,
+                                                                const double *__restrict__ rcell,
+                                                                const double *__restrict__ zv,
+                                                                const int *__restrict__ katm, double rcut,
+                                                                double *__restrict__ ewp)
+{
+    const double B1 = 0.0705230784, B2 = 0.0422820123, B3 = 0.0092705272;
+    const double B4 = 0.0001520143, B5 = 0.0002765672, B6 = 0.0000430638;
+    const double CERFC = 1.128379167;  // 2 / sqrt(pi), as cpsd.c rounds it
+    const int ii = blockIdx.x;
+    const long off = (long)ii * (2L * nion - ii - 1) / 2;
+    for (int jj = ii + 1 + threadIdx.x; jj < nion; jj += 256) {
+        const double dx = r1[3 * ii] - r1[3 * jj];
+        const double dy = r1[3 * ii + 1] - r1[3 * jj + 1];
+        const double dz = r1[3 * ii + 2] - r1[3 * jj + 2];
+        const double zz = zv[katm[ii]] * zv[katm[jj]];
+        double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (int l = 0; l < nsh; ++l) {
+            const double x = rcell[l] + dx, y = rcell[l + nsh] + dy, z = rcell[l + 2 * nsh] + dz;
+            const double r = sqrt(x * x + y * y + z * z);
+            const double wr = r / rcut;
+            double aa = (1.0 + wr * (B1 + wr * (B2 + wr * (B3 + wr * (B4 + wr * (B5 + wr * B6))))));
+            aa *= aa * aa * aa;
+            const double erfc = 1.0 / (aa * aa * aa * aa);
+            const double ad = zz * (erfc + CERFC * wr * exp(-wr * wr)) / (r * r * r);
+            s1 += x * ad;
+            s2 += y * ad;
+            s3 += z * ad;
+        }
+        const long pr = off + (jj - ii - 1);
+        ewp[3 * pr] = s1;
+        ewp[3 * pr + 1] = s2;
+        ewp[3 * pr + 2] = s3;
+    }
+}
+
+// fion = local + k-space Ewald - nonlocal + real-space Ewald, and the ion SD
+// step r2 = r1 + dti fion (cpsd.c:401-411); one thread per ion, fixed order.
+__global__ void force_total_kernel(int nion, double nl_factor, const int *__restrict__ proj_off,
+                                   const int *__restrict__ lmmax, const int *__restrict__ katm,
+                                   const double *__restrict__ fpart, const double *__restrict__ fnl,
+                                   const double *__restrict__ ewp, const double *__restrict__ dti,
+                                   const double *__restrict__ r1, double *__restrict__ fion,
+                                   double *__restrict__ r2)
+{
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= nion) return;
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int ch = 0; ch < kForceChunks; ++ch)
+        for (int k = 0; k < 3; ++k) f[k] += fpart[((long)ch * nion + ii) * 3 + k];
+    const int nl = lmmax[katm[ii]];
+    for (int l = 0; l < nl; ++l)
+        for (int k = 0; k < 3; ++k) f[k] -= nl_factor * fnl[3 * (proj_off[ii] + l) + k];
+    for (int a = 0; a < ii; ++a) {  // pairs (a, ii) enter with a minus sign (cpsd.c:359-361)
+        const long pr = (long)a * (2L * nion - a - 1) / 2 + (ii - a - 1);
+        for (int k = 0; k < 3; ++k) f[k] -= ewp[3 * pr + k];
+    }
+    const long off = (long)ii * (2L * nion - ii - 1) / 2;
+    for (int b = ii + 1; b < nion; ++b)  // pairs (ii, b): plus (cpsd.c:356-358)
+        for (int k = 0; k < 3; ++k) f[k] += ewp[3 * (off + b - ii - 1) + k];
+    for (int k = 0; k < 3; ++k) {
+        fion[3 * ii + k] = f[k];
+        r2[3 * ii + k] = r1[3 * ii + k] + dti[ii] * f[k];
+    }
+}
+
 // kinetic part of -H psi: c2 = -tg c1, ccpsdv3/cpsd.c:212-221
 __global__ void kinetic_kernel(int nb, int npw_pad, long ldc, const double *__restrict__ tg,
                                const cx<double> *__restrict__ c1, cx<double> *__restrict__ c2)
@@ -134,14 +270,17 @@ __global__ void kinetic_kernel(int nb, int npw_pad, long ldc, const double *__re
 
 // coefficients of the KB back-projection, ccpsdv3/cpsd.c:289:
 // coefT[b][P] = -beta[P][b] * scal2 / vnlnrm[P]
+// (and, for the nonlocal force, the same in [P][b] order when coefP is given)
 __global__ void kb_coef_kernel(int nproj, int nb, const double *__restrict__ beta,
                                const double *__restrict__ vnlnrm_p, double scal2,
-                               double *__restrict__ coefT)
+                               double *__restrict__ coefT, double *__restrict__ coefP)
 {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= nproj * nb) return;
     const int P = id / nb, b = id % nb;
-    coefT[(long)b * nproj + P] = -beta[id] * scal2 / vnlnrm_p[P];
+    const double v = -beta[id] * scal2 / vnlnrm_p[P];
+    coefT[(long)b * nproj + P] = v;
+    if (coefP) coefP[id] = v;
 }
 
 // ------------------------------------------------------------ density + xc

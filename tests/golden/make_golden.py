@@ -47,6 +47,19 @@ CASES = [
 ]
 
 
+def _moving(spec):
+    spec.move = 1
+    return spec
+
+
+# move = 1 (ion forces and the ion SD step): positions and forces per call
+MOVE_CASES = [
+    ("move_small_h2_16", lambda: _moving(configs.small_h2(16)), 3, 2, 1),
+    ("move_small_diamond_24", lambda: _moving(configs.small_diamond(24, 4)), 3, 2, 4),
+    ("move_small_diamond_32", lambda: _moving(configs.small_diamond(32, 40, ecut=25.0, seed=12)), 2, 2, 4),
+]
+
+
 def input_digest(inp) -> str:
     h = hashlib.sha256()
     for a in (inp.c2, inp.vl, inp.vnl, inp.vnlnrm, inp.tg, inp.vc, inp.vg, inp.masker1, inp.r2,
@@ -65,17 +78,22 @@ def run_case(ref, name, mk, ncalls, inner, keep):
     spec = mk()
     inp = inputs.build_inputs(spec)
     st = oracle.State(inp)
-    E, de, dc = [], [], []
+    E, de, dc, dr, r2, fion = [], [], [], [], [], []
     for _ in range(ncalls):
         ref.run(inp, inner, st)
         E.append(st.E.copy())
         de.append(st.deltae)
         dc.append(st.deltac)
+        dr.append(st.deltar)
+        r2.append(st.r2.copy())
+        fion.append(st.fion.copy())
     dn = st.dn.reshape(inp.ispin, inp.nfft, inp.nfft, inp.nfft + 2)[..., :inp.nfft]
     out = dict(E=np.array(E), deltae=np.array(de), deltac=np.array(dc), hml=st.hml, lmd=st.lmd,
                c2=packed(inp, st.c2, keep), cpsi=packed(inp, st.cpsi, keep),
                dn_sum=dn.sum(axis=(1, 2, 3)), dn_sq=(dn * dn).sum(axis=(1, 2, 3)),
                dn_plane0=np.ascontiguousarray(dn[:, 0]), inner=np.array(inner))
+    if spec.move:
+        out.update(deltar=np.array(dr), r2=np.array(r2), fion=np.array(fion), r1=st.r1.copy())
     np.savez_compressed(os.path.join(HERE, "ref_%s.npz" % name), **out)
     print("%-18s calls=%d inner=%d  E=%.12f" % (name, ncalls, inner, st.E[0]))
     return input_digest(inp)
@@ -106,7 +124,7 @@ def run_main(name, mk, inner, outer):
 def main():
     ref = oracle.ReferenceBuild()
     digests = {}
-    for name, mk, ncalls, inner, keep in CASES:
+    for name, mk, ncalls, inner, keep in CASES + MOVE_CASES:
         digests[name] = run_case(ref, name, mk, ncalls, inner, keep)
     digests["main_small_diamond_24"] = run_main("small_diamond_24", lambda: configs.small_diamond(24, 4), 2, 3)
     with open(os.path.join(HERE, "inputs.json"), "w") as f:

@@ -6,6 +6,8 @@ energy of every cpsd() call; matrices and orbitals to ~1e-10.
 """
 import os
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -80,6 +82,56 @@ def test_dropin_cpsd_matches_reference(golden, name):
     check_against_golden(inp, golden(name), rows, st)
     # cpsi leaves as c2 - c1, full box (cpsd.c:650-651)
     assert np.array_equal(st.cpsi, st.c2 - st.c1) or np.abs(st.cpsi - (st.c2 - st.c1)).max() < 1e-15
+
+
+def _moving(spec):
+    spec.move = 1
+    return spec
+
+
+# move = 1: ion forces and the ion SD step (tests/golden/make_golden.py MOVE_CASES)
+MOVE_CASES = {
+    "move_small_h2_16": (lambda: _moving(configs.small_h2(16)), 3, 2),
+    "move_small_diamond_24": (lambda: _moving(configs.small_diamond(24, 4)), 3, 2),
+    "move_small_diamond_32": (lambda: _moving(configs.small_diamond(32, 40, ecut=25.0, seed=12)), 2, 2),
+}
+F_TOL = 1e-9  # Ha/bohr
+
+
+@pytest.mark.parametrize("name", list(MOVE_CASES))
+def test_ion_motion_matches_reference(golden, name):
+    """move = 1 on the resident cell: energies, forces (local, nonlocal,
+    k-space and real-space Ewald), positions and deltar of every call against
+    the reference build."""
+    mk, ncalls, inner = MOVE_CASES[name]
+    g = golden(name)
+    inp = inputs.build_inputs(mk())
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    st = api.State(inp)
+    for k in range(ncalls):
+        cell.run(inner, move=1)
+        cell.get_state(st)
+        assert abs(cell.E[0] - g["E"][k, 0]) < E_TOL
+        assert np.abs(st.fion - g["fion"][k]).max() < F_TOL
+        assert np.abs(st.r2 - g["r2"][k]).max() < 1e-12
+        assert abs(cell.deltar - g["deltar"][k]) < F_TOL
+    assert np.abs(st.lmd - g["lmd"]).max() < 1e-9
+    cell.close()
+
+
+def test_dropin_cpsd_with_ion_motion_matches_reference(golden):
+    """The reference-facing cpsd() with move = 1, called like main.c does."""
+    mk, ncalls, inner = MOVE_CASES["move_small_diamond_24"]
+    g = golden("move_small_diamond_24")
+    inp = inputs.build_inputs(mk())
+    st = api.State(inp)
+    for k in range(ncalls):
+        api.cpsd(inp, st, inner, move=1)
+        assert abs(st.E[0] - g["E"][k, 0]) < E_TOL
+        assert np.abs(st.fion - g["fion"][k]).max() < F_TOL
+        assert np.abs(st.r2 - g["r2"][k]).max() < 1e-12
+        assert abs(st.deltar - g["deltar"][k]) < F_TOL
 
 
 def test_lagrange_warning_matches_reference_quirk():
@@ -212,10 +264,18 @@ def test_full_size_cell_properties():
 def test_error_paths():
     """Bad inputs come back as status codes, never as a device fault."""
     inp = inputs.build_inputs(configs.small_h2(16))
-    st = api.State(inp)
+    # move = 1 without the G vectors and masses it needs
+    L = lib.load()
+    cell = api.GpuCell(inp)
+    nul = ctypes.c_void_p()
+    assert L.cpsd_gpu_set_tables(cell.h, api._ptr(inp.katm), nul, api._ptr(inp.zv), api._ptr(inp.rcell), nul,
+                                 api._ptr(inp.tg), api._ptr(inp.vc), api._ptr(inp.vg), api._ptr(inp.lmmax),
+                                 api._ptr(inp.vnlnrm), api._ptr(inp.vl), api._ptr(inp.vnl)) == 0
+    cell.set_state(inp.c2, inp.r2)
     with pytest.raises(lib.CpsdError) as e:
-        api.cpsd(inp, st, 1, move=1)
+        cell.run(1, move=1)
     assert e.value.status == lib.CPSD_ERR_MOVE
+    cell.close()
     bad = inputs.build_inputs(configs.small_h2(16))
     bad.c2 = bad.c2.copy()
     out_of_mask = np.flatnonzero(bad.masker1 == 0)[5]

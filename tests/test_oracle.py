@@ -22,7 +22,21 @@ CASES = {
     "h2_dimer_32": (lambda: configs.h2_dimer_32(), 200, 1),
     "diamond8_64": (lambda: configs.diamond8_64(), 4, 2),
 }
+
+
+def _moving(spec):
+    spec.move = 1
+    return spec
+
+
+# move = 1: ion forces and the ion SD step (make_golden.MOVE_CASES)
+MOVE_CASES = {
+    "move_small_h2_16": (lambda: _moving(configs.small_h2(16)), 3, 2),
+    "move_small_diamond_24": (lambda: _moving(configs.small_diamond(24, 4)), 3, 2),
+    "move_small_diamond_32": (lambda: _moving(configs.small_diamond(32, 40, ecut=25.0, seed=12)), 2, 2),
+}
 E_TOL = 1e-9  # Ha, total energy parity bar
+F_TOL = 1e-9  # Ha/bohr, force parity bar
 
 
 @pytest.mark.parametrize("n", [8, 12, 16, 24, 32, 48, 64])
@@ -99,7 +113,7 @@ def test_inputs_match_fixture_digests():
     from make_golden import input_digest  # noqa: E402
     with open(os.path.join(GOLDEN, "inputs.json")) as f:
         want = json.load(f)
-    for name, (mk, _, _) in CASES.items():
+    for name, (mk, _, _) in list(CASES.items()) + list(MOVE_CASES.items()):
         assert input_digest(inputs.build_inputs(mk())) == want[name], name
 
 
@@ -147,6 +161,23 @@ def test_restatement_matches_reference_build(restatement, golden, name):
     keep = g["c2"].shape[0]
     assert np.abs(packed(inp, st.c2, keep) - g["c2"]).max() < 1e-10
     assert np.abs(packed(inp, st.cpsi, keep) - g["cpsi"]).max() < 1e-10
+
+
+@pytest.mark.parametrize("name", list(MOVE_CASES))
+def test_restatement_matches_reference_build_with_ion_motion(restatement, golden, name):
+    """move = 1: energies, forces, positions and deltar of every call against
+    the reference's own cpsd() (golden vectors)."""
+    mk, ncalls, inner = MOVE_CASES[name]
+    g = golden(name)
+    inp = inputs.build_inputs(mk())
+    st = oracle.State(inp)
+    for k in range(ncalls):
+        restatement.run(inp, inner, st)
+        assert abs(st.E[0] - g["E"][k, 0]) < E_TOL
+        assert np.abs(st.fion - g["fion"][k]).max() < F_TOL
+        assert np.abs(st.r2 - g["r2"][k]).max() < 1e-12
+        assert abs(st.deltar - g["deltar"][k]) < F_TOL
+    assert np.abs(st.lmd - g["lmd"]).max() < 1e-9
 
 
 def test_restatement_matches_reference_main(restatement):
