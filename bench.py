@@ -160,20 +160,21 @@ def cpu_reference(inp, budget_s, min_calls=3, inner=1):
 
 # ----------------------------------------------------------------- GPU arm
 def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True, precision=0, gemm=0):
+    """Device time of `steps` cpsd() calls of `inner` SD steps on a resident
+    cell.  The timed calls run the production schedule (no phase events: the
+    step's second stream overlaps the density chain); the per-phase times
+    come from two extra calls with phase events, which serialise the step."""
     from cpsd_b200 import api
     cell = api.GpuCell(inp, precision=precision)
     if gemm:
         cell.set_gemm(gemm)
     cell.set_state(inp.c2, inp.r2)
-    if want_phases:
-        cell.phase_timing(True)
     stream = torch.cuda.ExternalStream(cell.stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(warmup):
         cell.run(inner)
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(steps)]
-    phases = {}
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -184,18 +185,23 @@ def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True, precisio
         events[k][0].record(stream)
         cell.run(inner)
         events[k][1].record(stream)
-        if want_phases:
-            for name, ms in cell.phase_times().items():
-                phases.setdefault(name, []).append(ms)
     torch.cuda.synchronize()
     launches = cell.counters()[0] - l0
     if dist is not None:
         dist.barrier()
     total_ms = sum(a.elapsed_time(b) for a, b in events)
+    ph = {}
+    if want_phases:
+        cell.phase_timing(True)
+        phases = {}
+        for _ in range(2):
+            cell.run(inner)
+            for name, ms in cell.phase_times().items():
+                phases.setdefault(name, []).append(ms)
+        ph = {k: sum(v) / len(v) for k, v in phases.items()}
     geo = cell.geometry()
     E = cell.E.copy()
     cell.close()
-    ph = {k: sum(v) / len(v) for k, v in phases.items()}
     return total_ms, launches, ph, geo, E
 
 

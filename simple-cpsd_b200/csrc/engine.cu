@@ -356,6 +356,11 @@ struct cpsd_gpu_ctx {
     bool use_graph = true;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // one captured SD step per ping-pong parity
     int graph_launches = 0;
+    // second stream of a step: structure factors, projectors and the kinetic +
+    // nonlocal part of -H psi run beside the density -> potential chain
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_sf = nullptr, ev_side = nullptr;
+    cudaStream_t cs = nullptr;  // the stream the GEMM helpers launch on
     bool lag_tile = false;  // 4 x 4 tiled solver (<= 128 bands, 16-CTA clusters schedulable)
     int lag_cluster = 8;  // CTAs per cluster of the Lagrange solver (16 where schedulable)
     int lag_lb = 0;       // its row-tile width
@@ -472,7 +477,7 @@ int gemm_tn_batch(cpsd_gpu_ctx *c, int M, int N, int K, int nprod, const double 
     if (nprod > kTnMaxProd) return CPSD_ERR_ARG;
     const bool tc = (c->gemm_mode & which) != 0 && c->precision == CPSD_PREC_MIXED;
     c->nlaunch += launch_tn(M, N, K, nprod, A, lda, B, ldb, w, alpha, beta, C, ldc, tc, c->gws, c->gemm_ws_elems,
-                            c->flags + 2, c->st);
+                            c->flags + 2, c->cs);
     return CPSD_OK;
 }
 
@@ -498,7 +503,7 @@ int overlaps3(cpsd_gpu_ctx *c, int m, int K, long ld, const double *C2, const do
     while ((size_t)splits * 3 * mm > c->gemm_ws_elems && splits > 1) --splits;
     const int kchunk = (int)(cdiv(cdiv(K, splits), kOvBK) * kOvBK);
     splits = cdiv(K, kchunk);
-    tc_overlaps3_kernel<<<(unsigned)splits, kTcThreads, kOvSmem, c->st>>>(m, K, ld, C2, C1, c->w, kchunk,
+    tc_overlaps3_kernel<<<(unsigned)splits, kTcThreads, kOvSmem, c->cs>>>(m, K, ld, C2, C1, c->w, kchunk,
                                                                          (int)splits, c->gws, c->flags + 2);
     TnBatch bt{};
     for (int q = 0; q < 3; ++q) {
@@ -508,7 +513,7 @@ int overlaps3(cpsd_gpu_ctx *c, int m, int K, long ld, const double *C2, const do
     }
     bt.nprod = 3;
     bt.splits = (int)splits;
-    splitk_reduce_kernel<<<(unsigned)cdiv(mm * 3 * 32, 256), 256, 0, c->st>>>(m, m, m, c->gws, 1.0, 0.0, bt);
+    splitk_reduce_kernel<<<(unsigned)cdiv(mm * 3 * 32, 256), 256, 0, c->cs>>>(m, m, m, c->gws, 1.0, 0.0, bt);
     c->nlaunch += 2;
     return CPSD_OK;
 }
@@ -522,11 +527,11 @@ void gemm_nn(cpsd_gpu_ctx *c, int NJ, int K, int L, double alpha, const double *
     if (NJ <= 0 || L <= 0) return;
     if ((c->gemm_mode & which) != 0 && c->precision == CPSD_PREC_MIXED) {
         dim3 grid((unsigned)cdiv(K, kTcN), (unsigned)cdiv(NJ, kTcM));
-        tc_gemm_nn_kernel<<<grid, kTcThreads, kTcSmem, c->st>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo,
+        tc_gemm_nn_kernel<<<grid, kTcThreads, kTcSmem, c->cs>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo,
                                                                 c->flags + 2);
     } else {
         dim3 grid((unsigned)cdiv(K, GB), (unsigned)cdiv(NJ, GB));
-        gemm_nn_kernel<<<grid, 256, 0, c->st>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo);
+        gemm_nn_kernel<<<grid, 256, 0, c->cs>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo);
     }
     c->nlaunch += 1;
 }
@@ -556,6 +561,80 @@ int one_step(cpsd_gpu_ctx *c)
     const int K = 2 * c->npw_pad;
     const long ldr = 2L * c->npw_pad;
     CK(cudaMemcpyAsync(c->r1, c->r2, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToDevice, s));  // cpsd.c:174
+    // The structure factors, projectors and the kinetic + nonlocal part of
+    // -H psi need only c1 and the ions: they run on a second stream beside
+    // the density -> potential -> V psi chain, joined before the SD update.
+    // With phase timing on, everything stays on one stream so the phases add up.
+    const bool fork = !c->phase_timing;
+    cudaStream_t side = fork ? c->st2 : s;
+    // phase factors, local psp and projectors: cpsd.c:208, 224-286
+    auto issue_sf = [&]() {
+        if (c->nion > 0) {
+            phase_tables_kernel<<<(unsigned)cdiv(3 * c->nion, 128), 128, 0, side>>>(c->nion, c->n, c->unitg, c->r1,
+                                                                                 c->ex1, c->ex2, c->ex3);
+            c->nlaunch += 1;
+        }
+        VlocArgs va{};
+        va.npw = c->npw;
+        va.npw_pad = c->npw_pad;
+        va.n = c->n;
+        va.nh = c->nh;
+        va.nion = c->nion;
+        va.pt_i = c->pt_i;
+        va.pt_j = c->pt_j;
+        va.pt_k = c->pt_k;
+        va.katm = c->katm;
+        va.zv = c->zv;
+        va.ex1 = c->ex1;
+        va.ex2 = c->ex2;
+        va.ex3 = c->ex3;
+        va.vl = c->vl;
+        va.vnl = c->vnl;
+        va.lmmax = c->lmmax;
+        va.proj_off = c->proj_off;
+        va.s = c->sfac;
+        va.vall = c->vall;
+        va.proj = c->proj;
+        vloc_proj_kernel<<<(unsigned)cdiv(c->npw_pad, 128), 128, 0, side>>>(va); c->nlaunch += 1;
+    };
+    // kinetic + nonlocal part of -H psi into c2, cpsd.c:212-221, 287-290
+    auto issue_knl = [&]() -> int {
+        c->cs = side;
+        kinetic_kernel<<<(unsigned)cdiv((long)c->nb * c->npw_pad, 256), 256, 0, side>>>(c->nb, c->npw_pad, c->ldc,
+                                                                                       c->tg, c1, c2);
+        c->nlaunch += 1;
+        if (c->nproj > 0) {
+            int rc = gemm_tn(c, c->nproj, c->nb, K, (const double *)c->proj, ldr, (const double *)c1, ldr, c->w,
+                             1.0, 0.0, c->beta, c->nb, TN_PROJECTOR);
+            if (rc) {
+                c->cs = s;
+                return rc;
+            }
+            kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, side>>>(
+                c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT, c->move ? c->coefP : nullptr);
+            c->nlaunch += 1;
+            gemm_nn(c, c->nb, K, c->nproj, 1.0, c->coefT, c->nproj, (const double *)c->proj, ldr, 1.0,
+                    (double *)c2, ldr, TN_PROJECTOR);
+            if (c->move) {  // nonlocal force: Y_P = sum_b sw1(P, b) c1_b, then sum_G G Im(conj(chi_P) Y_P)
+                gemm_nn(c, c->nproj, K, c->nb, 1.0, c->coefP, c->nb, (const double *)c1, ldr, 0.0,
+                        (double *)c->Ynl, ldr);
+                force_nonlocal_kernel<<<c->nproj, 256, 0, side>>>(c->npw, c->ldc, c->w, c->Gv, c->proj, c->Ynl,
+                                                                 c->fnl);
+                c->nlaunch += 1;
+            }
+        }
+        c->cs = s;
+        return CPSD_OK;
+    };
+    if (fork) {
+        CK(cudaEventRecord(c->ev_fork, s));
+        CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+        issue_sf();
+        CK(cudaEventRecord(c->ev_sf, c->st2));
+        int rc = issue_knl();
+        if (rc) return rc;
+        CK(cudaEventRecord(c->ev_side, c->st2));
+    }
 
     mark(c, 0);
     // psi(G) -> psi(r) and the density, cpsd.c:177-194
@@ -576,39 +655,13 @@ int one_step(cpsd_gpu_ctx *c)
     c->fft->plane(PM_FWDREAL, c->g, c->Taux, pf, 1, s); c->nlaunch += 1;
     c->fft->fwd_z_store(c->g, c->Taux, c->dng, c->ldc, 1.0, 1, s); c->nlaunch += 1;
     mark(c, 4);
-    // phase factors, local psp, projectors, V(G): cpsd.c:208, 224-286, 373-379
-    if (c->nion > 0)
-    {
-        phase_tables_kernel<<<(unsigned)cdiv(3 * c->nion, 128), 128, 0, s>>>(c->nion, c->n, c->unitg, c->r1,
-                                                                              c->ex1, c->ex2, c->ex3);
-        c->nlaunch += 1;
-    }
-    VlocArgs va{};
-    va.npw = c->npw;
-    va.npw_pad = c->npw_pad;
-    va.n = c->n;
-    va.nh = c->nh;
-    va.nion = c->nion;
-    va.pt_i = c->pt_i;
-    va.pt_j = c->pt_j;
-    va.pt_k = c->pt_k;
-    va.katm = c->katm;
-    va.zv = c->zv;
-    va.ex1 = c->ex1;
-    va.ex2 = c->ex2;
-    va.ex3 = c->ex3;
-    va.vl = c->vl;
-    va.vnl = c->vnl;
-    va.lmmax = c->lmmax;
-    va.proj_off = c->proj_off;
-    va.vc = c->vc;
-    va.dng = c->dng;
-    va.scal2 = c->scal2;
-    va.s = c->sfac;
-    va.vall = c->vall;
-    va.Vg = c->Vg;
-    va.proj = c->proj;
-    vloc_proj_kernel<<<(unsigned)cdiv(c->npw_pad, 128), 128, 0, s>>>(va); c->nlaunch += 1;
+    if (fork)
+        CK(cudaStreamWaitEvent(s, c->ev_sf, 0));
+    else
+        issue_sf();
+    // V(G), cpsd.c:373-379
+    vg_kernel<<<(unsigned)cdiv(c->npw, 128), 128, 0, s>>>(c->npw, c->vall, c->dng, c->vc, c->scal2, c->Vg);
+    c->nlaunch += 1;
     if (c->move && c->nion > 0) {  // local, k-space and real-space Ewald forces
         ForceArgs fa{};
         fa.npw = c->npw;
@@ -647,30 +700,9 @@ int one_step(cpsd_gpu_ctx *c)
     pv.nout = c->ispin;
     c->fft->plane(PM_INVREAL, c->g, c->Taux, pv, 1, s); c->nlaunch += 1;
     mark(c, 6);
-    // kinetic + nonlocal part of -H psi, cpsd.c:212-221, 287-290
-    kinetic_kernel<<<(unsigned)cdiv((long)c->nb * c->npw_pad, 256), 256, 0, s>>>(c->nb, c->npw_pad, c->ldc,
-                                                                                c->tg, c1, c2); c->nlaunch += 1;
-    if (c->nproj > 0) {
-        int rc = gemm_tn(c, c->nproj, c->nb, K, (const double *)c->proj, ldr, (const double *)c1, ldr, c->w,
-                         1.0, 0.0, c->beta, c->nb, TN_PROJECTOR);
+    if (!fork) {
+        int rc = issue_knl();
         if (rc) return rc;
-        kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, s>>>(
-            c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT, c->move ? c->coefP : nullptr);
-        c->nlaunch += 1;
-        gemm_nn(c, c->nb, K, c->nproj, 1.0, c->coefT, c->nproj, (const double *)c->proj, ldr, 1.0,
-                (double *)c2, ldr, TN_PROJECTOR);
-        if (c->move) {  // nonlocal force: Y_P = sum_b sw1(P, b) c1_b, then sum_G G Im(conj(chi_P) Y_P)
-            gemm_nn(c, c->nproj, K, c->nb, 1.0, c->coefP, c->nb, (const double *)c1, ldr, 0.0, (double *)c->Ynl,
-                    ldr);
-            force_nonlocal_kernel<<<c->nproj, 256, 0, s>>>(c->npw, c->ldc, c->w, c->Gv, c->proj, c->Ynl, c->fnl);
-            c->nlaunch += 1;
-        }
-    }
-    if (c->move && c->nion > 0) {  // total force and the ion step r2 = r1 + dti fion
-        force_total_kernel<<<(unsigned)cdiv(c->nion, 128), 128, 0, s>>>(
-            c->nion, 2.0 * (c->ispin == 1 ? 2.0 : 1.0), c->proj_off, c->lmmax, c->katm, c->fpart, c->fnl, c->ewp,
-            c->dti, c->r1, c->fion, c->r2);
-        c->nlaunch += 1;
     }
     mark(c, 7);
     // (V + xc) psi back to G, -H psi and the SD step, cpsd.c:384-400
@@ -680,6 +712,13 @@ int one_step(cpsd_gpu_ctx *c)
     pp.ne0 = (c->ispin == 2) ? c->ne0 : c->nb;
     c->fft->plane(PM_APPLYV, c->g, c->Tb, pp, c->nb, s); c->nlaunch += 1;
     mark(c, 8);
+    if (fork) CK(cudaStreamWaitEvent(s, c->ev_side, 0));  // kinetic + nonlocal c2 is in place
+    if (c->move && c->nion > 0) {  // total force and the ion step r2 = r1 + dti fion
+        force_total_kernel<<<(unsigned)cdiv(c->nion, 128), 128, 0, s>>>(
+            c->nion, 2.0 * (c->ispin == 1 ? 2.0 : 1.0), c->proj_off, c->lmmax, c->katm, c->fpart, c->fnl, c->ewp,
+            c->dti, c->r1, c->fion, c->r2);
+        c->nlaunch += 1;
+    }
     ZEpilogue e{};
     e.c2 = c2;
     e.c1 = c1;
@@ -1158,6 +1197,11 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     c->ldc = h.npw_pad;
     CK(cudaSetDevice(p->device));
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_sf, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_side, cudaEventDisableTiming));
+    c->cs = c->st;
     // the fused density plane must fit in shared memory
     int optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
@@ -1966,6 +2010,9 @@ void cpsd_gpu_destroy(cpsd_gpu_ctx *c)
     for (auto &e : c->pev)
         if (e) cudaEventDestroy(e);
     c->ar.release();
+    for (cudaEvent_t e : {c->ev_fork, c->ev_sf, c->ev_side})
+        if (e) cudaEventDestroy(e);
+    if (c->st2) cudaStreamDestroy(c->st2);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
 }

@@ -75,10 +75,7 @@ struct VlocArgs {
     const double *vnl;  // [nkatm][9][npw]
     const int *lmmax;   // [nkatm]
     const int *proj_off;  // [nion] first projector row of each ion
-    const double *vc;   // [npw]
-    const cx<double> *dng;
-    double scal2;
-    cx<double> *s, *vall, *Vg;
+    cx<double> *s, *vall;
     cx<double> *proj;   // [nproj][npw_pad]
 };
 
@@ -115,9 +112,17 @@ __global__ void vloc_proj_kernel(VlocArgs a)
     }
     a.s[p] = s;
     a.vall[p] = vall;
-    const double vc = a.vc[p];
-    const cx<double> d = a.dng[p];
-    a.Vg[p] = cx<double>{vall.x * a.scal2 + d.x * vc, vall.y * a.scal2 + d.y * vc};
+}
+
+// V(G) = vall / omega + dng vc (cpsd.c:373-379), once the density is known
+__global__ void vg_kernel(int npw, const cx<double> *__restrict__ vall, const cx<double> *__restrict__ dng,
+                          const double *__restrict__ vc, double scal2, cx<double> *__restrict__ Vg)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npw) return;
+    const cx<double> v = vall[p], d = dng[p];
+    const double k = vc[p];
+    Vg[p] = cx<double>{v.x * scal2 + d.x * k, v.y * scal2 + d.y * k};
 }
 
 // ------------------------------------------------------------ ion forces

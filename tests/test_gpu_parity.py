@@ -333,6 +333,26 @@ def test_graphs_and_direct_launches_agree():
     assert np.array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("move", [0, 1])
+def test_two_stream_step_equals_serial_step(move):
+    """The production step runs the projector / kinetic / nonlocal branch on
+    a second stream beside the density chain; with phase timing on, the same
+    kernels run on one stream.  Both orders give the same bits."""
+    inp = inputs.build_inputs(configs.small_diamond(24, 6, ecut=20.0, seed=13))
+    out = []
+    for serial in (False, True):
+        cell = api.GpuCell(inp)
+        cell.phase_timing(serial)
+        cell.set_state(inp.c2, inp.r2)
+        E = [cell.run(2, move=move).copy() for _ in range(3)]
+        st = api.State(inp)
+        cell.get_state(st)
+        out.append((np.array(E), st.c2.copy(), st.r2.copy()))
+        cell.close()
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(oracle.REFERENCE_SO), "dcpsdv3_b200.x")),
                     reason="drop-in build of the reference main() absent")
 def test_reference_main_linked_against_library(tmp_path):
