@@ -29,9 +29,11 @@ stiff ones.  Targets are clipped to the kernel's range [LOGK_MIN, LOGK_MAX].
 
 Use is guarded: energies are compared every `inner` steps and a block that
 raises the energy, or whose Lagrange iteration did not converge, is redone
-from its start with plain SD, so the converged answer is plain SD's (the fixed
-point H psi = psi Lambda does not depend on K).  A trust region bounds log K:
-it shrinks after a rejected block and grows back after accepted ones.
+from its start with plain SD, so every path is monotone in the energy and the
+stationary points are plain SD's (H psi = psi Lambda does not depend on K);
+on cells with several stationary points a path may still end in a different
+one than plain SD from the same start.  A trust region bounds log K: it
+shrinks after a rejected block and grows back after accepted ones.
 """
 from __future__ import annotations
 
@@ -316,27 +318,29 @@ def load_pretrained(path: str = PRETRAINED) -> api.Mlp:
 
 
 def evaluate(inp, mlp: api.Mlp, inner: int, tol_per_ion: float, learned_steps: int, plain_steps: int,
-             verify_steps: int, precision: int = 1, gemm: int = 3, refine_per_ion: float = 1e-7) -> dict:
-    """Time to tol_per_ion (Ha per ion) of the learned mixed-precision path and
-    of plain FP64 SD on one cell.
+             verify_steps: int, precision: int = 1, gemm: int = 3, refine_per_ion: float = 1e-8) -> dict:
+    """Steps and wall time to tol_per_ion (Ha per ion) of the learned
+    mixed-precision path and of plain FP64 SD on one cell.
 
-    The converged energy is taken without trusting either run to finish:
-    plain FP64 SD is continued for verify_steps from the learned run's end
-    state, and its final energy is e_conv (the continuation's drift is
-    reported: a learned end state that is not stationary under plain SD
-    shows up there).  Plain SD then runs from the initial state until it is
-    within tolerance of e_conv or plain_steps."""
+    SD with fixed occupations can end near a metastable stationary point
+    (plain SD continued from it barely moves), and different paths can end in
+    different ones.  So the reference energy is the lowest energy any run
+    reaches: the learned run, plain FP64 SD continued for verify_steps from
+    its end state, and plain FP64 SD run for its whole budget from the
+    initial state.  Each path's time to tolerance is measured against it, and
+    the learned end state's distance from it is reported."""
     nion = inp.nion
     tol = tol_per_ion * nion
     lrn = run(inp, None, tol_per_ion, learned_steps, inner, mlp=mlp, precision=precision, gemm=gemm,
               refine_per_ion=refine_per_ion, keep_state=True)
     ver = run(inp, None, tol_per_ion, verify_steps, inner, start_c2=lrn.final_c2)
-    e_conv = ver.energies[-1]
-    plain = run(inp, e_conv, tol_per_ion, plain_steps, inner)
-    ls, lt = first_within(lrn, e_conv, tol, inner)
-    ps, pt = first_within(plain, e_conv, tol, inner)
+    plain = run(inp, None, tol_per_ion, plain_steps, inner)
+    e_best = min(min(lrn.energies), min(ver.energies), min(plain.energies))
+    ls, lt = first_within(lrn, e_best, tol, inner)
+    ps, pt = first_within(plain, e_best, tol, inner)
     out = {"nion": nion, "nbands": int(inp.nbands), "npw": int(inp.npw), "nfft": int(inp.nfft),
-           "tol_per_ion": tol_per_ion, "e_conv": e_conv,
+           "tol_per_ion": tol_per_ion, "e_best": e_best,
+           "learned_end_minus_best_per_ion": (lrn.energies[-1] - e_best) / nion,
            "verify_drift_per_ion": abs(ver.energies[-1] - lrn.energies[-1]) / nion,
            "verify_steps": verify_steps,
            "learned": {"steps_to_tol": ls, "seconds_to_tol": lt, "steps_run": lrn.steps,
@@ -344,8 +348,7 @@ def evaluate(inp, mlp: api.Mlp, inner: int, tol_per_ion: float, learned_steps: i
                        "fp64_refinement_from_step": lrn.refine_step, "final_energy": lrn.energies[-1],
                        "precision": "mixed" if precision else "fp64", "gemm": gemm},
            "plain_fp64": {"steps_to_tol": ps, "seconds_to_tol": pt, "steps_run": plain.steps,
-                          "seconds_run": plain.seconds[-1], "final_energy": plain.energies[-1]},
-           "plain_final_minus_e_conv_per_ion": (plain.energies[-1] - e_conv) / nion}
+                          "seconds_run": plain.seconds[-1], "final_energy": plain.energies[-1]}}
     if ps and ls:
         out["speedup_time"] = pt / lt
         out["speedup_steps"] = ps / ls
@@ -413,9 +416,26 @@ if __name__ == "__main__":
     ap.add_argument("--horizon", type=int, default=32)
     ap.add_argument("--headline", action="store_true",
                     help="8- and 64-atom training, timed learned mixed path vs plain FP64")
+    ap.add_argument("--evaluate", default=None, help="time one cell (a configs name) with the committed network")
+    ap.add_argument("--seed", type=int, default=6000)
+    ap.add_argument("--learned-steps", type=int, default=30000)
+    ap.add_argument("--plain-steps", type=int, default=200000)
+    ap.add_argument("--verify-steps", type=int, default=5000)
     a = ap.parse_args()
     if a.headline:
         print(json.dumps(headline(out=a.out, weights=a.weights), indent=1))
+        raise SystemExit(0)
+    if a.evaluate:
+        from . import configs
+        mlp = load_pretrained()
+        res = evaluate(inputs.build_inputs(configs.NAMED[a.evaluate](seed=a.seed)), mlp, a.inner, 1e-6,
+                       a.learned_steps, a.plain_steps, a.verify_steps)
+        res["cell"] = "%s seed %d" % (a.evaluate, a.seed)
+        mlp.close()
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(res, f, indent=1)
+        print(json.dumps(res, indent=1))
         raise SystemExit(0)
     r = experiment(a.train, a.eval, a.traj_steps, a.inner, 10, a.train_steps, 1e-6, a.max_steps, a.out, a.weights,
                    a.horizon)

@@ -141,6 +141,7 @@ struct FftOps {
                              int nb, cudaStream_t s) = 0;
     virtual void fwd_z_sd(const Geom &g, const void *Tb, const ZEpilogue &e, int nb, cudaStream_t s) = 0;
     virtual void plane(int mode, const Geom &g, void *Tb, const PlaneArgs &a, int nchunks, cudaStream_t s) = 0;
+    virtual int plane_ctas_per_sm(int mode) const = 0;  // resident CTAs of a plane pass
 };
 
 template <typename T, int NF>
@@ -270,6 +271,12 @@ struct FftOpsT final : FftOps {
         }
     }
     bool mode_ok(int mode) const { return psmem[mode] != 0; }
+    int plane_ctas_per_sm(int mode) const override
+    {
+        const bool two = (mode == PM_DENSITY) ? plane_has_two_cta_build<NF, PM_DENSITY>() && two_cta[mode]
+                                              : two_cta[mode];
+        return two ? 2 : 1;
+    }
 };
 
 bool grid_supported(int n)
@@ -1272,11 +1279,32 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
         CK(ar.alloc(&t, tbytes));
         c->Taux = t;
     }
-    // density chunks: about two CTAs per SM over the z planes, never across spins
+    // density chunks (bands summed by one CTA per z plane): the count that
+    // minimises waves x bands per CTA over the SMs' resident slots, the
+    // smallest such count (fewer partial densities to add); never across spins
     {
-        const int want = std::max(1, (int)cdiv(2 * 148, c->n));
-        c->nchunk0 = std::min(c->ne0, c->ispin == 2 ? std::max(1, want / 2) : want);
-        c->nchunk1 = (c->ispin == 2 && c->ne1 > 0) ? std::min(c->ne1, std::max(1, want / 2)) : 0;
+        int sms = 148;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
+        const long slots = (long)sms * c->fft->plane_ctas_per_sm(PM_DENSITY);
+        auto best_chunks = [&](int bands, int planes_per_chunk_group) {
+            int best = 1;
+            long best_cost = -1;
+            for (int ch = 1; ch <= std::min(bands, 64); ++ch) {
+                const long cost = cdiv((long)planes_per_chunk_group * ch, slots) * cdiv(bands, ch);
+                if (best_cost < 0 || cost < best_cost) {
+                    best_cost = cost;
+                    best = ch;
+                }
+            }
+            return best;
+        };
+        if (c->ispin == 1) {
+            c->nchunk0 = best_chunks(c->ne0, c->n);
+            c->nchunk1 = 0;
+        } else {  // both spins share the launch: plan each with half of the slots
+            c->nchunk0 = best_chunks(c->ne0, 2 * c->n);
+            c->nchunk1 = c->ne1 > 0 ? best_chunks(c->ne1, 2 * c->n) : 0;
+        }
         std::vector<int> b0;
         for (int q = 0; q <= c->nchunk0; ++q) b0.push_back((int)((long)c->ne0 * q / c->nchunk0));
         for (int q = 1; q <= c->nchunk1; ++q) b0.push_back(c->ne0 + (int)((long)c->ne1 * q / c->nchunk1));
