@@ -429,7 +429,7 @@ struct TnPlan {
 
 TnPlan tn_plan(int M, int N, int K, int nprod, bool tc, size_t ws_elems)
 {
-    const int tm = tc ? kTcM : GB, tn = tc ? kTcN : GB, bk = tc ? kTcBK : GK;
+    const int tm = tc ? kTcM : kDmT, tn = tc ? kTcN : kDmT, bk = tc ? kTcBK : kDmK;
     const long tiles = cdiv(M, tm) * cdiv(N, tn) * nprod;
     long splits = std::max<long>(1, cdiv(2 * 148, tiles));
     splits = std::min<long>(splits, std::max<long>(1, K / 64));
@@ -439,7 +439,7 @@ TnPlan tn_plan(int M, int N, int K, int nprod, bool tc, size_t ws_elems)
 }
 
 // C_q = alpha A_q' W B_q (+ beta C_q), q < nprod: split-K partial products
-// (FP64 CUDA cores, or 3xTF32 on tcgen05 when tc) and a fixed-order FP64
+// (FP64 tensor cores, or 3xTF32 on tcgen05 when tc) and a fixed-order FP64
 // reduction.  Returns the number of launches.
 int launch_tn(int M, int N, int K, int nprod, const double *const *A, long lda, const double *const *B, long ldb,
               const double *w, double alpha, double beta, double *const *C, long ldc, bool tc, double *ws,
@@ -458,8 +458,8 @@ int launch_tn(int M, int N, int K, int nprod, const double *const *A, long lda, 
         dim3 grid((unsigned)cdiv(M, kTcM), (unsigned)cdiv(N, kTcN), (unsigned)(pl.splits * nprod));
         tc_gemm_tn_kernel<<<grid, kTcThreads, kTcSmem, s>>>(M, N, K, lda, ldb, w, pl.kchunk, bt, ws, err);
     } else {
-        dim3 grid((unsigned)cdiv(M, GB), (unsigned)cdiv(N, GB), (unsigned)(pl.splits * nprod));
-        gemm_tn_w_kernel<<<grid, 256, 0, s>>>(M, N, K, lda, ldb, w, pl.kchunk, bt, ws);
+        dim3 grid((unsigned)cdiv(M, kDmT), (unsigned)cdiv(N, kDmT), (unsigned)(pl.splits * nprod));
+        gemm_tn_dmma_kernel<<<grid, kDmThreads, 0, s>>>(M, N, K, lda, ldb, w, pl.kchunk, bt, ws);
     }
     splitk_reduce_kernel<<<(unsigned)cdiv((long)M * N * nprod * 32, 256), 256, 0, s>>>(M, N, ldc, ws, alpha, beta,
                                                                                        bt);
@@ -537,8 +537,8 @@ void gemm_nn(cpsd_gpu_ctx *c, int NJ, int K, int L, double alpha, const double *
         tc_gemm_nn_kernel<<<grid, kTcThreads, kTcSmem, c->cs>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo,
                                                                 c->flags + 2);
     } else {
-        dim3 grid((unsigned)cdiv(K, GB), (unsigned)cdiv(NJ, GB));
-        gemm_nn_kernel<<<grid, 256, 0, c->cs>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo);
+        dim3 grid((unsigned)cdiv(K, kDmT), (unsigned)cdiv(NJ, kDmT));
+        gemm_nn_dmma_kernel<<<grid, kDmThreads, 0, c->cs>>>(NJ, K, L, alpha, Mat, ldm, B, ldb, beta, Out, ldo);
     }
     c->nlaunch += 1;
 }

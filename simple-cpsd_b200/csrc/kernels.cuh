@@ -417,7 +417,7 @@ __global__ void density_xc_kernel(XcArgs a)
 // K counts reals, the weight is per complex pair (w[k/2]): the Gamma-point
 // dot of ccpsdv3/gcdotc.c as a matrix product.  Up to kTnMaxProd products of
 // the same shape share one launch (blockIdx.z = prod * splits + split).
-constexpr int GB = 64, GK = 16, kTnMaxProd = 4;
+constexpr int kTnMaxProd = 4;
 
 struct TnBatch {
     const double *A[kTnMaxProd];
@@ -425,58 +425,6 @@ struct TnBatch {
     double *C[kTnMaxProd];
     int nprod, splits;
 };
-
-__global__ void __launch_bounds__(256)
-gemm_tn_w_kernel(int M, int N, int K, long lda, long ldb, const double *__restrict__ w, int kchunk,
-                 const __grid_constant__ TnBatch bt, double *__restrict__ part)
-{
-    __shared__ double As[GK][GB + 1], Bs[GK][GB + 1];
-    const int prod = blockIdx.z / bt.splits, split = blockIdx.z % bt.splits;
-    const double *__restrict__ A = bt.A[prod];
-    const double *__restrict__ B = bt.B[prod];
-    const int i0 = blockIdx.x * GB, j0 = blockIdx.y * GB;
-    const int k0 = split * kchunk;
-    const int k1 = min(K, k0 + kchunk);
-    const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
-    double acc[4][4] = {};
-    for (int kk = k0; kk < k1; kk += GK) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int e = tid + 256 * q;
-            const int row = e / GK, kl = e % GK;
-            const int k = kk + kl;
-            double av = 0.0, bv = 0.0;
-            if (k < k1) {
-                if (i0 + row < M) av = A[(long)(i0 + row) * lda + k] * (w ? w[k >> 1] : 1.0);
-                if (j0 + row < N) bv = B[(long)(j0 + row) * ldb + k];
-            }
-            As[kl][row] = av;
-            Bs[kl][row] = bv;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kl = 0; kl < GK; ++kl) {
-            double a[4], b[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) a[r] = As[kl][ty + 16 * r];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) b[c] = Bs[kl][tx + 16 * c];
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
-        }
-        __syncthreads();
-    }
-    double *out = part + ((long)prod * bt.splits + split) * M * N;
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int i = i0 + ty + 16 * r, j = j0 + tx + 16 * c;
-            if (i < M && j < N) out[(long)i * N + j] = acc[r][c];
-        }
-}
 
 // C_prod[i*ldc+j] = alpha * sum_s part[prod][s][i][j] (+ beta C): one warp
 // per output, lanes stride over the splits, then a fixed xor butterfly, so
@@ -502,56 +450,196 @@ __global__ void splitk_reduce_kernel(int M, int N, long ldc, const double *__res
     }
 }
 
-// Out[j*ldo+k] = beta*Out + alpha * sum_l Mat[l + j*ldm] * B[l*ldb + k]
-// (the reference's dgemm('N','N') on column-major psi blocks, cpsd.c:483-488)
-__global__ void __launch_bounds__(256)
-gemm_nn_kernel(int NJ, int K, int L, double alpha, const double *__restrict__ Mat, long ldm,
-               const double *__restrict__ B, long ldb, double beta, double *__restrict__ Out, long ldo)
+// ------------------------------------------------------------ FP64 tensor-core GEMMs
+// Two products on the FP64 tensor cores (mma.sync m8n8k4 f64: exact FP64
+// products, FP64 sums): the split-K weighted TN partials above and the
+// back-projection NN product (the reference's dgemm('N','N') on
+// column-major psi blocks, cpsd.c:483-488).  A CTA of four warps owns a 64x64 output
+// tile, each warp a 32x32 quadrant of 4x4 fragments of 8x8.  A shared tile
+// holds 16 values of the contraction index per row; MMA step s (0..3) feeds
+// fragment k-slot q with tile column 4q+s, so one lane's four values for a
+// tile are a contiguous 32-byte run (two 16-byte loads).  The next tile is
+// fetched into registers while the current one is multiplied: two shared
+// buffers, one barrier per tile.  Row strides keep every shared access free
+// of bank conflicts: kDmS = 18 puts consecutive rows 9 16-byte units apart,
+// kDmSB = 65 (NN B tile, [l][k]) staggers the four k-slots by one bank.
+constexpr int kDmT = 64, kDmK = 16, kDmThreads = 128, kDmS = 18, kDmSB = 65;
+
+CPSD_D void dmma(double &d0, double &d1, double a, double b)
 {
-    __shared__ double Ms[GK][GB + 1], Bs[GK][GB + 1];
-    const int k0 = blockIdx.x * GB, j0 = blockIdx.y * GB;
-    const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
-    double acc[4][4] = {};
-    for (int l0 = 0; l0 < L; l0 += GK) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// The four k-steps of a lane's fragment row of a [row][k] tile.
+CPSD_D void dm_frag(const double *t, int row, int fq, double (&v)[4])
+{
+    const double2 x = *reinterpret_cast<const double2 *>(t + row * kDmS + 4 * fq);
+    const double2 y = *reinterpret_cast<const double2 *>(t + row * kDmS + 4 * fq + 2);
+    v[0] = x.x;
+    v[1] = x.y;
+    v[2] = y.x;
+    v[3] = y.y;
+}
+
+// part[prod][split][i][j] as above; grid (M tiles, N tiles, nprod * splits).
+__global__ void __launch_bounds__(kDmThreads)
+gemm_tn_dmma_kernel(int M, int N, int K, long lda, long ldb, const double *__restrict__ w, int kchunk,
+                    const __grid_constant__ TnBatch bt, double *__restrict__ part)
+{
+    __shared__ __align__(16) double As[2][kDmT * kDmS], Bs[2][kDmT * kDmS];
+    const int prod = blockIdx.z / bt.splits, split = blockIdx.z % bt.splits;
+    const double *__restrict__ A = bt.A[prod];
+    const double *__restrict__ B = bt.B[prod];
+    const int i0 = blockIdx.x * kDmT, j0 = blockIdx.y * kDmT;
+    const int k0 = split * kchunk, k1 = min(K, k0 + kchunk);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32, fr = lane >> 2, fq = lane & 3;
+    double ra[4][2], rb[4][2];
+    // loader: pass q moves reals (2p, 2p+1) of tile row e>>3, e = tid + 128q, p = e&7
+    auto fetch = [&](int kk) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int e = tid + 256 * q;
-            {  // Mat tile: l fastest
-                const int jj = e / GK, ll = e % GK;
-                const int l = l0 + ll, j = j0 + jj;
-                Ms[ll][jj] = (l < L && j < NJ) ? Mat[l + (long)j * ldm] : 0.0;
-            }
-            {  // B tile: k fastest
-                const int ll = e / GB, kk = e % GB;
-                const int l = l0 + ll, k = k0 + kk;
-                Bs[ll][kk] = (l < L && k < K) ? B[(long)l * ldb + k] : 0.0;
+            const int e = tid + kDmThreads * q, row = e >> 3, k = kk + 2 * (e & 7);
+            const int i = i0 + row, j = j0 + row;
+            const double wk = (w != nullptr && k < k1) ? w[k >> 1] : 1.0;  // k even: one weight per pair
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const bool ok = k + h < k1;
+                ra[q][h] = (ok && i < M) ? A[(long)i * lda + k + h] * wk : 0.0;
+                rb[q][h] = (ok && j < N) ? B[(long)j * ldb + k + h] : 0.0;
             }
         }
-        __syncthreads();
+    };
+    auto stash = [&](int buf) {
 #pragma unroll
-        for (int ll = 0; ll < GK; ++ll) {
-            double a[4], b[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) a[r] = Ms[ll][ty + 16 * r];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) b[c] = Bs[ll][tx + 16 * c];
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        for (int q = 0; q < 4; ++q) {
+            const int e = tid + kDmThreads * q, off = (e >> 3) * kDmS + 2 * (e & 7);
+            *reinterpret_cast<double2 *>(&As[buf][off]) = make_double2(ra[q][0], ra[q][1]);
+            *reinterpret_cast<double2 *>(&Bs[buf][off]) = make_double2(rb[q][0], rb[q][1]);
         }
+    };
+    double acc[4][4][2] = {};
+    int buf = 0;
+    if (k0 < k1) {
+        fetch(k0);
+        stash(0);
+    }
+    __syncthreads();
+    for (int kk = k0; kk < k1; kk += kDmK) {
+        const bool more = kk + kDmK < k1;
+        if (more) fetch(kk + kDmK);
+        double a[4][4], b[4][4];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            dm_frag(As[buf], wr + 8 * f + fr, fq, a[f]);
+            dm_frag(Bs[buf], wc + 8 * f + fr, fq, b[f]);
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+            for (int fi = 0; fi < 4; ++fi)
+#pragma unroll
+                for (int fj = 0; fj < 4; ++fj) dmma(acc[fi][fj][0], acc[fi][fj][1], a[fi][s], b[fj][s]);
+        if (more) stash(buf ^ 1);
         __syncthreads();
+        buf ^= 1;
+    }
+    double *out = part + ((long)prod * bt.splits + split) * M * N;
+#pragma unroll
+    for (int fi = 0; fi < 4; ++fi) {
+        const int i = i0 + wr + 8 * fi + fr;
+        if (i >= M) continue;
+#pragma unroll
+        for (int fj = 0; fj < 4; ++fj)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int j = j0 + wc + 8 * fj + 2 * fq + h;
+                if (j < N) out[(long)i * N + j] = acc[fi][fj][h];
+            }
+    }
+}
+
+// Out[j*ldo+k] = beta*Out + alpha * sum_l
+// Mat[l + j*ldm] * B[l*ldb + k]; grid x over 64-wide k tiles, y over j tiles.
+__global__ void __launch_bounds__(kDmThreads)
+gemm_nn_dmma_kernel(int NJ, int K, int L, double alpha, const double *__restrict__ Mat, long ldm,
+                    const double *__restrict__ B, long ldb, double beta, double *__restrict__ Out, long ldo)
+{
+    __shared__ __align__(16) double Ms[2][kDmT * kDmS], Bs[2][kDmK * kDmSB];
+    const int k0 = blockIdx.x * kDmT, j0 = blockIdx.y * kDmT;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32, fr = lane >> 2, fq = lane & 3;
+    double rm[4][2], rb[8];
+    auto fetch = [&](int l0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {  // Mat: tile row j = e>>3, l pair (2p, 2p+1)
+            const int e = tid + kDmThreads * q, j = j0 + (e >> 3), l = l0 + 2 * (e & 7);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) rm[q][h] = (j < NJ && l + h < L) ? Mat[(long)j * ldm + l + h] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {  // B: tile row l = e>>6, column k = e&63
+            const int e = tid + kDmThreads * q, l = l0 + (e >> 6), k = k0 + (e & 63);
+            rb[q] = (l < L && k < K) ? B[(long)l * ldb + k] : 0.0;
+        }
+    };
+    auto stash = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = tid + kDmThreads * q;
+            *reinterpret_cast<double2 *>(&Ms[buf][(e >> 3) * kDmS + 2 * (e & 7)]) = make_double2(rm[q][0], rm[q][1]);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int e = tid + kDmThreads * q;
+            Bs[buf][(e >> 6) * kDmSB + (e & 63)] = rb[q];
+        }
+    };
+    double acc[4][4][2] = {};
+    int buf = 0;
+    if (L > 0) {
+        fetch(0);
+        stash(0);
+    }
+    __syncthreads();
+    for (int l0 = 0; l0 < L; l0 += kDmK) {
+        const bool more = l0 + kDmK < L;
+        if (more) fetch(l0 + kDmK);
+        double a[4][4];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) dm_frag(Ms[buf], wr + 8 * f + fr, fq, a[f]);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const double *bs = Bs[buf] + (4 * fq + s) * kDmSB + wc + fr;
+            double b[4];
+#pragma unroll
+            for (int fj = 0; fj < 4; ++fj) b[fj] = bs[8 * fj];
+#pragma unroll
+            for (int fi = 0; fi < 4; ++fi)
+#pragma unroll
+                for (int fj = 0; fj < 4; ++fj) dmma(acc[fi][fj][0], acc[fi][fj][1], a[fi][s], b[fj]);
+        }
+        if (more) stash(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+    for (int fi = 0; fi < 4; ++fi) {
+        const int j = j0 + wr + 8 * fi + fr;
+        if (j >= NJ) continue;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int j = j0 + ty + 16 * r, k = k0 + tx + 16 * c;
-            if (j < NJ && k < K) {
-                double *o = Out + (long)j * ldo + k;
-                *o = alpha * acc[r][c] + (beta == 0.0 ? 0.0 : beta * *o);
+        for (int fj = 0; fj < 4; ++fj)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = k0 + wc + 8 * fj + 2 * fq + h;
+                if (k < K) {
+                    double *o = Out + (long)j * ldo + k;
+                    *o = alpha * acc[fi][fj][h] + (beta == 0.0 ? 0.0 : beta * *o);
+                }
             }
-        }
+    }
 }
 
 // ------------------------------------------------------------ Lagrange multipliers

@@ -3,7 +3,7 @@
 //
 //   part[prod][split][i][j] = sum_{k in chunk} (w_k A[i][k]) B[j][k]
 //
-// the same contract as gemm_tn_w_kernel (kernels.cuh): A and B FP64 in HBM,
+// the same contract as gemm_tn_dmma_kernel (kernels.cuh): A and B FP64 in HBM,
 // rows K-contiguous, weight per complex pair.  Each stage converts a 128 x 32
 // slab of each operand to a TF32 pair x = hi + lo and one elected thread
 // issues the three products hi*hi + hi*lo + lo*hi (tcgen05.mma kind::tf32,
@@ -423,7 +423,7 @@ tc_overlaps3_kernel(int m, int K, long ld, const double *__restrict__ X, const d
 
 // ------------------------------------------------------------- NN products
 // tc_gemm_nn_kernel: Out[j][k] = beta Out[j][k] + alpha sum_l Mat[j][l] B[l][k]
-// (the contract of gemm_nn_kernel: back-projection, residual and constraint
+// (the contract of gemm_nn_dmma_kernel: back-projection, residual and constraint
 // products with K the long grid dimension) in 3xTF32 on tcgen05.  CTA tile:
 // 128 rows j x 128 columns k, the reduction over l in slabs of 32.  Mat
 // rows are l-contiguous (K-major as loaded); B rows are k-contiguous, so B is
