@@ -30,6 +30,13 @@ Signature g_sig;
 
 }  // namespace
 
+// engine.cu: cpsd_gpu_run, then the host-layout outputs, with c1 and cpsi
+// zeroed on host threads during the run (c2 must have just gone through
+// cpsd_gpu_set_state).
+int cpsd_dropin_run_fetch(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae, double *deltac,
+                          double *deltar, double *c1, double *c2, double *cpsi, double *dn, double *hml,
+                          double *lmd, double *r1, double *r2, double *fion);
+
 extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, const int ispin, const int *ne,
                              const int nfft, const int nfft3d, const int n2ft3d, const double *unitg,
                              const double omega, const double dt, const double fmass, const int *katm,
@@ -89,10 +96,8 @@ extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, co
     if (rc) return rc;
     rc = cpsd_gpu_set_state(c, c2, r2);
     if (rc) return rc;
-    const int run = cpsd_gpu_run(c, inner, move, E, deltae, deltac, deltar);
-    if (run != CPSD_OK && run != CPSD_WARN_LAGRANGE) return run;
-    rc = cpsd_gpu_get_state(c, c1, c2, cpsi, dn, hml, lmd, r1, r2, fion);
-    return rc ? rc : run;
+    return cpsd_dropin_run_fetch(c, inner, move, E, deltae, deltac, deltar, c1, c2, cpsi, dn, hml, lmd, r1, r2,
+                                 fion);
 }
 
 extern "C" cpsd_gpu_ctx *cpsd_gpu_dropin_context(void)

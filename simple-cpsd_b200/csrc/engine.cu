@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "cpsd_b200.h"
 #include "fft.cuh"
+#include "host_pool.h"
 #include "kernels.cuh"
 #include "mlp.cuh"
 #include "tc_gemm.cuh"
@@ -413,7 +414,16 @@ struct cpsd_gpu_ctx {
     double *beta = nullptr, *coefT = nullptr, *Mov = nullptr, *gws = nullptr, *lag = nullptr;
     double *lmd = nullptr, *hml = nullptr, *Edev = nullptr, *red = nullptr;
     int *chunk_dens = nullptr, *chunk_band = nullptr, *flags = nullptr;
-    double *full = nullptr;  // (ne0+ne1) * n2ft3d staging for host layout conversion
+    double *full = nullptr;  // ispin * n2ft3d: the density in the reference's padded layout
+    // pinned host staging of two packed band sets (nb x ldc each): the sphere
+    // is all that crosses PCIe for the host-layout orbitals
+    struct Pinned {
+        cx<double> *p = nullptr;
+        ~Pinned()
+        {
+            if (p) cudaFreeHost(p);
+        }
+    } hstage;
     int pblocks = 0, bblocks = 0, gblocks = 0;
     double *ppart = nullptr, *bpart = nullptr, *gpart = nullptr;
 };
@@ -1050,7 +1060,170 @@ int batch_step(cpsd_gpu_batch *b)
     return CPSD_OK;
 }
 
+// ------------------------------------------------- host-layout orbitals
+// The reference keeps every band on the full half-box grid (nfft3d complex
+// values), zero outside the plane-wave sphere (ccpsdv3/cpsd.c:171-205 reads
+// and writes c1, c2, cpsi there).  Only the sphere crosses PCIe: host threads
+// gather it into pinned staging (checking that the rest is zero) and write
+// the grids back as zeros plus the scattered sphere.
+
+// Slices of one band's grid for the host threads (about 512 KB each).
+long grid_slices(const cpsd_gpu_ctx *c)
+{
+    return std::max<long>(1, cdiv(c->nfft3d * (long)sizeof(cx<double>), 512L << 10));
+}
+
+// c->hstage[b][p] = full[b][pt_idx[p]], zero past npw; returns the number of
+// nonzero points outside the sphere.
+long host_gather(cpsd_gpu_ctx *c, const double *full)
+{
+    const cx<double> *src = reinterpret_cast<const cx<double> *>(full);
+    const int *inv = c->hg.inv_idx.data();
+    const long S = grid_slices(c), per = cdiv(c->nfft3d, S);
+    std::atomic<long> outside{0};
+    cpsd_host::Pool::get().run((int)(c->nb * S), [&](int t) {
+        const int b = (int)(t / S);
+        const long g0 = (t % S) * per, g1 = std::min(c->nfft3d, g0 + per);
+        const cx<double> *sb = src + (long)b * c->nfft3d;
+        cx<double> *d = c->hstage.p + (long)b * c->ldc;
+        long bad = 0;
+        for (long g = g0; g < g1; ++g) {
+            const int p = inv[g];
+            if (p >= 0)
+                d[p] = sb[g];
+            else
+                bad += (sb[g].x != 0.0 || sb[g].y != 0.0);
+        }
+        if (t % S == 0)
+            for (long p = c->npw; p < c->ldc; ++p) d[p] = cx<double>{0.0, 0.0};
+        if (bad) outside += bad;
+    });
+    return outside.load();
+}
+
+// Zero every band grid of the listed host arrays (nb x nfft3d complex each).
+std::function<void(int)> zero_grids_task(const cpsd_gpu_ctx *c, std::vector<double *> grids, int *items)
+{
+    const long S = grid_slices(c), per = cdiv(c->nfft3d, S), nb = c->nb, nfft3d = c->nfft3d;
+    *items = (int)(grids.size() * nb * S);
+    return [grids, S, per, nb, nfft3d](int t) {
+        const long gi = t / (nb * S), r = t % (nb * S), b = r / S;
+        const long g0 = (r % S) * per, g1 = std::min(nfft3d, g0 + per);
+        if (g1 > g0) memset(grids[gi] + 2 * (b * nfft3d + g0), 0, sizeof(cx<double>) * (g1 - g0));
+    };
+}
+
+// Bits of get_state_host's `zeroed`: host grids known to be zero outside the sphere.
+enum { ZERO_C1 = 1, ZERO_C2 = 2, ZERO_CPSI = 4 };
+
+int get_state_host(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double *dn, double *hml, double *lmd,
+                   double *r1, double *r2, double *fion, unsigned zeroed)
+{
+    if (!c) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    cudaStream_t s = c->st;
+    const long P = (long)c->nb * c->ldc;
+    const size_t pb = sizeof(cx<double>) * P;
+    const cx<double> *cc2 = c->cbuf[c->cur], *cc1 = c->ran ? c->cbuf[c->cur ^ 1] : cc2;
+    cx<double> *h2 = c->hstage.p, *h1 = c->hstage.p + P;
+    if (c2 || cpsi) {
+        CK(cudaMemcpyAsync(h2, cc2, pb, cudaMemcpyDeviceToHost, s));
+        c->d2h += (long long)pb;
+    }
+    if (c1 || cpsi) {
+        CK(cudaMemcpyAsync(h1, cc1, pb, cudaMemcpyDeviceToHost, s));
+        c->d2h += (long long)pb;
+    }
+    const long ne02 = (long)c->ne0 * c->ne0, ne12 = (long)c->ne1 * c->ne1;
+    if (dn) {
+        const long tot = (long)c->ispin * c->n2ft3d;
+        pad_real_kernel<<<(unsigned)cdiv(tot, 256), 256, 0, s>>>(c->ispin, c->n, c->dn, c->full);
+        CK(cudaMemcpyAsync(dn, c->full, sizeof(double) * tot, cudaMemcpyDeviceToHost, s));
+        c->nlaunch += 1;
+        c->d2h += (long long)sizeof(double) * tot;
+    }
+    c->d2h += (long long)sizeof(double) * ((hml ? ne02 + ne12 : 0) + (lmd ? ne02 + ne12 : 0) +
+                                          (c->nion > 0 ? ((r1 ? 3 : 0) + (r2 ? 3 : 0)) * c->nion : 0));
+    if (hml) CK(cudaMemcpyAsync(hml, c->hml, sizeof(double) * (ne02 + ne12), cudaMemcpyDeviceToHost, s));
+    if (lmd) CK(cudaMemcpyAsync(lmd, c->lmd, sizeof(double) * (ne02 + ne12), cudaMemcpyDeviceToHost, s));
+    if (c->nion > 0) {
+        if (r1) CK(cudaMemcpyAsync(r1, c->r1, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
+        if (r2) CK(cudaMemcpyAsync(r2, c->r2, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
+        // the forces exist only after a move = 1 run (cpsd.c:246-364); as in
+        // the reference, fion is left untouched otherwise
+        if (fion && c->move) {
+            CK(cudaMemcpyAsync(fion, c->fion, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
+            c->d2h += (long long)sizeof(double) * 3 * c->nion;
+        }
+    }
+    // zero the grids that need it while the copies run, then scatter the sphere
+    std::vector<double *> zero;
+    if (c1 && !(zeroed & ZERO_C1)) zero.push_back(c1);
+    if (c2 && !(zeroed & ZERO_C2)) zero.push_back(c2);
+    if (cpsi && !(zeroed & ZERO_CPSI)) zero.push_back(cpsi);
+    auto &pool = cpsd_host::Pool::get();
+    if (!zero.empty()) {
+        int items = 0;
+        auto task = zero_grids_task(c, zero, &items);
+        pool.run(items, task);
+    }
+    CK(cudaStreamSynchronize(s));
+    struct Out {
+        double *host;
+        const cx<double> *a, *sub;
+    } outs[3] = {{c1, h1, nullptr}, {c2, h2, nullptr}, {cpsi, h2, h1}};  // cpsi = c2 - c1
+    std::vector<Out> todo;
+    for (const Out &o : outs)
+        if (o.host) todo.push_back(o);
+    const int *pt = c->hg.pt_idx.data();
+    pool.run((int)(todo.size() * c->nb), [&](int t) {
+        const Out &o = todo[t / c->nb];
+        const long b = t % c->nb;
+        cx<double> *d = reinterpret_cast<cx<double> *>(o.host) + b * c->nfft3d;
+        const cx<double> *a = o.a + b * c->ldc;
+        if (o.sub) {
+            const cx<double> *u = o.sub + b * c->ldc;
+            for (int p = 0; p < c->npw; ++p) d[pt[p]] = cx<double>{a[p].x - u[p].x, a[p].y - u[p].y};
+        } else {
+            for (int p = 0; p < c->npw; ++p) d[pt[p]] = a[p];
+        }
+    });
+    return CPSD_OK;
+}
+
 }  // namespace
+
+// The drop-in's run-and-fetch: c2 has just been read by cpsd_gpu_set_state,
+// which checked it is zero outside the sphere, so only its sphere is written
+// back; c1 and cpsi are zeroed by host threads while the GPU runs the steps.
+int cpsd_dropin_run_fetch(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae, double *deltac,
+                          double *deltar, double *c1, double *c2, double *cpsi, double *dn, double *hml,
+                          double *lmd, double *r1, double *r2, double *fion)
+{
+    if (!c) return CPSD_ERR_ARG;
+    const size_t gb = sizeof(double) * c->nb * c->n2ft3d;
+    auto apart = [gb](const double *x, const double *y) {
+        return !x || !y || (const char *)x + gb <= (const char *)y || (const char *)y + gb <= (const char *)x;
+    };
+    const bool separate = c2 && apart(c1, c2) && apart(cpsi, c2) && apart(c1, cpsi);
+    std::vector<double *> zero;
+    if (separate) {
+        if (c1) zero.push_back(c1);
+        if (cpsi) zero.push_back(cpsi);
+    }
+    auto &pool = cpsd_host::Pool::get();
+    if (!zero.empty()) {
+        int items = 0;
+        auto task = zero_grids_task(c, zero, &items);
+        pool.start(items, task);  // the pool is held until the wait below
+    }
+    const int run = cpsd_gpu_run(c, inner, move, E, deltae, deltac, deltar);
+    if (!zero.empty()) pool.wait();
+    if (run != CPSD_OK && run != CPSD_WARN_LAGRANGE) return run;
+    const unsigned zeroed = separate ? (ZERO_C1 | ZERO_C2 | ZERO_CPSI) : 0u;
+    const int rc = get_state_host(c, c1, c2, cpsi, dn, hml, lmd, r1, r2, fion, zeroed);
+    return rc ? rc : run;
+}
 
 // ====================================================================== C ABI
 extern "C" {
@@ -1345,7 +1518,8 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->ppart, 3 * c->pblocks));
     CK(ar.alloc(&c->bpart, (size_t)2 * nb * c->bblocks));
     CK(ar.alloc(&c->gpart, 2 * c->gblocks));
-    CK(ar.alloc(&c->full, (size_t)std::max(nb, c->ispin) * c->n2ft3d));
+    CK(ar.alloc(&c->full, (size_t)c->ispin * c->n2ft3d));
+    CK(cudaMallocHost((void **)&c->hstage.p, sizeof(cx<double>) * 2 * nb * c->ldc));
     CK(ar.alloc(&c->shell, (size_t)c->npw_pad));
     CK(ar.alloc(&c->dstep, 1));
     CK(ar.alloc(&c->pcap, 2));
@@ -1531,19 +1705,13 @@ int cpsd_gpu_set_state(cpsd_gpu_ctx *c, const double *c2, const double *r2)
     if (!c || !c2 || (c->nion > 0 && !r2)) return CPSD_ERR_ARG;
     CK(cudaSetDevice(c->prm.device));
     cudaStream_t s = c->st;
-    CK(cudaMemcpyAsync(c->full, c2, sizeof(double) * c->nb * c->n2ft3d, cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(c->flags + 1, 0, sizeof(int), s));
-    CK(cudaMemsetAsync(c->cbuf[c->cur], 0, sizeof(cx<double>) * c->nb * c->npw_pad, s));
-    pack_kernel<<<(unsigned)cdiv((long)c->nb * c->nfft3d, 256), 256, 0, s>>>(
-        c->nb, c->nfft3d, c->ldc, c->npw, c->inv_idx, (const cx<double> *)c->full, c->cbuf[c->cur], c->flags + 1);
+    CK(cudaStreamSynchronize(s));  // the staging buffer may still feed an earlier copy
+    if (host_gather(c, c2)) return CPSD_ERR_UNMASKED_PSI;  // device state untouched
+    const size_t pb = sizeof(cx<double>) * c->nb * c->ldc;
+    CK(cudaMemcpyAsync(c->cbuf[c->cur], c->hstage.p, pb, cudaMemcpyHostToDevice, s));
     if (c->nion > 0) CK(cudaMemcpyAsync(c->r2, r2, sizeof(double) * 3 * c->nion, cudaMemcpyHostToDevice, s));
-    int outside = 0;
-    CK(cudaMemcpyAsync(&outside, c->flags + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    c->h2d += (long long)sizeof(double) * (c->nb * c->n2ft3d + 3 * c->nion);
-    c->d2h += (long long)sizeof(int);
-    c->nlaunch += 1;
-    if (outside) return CPSD_ERR_UNMASKED_PSI;
+    c->h2d += (long long)pb + (long long)sizeof(double) * 3 * c->nion;
     c->state_ok = true;
     return CPSD_OK;
 }
@@ -1611,51 +1779,7 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
 int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double *dn, double *hml,
                        double *lmd, double *r1, double *r2, double *fion)
 {
-    if (!c) return CPSD_ERR_ARG;
-    CK(cudaSetDevice(c->prm.device));
-    cudaStream_t s = c->st;
-    const size_t fullb = sizeof(double) * c->nb * c->n2ft3d;
-    const cx<double> *cc2 = c->cbuf[c->cur], *cc1 = c->cbuf[c->cur ^ 1];
-    if (!c->ran) cc1 = cc2;
-    const unsigned ub = (unsigned)cdiv((long)c->nb * c->npw, 256);
-    struct Out {
-        double *host;
-        const cx<double> *a, *sub;
-    } outs[3] = {{c1, cc1, nullptr}, {c2, cc2, nullptr}, {cpsi, cc2, cc1}};
-    for (auto &o : outs) {
-        if (!o.host) continue;
-        CK(cudaMemsetAsync(c->full, 0, fullb, s));
-        unpack_kernel<<<ub, 256, 0, s>>>(c->nb, c->npw, c->ldc, c->pt_idx, o.a, o.sub, (cx<double> *)c->full,
-                                         c->nfft3d);
-        CK(cudaMemcpyAsync(o.host, c->full, fullb, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        c->nlaunch += 1;
-        c->d2h += (long long)fullb;
-    }
-    const long ne02 = (long)c->ne0 * c->ne0, ne12 = (long)c->ne1 * c->ne1;
-    if (dn) {
-        const long tot = (long)c->ispin * c->n2ft3d;
-        pad_real_kernel<<<(unsigned)cdiv(tot, 256), 256, 0, s>>>(c->ispin, c->n, c->dn, c->full);
-        CK(cudaMemcpyAsync(dn, c->full, sizeof(double) * tot, cudaMemcpyDeviceToHost, s));
-        c->nlaunch += 1;
-        c->d2h += (long long)sizeof(double) * tot;
-    }
-    c->d2h += (long long)sizeof(double) * ((hml ? ne02 + ne12 : 0) + (lmd ? ne02 + ne12 : 0) +
-                                          (c->nion > 0 ? ((r1 ? 3 : 0) + (r2 ? 3 : 0)) * c->nion : 0));
-    if (hml) CK(cudaMemcpyAsync(hml, c->hml, sizeof(double) * (ne02 + ne12), cudaMemcpyDeviceToHost, s));
-    if (lmd) CK(cudaMemcpyAsync(lmd, c->lmd, sizeof(double) * (ne02 + ne12), cudaMemcpyDeviceToHost, s));
-    if (c->nion > 0) {
-        if (r1) CK(cudaMemcpyAsync(r1, c->r1, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
-        if (r2) CK(cudaMemcpyAsync(r2, c->r2, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
-        // the forces exist only after a move = 1 run (cpsd.c:246-364); as in
-        // the reference, fion is left untouched otherwise
-        if (fion && c->move) {
-            CK(cudaMemcpyAsync(fion, c->fion, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToHost, s));
-            c->d2h += (long long)sizeof(double) * 3 * c->nion;
-        }
-    }
-    CK(cudaStreamSynchronize(s));
-    return CPSD_OK;
+    return get_state_host(c, c1, c2, cpsi, dn, hml, lmd, r1, r2, fion, 0u);
 }
 
 int cpsd_gpu_npw(const cpsd_gpu_ctx *c) { return c ? c->npw : 0; }

@@ -1481,39 +1481,6 @@ __global__ void __launch_bounds__(kFinalThreads) final_energy_kernel(FinalArgs a
 }
 
 // ------------------------------------------------------------ layout conversion
-// packed <-> reference half box: full[b][2*idx] <- packed[b][p]
-__global__ void unpack_kernel(int nb, int npw, long ldp, const int *__restrict__ pt_idx,
-                              const cx<double> *__restrict__ a, const cx<double> *__restrict__ sub,
-                              cx<double> *__restrict__ full, long nfft3d)
-{
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= (long)nb * npw) return;
-    const int b = (int)(id / npw), p = (int)(id % npw);
-    cx<double> v = a[(long)b * ldp + p];
-    if (sub) {
-        cx<double> u = sub[(long)b * ldp + p];
-        v = cx<double>{v.x - u.x, v.y - u.y};
-    }
-    full[(long)b * nfft3d + pt_idx[p]] = v;
-}
-
-// gather packed from the half box; count entries outside the sphere that are not zero
-__global__ void pack_kernel(int nb, long nfft3d, long ldp, int npw, const int *__restrict__ inv_idx,
-                            const cx<double> *__restrict__ full, cx<double> *__restrict__ packed,
-                            int *outside)
-{
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= (long)nb * nfft3d) return;
-    const int b = (int)(id / nfft3d);
-    const long g = id % nfft3d;
-    const cx<double> v = full[id];
-    const int p = inv_idx[g];
-    if (p >= 0)
-        packed[(long)b * ldp + p] = v;
-    else if (v.x != 0.0 || v.y != 0.0)
-        atomicAdd(outside, 1);
-}
-
 // real grid [ms][z][y][x] -> reference padded layout [ms][z][y][x(n+2)] with zero pads
 __global__ void pad_real_kernel(int nsets, int n, const double *__restrict__ src, double *__restrict__ dst)
 {

@@ -84,6 +84,40 @@ def test_dropin_cpsd_matches_reference(golden, name):
     assert np.array_equal(st.cpsi, st.c2 - st.c1) or np.abs(st.cpsi - (st.c2 - st.c1)).max() < 1e-15
 
 
+def _outside_sphere(inp, x):
+    return x.reshape(-1, inp.nfft3d, 2)[:, inp.masker1 == 0, :]
+
+
+def test_host_layout_outputs_overwrite_every_grid_point():
+    """c1 and cpsi are outputs only: NaN or other values in those buffers
+    before a call leave no trace (only the sphere crosses PCIe; host threads
+    write the zeros), and the results are bit-identical to calls whose
+    buffers started clean.  The resident get_state writes whole grids too."""
+    inp = inputs.build_inputs(configs.small_diamond(24, 4, ecut=16.0))
+    clean, dirty = api.State(inp), api.State(inp)
+    for fill in (np.nan, -3.0):
+        dirty.c1[:] = fill
+        dirty.cpsi[:] = 7.0
+        api.cpsd(inp, clean, 2)
+        api.cpsd(inp, dirty, 2)
+        for a, b in ((clean.c1, dirty.c1), (clean.c2, dirty.c2), (clean.cpsi, dirty.cpsi), (clean.dn, dirty.dn)):
+            assert np.array_equal(a, b)
+    for x in (clean.c1, clean.c2, clean.cpsi):
+        assert not _outside_sphere(inp, x).any()
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    cell.run(2)
+    ref, got = api.State(inp), api.State(inp)
+    for x in (got.c1, got.c2, got.cpsi):
+        x[:] = np.nan
+    cell.get_state(ref)
+    cell.get_state(got)
+    cell.close()
+    for a, b in ((ref.c1, got.c1), (ref.c2, got.c2), (ref.cpsi, got.cpsi)):
+        assert np.array_equal(a, b)
+        assert not _outside_sphere(inp, b).any()
+
+
 def _moving(spec):
     spec.move = 1
     return spec
