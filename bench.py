@@ -62,6 +62,31 @@ def phase_bytes(geo, nb, n, ispin):
     }
 
 
+def model_bytes(geo, nb, n, ispin, s_fft=16):
+    """Algorithmic bytes per launch under the transform model: a 3-D
+    transform is two passes, each one read and one write of the half box
+    (Nh = (n/2+1) n^2 complex, s_fft bytes each); packed coefficient streams
+    are nb*npw*16 bytes, real-grid fields n^3*8.  The engine's passes are z
+    (inv_z / fwd_z) and y+x planes (plane kernels), one model pass each.  The
+    V psi plane kernel also redoes each band's inverse plane pass instead of
+    storing psi(r); the model does not count that re-computation."""
+    pass_b = 2 * (n // 2 + 1) * n * n * s_fft
+    Pk = nb * geo["npw"] * 16
+    R = n ** 3 * 8
+    return {
+        "inv_z_bands": nb * pass_b + Pk,             # c1 in; inverse z pass of every band
+        "density_plane": nb * pass_b + ispin * R,    # inverse plane pass of every band; density out
+        "applyv_plane": nb * pass_b + ispin * R,     # forward plane pass of every band; V(r) in
+        "fwd_z_sd": nb * pass_b + 4 * Pk,            # forward z pass; c2, c1 in; cpsi, c2 out
+    }
+
+
+def step_model_bytes(nb, n, npw, s_fft=16):
+    """The same model for a whole SD step: 2 nb + 2 transforms, six packed
+    coefficient streams (c1, c2, H psi read and write), six real-grid fields."""
+    return (2 * nb + 2) * 4 * (n // 2 + 1) * n * n * s_fft + 6 * nb * npw * 16 + 6 * n ** 3 * 8
+
+
 def traffic_from_profile(kernel, workload):
     """dram bytes per launch from a committed ncu summary, if there is one."""
     path = os.path.join(REPO, "profiles", "%s_%s.txt" % (kernel, workload))
@@ -253,19 +278,31 @@ def e2e_dropin(inp, calls, inner):
     return calls * inner / dt, (h1 - h0) / calls, (d1 - d0) / calls, l1 - l0
 
 
-def roofline_entry(ph, geo, nb, n, ispin, workload):
+def roofline_entry(ph, geo, nb, n, ispin, workload, sd_step_ms):
+    """The longest single-kernel phase against the measured HBM copy rate,
+    with the model's bytes per launch (model_bytes); the pruned bytes the
+    kernel must move at least (phase_bytes) are given beside them, and the
+    whole SD step against the same model."""
     pb = phase_bytes(geo, nb, n, ispin)
-    cand = {k: v for k, v in ph.items() if k in pb and v > 0}
+    mb = model_bytes(geo, nb, n, ispin)
+    cand = {k: v for k, v in ph.items() if k in mb and v > 0}
     if not cand:
         return None
     top = max(cand, key=cand.get)
     peak, src = peaks()
-    achieved = pb[top] / (cand[top] * 1e-3) / 1e9
+    t = cand[top] * 1e-3
+    achieved = mb[top] / t / 1e9
     total = sum(v for v in ph.values() if v > 0)
+    sb = step_model_bytes(nb, n, geo["npw"])
+    step_gbs = sb / (sd_step_ms * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
             "peak_source": src, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": traffic_from_profile(top, workload), "algorithmic_bytes": pb[top],
-            "launch_ms": round(cand[top], 5), "share_of_step": round(cand[top] / total, 3) if total else None}
+            "traffic": traffic_from_profile(top, workload), "algorithmic_bytes": mb[top],
+            "bytes_model": "2 passes x (read + write) of the half box per 3-D transform, FP64",
+            "pruned_bytes": pb[top], "frac_pruned": round(pb[top] / t / 1e9 / peak, 4),
+            "launch_ms": round(cand[top], 5), "share_of_step": round(cand[top] / total, 3) if total else None,
+            "sd_step": {"bytes": sb, "ms": round(sd_step_ms, 5), "achieved": round(step_gbs, 1),
+                        "frac": round(step_gbs / peak, 4)}}
 
 
 def main():
@@ -361,7 +398,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if not prec_code else "f32+f64",
             "data": "synthetic (seeded)", "config": config, "gpu_launches": int(launches), "clocks": clocks,
             "final_energy": float(E[0])}
-    line["roofline"] = roofline_entry(ph, geo, inp.nbands, inp.nfft, inp.ispin, args.workload)
+    line["roofline"] = roofline_entry(ph, geo, inp.nbands, inp.nfft, inp.ispin, args.workload,
+                                      total_ms / (args.steps * args.inner))
     line["phases_ms"] = {k: round(v, 5) for k, v in ph.items()}
 
     if rank == 0 and not args.no_e2e:
@@ -418,7 +456,8 @@ def main():
             "value": 3 * args.inner / (tms * 1e-3), "unit": "steps/s",
             "ms_per_sd_step": tms / (3 * args.inner), "npw": big.npw, "nbands": big.nbands,
             "phases_ms": {k: round(v, 4) for k, v in ph3.items()},
-            "roofline": roofline_entry(ph3, geo3, big.nbands, big.nfft, big.ispin, "diamond64_128"),
+            "roofline": roofline_entry(ph3, geo3, big.nbands, big.nfft, big.ispin, "diamond64_128",
+                                       tms / (3 * args.inner)),
             "cpu_reference_s_per_step": 105.6}
     if rank == 0:
         print(json.dumps(line))
