@@ -126,9 +126,19 @@ def test_bench_roofline_helpers():
     pb = bench.phase_bytes(geo, 16, 64, 1)
     T = 16 * 64 * 300 * 16
     assert pb["applyv_plane"] == 2 * T + 64 ** 3 * 8
-    r = bench.roofline_entry({"applyv_plane": 0.01, "density_plane": 0.005}, geo, 16, 64, 1, "x")
+    r = bench.roofline_entry({"applyv_plane": 0.01, "density_plane": 0.005}, geo, 16, 64, 1, "x", 0.1)
     assert r["kernel"] == "applyv_plane" and r["unit"] == "GB/s" and r["bound"] == "hbm"
-    assert r["achieved"] == pytest.approx(pb["applyv_plane"] / 1e-5 / 1e9, rel=1e-3)
+    # transform model: one pass (read + write of the half box) per band, plus V(r)
+    Nh = 33 * 64 * 64
+    model = 16 * 2 * Nh * 16 + 64 ** 3 * 8
+    assert r["algorithmic_bytes"] == model
+    assert r["achieved"] == pytest.approx(model / 1e-5 / 1e9, rel=1e-3)
+    assert r["pruned_bytes"] == pb["applyv_plane"]
+    assert r["frac_pruned"] == pytest.approx(pb["applyv_plane"] / 1e-5 / 1e9 / r["peak"], rel=1e-3)
+    # whole step: (2 nb + 2) transforms, six coefficient streams, six grid fields
+    sb = 34 * 4 * Nh * 16 + 6 * 16 * 2483 * 16 + 6 * 64 ** 3 * 8
+    assert r["sd_step"]["bytes"] == sb
+    assert r["sd_step"]["achieved"] == pytest.approx(sb / 1e-4 / 1e9, rel=1e-3)
 
 
 def _rank_main(rank, world, port, q):
