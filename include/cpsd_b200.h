@@ -29,8 +29,10 @@ enum {
     CPSD_ERR_MOVE = 7,          /* move=1 requested but no G vectors / masses were given */
     CPSD_ERR_TIMEOUT = 8,       /* a bounded wait on the device ran out (tensor-core pipeline) */
     CPSD_ERR_SCRATCH = 9,       /* a problem larger than cpsd_overlap_tn_noalloc's static scratch */
-    CPSD_WARN_LAGRANGE = 10     /* (positive warning) Lagrange iteration hit 30 steps; the
+    CPSD_WARN_LAGRANGE = 10,    /* (positive warning) Lagrange iteration hit 30 steps; the
                                    reference prints "ierr=10" and continues (cpsd.c:477) */
+    CPSD_ERR_EIG = 11,          /* the epilogue's eigen solve of hml did not converge */
+    CPSD_ERR_IO = 12            /* an output file could not be written */
 };
 
 /* Human-readable text for a status code. */
@@ -151,6 +153,40 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
 /* Download the state cpsd() returns; any pointer may be NULL to skip it. */
 int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double *dn,
                        double *hml, double *lmd, double *r1, double *r2, double *fion);
+
+/*
+ * The run's epilogue, ccpsdv3/main.c:452-487, on the resident state after at
+ * least one cpsd_gpu_run (CPSD_ERR_ARG before).  Any output may be NULL:
+ *   ortho  <c1_i|c1_j> per spin (Gamma-point dots), hml's layout: the
+ *          orthonormality table main.c:455-467 prints for i <= j;
+ *   eig    eigenvalues of hml per spin, eig[ms*ne[0] + i], descending: what
+ *          esyev('V','U') + eigsrt leave (main.c:470-479);
+ *   vec    the eigenvectors, hml's layout, columns in eig's order (the hml
+ *          that main.c holds after esyev + eigsrt); a column's sign is not
+ *          fixed by the problem and may differ from LAPACK's.
+ * Then c1 <- c2 vec per spin on the device (main.c:481-487): a following
+ * cpsd_gpu_get_state returns the rotated orbitals main.c writes to ELCOUT.
+ * CPSD_ERR_EIG: the Jacobi solve did not converge (not seen in practice).
+ */
+int cpsd_gpu_epilogue(cpsd_gpu_ctx *c, double *ortho, double *eig, double *vec);
+
+/*
+ * ELCOUT as main.c:537-546 writes it: int icube, int nfft, double unit,
+ * int ispin, int ne[2], then (ne[0]+ne[1]) * (nfft+2)*nfft*nfft doubles of
+ * c1 (host layout), native byte order.  CPSD_ERR_IO if the file cannot be
+ * written.
+ */
+int cpsd_write_elcout(const char *path, int icube, int nfft, double unit, int ispin, const int *ne,
+                      const double *c1);
+
+/*
+ * IONOUT as main.c:549-566 writes it: nkatm; per kind "'<fname> ' <lmax>";
+ * nion; per ion "<katm+1> x y z 0.000000 0.000000 0.000000 " -- main.c
+ * zeroes r1 (:550) before printing it beside r2.  fname[ia] are the psp file
+ * names IONIN listed.
+ */
+int cpsd_write_ionout(const char *path, int nkatm, const char *const *fname, const int *lmax, int nion,
+                      const int *katm, const double *r2);
 
 /* Sphere size (packed G vectors per band) and the kernel launches of one SD step. */
 int cpsd_gpu_npw(const cpsd_gpu_ctx *c);

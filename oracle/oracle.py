@@ -177,3 +177,66 @@ class ReferenceBuild:
 
     def gssum(self, nfft: int, x: np.ndarray) -> float:
         return self.lib.gssum(ctypes.c_int(nfft), _ptr(x))
+
+    def gcdotc(self, nfft: int, a: np.ndarray, b: np.ndarray) -> float:
+        return self.lib.gcdotc(ctypes.c_int(nfft), _ptr(a), _ptr(b))
+
+    def eigsrt(self, D: np.ndarray, V: np.ndarray, n: int) -> None:
+        """The reference's eigsrt (ccpsdv3/eigsrt.c:9-36) in place; V column-major, ld n."""
+        self.lib.eigsrt(_ptr(D), _ptr(V), ctypes.c_int(n))
+
+
+def eigsrt(D: np.ndarray, V: np.ndarray) -> None:
+    """ccpsdv3/eigsrt.c:9-36 restated: selection sort into descending order,
+    ties to the later index; V[:, i] (eigenvector i) moves with D[i]."""
+    n = len(D)
+    for i in range(n - 1):
+        k, p = i, D[i]
+        for j in range(i + 1, n):
+            if D[j] >= p:
+                k, p = j, D[j]
+        if k != i:
+            D[k] = D[i]
+            D[i] = p
+            V[:, [i, k]] = V[:, [k, i]]
+
+
+def epilogue(inp, st: State, gcdotc, sort=eigsrt, matmul=None) -> dict:
+    """ccpsdv3/main.c:452-487 restated on a State after the last cpsd() call:
+
+    * ``ortho``: <c1_i|c1_j> (gcdotc, main.c:455-467), per spin in hml's layout;
+    * ``eig``, ``vec``: dsyev('V','U') of hml per spin (LAPACK, via scipy)
+      then eigsrt (main.c:470-479): eig[ms*ne0 + i] descending, vec in hml's
+      layout (column-major, ld ne[ms]);
+    * ``c1``: c2 V per spin (main.c:481-487), the orbitals ELCOUT holds.
+
+    ``gcdotc(nfft, a, b)`` is a checker's Gamma-point dot; ``sort(D, V)``
+    orders the eigenpairs (V as an array, column i = vector i); ``matmul(C2, V)``
+    returns C2 @ V for C2 of shape (n2ft3d, m) (numpy by default)."""
+    from scipy.linalg import lapack
+    ne = [int(inp.ne[0]), int(inp.ne[1])]
+    ne0 = ne[0]
+    n2 = inp.n2ft3d
+    ortho = np.zeros(ne[0] ** 2 + ne[1] ** 2)
+    vec = np.zeros_like(ortho)
+    eig = np.zeros(ne[0] + ne[1])
+    c1 = np.zeros_like(st.c2)
+    for ms in range(inp.ispin):
+        m, b0 = ne[ms], ms * ne0
+        o = ms * ne0 * ne0
+        for i in range(m):
+            for j in range(i, m):
+                w = gcdotc(inp.nfft, st.c1[(b0 + i) * n2:(b0 + i + 1) * n2], st.c1[(b0 + j) * n2:(b0 + j + 1) * n2])
+                ortho[o + i + j * m] = ortho[o + j + i * m] = w
+        H = st.hml[o:o + m * m].reshape(m, m).T  # H[i, j] = hml[i + j*m]
+        w, v, info = lapack.dsyev(np.array(H, order="F"), compute_v=1, lower=0)
+        assert info == 0
+        D = np.array(w)
+        V = np.array(v)
+        sort(D, V)
+        eig[ms * ne0:ms * ne0 + m] = D
+        vec[o:o + m * m] = V.T.ravel()  # column-major
+        C2 = st.c2[b0 * n2:(b0 + m) * n2].reshape(m, n2).T
+        C1 = matmul(C2, V) if matmul else C2 @ V
+        c1[b0 * n2:(b0 + m) * n2] = C1.T.ravel()
+    return {"ortho": ortho, "eig": eig, "vec": vec, "c1": c1}

@@ -221,6 +221,18 @@ class GpuCell:
         st.deltae, st.deltac, st.deltar = self.deltae, self.deltac, self.deltar
         return st
 
+    def epilogue(self) -> dict:
+        """The run's epilogue on the device (ccpsdv3/main.c:452-487): the
+        orthonormality table <c1_i|c1_j>, the eigenvalues of hml per spin in
+        descending order (eig[ms*ne0 + i]) with their eigenvectors (hml's
+        layout), and c1 <- c2 V, which get_state then returns."""
+        ne0, ne1 = int(self.inp.ne[0]), int(self.inp.ne[1])
+        ortho = np.zeros(ne0 * ne0 + ne1 * ne1)
+        vec = np.zeros_like(ortho)
+        eig = np.zeros(ne0 + ne1)
+        self._check(self._L.cpsd_gpu_epilogue(self.h, _ptr(ortho), _ptr(eig), _ptr(vec)), "cpsd_gpu_epilogue")
+        return {"ortho": ortho, "eig": eig, "vec": vec}
+
     def close(self) -> None:
         if getattr(self, "h", None):
             self._L.cpsd_gpu_destroy(self.h)
@@ -345,6 +357,35 @@ class Mlp:
             self.close()
         except Exception:
             pass
+
+
+def write_elcout(path: str, inp, c1: np.ndarray) -> None:
+    """ELCOUT as ccpsdv3/main.c:537-546 writes it (header, then c1)."""
+    L = _l.load()
+    ne = np.ascontiguousarray(inp.ne, dtype=np.int32)
+    c1 = np.ascontiguousarray(c1, dtype=np.float64)
+    if c1.size != int(ne.sum()) * inp.n2ft3d:
+        raise ValueError("c1 must hold (ne0+ne1) * n2ft3d doubles")
+    rc = L.cpsd_write_elcout(path.encode(), int(inp.spec.icube), int(inp.nfft), float(inp.spec.unit),
+                             int(inp.ispin), _ptr(ne), _ptr(c1))
+    if rc:
+        raise CpsdError(rc, "cpsd_write_elcout")
+
+
+def write_ionout(path: str, inp, fnames, r2: np.ndarray) -> None:
+    """IONOUT as ccpsdv3/main.c:549-566 writes it; fnames are the psp file
+    names of the kinds (as IONIN lists them)."""
+    L = _l.load()
+    species = inp.spec.species
+    if len(fnames) != len(species):
+        raise ValueError("one file name per kind")
+    names = (ctypes.c_char_p * len(fnames))(*[f.encode() for f in fnames])
+    lmax = np.array([sp.lmax for sp in species], dtype=np.int32)
+    katm = np.ascontiguousarray(inp.katm, dtype=np.int32)
+    r2 = np.ascontiguousarray(r2, dtype=np.float64)
+    rc = L.cpsd_write_ionout(path.encode(), len(fnames), names, _ptr(lmax), int(inp.nion), _ptr(katm), _ptr(r2))
+    if rc:
+        raise CpsdError(rc, "cpsd_write_ionout")
 
 
 def dropin_counters():

@@ -24,6 +24,8 @@ CPSD_ERR_MOVE = 7
 CPSD_ERR_TIMEOUT = 8
 CPSD_ERR_SCRATCH = 9
 CPSD_WARN_LAGRANGE = 10
+CPSD_ERR_EIG = 11
+CPSD_ERR_IO = 12
 
 CPSD_PREC_FP64 = 0
 CPSD_PREC_MIXED = 1
@@ -47,7 +49,8 @@ EXPORTS = [
     "cpsd_mlp_get_params", "cpsd_mlp_set_params", "cpsd_mlp_destroy", "cpsd_gpu_set_preconditioner",
     "cpsd_gpu_set_preconditioner_range", "cpsd_gpu_save_orbitals", "cpsd_gpu_restore_orbitals",
     "cpsd_gpu_get_packed", "cpsd_gpu_set_packed", "cpsd_gpu_get_sphere", "cpsd_gpu_set_gemm",
-    "cpsd_overlap_tn", "cpsd_overlap_tn_noalloc",
+    "cpsd_overlap_tn", "cpsd_overlap_tn_noalloc", "cpsd_gpu_epilogue", "cpsd_write_elcout",
+    "cpsd_write_ionout",
 ]
 
 
@@ -85,6 +88,9 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_gpu_set_state.argtypes = [_P, _P, _P]
     lib.cpsd_gpu_run.argtypes = [_P, _I, _I, _P, _P, _P, _P]
     lib.cpsd_gpu_get_state.argtypes = [_P] + [_P] * 9
+    lib.cpsd_gpu_epilogue.argtypes = [_P, _P, _P, _P]
+    lib.cpsd_write_elcout.argtypes = [ctypes.c_char_p, _I, _I, _D, _I, _P, _P]
+    lib.cpsd_write_ionout.argtypes = [ctypes.c_char_p, _I, ctypes.POINTER(ctypes.c_char_p), _P, _I, _P, _P]
     lib.cpsd_gpu_npw.argtypes = [_P]
     lib.cpsd_gpu_launches_per_step.argtypes = [_P]
     lib.cpsd_gpu_geometry.argtypes = [_P, _P]

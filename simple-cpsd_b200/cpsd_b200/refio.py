@@ -124,3 +124,39 @@ def parse_reference_stdout(text: str):
             if s.startswith(k):
                 final[idx] = float(s.split(":")[1].split("(")[0])
     return rows, final
+
+
+def parse_reference_epilogue(text: str):
+    """The epilogue tables main.c prints: the orthonormality rows
+    (ms, i, j, <c1_i|c1_j>), 1-based as printed (main.c:455-467), and the
+    orbital energies in Hartree (main.c:518-530; with two spins a line holds
+    one value of each)."""
+    ortho, eig = [], []
+    mode = None
+    for line in text.splitlines():
+        st = line.strip()
+        if st.startswith("orthonormality"):
+            mode = "o"
+            continue
+        if st.startswith("orbital energies"):
+            mode = "e"
+            continue
+        if mode == "o":
+            parts = st.split()
+            if len(parts) == 4:
+                try:
+                    ortho.append((int(parts[0]), int(parts[1]), int(parts[2]), float(parts[3])))
+                    continue
+                except ValueError:
+                    pass
+            if st:
+                mode = None
+        elif mode == "e":
+            if "eV)" not in st:
+                if st:
+                    mode = None
+                continue
+            for chunk in st.split("eV)"):
+                if "(" in chunk:
+                    eig.append(float(chunk.split("(")[0]))
+    return ortho, eig

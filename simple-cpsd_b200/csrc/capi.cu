@@ -125,6 +125,41 @@ extern "C" void cpsd(const int inner, const int move, const int nion, const int 
         printf("cpsd (B200): error %d: %s\n", rc, cpsd_gpu_strerror(rc));
 }
 
+// ====================================================================== epilogue files
+extern "C" int cpsd_write_elcout(const char *path, int icube, int nfft, double unit, int ispin, const int *ne,
+                                 const double *c1)
+{
+    if (!path || !ne || !c1 || nfft <= 0 || ne[0] < 0 || ne[1] < 0) return CPSD_ERR_ARG;
+    FILE *fp = fopen(path, "wb");
+    if (!fp) return CPSD_ERR_IO;
+    const size_t nn = (size_t)(ne[0] + ne[1]) * (size_t)(nfft + 2) * nfft * nfft;
+    bool ok = fwrite(&icube, sizeof(int), 1, fp) == 1 && fwrite(&nfft, sizeof(int), 1, fp) == 1 &&
+              fwrite(&unit, sizeof(double), 1, fp) == 1 && fwrite(&ispin, sizeof(int), 1, fp) == 1 &&
+              fwrite(ne, sizeof(int), 2, fp) == 2 && fwrite(c1, sizeof(double), nn, fp) == nn;
+    ok = (fclose(fp) == 0) && ok;
+    return ok ? CPSD_OK : CPSD_ERR_IO;
+}
+
+extern "C" int cpsd_write_ionout(const char *path, int nkatm, const char *const *fname, const int *lmax, int nion,
+                                 const int *katm, const double *r2)
+{
+    if (!path || nkatm < 0 || nion < 0 || (nkatm > 0 && (!fname || !lmax)) || (nion > 0 && (!katm || !r2)))
+        return CPSD_ERR_ARG;
+    FILE *fp = fopen(path, "w");
+    if (!fp) return CPSD_ERR_IO;
+    bool ok = fprintf(fp, "%d\n", nkatm) > 0;
+    for (int ia = 0; ia < nkatm && ok; ++ia) ok = fprintf(fp, "'%s ' %d\n", fname[ia], lmax[ia]) > 0;
+    ok = ok && fprintf(fp, "%d\n", nion) > 0;
+    for (int ii = 0; ii < nion && ok; ++ii) {
+        ok = fprintf(fp, "%d ", katm[ii] + 1) > 0;
+        for (int d = 0; d < 3 && ok; ++d) ok = fprintf(fp, "%lf ", r2[3 * ii + d]) > 0;
+        for (int d = 0; d < 3 && ok; ++d) ok = fprintf(fp, "%lf ", 0.0) > 0;
+        ok = ok && fprintf(fp, "\n") > 0;
+    }
+    ok = (fclose(fp) == 0) && ok;
+    return ok ? CPSD_OK : CPSD_ERR_IO;
+}
+
 // ====================================================================== 3-D FFT drop-ins
 namespace {
 

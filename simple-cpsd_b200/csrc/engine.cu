@@ -415,6 +415,9 @@ struct cpsd_gpu_ctx {
     double *lmd = nullptr, *hml = nullptr, *Edev = nullptr, *red = nullptr;
     int *chunk_dens = nullptr, *chunk_band = nullptr, *flags = nullptr;
     double *full = nullptr;  // ispin * n2ft3d: the density in the reference's padded layout
+    // epilogue (allocated on first use): Jacobi workspace, eigenpairs, overlaps
+    double *eigA = nullptr, *eigV = nullptr, *eigD = nullptr, *eigVec = nullptr, *ortho = nullptr;
+    int *eig_sweeps = nullptr;
     // pinned host staging of two packed band sets (nb x ldc each): the sphere
     // is all that crosses PCIe for the host-layout orbitals
     struct Pinned {
@@ -1334,7 +1337,9 @@ const char *cpsd_gpu_strerror(int status)
     case CPSD_ERR_BANDS: return "more than 256 bands in a spin channel";
     case CPSD_ERR_EMPTY_MASK: return "the cutoff mask selects no G vector";
     case CPSD_ERR_UNMASKED_PSI: return "orbital coefficients outside the cutoff mask";
-    case CPSD_ERR_MOVE: return "ionic motion (move=1) is not available";
+    case CPSD_ERR_MOVE: return "move=1 requested but no G vectors / masses were given";
+    case CPSD_ERR_EIG: return "the Jacobi eigen solve of hml did not converge in 60 sweeps";
+    case CPSD_ERR_IO: return "an output file could not be written";
     case CPSD_WARN_LAGRANGE: return "ierr=10: Lagrange-multiplier iteration did not converge in 30 steps";
     default: return "unknown status";
     }
@@ -1780,6 +1785,86 @@ int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, do
                        double *lmd, double *r1, double *r2, double *fion)
 {
     return get_state_host(c, c1, c2, cpsi, dn, hml, lmd, r1, r2, fion, 0u);
+}
+
+int cpsd_gpu_epilogue(cpsd_gpu_ctx *c, double *ortho, double *eig, double *vec)
+{
+    if (!c) return CPSD_ERR_ARG;
+    if (!c->ran) return CPSD_ERR_ARG;  // hml and c1 exist only after a run
+    CK(cudaSetDevice(c->prm.device));
+    cudaStream_t s = c->st;
+    const long ne02 = (long)c->ne0 * c->ne0;
+    if (!c->eigA) {
+        CK(c->ar.alloc(&c->eigA, (size_t)2 * ne02));
+        CK(c->ar.alloc(&c->eigV, (size_t)2 * ne02));
+        CK(c->ar.alloc(&c->eigD, (size_t)2 * c->ne0));
+        CK(c->ar.alloc(&c->eigVec, (size_t)2 * ne02));
+        CK(c->ar.alloc(&c->ortho, (size_t)2 * ne02));
+        CK(c->ar.alloc(&c->eig_sweeps, 2));
+    }
+    const cudaStream_t cs_saved = c->cs;
+    c->cs = s;
+    const int K = 2 * c->npw_pad;
+    const long ldr = 2L * c->npw_pad;
+    const double *c1 = (const double *)c->cbuf[c->cur ^ 1];
+    const double *c2 = (const double *)c->cbuf[c->cur];
+    // orthonormality of c1 (main.c:455-467): <c1_i|c1_j>, Gamma-point dots
+    if (ortho) {
+        for (int ms = 0; ms < c->ispin; ++ms) {
+            const int m = ms ? c->ne1 : c->ne0;
+            const long off = (long)(ms ? c->ne0 : 0) * ldr;
+            // row-major M x M from the TN product equals its column-major transpose (symmetric)
+            const int rc = gemm_tn(c, m, m, K, c1 + off, ldr, c1 + off, ldr, c->w, 1.0, 0.0, c->ortho + ms * ne02, m);
+            if (rc) {
+                c->cs = cs_saved;
+                return rc;
+            }
+        }
+    }
+    // eigenpairs of hml per spin (main.c:470-479)
+    EigArgs ea{};
+    ea.hml = c->hml;
+    ea.ne[0] = c->ne0;
+    ea.ne[1] = c->ispin == 2 ? c->ne1 : 0;
+    ea.ne0 = c->ne0;
+    ea.A = c->eigA;
+    ea.V = c->eigV;
+    ea.eig = c->eigD;
+    ea.vec = c->eigVec;
+    ea.sweeps = c->eig_sweeps;
+    jacobi_eig_kernel<<<c->ispin, kEigThreads, 0, s>>>(ea);
+    c->nlaunch += 1;
+    // c1 <- c2 V per spin (main.c:481-487): band j of c1 = sum_l V[l][j] band l of c2
+    double *c1w = (double *)c->cbuf[c->cur ^ 1];
+    for (int ms = 0; ms < c->ispin; ++ms) {
+        const int m = ms ? c->ne1 : c->ne0;
+        const long off = (long)(ms ? c->ne0 : 0) * ldr;
+        gemm_nn(c, m, K, m, 1.0, c->eigVec + ms * ne02, m, c2 + off, ldr, 0.0, c1w + off, ldr);
+    }
+    c->cs = cs_saved;
+    CK(cudaGetLastError());
+    int sweeps[2] = {0, 0};
+    CK(cudaMemcpyAsync(sweeps, c->eig_sweeps, sizeof(int) * c->ispin, cudaMemcpyDeviceToHost, s));
+    const long ne12 = (long)c->ne1 * c->ne1;
+    if (ortho) {
+        CK(cudaMemcpyAsync(ortho, c->ortho, sizeof(double) * ne02, cudaMemcpyDeviceToHost, s));
+        if (c->ispin == 2)
+            CK(cudaMemcpyAsync(ortho + ne02, c->ortho + ne02, sizeof(double) * ne12, cudaMemcpyDeviceToHost, s));
+    }
+    if (eig) {
+        CK(cudaMemcpyAsync(eig, c->eigD, sizeof(double) * c->ne0, cudaMemcpyDeviceToHost, s));
+        if (c->ispin == 2)
+            CK(cudaMemcpyAsync(eig + c->ne0, c->eigD + c->ne0, sizeof(double) * c->ne1, cudaMemcpyDeviceToHost, s));
+    }
+    if (vec) {
+        CK(cudaMemcpyAsync(vec, c->eigVec, sizeof(double) * ne02, cudaMemcpyDeviceToHost, s));
+        if (c->ispin == 2)
+            CK(cudaMemcpyAsync(vec + ne02, c->eigVec + ne02, sizeof(double) * ne12, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    for (int ms = 0; ms < c->ispin; ++ms)
+        if (sweeps[ms] > kEigMaxSweeps) return CPSD_ERR_EIG;
+    return CPSD_OK;
 }
 
 int cpsd_gpu_npw(const cpsd_gpu_ctx *c) { return c ? c->npw : 0; }

@@ -1493,3 +1493,181 @@ __global__ void pad_real_kernel(int nsets, int n, const double *__restrict__ src
     const long yz = r / (n + 2);
     dst[id] = (x < n) ? src[(long)ms * n * n * n + yz * n + x] : 0.0;
 }
+
+// ------------------------------------------------------------ epilogue eigenpairs
+// ccpsdv3/main.c:470-481: per spin, dsyev('V','U') of hml, then eigsrt
+// (ccpsdv3/eigsrt.c:9-36: selection sort into descending order, ties to the
+// later index, eigenvector columns moved with their values).  Here: cyclic
+// Jacobi, rounds of the round-robin pair order (n/2 disjoint pairs per
+// round, n padded to even with an idle index), so one round's rotations run
+// in parallel: rows of A, then columns of A and V.  Rotation and thresholds
+// follow the classical scheme (Rutishauser; as in Numerical Recipes
+// "jacobi"): t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)), theta =
+// (a_qq - a_pp) / (2 a_pq); in the first sweeps only |a_pq| above 0.2 S / n^2
+// (S = sum of |a_ij|, i < j) rotate; from the fifth sweep on an a_pq that
+// no longer changes a_pp or a_qq (|a_pp| + 100 |a_pq| == |a_pp|, the same
+// for a_qq) is set to zero.  The sweeps end when S is zero.  One CTA per
+// spin; A and V (column-major, ld n) live in global memory (L2).
+constexpr int kEigThreads = 1024, kEigMaxSweeps = 60;
+
+struct EigArgs {
+    const double *hml;   // per spin ms at hml + ms*ne0*ne0, column-major, ld ne[ms]; upper triangle read
+    int ne[2], ne0;
+    double *A, *V;       // workspace: per spin ne0*ne0 each
+    double *eig;         // eig[ms*ne0 + i], descending
+    double *vec;         // eigenvectors in hml's layout, columns in eig's order
+    int *sweeps;         // per spin: sweeps run (kEigMaxSweeps + 1: not converged)
+};
+
+__global__ void __launch_bounds__(kEigThreads) jacobi_eig_kernel(EigArgs a)
+{
+    __shared__ double rc[128], rs[128], rapp[128], raqq[128], rt[128], red[32];
+    __shared__ int rp[128], rq[128], perm[256];
+    __shared__ double sum_off;
+    const int ms = blockIdx.x, n = a.ne[ms], tid = threadIdx.x;
+    if (n <= 0) return;
+    const long off = (long)ms * a.ne0 * a.ne0;
+    const double *H = a.hml + off;
+    double *A = a.A + off, *V = a.V + off;
+    for (long e = tid; e < (long)n * n; e += kEigThreads) {
+        const int i = (int)(e % n), j = (int)(e / n);
+        A[e] = (i <= j) ? H[i + (long)j * n] : H[j + (long)i * n];
+        V[e] = (i == j) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const int np = n + (n & 1), half = np / 2, m1 = np - 1;
+    int sweep = 1;
+    for (; sweep <= kEigMaxSweeps; ++sweep) {
+        // S = sum_{i<j} |a_ij|
+        double v = 0.0;
+        for (long e = tid; e < (long)n * n; e += kEigThreads) {
+            const int i = (int)(e % n), j = (int)(e / n);
+            if (i < j) v += fabs(A[e]);
+        }
+        v = block_sum<kEigThreads>(v, red);
+        if (tid == 0) sum_off = v;
+        __syncthreads();
+        const double S = sum_off;
+        if (S == 0.0) break;
+        const double tresh = (sweep < 4) ? 0.2 * S / ((double)n * n) : 0.0;
+        for (int r = 0; r < m1; ++r) {
+            if (tid < half) {
+                int p, q;
+                if (tid == 0) {
+                    p = 0;
+                    q = 1 + r;
+                } else {
+                    p = 1 + (r + tid) % m1;
+                    q = 1 + (r - tid + m1) % m1;
+                }
+                if (p > q) {
+                    const int x = p;
+                    p = q;
+                    q = x;
+                }
+                double c = 1.0, s = 0.0, t = 0.0;
+                bool rot = false;
+                if (q < n) {
+                    const double app = A[p + (long)p * n], aqq = A[q + (long)q * n], apq = A[p + (long)q * n];
+                    const double g = 100.0 * fabs(apq);
+                    if (sweep > 4 && fabs(app) + g == fabs(app) && fabs(aqq) + g == fabs(aqq)) {
+                        A[p + (long)q * n] = 0.0;
+                        A[q + (long)p * n] = 0.0;
+                    } else if (fabs(apq) > tresh && apq != 0.0) {
+                        const double h = aqq - app;
+                        if (fabs(h) + g == fabs(h)) {
+                            t = apq / h;
+                        } else {
+                            const double theta = 0.5 * h / apq;
+                            t = 1.0 / (fabs(theta) + sqrt(1.0 + theta * theta));
+                            if (theta < 0.0) t = -t;
+                        }
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        s = t * c;
+                        rot = true;
+                        rapp[tid] = app;
+                        raqq[tid] = aqq;
+                        rt[tid] = t * apq;
+                    }
+                }
+                rp[tid] = rot ? p : -1;
+                rq[tid] = q;
+                rc[tid] = c;
+                rs[tid] = s;
+            }
+            __syncthreads();
+            // rows p, q of A: A <- P^T A
+            for (long e = tid; e < (long)half * n; e += kEigThreads) {
+                const int k = (int)(e / n), j = (int)(e % n), p = rp[k];
+                if (p < 0) continue;
+                const int q = rq[k];
+                const double c = rc[k], s = rs[k];
+                const double ap = A[p + (long)j * n], aq = A[q + (long)j * n];
+                A[p + (long)j * n] = c * ap - s * aq;
+                A[q + (long)j * n] = s * ap + c * aq;
+            }
+            __syncthreads();
+            // columns p, q of A and V: A <- A P, V <- V P
+            for (long e = tid; e < (long)half * n; e += kEigThreads) {
+                const int k = (int)(e / n), i = (int)(e % n), p = rp[k];
+                if (p < 0) continue;
+                const int q = rq[k];
+                const double c = rc[k], s = rs[k];
+                double *cp = A + (long)p * n, *cq = A + (long)q * n;
+                double x = cp[i], y = cq[i];
+                cp[i] = c * x - s * y;
+                cq[i] = s * x + c * y;
+                cp = V + (long)p * n;
+                cq = V + (long)q * n;
+                x = cp[i];
+                y = cq[i];
+                cp[i] = c * x - s * y;
+                cq[i] = s * x + c * y;
+            }
+            __syncthreads();
+            // the rotated 2 x 2 blocks (touched by their own rotation only):
+            // a_pp - t a_pq, a_qq + t a_pq and exact zeros off the diagonal
+            if (tid < half && rp[tid] >= 0) {
+                const int p = rp[tid], q = rq[tid];
+                A[p + (long)p * n] = rapp[tid] - rt[tid];
+                A[q + (long)q * n] = raqq[tid] + rt[tid];
+                A[p + (long)q * n] = 0.0;
+                A[q + (long)p * n] = 0.0;
+            }
+            __syncthreads();
+        }
+        // restore exact symmetry from the upper triangle
+        for (long e = tid; e < (long)n * n; e += kEigThreads) {
+            const int i = (int)(e % n), j = (int)(e / n);
+            if (i > j) A[e] = A[j + (long)i * n];
+        }
+        __syncthreads();
+    }
+    // eigsrt: descending selection sort, ties to the later index
+    if (tid == 0) {
+        for (int i = 0; i < n; ++i) perm[i] = i;
+        for (int i = 0; i < n - 1; ++i) {
+            int k = i;
+            double p = A[perm[i] + (long)perm[i] * n];
+            for (int j = i + 1; j < n; ++j) {
+                const double d = A[perm[j] + (long)perm[j] * n];
+                if (d >= p) {
+                    k = j;
+                    p = d;
+                }
+            }
+            if (k != i) {
+                const int x = perm[i];
+                perm[i] = perm[k];
+                perm[k] = x;
+            }
+        }
+        a.sweeps[ms] = sweep;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += kEigThreads) a.eig[(long)ms * a.ne0 + i] = A[perm[i] + (long)perm[i] * n];
+    for (long e = tid; e < (long)n * n; e += kEigThreads) {
+        const int i = (int)(e % n), j = (int)(e / n);
+        a.vec[off + i + (long)j * n] = V[i + (long)perm[j] * n];
+    }
+}

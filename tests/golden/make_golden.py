@@ -9,8 +9,14 @@ workloads and stores compact outputs:
   cutoff sphere, in half-box index order) and the density checksums.
 * ``ref_main_<name>.npz`` -- the reference's main() run from its own input
   files (ELCIN, CONTROL, IONIN, .vpp written by cpsd_b200.refio): the printed
-  per-iteration lines and final energy table.  This pins the table setup
-  (G, mask at the grid cutoff, tg/vc/vg, Ewald constant) to main.c's.
+  per-iteration lines and final energy table, the printed epilogue tables
+  (orthonormality, orbital energies), the packed c1 of ELCOUT and the text
+  of IONOUT.  This pins the table setup (G, mask at the grid cutoff,
+  tg/vc/vg, Ewald constant) and the epilogue to main.c's.
+* ``ref_epi_<name>.npz`` -- the epilogue of main.c:452-487 after the last
+  call, with the reference's own gcdotc and eigsrt and the LAPACK dsyev /
+  BLAS dgemm of the OpenBLAS the reference build links: the orthonormality
+  matrix, eigenvalues, eigenvectors and the packed rotated c1 (first 8 bands).
 * ``inputs.json`` -- SHA-256 of the generated inputs, so a change of the
   input builder is caught before parity is compared.
 
@@ -44,6 +50,12 @@ CASES = [
     ("small_diamond_48", lambda: configs.small_diamond(48, 6, ecut=30.0), 2, 2, 6),
     ("h2_dimer_32", lambda: configs.h2_dimer_32(), 200, 1, 1),
     ("diamond8_64", lambda: configs.diamond8_64(), 4, 2, 4),
+]
+
+# epilogue (main.c:452-487) after the calls: (name, spec builder, calls, inner)
+EPILOGUE_CASES = [
+    ("small_diamond_24", lambda: configs.small_diamond(24, 4), 3, 2),
+    ("small_diamond_32_40", lambda: configs.small_diamond(32, 40, ecut=25.0, seed=12), 2, 2),
 ]
 
 
@@ -99,6 +111,28 @@ def run_case(ref, name, mk, ncalls, inner, keep):
     return input_digest(inp)
 
 
+def run_epilogue(ref, name, mk, ncalls, inner):
+    from scipy.linalg import blas
+    inp = inputs.build_inputs(mk())
+    st = oracle.State(inp)
+    for _ in range(ncalls):
+        ref.run(inp, inner, st)
+
+    def ref_sort(D, V):  # the reference's eigsrt on a column-major copy
+        n = len(D)
+        Vc = np.ascontiguousarray(V.T).ravel()
+        ref.eigsrt(D, Vc, n)
+        V[:, :] = Vc.reshape(n, n).T
+
+    ep = oracle.epilogue(inp, st, ref.gcdotc, sort=ref_sort,
+                         matmul=lambda A, B: blas.dgemm(1.0, np.asfortranarray(A), np.asfortranarray(B)))
+    np.savez_compressed(os.path.join(HERE, "ref_epi_%s.npz" % name), ortho=ep["ortho"], eig=ep["eig"],
+                        vec=ep["vec"], c1=packed(inp, ep["c1"], min(8, inp.nbands)), hml=st.hml,
+                        E=st.E.copy(), ncalls=np.array(ncalls), inner=np.array(inner))
+    print("epilogue(%s): eig %s" % (name, np.array2string(ep["eig"][:4], precision=6)))
+    return input_digest(inp)
+
+
 def run_main(name, mk, inner, outer):
     """The reference's own main() on files written in its formats (grid cutoff)."""
     spec = mk()
@@ -111,12 +145,19 @@ def run_main(name, mk, inner, outer):
         refio.write_reference_inputs(d, inp, inner=inner, outer=outer)
         out = subprocess.run([exe], cwd=d, capture_output=True, check=True).stdout.decode("utf-8", "replace")
         elc = refio.read_elcin(os.path.join(d, "ELCOUT"))
+        with open(os.path.join(d, "IONOUT")) as f:
+            ionout = f.read()
     rows, final = refio.parse_reference_stdout(out)
+    ortho, eig = refio.parse_reference_epilogue(out)
     np.savez_compressed(os.path.join(HERE, "ref_main_%s.npz" % name), rows=np.array(rows),
                         final=np.array([final[i] for i in range(10)]), inner=np.array(inner),
                         outer=np.array(outer), ecut=np.array(spec.ecut_ry),
                         elcout_norms=np.array([np.sum(elc["c"].reshape(inp.nbands, -1)[b] ** 2)
-                                               for b in range(inp.nbands)]))
+                                               for b in range(inp.nbands)]),
+                        ortho_printed=np.array(ortho), eig_printed=np.array(eig),
+                        elcout_header=np.array([elc["icube"], elc["nfft"], elc["ispin"], *elc["ne"]]),
+                        elcout_unit=np.array(elc["unit"]), elcout_c1=packed(inp, elc["c"], inp.nbands),
+                        ionout=np.array(ionout))
     print("main(%s): %d iterations, E=%.10f" % (name, len(rows), final[0]))
     return input_digest(inp)
 
@@ -126,6 +167,8 @@ def main():
     digests = {}
     for name, mk, ncalls, inner, keep in CASES + MOVE_CASES:
         digests[name] = run_case(ref, name, mk, ncalls, inner, keep)
+    for name, mk, ncalls, inner in EPILOGUE_CASES:
+        digests["epi_" + name] = run_epilogue(ref, name, mk, ncalls, inner)
     digests["main_small_diamond_24"] = run_main("small_diamond_24", lambda: configs.small_diamond(24, 4), 2, 3)
     with open(os.path.join(HERE, "inputs.json"), "w") as f:
         json.dump(digests, f, indent=1, sort_keys=True)

@@ -461,3 +461,88 @@ def test_mixed_precision_tracks_fp64(restatement):
     restatement.run(inp, 1, probe)
     assert abs(cell.E[0] - probe.E[0]) < E_TOL
     cell.close()
+
+
+# epilogue of main.c:452-487 (tests/golden/make_golden.py EPILOGUE_CASES)
+from test_oracle import EPI_CASES, align_bands, align_columns  # noqa: E402
+
+
+def _packed_bands(inp, c, nb):
+    pts = np.flatnonzero(inp.masker1)
+    return c.reshape(inp.nbands, inp.nfft3d, 2)[:nb, pts, :]
+
+
+@pytest.mark.parametrize("name", list(EPI_CASES))
+def test_epilogue_matches_reference(golden, name):
+    """On the device: the orthonormality table, the eigenpairs of hml
+    (descending, the reference's eigsrt order; Jacobi vectors compared up to
+    each column's sign) and c1 <- c2 V, against the reference's own gcdotc,
+    eigsrt and LAPACK after the same cpsd() calls."""
+    g = golden("epi_" + name)
+    inp = inputs.build_inputs(EPI_CASES[name]())
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    for _ in range(int(g["ncalls"])):
+        cell.run(int(g["inner"]))
+    before = api.State(inp)
+    cell.get_state(before)
+    assert np.abs(before.hml - g["hml"]).max() < 1e-9
+    ep = cell.epilogue()
+    after = api.State(inp)
+    cell.get_state(after)
+    cell.close()
+    m = int(inp.ne[0])
+    assert np.abs(ep["ortho"] - g["ortho"]).max() < 1e-12
+    assert np.abs(ep["eig"] - g["eig"]).max() < 1e-9
+    V, Vg = ep["vec"][:m * m].reshape(m, m).T, g["vec"][:m * m].reshape(m, m).T
+    assert np.abs(align_columns(Vg, V) - Vg).max() < 1e-8
+    assert np.abs(V.T @ V - np.eye(m)).max() < 1e-13
+    got = _packed_bands(inp, after.c1, g["c1"].shape[0])
+    assert np.abs(align_bands(g["c1"], got) - g["c1"]).max() < 1e-9
+    assert np.array_equal(after.c2, before.c2)  # the epilogue leaves c2 alone
+
+
+def test_epilogue_files_reproduce_reference_main(tmp_path):
+    """The reference main()'s run (ELCIN/CONTROL/IONIN from the same inputs)
+    finished on the device: printed orbital energies, the ELCOUT the library
+    writes (header bytes, c1 up to each band's sign) and IONOUT's text."""
+    from cpsd_b200 import refio
+    g = np.load(os.path.join(GOLDEN, "ref_main_small_diamond_24.npz"))
+    spec = configs.small_diamond(24, 4)
+    spec.ecut_ry = float(g["ecut"])
+    inp = inputs.build_inputs(spec)
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    for _ in g["rows"]:
+        cell.run(int(g["inner"]))
+    ep = cell.epilogue()
+    st = api.State(inp)
+    cell.get_state(st)
+    cell.close()
+    m = int(inp.ne[0])
+    for ms, i, j, w in g["ortho_printed"]:
+        assert abs(ep["ortho"][int(i) - 1 + (int(j) - 1) * m] - w) <= 5e-8 * abs(w) + 1e-15
+    assert np.allclose(ep["eig"], g["eig_printed"], rtol=1e-7, atol=0)
+    path = str(tmp_path / "ELCOUT")
+    api.write_elcout(path, inp, st.c1)
+    back = refio.read_elcin(path)
+    icube, nfft, ispin, ne0, ne1 = (int(x) for x in g["elcout_header"])
+    assert (back["icube"], back["nfft"], back["ispin"], back["ne"]) == (icube, nfft, ispin, (ne0, ne1))
+    assert back["unit"] == float(g["elcout_unit"])
+    got = _packed_bands(inp, back["c"], inp.nbands)
+    assert np.abs(align_bands(g["elcout_c1"], got) - g["elcout_c1"]).max() < 1e-9
+    assert not np.delete(back["c"].reshape(inp.nbands, inp.nfft3d, 2), np.flatnonzero(inp.masker1), axis=1).any()
+    path = str(tmp_path / "IONOUT")
+    api.write_ionout(path, inp, ["C0.vpp"], st.r2)
+    with open(path) as f:
+        assert f.read() == str(g["ionout"])
+
+
+def test_epilogue_needs_a_run():
+    inp = inputs.build_inputs(configs.small_diamond(24, 4))
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    with pytest.raises(lib.CpsdError) as e:
+        cell.epilogue()
+    assert e.value.status == lib.CPSD_ERR_ARG
+    cell.close()

@@ -115,6 +115,8 @@ def test_inputs_match_fixture_digests():
         want = json.load(f)
     for name, (mk, _, _) in list(CASES.items()) + list(MOVE_CASES.items()):
         assert input_digest(inputs.build_inputs(mk())) == want[name], name
+    for name, mk in EPI_CASES.items():
+        assert input_digest(inputs.build_inputs(mk())) == want["epi_" + name], name
 
 
 def test_orbitals_orthonormal_and_hermitian():
@@ -203,3 +205,87 @@ def test_lagrange_off_by_one_quirk_single_band(restatement):
     st = oracle.State(inp)
     restatement.run(inp, 3, st)
     assert st.lagrange_fail == 3
+
+
+# epilogue of main.c:452-487 (tests/golden/make_golden.py EPILOGUE_CASES)
+EPI_CASES = {
+    "small_diamond_24": lambda: configs.small_diamond(24, 4),
+    "small_diamond_32_40": lambda: configs.small_diamond(32, 40, ecut=25.0, seed=12),
+}
+
+
+def align_columns(ref, got):
+    """got with each column's sign chosen to match ref (an eigenvector's
+    sign is not fixed by the problem); columns are the last axis."""
+    s = np.sign((ref.reshape(-1, ref.shape[-1]) * got.reshape(-1, got.shape[-1])).sum(axis=0))
+    s[s == 0] = 1.0
+    return got * s
+
+
+def align_bands(ref, got):
+    """Packed orbitals (band, point, re/im): each band's sign chosen to match ref."""
+    s = np.sign(np.einsum("bpc,bpc->b", ref, got))
+    s[s == 0] = 1.0
+    return got * s[:, None, None]
+
+
+def _packed(inp, c, nb):
+    pts = np.flatnonzero(inp.masker1)
+    return c.reshape(inp.nbands, inp.nfft3d, 2)[:nb, pts, :]
+
+
+@pytest.mark.parametrize("name", list(EPI_CASES))
+def test_restatement_epilogue_matches_reference(restatement, golden, name):
+    """Orthonormality table, eigenpairs of hml (descending, eigsrt order) and
+    c1 <- c2 V, from the restatement's state, against the reference's own
+    gcdotc / eigsrt and its LAPACK."""
+    g = golden("epi_" + name)
+    inp = inputs.build_inputs(EPI_CASES[name]())
+    st = oracle.State(inp)
+    for _ in range(int(g["ncalls"])):
+        restatement.run(inp, int(g["inner"]), st)
+    assert np.abs(st.hml - g["hml"]).max() < 1e-9
+    ep = oracle.epilogue(inp, st, restatement.gcdotc)
+    m = int(inp.ne[0])
+    assert np.abs(ep["ortho"] - g["ortho"]).max() < 1e-12
+    assert np.abs(ep["eig"] - g["eig"]).max() < 1e-9
+    assert np.all(np.diff(ep["eig"][:m]) <= 0)
+    V, Vg = ep["vec"][:m * m].reshape(m, m).T, g["vec"][:m * m].reshape(m, m).T
+    assert np.abs(align_columns(Vg, V) - Vg).max() < 1e-8
+    got = _packed(inp, ep["c1"], g["c1"].shape[0])
+    assert np.abs(align_bands(g["c1"], got) - g["c1"]).max() < 1e-9
+
+
+def test_restatement_epilogue_matches_reference_main(restatement, tmp_path):
+    """The reference main()'s printed epilogue tables, its ELCOUT and its
+    IONOUT: the restatement's epilogue and this library's file writers
+    (host code, no GPU) reproduce them."""
+    from cpsd_b200 import api, refio
+    g = np.load(os.path.join(GOLDEN, "ref_main_small_diamond_24.npz"))
+    spec = configs.small_diamond(24, 4)
+    spec.ecut_ry = float(g["ecut"])
+    inp = inputs.build_inputs(spec)
+    st = oracle.State(inp)
+    for _ in g["rows"]:
+        restatement.run(inp, int(g["inner"]), st)
+    ep = oracle.epilogue(inp, st, restatement.gcdotc)
+    m = int(inp.ne[0])
+    for ms, i, j, w in g["ortho_printed"]:
+        assert abs(ep["ortho"][int(i) - 1 + (int(j) - 1) * m] - w) <= 5e-8 * abs(w) + 1e-15
+    assert np.allclose(ep["eig"], g["eig_printed"], rtol=1e-7, atol=0)
+    got = _packed(inp, ep["c1"], inp.nbands)
+    assert np.abs(align_bands(g["elcout_c1"], got) - g["elcout_c1"]).max() < 1e-9
+    # ELCOUT and IONOUT through the library's writers
+    path = str(tmp_path / "ELCOUT")
+    api.write_elcout(path, inp, ep["c1"])
+    back = refio.read_elcin(path)
+    icube, nfft, ispin, ne0, ne1 = (int(x) for x in g["elcout_header"])
+    assert (back["icube"], back["nfft"], back["ispin"], back["ne"]) == (icube, nfft, ispin, (ne0, ne1))
+    assert back["unit"] == float(g["elcout_unit"])
+    assert np.array_equal(back["c"], ep["c1"])
+    assert os.path.getsize(path) == 4 * 2 + 8 + 4 * 3 + 8 * inp.nbands * inp.n2ft3d
+    path = str(tmp_path / "IONOUT")
+    api.write_ionout(path, inp, ["C0.vpp"], st.r2)
+    with open(path) as f:
+        assert f.read() == str(g["ionout"])
+
