@@ -183,6 +183,42 @@ def cpu_reference(inp, budget_s, min_calls=3, inner=1):
     return calls * inner / dt, kind, calls, dt
 
 
+def time_kbpp(nfft=128, lmax=3, unit=20.5, reps=3, ref=True):
+    """The input pipeline's KB tables (cpsd_gpu_kbpp: host arrays in and out,
+    copies included) on the 128^3 grid of the 64-atom cell, s+p+d channels,
+    501 radial points; beside it the reference's own kbpp() (oracle/_ref,
+    one host thread, as the formatter runs) on the same table and grid."""
+    import numpy as np
+    from cpsd_b200 import api, inputs, psp
+    t = psp.radial_table(lmax, seed=3)
+    _, _, unitg = inputs.get_cube(1, unit)
+    G = inputs.get_g(nfft, unitg)
+    nfft3d = (nfft // 2 + 1) * nfft * nfft
+    api.kbpp(t, G, nfft3d)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        vl, vnl, _, _ = api.kbpp(t, G, nfft3d)
+    gpu_s = (time.perf_counter() - t0) / reps
+    out = {"grid": nfft, "g_points": nfft3d, "radial_points": t.nrho, "lmax": lmax,
+           "gpu_e2e_ms": round(gpu_s * 1e3, 3), "timing": "host wall clock around the C-ABI call, mean of %d" % reps,
+           "bytes_h2d": 8 * (3 * nfft3d + (2 * lmax + 3) * t.nrho),
+           "bytes_d2h": 8 * (1 + lmax * lmax) * nfft3d}
+    if ref:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle  # test infrastructure: only the baseline leg runs it
+        try:
+            t0 = time.perf_counter()
+            rvl, rvnl, _, _ = oracle.reference_kbpp(t.zv, lmax, t.rho, t.vp, t.wp, t.drho, G, nfft3d)
+            ref_s = time.perf_counter() - t0
+            out["reference_cpu_s"] = round(ref_s, 3)
+            out["reference_cores"] = 1
+            out["speedup_e2e"] = round(ref_s / gpu_s, 1)
+            out["max_rel_diff_vl"] = float(np.abs(vl - rvl).max() / np.abs(rvl).max())
+        except FileNotFoundError:
+            out["reference_cpu_s"] = None
+    return out
+
+
 # ----------------------------------------------------------------- GPU arm
 def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True, precision=0, gemm=0):
     """Device time of `steps` cpsd() calls of `inner` SD steps on a resident
@@ -452,6 +488,8 @@ def main():
                           "ms_per_sd_step": tmt / (3 * args.inner),
                           "phases_ms": {k: round(v, 4) for k, v in ph3t.items()}}
         line["extra"] = extra
+        # input pipeline: KB tables of a tabulated psp on the 128^3 grid
+        extra["kbpp_128"] = time_kbpp()
         extra["diamond64_128"] = {
             "value": 3 * args.inner / (tms * 1e-3), "unit": "steps/s",
             "ms_per_sd_step": tms / (3 * args.inner), "npw": big.npw, "nbands": big.nbands,

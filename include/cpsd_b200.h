@@ -188,6 +188,30 @@ int cpsd_write_elcout(const char *path, int icube, int nfft, double unit, int is
 int cpsd_write_ionout(const char *path, int nkatm, const char *const *fname, const int *lmax, int nion,
                       const int *katm, const double *r2);
 
+/*
+ * Input pipeline.  Replaces kbpp() of ckbppv3/dkbppv3.c (kbppv3.c:335-444),
+ * same arguments and meanings: Kleinman-Bylander tables on the half-box G
+ * grid (G as get_g lays it out, 3 * nfft3d) from tabulated radial data --
+ * rho[nrho] on a uniform grid of step drho, vp and wp [(lmax+1) * nrho],
+ * channel lmax the local one.  As kbpp() does, vp's nonlocal channels are
+ * replaced by vp_l - vp_lmax.  Out: vl[nfft3d], vnl[lmax^2 * nfft3d],
+ * vnlnrm[lmax^2].  The per-G integrals run on the GPU (one thread per G;
+ * the tables in shared memory), lmax <= 3, nrho <= 4095.
+ */
+int cpsd_gpu_kbpp(double zv, int lmax, int nrho, double drho, const double *rho, double *vp, const double *wp,
+                  int nfft3d, const double *G, double *vl, double *vnl, double *vnlnrm);
+
+/*
+ * The initial orbitals of cmakepsi/dmakepsi.c:93-140: one plane wave per
+ * band from PSI0.DAT rows (waves[4n..4n+3] = i j k l; coefficient 1, 1/sqrt(2)
+ * or i/sqrt(2) for l = 0, > 0, < 0; on the kx = 0 plane also the Hermitian
+ * partner), written into psi[(ne[0] + ne[1]) * (nfft+2)*nfft*nfft] in the
+ * ELCIN layout; spin 1 reuses the first ne[1] rows, as the reference does.
+ * Host code (a few stores per band); cpsd_write_elcout writes the file.
+ * CPSD_ERR_ARG for an index outside the half box.
+ */
+int cpsd_makepsi(int nfft, int ispin, const int *ne, const int *waves, double *psi);
+
 /* Sphere size (packed G vectors per band) and the kernel launches of one SD step. */
 int cpsd_gpu_npw(const cpsd_gpu_ctx *c);
 int cpsd_gpu_launches_per_step(const cpsd_gpu_ctx *c);

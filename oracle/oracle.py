@@ -122,6 +122,29 @@ def _fft(fn, A: np.ndarray, nfft: int) -> None:
        None, i(0))
 
 
+KBPP_SO = os.path.join(HERE, "_ref", "libkbpp_ref.so")
+
+
+def reference_kbpp(zv: float, lmax: int, rho: np.ndarray, vp: np.ndarray, wp: np.ndarray, drho: float,
+                   G: np.ndarray, nfft3d: int, path: str = KBPP_SO):
+    """The reference's own kbpp() (ckbppv3/dkbppv3.c, compiled unmodified into
+    oracle/_ref/libkbpp_ref.so): returns (vl, vnl, vnlnrm, vp after the call)."""
+    if not os.path.exists(path):
+        raise FileNotFoundError(path + " (build with: make -C oracle ref)")
+    lib = ctypes.CDLL(path)
+    D = ctypes.c_double
+    vp = np.array(vp, dtype=np.float64)
+    lmmax = lmax * lmax
+    vl = np.zeros(nfft3d)
+    vnl = np.zeros(max(lmmax, 1) * nfft3d)
+    vnlnrm = np.zeros(max(lmmax, 1))
+    lib.kbpp(D(zv), ctypes.c_int(lmax), ctypes.c_int(len(rho)), D(drho),
+             _ptr(np.ascontiguousarray(rho, dtype=np.float64)), _ptr(vp),
+             _ptr(np.ascontiguousarray(wp, dtype=np.float64)), ctypes.c_int(nfft3d),
+             _ptr(np.ascontiguousarray(G, dtype=np.float64)), _ptr(vl), _ptr(vnl), _ptr(vnlnrm))
+    return vl, vnl[:lmmax * nfft3d], vnlnrm[:lmmax], vp
+
+
 class ReferenceBuild:
     """The reference's own cpsd() (oracle/_ref/libcpsd_ref.so)."""
 
@@ -240,3 +263,82 @@ def epilogue(inp, st: State, gcdotc, sort=eigsrt, matmul=None) -> dict:
         C1 = matmul(C2, V) if matmul else C2 @ V
         c1[b0 * n2:(b0 + m) * n2] = C1.T.ravel()
     return {"ortho": ortho, "eig": eig, "vec": vec, "c1": c1}
+
+
+def simp(f: np.ndarray, h: float) -> np.ndarray:
+    """simp() of ckbppv3/dkbppv3.c along the last axis:
+    h/3 (2 sum_even f + 4 sum_odd f - f_0 - f_{n-1})."""
+    s = 2.0 * f[..., 0::2].sum(axis=-1) + 4.0 * f[..., 1::2].sum(axis=-1) - f[..., 0] - f[..., -1]
+    return s * (h / 3.0)
+
+
+def kbpp(zv: float, lmax: int, rho: np.ndarray, vp: np.ndarray, wp: np.ndarray, drho: float,
+         G: np.ndarray, nfft3d: int, chunk: int = 2048):
+    """kbpp() of ckbppv3/dkbppv3.c (kbppv3.c:335-444) restated with numpy:
+    returns (vl, vnl, vnlnrm, vp with its nonlocal channels minus the local one)."""
+    n = len(rho)
+    vp = np.array(vp, dtype=np.float64).reshape(lmax + 1, n)
+    wp = np.asarray(wp, dtype=np.float64).reshape(lmax + 1, n)
+    for l in range(lmax):
+        vp[l] -= vp[lmax]
+    lmmax = lmax * lmax
+    vnlnrm = np.zeros(lmmax)
+    for l in range(lmax):
+        vnlnrm[l * l:(l + 1) * (l + 1)] = simp(vp[l] * wp[l] * wp[l], drho)
+    fourpi = 4.0 * np.pi
+    p0, p1, p2 = np.sqrt(fourpi), np.sqrt(3.0 * fourpi), np.sqrt(15.0 * fourpi)
+    vl = np.zeros(nfft3d)
+    vnl = np.zeros((lmmax, nfft3d))
+    G = np.asarray(G).reshape(3, nfft3d)
+    for k0 in range(1, nfft3d, chunk):
+        k = np.arange(k0, min(nfft3d, k0 + chunk))
+        g = G[:, k]
+        q = np.sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2])
+        gx, gy, gz = g[0] / q, g[1] / q, g[2] / q
+        x = q[:, None] * rho[None, :]
+        sn, cs = np.sin(x), np.cos(x)
+        if lmax > 2:
+            a = 3.0 * (sn / x - cs) / x - sn
+            f = a * wp[2] * vp[2]
+            f[:, 0] = 0.0
+            d = p2 * simp(f, drho) / q
+            vnl[4, k] = d * (3.0 * gz * gz - 1.0) / (2.0 * np.sqrt(3.0))
+            vnl[5, k] = d * gx * gy
+            vnl[6, k] = d * gy * gz
+            vnl[7, k] = d * gz * gx
+            vnl[8, k] = d * (gx * gx - gy * gy) / 2.0
+        if lmax > 1:
+            f = (sn / x - cs) * wp[1] * vp[1]
+            f[:, 0] = 0.0
+            p = p1 * simp(f, drho) / q
+            vnl[1, k], vnl[2, k], vnl[3, k] = p * gx, p * gy, p * gz
+        if lmax > 0:
+            vnl[0, k] = p0 * simp(sn * wp[0] * vp[0], drho) / q
+        vl[k] = simp(rho * vp[lmax] * sn, drho) * fourpi / q - zv * fourpi * cs[:, -1] / (q * q)
+    vl[0] = fourpi * simp(vp[lmax] * (rho * rho), drho) + 2.0 * np.pi * zv * rho[-1] * rho[-1]
+    if lmax > 0:
+        vnl[0, 0] = p0 * simp(rho * wp[0] * vp[0], drho)
+    return vl, vnl.ravel(), vnlnrm, vp.ravel()
+
+
+def makepsi(nfft: int, ispin: int, ne, waves) -> np.ndarray:
+    """cmakepsi/dmakepsi.c:93-140 restated: one plane wave per band (PSI0.DAT
+    rows i j k l), its Hermitian partner on the kx = 0 plane; spin 1 reuses
+    the first ne[1] rows."""
+    nh = nfft // 2 + 1
+    nfft3 = (nfft + 2) * nfft * nfft
+    s = 1.0 / np.sqrt(2.0)
+    bands = []
+    for ms in range(ispin):
+        for n in range(int(ne[ms])):
+            i, j, k, l = (int(v) for v in waves[n])
+            c = (0.0, s) if l < 0 else ((1.0, 0.0) if l == 0 else (s, 0.0))
+            b = np.zeros(nfft3)
+            k2, k3 = (j + nfft) % nfft, (k + nfft) % nfft
+            idx = 2 * (i + k2 * nh + k3 * nh * nfft)
+            b[idx], b[idx + 1] = c
+            if i == 0:
+                idx = 2 * (((nfft - k2) % nfft) * nh + ((nfft - k3) % nfft) * nh * nfft)
+                b[idx], b[idx + 1] = c[0], -c[1]
+            bands.append(b)
+    return np.concatenate(bands)

@@ -388,6 +388,41 @@ def write_ionout(path: str, inp, fnames, r2: np.ndarray) -> None:
         raise CpsdError(rc, "cpsd_write_ionout")
 
 
+def kbpp(table, G: np.ndarray, nfft3d: int):
+    """Kleinman-Bylander tables on the half-box grid from a radial table
+    (ckbppv3/dkbppv3.c kbpp(), on the GPU): returns (vl, vnl, vnlnrm, vp)
+    with vp's nonlocal channels replaced by vp_l - vp_lmax, as kbpp() leaves
+    them."""
+    L = _l.load()
+    lmax = int(table.lmax)
+    vp = np.array(table.vp, dtype=np.float64)
+    vl = np.zeros(nfft3d)
+    vnl = np.zeros(max(lmax * lmax, 1) * nfft3d)
+    vnlnrm = np.zeros(max(lmax * lmax, 1))
+    rc = L.cpsd_gpu_kbpp(float(table.zv), lmax, int(table.nrho), float(table.drho),
+                         _ptr(np.ascontiguousarray(table.rho, dtype=np.float64)), _ptr(vp),
+                         _ptr(np.ascontiguousarray(table.wp, dtype=np.float64)), int(nfft3d),
+                         _ptr(np.ascontiguousarray(G, dtype=np.float64)), _ptr(vl), _ptr(vnl), _ptr(vnlnrm))
+    if rc:
+        raise CpsdError(rc, "cpsd_gpu_kbpp")
+    return vl, vnl[:lmax * lmax * nfft3d], vnlnrm[:lmax * lmax], vp
+
+
+def makepsi(nfft: int, ispin: int, ne, waves) -> np.ndarray:
+    """The initial plane-wave orbitals of cmakepsi/dmakepsi.c in the ELCIN
+    layout; waves: the PSI0.DAT rows (i, j, k, l), at least ne[0] of them."""
+    L = _l.load()
+    ne = np.ascontiguousarray(ne, dtype=np.int32)
+    w = np.ascontiguousarray(np.asarray(waves, dtype=np.int32)[:int(ne[0])].ravel())
+    if w.size != 4 * int(ne[0]):
+        raise ValueError("need ne[0] rows of (i, j, k, l)")
+    psi = np.zeros((int(ne[0]) + (int(ne[1]) if ispin == 2 else 0)) * (nfft + 2) * nfft * nfft)
+    rc = L.cpsd_makepsi(int(nfft), int(ispin), _ptr(ne), _ptr(w), _ptr(psi))
+    if rc:
+        raise CpsdError(rc, "cpsd_makepsi")
+    return psi
+
+
 def dropin_counters():
     """Counters of the context the drop-in cpsd() keeps between calls."""
     L = _l.load()

@@ -50,7 +50,7 @@ EXPORTS = [
     "cpsd_gpu_set_preconditioner_range", "cpsd_gpu_save_orbitals", "cpsd_gpu_restore_orbitals",
     "cpsd_gpu_get_packed", "cpsd_gpu_set_packed", "cpsd_gpu_get_sphere", "cpsd_gpu_set_gemm",
     "cpsd_overlap_tn", "cpsd_overlap_tn_noalloc", "cpsd_gpu_epilogue", "cpsd_write_elcout",
-    "cpsd_write_ionout",
+    "cpsd_write_ionout", "cpsd_gpu_kbpp", "cpsd_makepsi",
 ]
 
 
@@ -89,6 +89,8 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_gpu_run.argtypes = [_P, _I, _I, _P, _P, _P, _P]
     lib.cpsd_gpu_get_state.argtypes = [_P] + [_P] * 9
     lib.cpsd_gpu_epilogue.argtypes = [_P, _P, _P, _P]
+    lib.cpsd_gpu_kbpp.argtypes = [_D, _I, _I, _D, _P, _P, _P, _I, _P, _P, _P, _P]
+    lib.cpsd_makepsi.argtypes = [_I, _I, _P, _P, _P]
     lib.cpsd_write_elcout.argtypes = [ctypes.c_char_p, _I, _I, _D, _I, _P, _P]
     lib.cpsd_write_ionout.argtypes = [ctypes.c_char_p, _I, ctypes.POINTER(ctypes.c_char_p), _P, _I, _P, _P]
     lib.cpsd_gpu_npw.argtypes = [_P]

@@ -39,10 +39,12 @@ def read_elcin(path: str):
 
 def write_vpp(path: str, icube: int, nfft: int, unit: float, atom: str, amass: float,
               zv: float, lmax: int, rc: Sequence[float], vnlnrm: np.ndarray,
-              vl: np.ndarray, vnl: np.ndarray) -> None:
+              vl: np.ndarray, vnl: np.ndarray, pad: str = " ") -> None:
+    """pad fills a one-letter atom name: the psp formatter's own files carry
+    the string terminator there (pad="\\0", its fscanf("%s") into char[2])."""
     lmmax = lmax * lmax
     nfft3d = (nfft // 2 + 1) * nfft * nfft
-    a = (atom + "  ")[:2].encode()
+    a = (atom + pad + pad)[:2].encode("latin-1")
     with open(path, "wb") as f:
         f.write(struct.pack("=iid", icube, nfft, unit))
         f.write(a)
@@ -160,3 +162,34 @@ def parse_reference_epilogue(text: str):
                 if "(" in chunk:
                     eig.append(float(chunk.split("(")[0]))
     return ortho, eig
+
+
+def read_vpp(path: str):
+    """A ``.vpp`` file (the formatter's DATAOUT), as main.c:264-284 reads it."""
+    with open(path, "rb") as f:
+        icube, nfft, unit = struct.unpack("=iid", f.read(16))
+        atom = f.read(2).decode("latin-1")
+        amass, zv, lmax = struct.unpack("=ddi", f.read(20))
+        nfft3d = (nfft // 2 + 1) * nfft * nfft
+        lmmax = lmax * lmax
+        rd = lambda m: np.frombuffer(f.read(8 * m), dtype=np.float64).copy()  # noqa: E731
+        rc = rd(lmax + 1)
+        vnlnrm = rd(lmmax)
+        vl = rd(nfft3d)
+        vnl = rd(lmmax * nfft3d)
+    return dict(icube=icube, nfft=nfft, unit=unit, atom=atom, amass=amass, zv=zv, lmax=lmax, rc=rc,
+                vnlnrm=vnlnrm, vl=vl, vnl=vnl)
+
+
+def write_aimd_param(path: str, icube: int, unit: float, nfft: int, ispin: int, ne: Sequence[int]) -> None:
+    """aimd.param as dkbppv3.c / dmakepsi.c read it: icube, unit, nfft, ispin ne0 ne1."""
+    with open(path, "w") as f:
+        f.write("%d %.17e %d\n%d %d %d\n" % (icube, unit, nfft, ispin, int(ne[0]), int(ne[1])))
+
+
+def write_psi0(path: str, waves) -> None:
+    """PSI0.DAT: one row "i j k l" per band (cmakepsi/dmakepsi.c:93-107)."""
+    with open(path, "w") as f:
+        for i, j, k, l in waves:
+            f.write(" %d %d %d %d\n" % (i, j, k, l))
+

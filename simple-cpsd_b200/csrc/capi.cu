@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "cpsd_b200.h"
 #include "fft.cuh"
+#include "pipeline.cuh"
 
 namespace {
 
@@ -123,6 +124,125 @@ extern "C" void cpsd(const int inner, const int move, const int nion, const int 
         printf("ierr=10\n");  // the reference's message for the same condition (cpsd.c:477)
     else if (rc != CPSD_OK)
         printf("cpsd (B200): error %d: %s\n", rc, cpsd_gpu_strerror(rc));
+}
+
+// ====================================================================== input pipeline
+namespace {
+
+// simp() of ckbppv3/dkbppv3.c, in its order of operations
+double host_simp(int n, const double *y, double h)
+{
+    double s2 = 0.0, s4 = 0.0;
+    for (int i = 0; i < n; i += 2) s2 += y[i];
+    for (int i = 1; i < n; i += 2) s4 += y[i];
+    double s = 2.0 * s2 + 4.0 * s4 - y[0] - y[n - 1];
+    return s * (h / 3.0);
+}
+
+struct DevBuf {
+    double *p = nullptr;
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+extern "C" int cpsd_gpu_kbpp(double zv, int lmax, int nrho, double drho, const double *rho, double *vp,
+                             const double *wp, int nfft3d, const double *G, double *vl, double *vnl,
+                             double *vnlnrm)
+{
+    if (lmax < 0 || lmax > 3 || nrho < 2 || nrho > kKbppMaxRho || nfft3d < 1 || !rho || !vp || !wp || !G ||
+        !vl || (lmax > 0 && (!vnl || !vnlnrm)))
+        return CPSD_ERR_ARG;
+    const long N = nfft3d, n = nrho, lmmax = (long)lmax * lmax;
+    // kbpp(): nonlocal channels relative to the local one, then their norms
+    for (int l = 0; l < lmax; ++l)
+        for (long i = 0; i < n; ++i) vp[i + l * n] -= vp[i + lmax * n];
+    std::vector<double> f(n);
+    for (int l = 0; l < lmax; ++l) {
+        for (long i = 0; i < n; ++i) f[i] = vp[i + l * n] * wp[i + l * n] * wp[i + l * n];
+        const double a = host_simp(nrho, f.data(), drho);
+        for (int i = l * l; i < (l + 1) * (l + 1); ++i) vnlnrm[i] = a;
+    }
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return CPSD_ERR_CUDA;
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{s};
+    DevBuf dr, dvp, dwp, dG, dvl, dvnl;
+    const size_t tab = sizeof(double) * (lmax + 1) * n;
+    if (cudaMalloc(&dr.p, sizeof(double) * n) != cudaSuccess || cudaMalloc(&dvp.p, tab) != cudaSuccess ||
+        cudaMalloc(&dwp.p, tab) != cudaSuccess || cudaMalloc(&dG.p, sizeof(double) * 3 * N) != cudaSuccess ||
+        cudaMalloc(&dvl.p, sizeof(double) * N) != cudaSuccess ||
+        (lmmax > 0 && cudaMalloc(&dvnl.p, sizeof(double) * lmmax * N) != cudaSuccess))
+        return CPSD_ERR_CUDA;
+    if (cudaMemcpyAsync(dr.p, rho, sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dvp.p, vp, tab, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dwp.p, wp, tab, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dG.p, G, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return CPSD_ERR_CUDA;
+    const size_t smem = kbpp_smem_bytes(nrho);
+    if (cudaFuncSetAttribute(kbpp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return CPSD_ERR_CUDA;
+    KbppArgs a{};
+    a.nfft3d = nfft3d;
+    a.nrho = nrho;
+    a.lmax = lmax;
+    a.drho = drho;
+    a.zv = zv;
+    a.rho = dr.p;
+    a.vp = dvp.p;
+    a.wp = dwp.p;
+    a.G = dG.p;
+    a.vl = dvl.p;
+    a.vnl = dvnl.p;
+    const long blocks = std::max<long>(1, std::min<long>((N + kKbppThreads - 1) / kKbppThreads, 148L * 16));
+    kbpp_kernel<<<(unsigned)blocks, kKbppThreads, smem, s>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return CPSD_ERR_CUDA;
+    if (cudaMemcpyAsync(vl, dvl.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        (lmmax > 0 &&
+         cudaMemcpyAsync(vnl, dvnl.p, sizeof(double) * lmmax * N, cudaMemcpyDeviceToHost, s) != cudaSuccess))
+        return CPSD_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return CPSD_ERR_CUDA;
+    return CPSD_OK;
+}
+
+extern "C" int cpsd_makepsi(int nfft, int ispin, const int *ne, const int *waves, double *psi)
+{
+    if (nfft < 2 || (nfft & 1) || (ispin != 1 && ispin != 2) || !ne || !waves || !psi || ne[0] < 0 ||
+        ne[1] < 0 || (ispin == 2 && ne[1] > ne[0]))
+        return CPSD_ERR_ARG;
+    const int nh = nfft / 2 + 1;
+    const long nfft3 = (long)(nfft + 2) * nfft * nfft;
+    // PSI0.DAT rows "i j k l" (cmakepsi/dmakepsi.c:93-107): G index and the
+    // coefficient: l < 0 -> i/sqrt(2), l == 0 -> 1, l > 0 -> 1/sqrt(2)
+    const double scale = 1.0 / sqrt(2.0);
+    for (int n = 0; n < ne[0]; ++n) {
+        const int i = waves[4 * n], j = waves[4 * n + 1], k = waves[4 * n + 2];
+        if (i < 0 || i >= nh || j <= -nfft || j >= nfft || k <= -nfft || k >= nfft) return CPSD_ERR_ARG;
+    }
+    double *band = psi;
+    for (int ms = 0; ms < ispin; ++ms)
+        for (int n = 0; n < (ms ? ne[1] : ne[0]); ++n) {  // spin 1 reuses the first ne[1] rows (dmakepsi.c:117)
+            const int *w = waves + 4 * n;
+            const int k1 = w[0], k2 = (w[1] + nfft) % nfft, k3 = (w[2] + nfft) % nfft, l = w[3];
+            const double re = l < 0 ? 0.0 : (l == 0 ? 1.0 : scale), im = l < 0 ? scale : 0.0;
+            memset(band, 0, sizeof(double) * nfft3);
+            long idx = 2L * (k1 + (long)k2 * nh + (long)k3 * nh * nfft);
+            band[idx] = re;
+            band[idx + 1] = im;
+            if (k1 == 0) {  // the Hermitian partner on the kx = 0 plane
+                const int kk2 = (nfft - k2) % nfft, kk3 = (nfft - k3) % nfft;
+                idx = 2L * (k1 + (long)kk2 * nh + (long)kk3 * nh * nfft);
+                band[idx] = re;
+                band[idx + 1] = -im;
+            }
+            band += nfft3;
+        }
+    return CPSD_OK;
 }
 
 // ====================================================================== epilogue files

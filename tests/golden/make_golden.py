@@ -17,6 +17,14 @@ workloads and stores compact outputs:
   call, with the reference's own gcdotc and eigsrt and the LAPACK dsyev /
   BLAS dgemm of the OpenBLAS the reference build links: the orthonormality
   matrix, eigenvalues, eigenvectors and the packed rotated c1 (first 8 bands).
+* ``ref_kbpp_<name>.npz`` -- the reference's own kbpp() (ckbppv3/dkbppv3.c,
+  oracle/_ref/libkbpp_ref.so) on a seeded radial table (cpsd_b200.psp):
+  vl, vnl, vnlnrm and vp as the call leaves it; ``ref_kbpp_main.npz`` --
+  the formatter program itself (oracle/_ref/dkbppv3.x) on aimd.param, the
+  table file and its "highest L" prompt: the DATAOUT bytes.
+* ``ref_makepsi.npz`` -- the reference's initial-orbital program
+  (oracle/_ref/dmakepsi.x) on aimd.param and a PSI0.DAT: the ELCIN it
+  writes, as header plus the nonzero entries.
 * ``inputs.json`` -- SHA-256 of the generated inputs, so a change of the
   input builder is caught before parity is compared.
 
@@ -39,7 +47,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(REPO, "simple-cpsd_b200"))
 sys.path.insert(0, os.path.join(REPO, "oracle"))
 
-from cpsd_b200 import configs, inputs, refio  # noqa: E402
+from cpsd_b200 import configs, inputs, psp, refio  # noqa: E402
 import oracle  # noqa: E402
 
 # (name, spec builder, number of cpsd() calls, inner steps per call, bands of c2 kept)
@@ -70,6 +78,76 @@ MOVE_CASES = [
     ("move_small_diamond_24", lambda: _moving(configs.small_diamond(24, 4)), 3, 2, 4),
     ("move_small_diamond_32", lambda: _moving(configs.small_diamond(32, 40, ecut=25.0, seed=12)), 2, 2, 4),
 ]
+
+
+# kbpp(): (name, lmax, table seed, nfft); the cube is icube 1, a = 10.26
+KBPP_CASES = [("l1", 1, 1, 12), ("l2", 2, 2, 12), ("l3", 3, 3, 12)]
+KBPP_UNIT = 10.26
+
+
+def plane_waves(nfft: int, count: int):
+    """PSI0.DAT-style rows: half-box G by increasing |k|^2 (ties in loop
+    order), the first as l = 0, then each G as l = -1 and l = +1."""
+    h = nfft // 2
+    ks = [(i, j, k) for k in range(-h + 1, h) for j in range(-h + 1, h) for i in range(0, h)
+          if (i, j, k) != (0, 0, 0) and (i > 0 or j > 0 or (j == 0 and k > 0))]
+    ks.sort(key=lambda t: t[0] ** 2 + t[1] ** 2 + t[2] ** 2)
+    rows = [(0, 0, 0, 0)]
+    for t in ks:
+        rows += [t + (-1,), t + (1,)]
+    return rows[:count]
+
+
+def table_digest(t) -> str:
+    h = hashlib.sha256()
+    for a in (t.rho, t.vp, t.wp, t.rc, np.array([t.zv, t.amass, t.drho, t.lmax])):
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def run_kbpp(name, lmax, seed, nfft):
+    t = psp.radial_table(lmax, seed=seed)
+    _, _, unitg = inputs.get_cube(1, KBPP_UNIT)
+    nfft3d = (nfft // 2 + 1) * nfft * nfft
+    vl, vnl, vnlnrm, vp = oracle.reference_kbpp(t.zv, lmax, t.rho, t.vp, t.wp, t.drho,
+                                                inputs.get_g(nfft, unitg), nfft3d)
+    np.savez_compressed(os.path.join(HERE, "ref_kbpp_%s.npz" % name), vl=vl, vnl=vnl, vnlnrm=vnlnrm, vp=vp,
+                        lmax=np.array(lmax), seed=np.array(seed), nfft=np.array(nfft))
+    print("kbpp(%s): vl(G=0)=%.10f vnlnrm=%s" % (name, vl[0], np.array2string(vnlnrm, precision=6)))
+    return table_digest(t)
+
+
+def run_kbpp_main(lmax=3, seed=3, nfft=12, highest_l=2):
+    """The formatter program: aimd.param + table file + the prompt's answer."""
+    t = psp.radial_table(lmax, seed=seed)
+    exe = os.path.join(REPO, "oracle", "_ref", "dkbppv3.x")
+    with tempfile.TemporaryDirectory() as d:
+        refio.write_aimd_param(os.path.join(d, "aimd.param"), 1, KBPP_UNIT, nfft, 1, (4, 0))
+        psp.write_table(os.path.join(d, "C.dat"), t)
+        subprocess.run([exe, "C.dat"], cwd=d, input=b"%d\n" % highest_l, capture_output=True, check=True)
+        with open(os.path.join(d, "DATAOUT"), "rb") as f:
+            data = f.read()
+    np.savez_compressed(os.path.join(HERE, "ref_kbpp_main.npz"), dataout=np.frombuffer(data, dtype=np.uint8),
+                        lmax=np.array(lmax), seed=np.array(seed), nfft=np.array(nfft),
+                        highest_l=np.array(highest_l))
+    print("dkbppv3.x: DATAOUT %d bytes" % len(data))
+    return table_digest(t)
+
+
+def run_makepsi(nfft=12, ispin=2, ne=(6, 4)):
+    rows = plane_waves(nfft, ne[0])
+    exe = os.path.join(REPO, "oracle", "_ref", "dmakepsi.x")
+    with tempfile.TemporaryDirectory() as d:
+        refio.write_aimd_param(os.path.join(d, "aimd.param"), 1, KBPP_UNIT, nfft, ispin, ne)
+        refio.write_psi0(os.path.join(d, "PSI0.DAT"), rows)
+        subprocess.run([exe, "ELCIN"], cwd=d, capture_output=True, check=True)
+        elc = refio.read_elcin(os.path.join(d, "ELCIN"))
+    c = elc["c"]
+    nz = np.flatnonzero(c)
+    np.savez_compressed(os.path.join(HERE, "ref_makepsi.npz"), rows=np.array(rows, dtype=np.int32),
+                        header=np.array([elc["icube"], elc["nfft"], elc["ispin"], *elc["ne"]]),
+                        unit=np.array(elc["unit"]), size=np.array(c.size), nz=nz, values=c[nz])
+    print("dmakepsi.x: %d bands, %d nonzeros" % (sum(ne), len(nz)))
 
 
 def input_digest(inp) -> str:
@@ -170,6 +248,10 @@ def main():
     for name, mk, ncalls, inner in EPILOGUE_CASES:
         digests["epi_" + name] = run_epilogue(ref, name, mk, ncalls, inner)
     digests["main_small_diamond_24"] = run_main("small_diamond_24", lambda: configs.small_diamond(24, 4), 2, 3)
+    for name, lmax, seed, nfft in KBPP_CASES:
+        digests["kbpp_" + name] = run_kbpp(name, lmax, seed, nfft)
+    digests["kbpp_main"] = run_kbpp_main()
+    run_makepsi()
     with open(os.path.join(HERE, "inputs.json"), "w") as f:
         json.dump(digests, f, indent=1, sort_keys=True)
     with open(os.path.join(REPO, "oracle", "_ref", "BUILD_INFO.txt")) as f:

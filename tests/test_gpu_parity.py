@@ -546,3 +546,68 @@ def test_epilogue_needs_a_run():
         cell.epilogue()
     assert e.value.status == lib.CPSD_ERR_ARG
     cell.close()
+
+
+# input pipeline (tests/golden/make_golden.py KBPP_CASES, run_kbpp_main)
+from test_oracle import KBPP_CASES, assert_kbpp_close, kbpp_case  # noqa: E402
+
+
+@pytest.mark.parametrize("name", list(KBPP_CASES))
+def test_kbpp_matches_reference(golden, name):
+    """cpsd_gpu_kbpp (one thread per G, the radial tables in shared memory)
+    against the reference's own compiled kbpp() on the same table and grid:
+    s, p and d channels, the local part with its long-range term, G = 0."""
+    g, t, G, nfft3d = kbpp_case(golden, name)
+    got = api.kbpp(t, G, nfft3d)
+    assert_kbpp_close(got, g, 1e-13)
+
+
+def test_psp_formatter_reproduces_reference_dataout(tmp_path):
+    """psp.format_vpp (kbpp on the GPU) writes the .vpp file the reference's
+    formatter program wrote for the same table, grid and "highest L" answer
+    (a lower answer than the table's lmax makes that channel the local one)."""
+    from cpsd_b200 import psp, refio
+    g = np.load(os.path.join(GOLDEN, "ref_kbpp_main.npz"))
+    ref_path = str(tmp_path / "DATAOUT.ref")
+    with open(ref_path, "wb") as f:
+        f.write(g["dataout"].tobytes())
+    t = psp.radial_table(int(g["lmax"]), seed=int(g["seed"]))
+    path = str(tmp_path / "DATAOUT")
+    psp.format_vpp(path, t, 1, 10.26, int(g["nfft"]), int(g["highest_l"]))
+    a, b = refio.read_vpp(path), refio.read_vpp(ref_path)
+    assert os.path.getsize(path) == os.path.getsize(ref_path)
+    with open(path, "rb") as f:
+        assert f.read(38) == g["dataout"].tobytes()[:38]  # icube, nfft, unit, atom, amass, zv, lmax
+    for k in ("icube", "nfft", "unit", "atom", "amass", "zv", "lmax"):
+        assert a[k] == b[k], k
+    assert np.array_equal(a["rc"], b["rc"])
+    assert np.abs(a["vnlnrm"] - b["vnlnrm"]).max() <= 1e-15 * np.abs(b["vnlnrm"]).max()
+    assert np.abs(a["vl"] - b["vl"]).max() <= 1e-13 * np.abs(b["vl"]).max()
+    assert np.abs(a["vnl"] - b["vnl"]).max() <= 1e-13 * np.abs(b["vnl"]).max()
+
+
+def test_pipeline_inputs_drive_the_sd_path(restatement):
+    """Radial table -> kbpp on the GPU -> vl, vnl, vnlnrm; plane-wave start
+    orbitals from makepsi; SD steps on those inputs on the GPU equal the
+    restatement's on the same arrays."""
+    from cpsd_b200 import psp
+    inp = inputs.build_inputs(configs.small_diamond(24, 4, ecut=20.0))
+    t = psp.radial_table(2, seed=2)
+    vl, vnl, vnlnrm, _ = api.kbpp(t, inp.G, inp.nfft3d)
+    inp.vl[:] = vl
+    inp.vnl[:] = 0.0
+    inp.vnl[:4 * inp.nfft3d] = vnl
+    inp.vnlnrm[:] = 0.0
+    inp.vnlnrm[:4] = vnlnrm
+    inp.c2 = api.makepsi(inp.nfft, 1, (4, 0), [(0, 0, 0, 0), (1, 0, 0, -1), (1, 0, 0, 1), (0, 1, 0, -1)])
+    so = oracle.State(inp)
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    for _ in range(2):
+        restatement.run(inp, 2, so)
+        cell.run(2)
+        assert abs(cell.E[0] - so.E[0]) < E_TOL
+    st = api.State(inp)
+    cell.get_state(st)
+    cell.close()
+    assert np.abs(st.c2 - so.c2).max() < 1e-10

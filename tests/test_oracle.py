@@ -289,3 +289,74 @@ def test_restatement_epilogue_matches_reference_main(restatement, tmp_path):
     with open(path) as f:
         assert f.read() == str(g["ionout"])
 
+
+
+# input pipeline: tests/golden/make_golden.py KBPP_CASES, run_kbpp_main, run_makepsi
+KBPP_CASES = {"l1": 1, "l2": 2, "l3": 3}
+
+
+def kbpp_case(golden, name):
+    from cpsd_b200 import psp
+    g = golden("kbpp_" + name)
+    t = psp.radial_table(int(g["lmax"]), seed=int(g["seed"]))
+    nfft = int(g["nfft"])
+    _, _, unitg = inputs.get_cube(1, 10.26)
+    return g, t, inputs.get_g(nfft, unitg), (nfft // 2 + 1) * nfft * nfft
+
+
+def assert_kbpp_close(got, g, rel):
+    vl, vnl, vnlnrm, vp = got
+    scale = np.abs(g["vl"]).max()
+    assert np.abs(vl - g["vl"]).max() <= rel * scale
+    if g["vnl"].size:
+        assert np.abs(vnl - g["vnl"]).max() <= rel * np.abs(g["vnl"]).max()
+    assert np.abs(vnlnrm - g["vnlnrm"]).max() <= rel * max(1.0, np.abs(g["vnlnrm"]).max())
+    assert np.array_equal(vp, g["vp"])  # vp_l - vp_lmax, the same subtraction
+
+
+def test_pipeline_tables_match_fixture_digests():
+    sys.path.insert(0, GOLDEN)
+    from make_golden import KBPP_CASES as KC, table_digest  # noqa: E402
+    from cpsd_b200 import psp
+    with open(os.path.join(GOLDEN, "inputs.json")) as f:
+        want = json.load(f)
+    for name, lmax, seed, _ in KC:
+        assert table_digest(psp.radial_table(lmax, seed=seed)) == want["kbpp_" + name]
+    assert table_digest(psp.radial_table(3, seed=3)) == want["kbpp_main"]
+
+
+@pytest.mark.parametrize("name", list(KBPP_CASES))
+def test_kbpp_restatement_matches_reference(golden, name):
+    """kbpp() restated (numpy) against the reference's own compiled kbpp()."""
+    g, t, G, nfft3d = kbpp_case(golden, name)
+    got = oracle.kbpp(t.zv, t.lmax, t.rho, t.vp, t.wp, t.drho, G, nfft3d)
+    assert_kbpp_close(got, g, 1e-13)
+
+
+def test_psp_table_file_round_trip(tmp_path):
+    """psp.write_table writes what dkbppv3.c main() reads; read_table reads it back."""
+    from cpsd_b200 import psp
+    t = psp.radial_table(3, seed=3)
+    path = str(tmp_path / "C.dat")
+    psp.write_table(path, t)
+    b = psp.read_table(path)
+    assert (b.atom, b.zv, b.amass, b.lmax, b.drho) == (t.atom, t.zv, t.amass, t.lmax, t.drho)
+    for x, y in ((b.rc, t.rc), (b.rho, t.rho), (b.vp, t.vp), (b.wp, t.wp)):
+        assert np.array_equal(x, y)
+
+
+def test_makepsi_matches_reference():
+    """The initial orbitals: the library's host code (no GPU needed) and the
+    restatement against the ELCIN the reference's dmakepsi.x wrote, bit for
+    bit (plane waves, Hermitian partners on kx = 0, spin 1 reusing rows)."""
+    from cpsd_b200 import api
+    g = np.load(os.path.join(GOLDEN, "ref_makepsi.npz"))
+    icube, nfft, ispin, ne0, ne1 = (int(x) for x in g["header"])
+    want = np.zeros(int(g["size"]))
+    want[g["nz"]] = g["values"]
+    for psi in (api.makepsi(nfft, ispin, (ne0, ne1), g["rows"]),
+                oracle.makepsi(nfft, ispin, (ne0, ne1), g["rows"])):
+        assert psi.size == want.size
+        assert np.array_equal(psi, want)
+    with pytest.raises(Exception):
+        api.makepsi(nfft, ispin, (ne0, ne1), [(nfft, 0, 0, 0)] * ne0)  # kx outside the half box
