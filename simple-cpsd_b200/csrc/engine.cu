@@ -3,6 +3,10 @@
 // step is a fixed sequence of kernel launches on the context's stream.
 #include <cuda_runtime.h>
 
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -414,7 +418,6 @@ struct cpsd_gpu_ctx {
     double *beta = nullptr, *coefT = nullptr, *Mov = nullptr, *gws = nullptr, *lag = nullptr;
     double *lmd = nullptr, *hml = nullptr, *Edev = nullptr, *red = nullptr;
     int *chunk_dens = nullptr, *chunk_band = nullptr, *flags = nullptr;
-    double *full = nullptr;  // ispin * n2ft3d: the density in the reference's padded layout
     // epilogue (allocated on first use): Jacobi workspace, eigenpairs, overlaps
     double *eigA = nullptr, *eigV = nullptr, *eigD = nullptr, *eigVec = nullptr, *ortho = nullptr;
     int *eig_sweeps = nullptr;
@@ -427,6 +430,9 @@ struct cpsd_gpu_ctx {
             if (p) cudaFreeHost(p);
         }
     } hstage;
+    Pinned tstage;  // packed tables of cpsd_gpu_set_tables
+    size_t tstage_bytes = 0;
+    Pinned dstage;  // the density (ispin * n^3) on its way to the padded host layout
     int pblocks = 0, bblocks = 0, gblocks = 0;
     double *ppart = nullptr, *bpart = nullptr, *gpart = nullptr;
 };
@@ -1070,6 +1076,38 @@ int batch_step(cpsd_gpu_batch *b)
 // gather it into pinned staging (checking that the rest is zero) and write
 // the grids back as zeros plus the scattered sphere.
 
+// Pinned staging of the packed tables: slices handed out in order (16-byte
+// aligned), each copied to its device array by one cudaMemcpyAsync.
+struct Stager {
+    char *base;
+    size_t cap;
+    cudaStream_t s;
+    size_t off = 0;
+    bool full = false;
+    cudaError_t err = cudaSuccess;
+    long long bytes = 0;
+    template <typename T>
+    T *slice(size_t n)
+    {
+        const size_t b = (n * sizeof(T) + 15) / 16 * 16;
+        if (off + b > cap) {
+            full = true;
+            return reinterpret_cast<T *>(base);
+        }
+        T *p = reinterpret_cast<T *>(base + off);
+        off += b;
+        return p;
+    }
+    bool ok() const { return !full; }
+    template <typename T>
+    void put(T *dst, const T *src, size_t n)
+    {
+        if (n == 0 || err != cudaSuccess) return;
+        err = cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
+        bytes += (long long)(n * sizeof(T));
+    }
+};
+
 // Slices of one band's grid for the host threads (about 512 KB each).
 long grid_slices(const cpsd_gpu_ctx *c)
 {
@@ -1104,6 +1142,24 @@ long host_gather(cpsd_gpu_ctx *c, const double *full)
     return outside.load();
 }
 
+// Zero n doubles.  On x86-64 with non-temporal stores: the lines are only
+// written, so they need not be read for ownership first; scalar stores at
+// the unaligned ends, and a store fence so that later stores from other
+// threads (the scatter of the sphere) land after these.
+void zero_stream(double *p, size_t n)
+{
+#if defined(__x86_64__)
+    size_t i = 0;
+    for (; i < n && (reinterpret_cast<uintptr_t>(p + i) & 15) != 0; ++i) p[i] = 0.0;
+    const __m128d z = _mm_setzero_pd();
+    for (; i + 2 <= n; i += 2) _mm_stream_pd(p + i, z);
+    for (; i < n; ++i) p[i] = 0.0;
+    _mm_sfence();
+#else
+    memset(p, 0, sizeof(double) * n);
+#endif
+}
+
 // Zero every band grid of the listed host arrays (nb x nfft3d complex each).
 std::function<void(int)> zero_grids_task(const cpsd_gpu_ctx *c, std::vector<double *> grids, int *items)
 {
@@ -1112,7 +1168,7 @@ std::function<void(int)> zero_grids_task(const cpsd_gpu_ctx *c, std::vector<doub
     return [grids, S, per, nb, nfft3d](int t) {
         const long gi = t / (nb * S), r = t % (nb * S), b = r / S;
         const long g0 = (r % S) * per, g1 = std::min(nfft3d, g0 + per);
-        if (g1 > g0) memset(grids[gi] + 2 * (b * nfft3d + g0), 0, sizeof(cx<double>) * (g1 - g0));
+        if (g1 > g0) zero_stream(grids[gi] + 2 * (b * nfft3d + g0), (size_t)2 * (g1 - g0));
     };
 }
 
@@ -1138,12 +1194,10 @@ int get_state_host(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double
         c->d2h += (long long)pb;
     }
     const long ne02 = (long)c->ne0 * c->ne0, ne12 = (long)c->ne1 * c->ne1;
-    if (dn) {
-        const long tot = (long)c->ispin * c->n2ft3d;
-        pad_real_kernel<<<(unsigned)cdiv(tot, 256), 256, 0, s>>>(c->ispin, c->n, c->dn, c->full);
-        CK(cudaMemcpyAsync(dn, c->full, sizeof(double) * tot, cudaMemcpyDeviceToHost, s));
-        c->nlaunch += 1;
-        c->d2h += (long long)sizeof(double) * tot;
+    double *dst = reinterpret_cast<double *>(c->dstage.p);
+    if (dn) {  // unpadded into pinned staging; the host adds the two pad reals per x line
+        CK(cudaMemcpyAsync(dst, c->dn, sizeof(double) * c->ispin * c->n3, cudaMemcpyDeviceToHost, s));
+        c->d2h += (long long)sizeof(double) * c->ispin * c->n3;
     }
     c->d2h += (long long)sizeof(double) * ((hml ? ne02 + ne12 : 0) + (lmd ? ne02 + ne12 : 0) +
                                           (c->nion > 0 ? ((r1 ? 3 : 0) + (r2 ? 3 : 0)) * c->nion : 0));
@@ -1171,6 +1225,17 @@ int get_state_host(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double
         pool.run(items, task);
     }
     CK(cudaStreamSynchronize(s));
+    if (dn) {  // [ms][z][y][x] -> the reference's [ms][z][y][x(n+2)], pads zero (cpsd.c:185-194)
+        const int n = c->n;
+        const long lines = (long)c->ispin * n * n, per = 1024;
+        pool.run((int)cdiv(lines, per), [&](int t) {
+            for (long l = t * per; l < std::min(lines, (t + 1) * per); ++l) {
+                memcpy(dn + l * (n + 2), dst + l * n, sizeof(double) * n);
+                dn[l * (n + 2) + n] = 0.0;
+                dn[l * (n + 2) + n + 1] = 0.0;
+            }
+        });
+    }
     struct Out {
         double *host;
         const cx<double> *a, *sub;
@@ -1523,8 +1588,15 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->ppart, 3 * c->pblocks));
     CK(ar.alloc(&c->bpart, (size_t)2 * nb * c->bblocks));
     CK(ar.alloc(&c->gpart, 2 * c->gblocks));
-    CK(ar.alloc(&c->full, (size_t)c->ispin * c->n2ft3d));
     CK(cudaMallocHost((void **)&c->hstage.p, sizeof(cx<double>) * 2 * nb * c->ldc));
+    {
+        // every slice cpsd_gpu_set_tables packs, each rounded up to 16 bytes
+        const size_t P = (size_t)c->npw_pad, K = (size_t)c->nkatm, I = (size_t)std::max(nion, 1);
+        c->tstage_bytes = 8 * (3 * P + P + K * P + 9 * K * P + K + 9 + 3 * (size_t)c->nsh + K + 2 * I + 9 * I +
+                               3 * P) + 16 * 16;
+        CK(cudaMallocHost((void **)&c->tstage.p, c->tstage_bytes));
+        CK(cudaMallocHost((void **)&c->dstage.p, sizeof(double) * c->ispin * c->n3));
+    }
     CK(ar.alloc(&c->shell, (size_t)c->npw_pad));
     CK(ar.alloc(&c->dstep, 1));
     CK(ar.alloc(&c->pcap, 2));
@@ -1628,31 +1700,21 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
     CK(cudaSetDevice(c->prm.device));
     const HostGeom &h = c->hg;
     const int nkatm = c->nkatm;
-    std::vector<double> ptg(c->npw_pad, 0.0), pvc(c->npw_pad, 0.0), pvg(c->npw_pad, 0.0);
-    for (int p = 0; p < c->npw; ++p) {
-        ptg[p] = tg[h.pt_idx[p]];
-        pvc[p] = vc[h.pt_idx[p]];
-        pvg[p] = vg[h.pt_idx[p]];
-    }
-    std::vector<double> pvl((size_t)nkatm * c->npw), pvnl((size_t)nkatm * 9 * c->npw, 0.0);
-    for (int ia = 0; ia < nkatm; ++ia) {
+    for (int ia = 0; ia < nkatm; ++ia)
         if (lmmax[ia] < 0 || lmmax[ia] > 9) return CPSD_ERR_ARG;
-        for (int p = 0; p < c->npw; ++p) pvl[(size_t)ia * c->npw + p] = vl[(size_t)ia * c->nfft3d + h.pt_idx[p]];
-        for (int l = 0; l < lmmax[ia]; ++l)
-            for (int p = 0; p < c->npw; ++p)
-                pvnl[((size_t)ia * 9 + l) * c->npw + p] = vnl[((size_t)ia * 9 + l) * c->nfft3d + h.pt_idx[p]];
-    }
     std::vector<int> off(std::max(c->nion, 1), 0), hk(std::max(c->nion, 1), 0);
-    std::vector<double> pn;
     int np = 0;
     for (int ii = 0; ii < c->nion; ++ii) {
         const int ia = katm[ii];
         if (ia < 0 || ia >= nkatm) return CPSD_ERR_ARG;
         hk[ii] = ia;
         off[ii] = np;
-        for (int l = 0; l < lmmax[ia]; ++l) pn.push_back(vnlnrm[ia * 9 + l]);
         np += lmmax[ia];
     }
+    const bool motion = G && amass && c->nion > 0;
+    if (motion)
+        for (int ia = 0; ia < nkatm; ++ia)
+            if (!(amass[ia] > 0)) return CPSD_ERR_ARG;
     if (np != c->nproj || !c->proj) {
         drop_graphs(c);
         if (np > 0) {
@@ -1663,44 +1725,79 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
         }
         c->nproj = np;
     }
-    CK(cudaMemcpy(c->tg, ptg.data(), sizeof(double) * c->npw_pad, cudaMemcpyHostToDevice));
-    {
-        double tmax = 0.0;
-        for (int p = 0; p < c->npw; ++p) tmax = std::max(tmax, ptg[p]);
-        c->tmax = tmax > 0 ? tmax : 1.0;
-        std::vector<int> sh(c->npw_pad, 0);
-        for (int p = 0; p < c->npw; ++p)
-            sh[p] = std::min(kShells - 1, (int)(ptg[p] / c->tmax * kShells));
-        CK(cudaMemcpy(c->shell, sh.data(), sizeof(int) * c->npw_pad, cudaMemcpyHostToDevice));
+    // pack into pinned staging (the previous upload from it has finished
+    // once the stream is idle), then one asynchronous copy per table
+    CK(cudaStreamSynchronize(c->st));
+    Stager sg{reinterpret_cast<char *>(c->tstage.p), c->tstage_bytes, c->st};
+    const int npw = c->npw, npw_pad = c->npw_pad;
+    const int *pt = h.pt_idx.data();
+    double *ptg = sg.slice<double>(npw_pad), *pvc = sg.slice<double>(npw_pad), *pvg = sg.slice<double>(npw_pad);
+    int *sh = sg.slice<int>(npw_pad);
+    double *pvl = sg.slice<double>((size_t)nkatm * npw), *pvnl = sg.slice<double>((size_t)nkatm * 9 * npw);
+    double *pzv = sg.slice<double>(nkatm), *pug = sg.slice<double>(9), *prc = sg.slice<double>(3 * c->nsh);
+    int *plm = sg.slice<int>(nkatm), *pk = sg.slice<int>(c->nion), *po = sg.slice<int>(c->nion);
+    double *pn = sg.slice<double>(np), *pg = sg.slice<double>(motion ? (size_t)3 * npw : 0);
+    if (!sg.ok()) return CPSD_ERR_ARG;  // more kinds / ions than the context was created for
+    double tmax = 0.0;
+    for (int p = 0; p < npw_pad; ++p) {
+        const bool in = p < npw;
+        ptg[p] = in ? tg[pt[p]] : 0.0;
+        pvc[p] = in ? vc[pt[p]] : 0.0;
+        pvg[p] = in ? vg[pt[p]] : 0.0;
+        tmax = std::max(tmax, ptg[p]);
     }
-    CK(cudaMemcpy(c->vc, pvc.data(), sizeof(double) * c->npw_pad, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->vg, pvg.data(), sizeof(double) * c->npw_pad, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->vl, pvl.data(), sizeof(double) * pvl.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->vnl, pvnl.data(), sizeof(double) * pvnl.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->zv, zv, sizeof(double) * nkatm, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->lmmax, lmmax, sizeof(int) * nkatm, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->unitg, c->prm.unitg, sizeof(double) * 9, cudaMemcpyHostToDevice));
+    c->tmax = tmax > 0 ? tmax : 1.0;
+    for (int p = 0; p < npw_pad; ++p) sh[p] = p < npw ? std::min(kShells - 1, (int)(ptg[p] / c->tmax * kShells)) : 0;
+    for (int ia = 0; ia < nkatm; ++ia) {
+        for (int p = 0; p < npw; ++p) pvl[(size_t)ia * npw + p] = vl[(size_t)ia * c->nfft3d + pt[p]];
+        for (int l = 0; l < 9; ++l) {
+            double *d = pvnl + ((size_t)ia * 9 + l) * npw;
+            if (l < lmmax[ia]) {
+                const double *src = vnl + ((size_t)ia * 9 + l) * c->nfft3d;
+                for (int p = 0; p < npw; ++p) d[p] = src[pt[p]];
+            } else {
+                memset(d, 0, sizeof(double) * npw);
+            }
+        }
+    }
+    memcpy(pzv, zv, sizeof(double) * nkatm);
+    memcpy(pug, c->prm.unitg, sizeof(double) * 9);
+    if (c->nsh > 0) memcpy(prc, rcell, sizeof(double) * 3 * c->nsh);
+    memcpy(plm, lmmax, sizeof(int) * nkatm);
     if (c->nion > 0) {
-        CK(cudaMemcpy(c->katm, hk.data(), sizeof(int) * c->nion, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(c->proj_off, off.data(), sizeof(int) * c->nion, cudaMemcpyHostToDevice));
+        memcpy(pk, hk.data(), sizeof(int) * c->nion);
+        memcpy(po, off.data(), sizeof(int) * c->nion);
     }
-    if (c->nsh > 0) CK(cudaMemcpy(c->rcell, rcell, sizeof(double) * 3 * c->nsh, cudaMemcpyHostToDevice));
-    if (np > 0) CK(cudaMemcpy(c->vnlnrm_p, pn.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
+    for (int ii = 0, q = 0; ii < c->nion; ++ii)
+        for (int l = 0; l < lmmax[hk[ii]]; ++l) pn[q++] = vnlnrm[hk[ii] * 9 + l];
+    if (motion)
+        for (int d = 0; d < 3; ++d)
+            for (int p = 0; p < npw; ++p) pg[(size_t)d * npw + p] = G[(size_t)d * c->nfft3d + pt[p]];
+    sg.put(c->tg, ptg, npw_pad);
+    sg.put(c->shell, sh, npw_pad);
+    sg.put(c->vc, pvc, npw_pad);
+    sg.put(c->vg, pvg, npw_pad);
+    sg.put(c->vl, pvl, (size_t)nkatm * npw);
+    sg.put(c->vnl, pvnl, (size_t)nkatm * 9 * npw);
+    sg.put(c->zv, pzv, nkatm);
+    sg.put(c->lmmax, plm, nkatm);
+    sg.put(c->unitg, pug, 9);
+    if (c->nion > 0) {
+        sg.put(c->katm, pk, c->nion);
+        sg.put(c->proj_off, po, c->nion);
+    }
+    if (c->nsh > 0) sg.put(c->rcell, prc, 3 * c->nsh);
+    if (np > 0) sg.put(c->vnlnrm_p, pn, np);
     // ion motion needs the G vectors (packed like tg) and the masses
     c->motion_ok = false;
-    if (G && amass && c->nion > 0) {
-        std::vector<double> pg((size_t)3 * c->npw);
-        for (int d = 0; d < 3; ++d)
-            for (int p = 0; p < c->npw; ++p) pg[(size_t)d * c->npw + p] = G[(size_t)d * c->nfft3d + h.pt_idx[p]];
-        CK(cudaMemcpy(c->Gv, pg.data(), sizeof(double) * pg.size(), cudaMemcpyHostToDevice));
+    if (motion) {
+        sg.put(c->Gv, pg, (size_t)3 * npw);
         c->amass_h.assign(amass, amass + nkatm);
-        for (double m : c->amass_h)
-            if (!(m > 0)) return CPSD_ERR_ARG;
         c->motion_ok = true;
     }
-    CK(cudaDeviceSynchronize());
-    c->h2d += (long long)sizeof(double) * (3 * c->npw_pad + (long)pvl.size() + (long)pvnl.size() + nkatm + 9 + np +
-                                          3 * c->nsh) + (long long)sizeof(int) * (nkatm + 2 * c->nion);
+    CK(sg.err);
+    CK(cudaStreamSynchronize(c->st));
+    c->h2d += sg.bytes;
     c->tables_ok = true;
     return CPSD_OK;
 }

@@ -1480,20 +1480,6 @@ __global__ void __launch_bounds__(kFinalThreads) final_energy_kernel(FinalArgs a
     a.E[11] = dc / a.dte;
 }
 
-// ------------------------------------------------------------ layout conversion
-// real grid [ms][z][y][x] -> reference padded layout [ms][z][y][x(n+2)] with zero pads
-__global__ void pad_real_kernel(int nsets, int n, const double *__restrict__ src, double *__restrict__ dst)
-{
-    const long n2r = (long)(n + 2) * n * n;
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= (long)nsets * n2r) return;
-    const int ms = (int)(id / n2r);
-    const long r = id % n2r;
-    const int x = (int)(r % (n + 2));
-    const long yz = r / (n + 2);
-    dst[id] = (x < n) ? src[(long)ms * n * n * n + yz * n + x] : 0.0;
-}
-
 // ------------------------------------------------------------ epilogue eigenpairs
 // ccpsdv3/main.c:470-481: per spin, dsyev('V','U') of hml, then eigsrt
 // (ccpsdv3/eigsrt.c:9-36: selection sort into descending order, ties to the
