@@ -810,7 +810,7 @@ int one_step(cpsd_gpu_ctx *c)
     la.fail = c->flags;
     la.lb = c->lag_lb;
     if (c->ne0 <= kLagSmallMax)
-        lagrange_small_kernel<<<1, kLagThreads, sizeof(double) * 7 * ne02, s>>>(la);
+        lagrange_small_kernel<<<1, kLagThreads, lag_small_smem_bytes(c->ne0), s>>>(la);
     else if (c->lag_tile) {
         cudaLaunchConfig_t cfg{};
         cudaLaunchAttribute attr[1];
@@ -1613,7 +1613,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->py, (size_t)nb * kShells));
     if (c->ne0 <= kLagSmallMax)
         CK(cudaFuncSetAttribute(lagrange_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(double) * 7 * kLagSmallMax * kLagSmallMax)));
+                                (int)lag_small_smem_bytes(kLagSmallMax)));
     else {
         // 16-CTA clusters where the device can schedule them, else the portable 8
         CK(cudaFuncSetAttribute(lagrange_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));

@@ -905,85 +905,133 @@ __global__ void __launch_bounds__(kLagThreads) lagrange_kernel(LagArgs a)
 // every matrix in shared memory; block barriers instead of cluster barriers.
 constexpr int kLagSmallMax = 32;
 
+// Smem layout of lagrange_small_kernel: seven matrices padded to mp = m
+// rounded up to 8, leading dimension mp + 4 (fragment loads of lanes
+// 4r + k hit 16 different banks), then the unpadded differences.
+CPSD_HD int lag_small_mp(int m) { return (m + 7) / 8 * 8; }
+CPSD_HD int lag_small_ld(int m) { return lag_small_mp(m) + 4; }
+inline size_t lag_small_smem_bytes(int ne0)
+{
+    return sizeof(double) * ((size_t)7 * lag_small_mp(ne0) * lag_small_ld(ne0) + (size_t)ne0 * ne0);
+}
+
+// One 8 x 8 tile of P = A B (column-major, leading dimension ld, inner
+// dimension kd, a multiple of 4) on the FP64 tensor cores: a lane's
+// fragment d[0..1] holds P(i0 + lane/4, j0 + 2 (lane%4) + e).
+CPSD_D void lag_tile_mma(const double *A, const double *B, int ld, int kd, int i0, int j0, int lane,
+                         double (&d)[2])
+{
+    const int r = lane >> 2, q = lane & 3;
+    d[0] = d[1] = 0.0;
+    for (int k0 = 0; k0 < kd; k0 += 4) dmma(d[0], d[1], A[(i0 + r) + (k0 + q) * ld], B[(k0 + q) + (j0 + r) * ld]);
+}
+
+// cpsd.c:420-479 for m <= kLagSmallMax bands: one CTA; the four m x m
+// products of an iteration on the FP64 tensor cores (mma.sync m8n8k4),
+// 8 x 8 tiles spread over the warps; two barriers per iteration.
 __global__ void __launch_bounds__(kLagThreads) lagrange_small_kernel(LagArgs a)
 {
-    constexpr int MM = kLagSmallMax * kLagSmallMax;
-    extern __shared__ double lag_sm[];  // 7 * ne0^2 doubles (dynamic)
-    const int ld = a.ne0 * a.ne0;
-    double *s11 = lag_sm, *s12 = lag_sm + ld, *s21 = lag_sm + 2 * ld, *s22 = lag_sm + 3 * ld;
-    double *st1 = lag_sm + 4 * ld;
-    double *X[2] = {lag_sm + 5 * ld, lag_sm + 6 * ld};
-    __shared__ double shv[kLagThreads / 32];
-    __shared__ int shi[kLagThreads / 32];
-    __shared__ int s_done;
-    const int tid = threadIdx.x;
+    constexpr int NW = kLagThreads / 32;
+    constexpr int TMAX = (kLagSmallMax / 8) * (kLagSmallMax / 8);  // tiles of the largest matrix
+    constexpr int TPW = (TMAX + NW - 1) / NW;                      // tiles per warp
+    extern __shared__ double lag_sm[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long ne02 = (long)a.ne0 * a.ne0;
+    // the layout is sized for ne0 (ne1 <= ne0 reuses it)
+    const int LD = lag_small_ld(a.ne0), SZ = lag_small_mp(a.ne0) * LD;
+    double *s11 = lag_sm, *s12 = lag_sm + SZ, *s21 = lag_sm + 2 * SZ, *s22 = lag_sm + 3 * SZ;
+    double *st1 = lag_sm + 4 * SZ;
+    double *X[2] = {lag_sm + 5 * SZ, lag_sm + 6 * SZ};
+    // sa1 - sa0 of each iteration (cpsd.c:469) at the reference's unpadded
+    // index i + j m: what the reference keeps in st1 for its convergence
+    // read; entries past m^2 keep the last ones written, as st1's do there
+    double *dif = lag_sm + 7 * SZ;
+    __shared__ double shv[NW];
+    __shared__ int shi[NW];
     for (int ms = 0; ms < a.ispin; ++ms) {
         const int m = ms ? a.ne1 : a.ne0;
-        const int kk = m * m;
+        const long kk = (long)m * m;
         if (m == 0) continue;
+        const int mp = lag_small_mp(m), ld = lag_small_ld(m), nt = (mp / 8) * (mp / 8);
         const double *M22 = a.M22[ms], *M21 = a.M21[ms], *M11 = a.M11[ms];
         const double dte = a.dte;
-        for (int e = tid; e < kk; e += kLagThreads) {  // cpsd.c:420-437
-            const int i = e % m, j = e / m;
-            double v22, v21, v12, v11;
-            if (i == j) {
-                v22 = (1.0 - M22[i * m + i]) * 0.5 / dte;
-                v21 = (1.0 - M21[i * m + i]) * 0.5;
-                v12 = v21;
-                v11 = -M11[i * m + i] * 0.5 * dte;
-            } else {
-                const int lo = i < j ? i : j, hi = i < j ? j : i;
-                v22 = -M22[lo * m + hi] * 0.5 / dte;
-                v21 = -M21[lo * m + hi] * 0.5;
-                v12 = -M21[hi * m + lo] * 0.5;
-                v11 = -M11[lo * m + hi] * 0.5 * dte;
+        for (int e = tid; e < mp * ld; e += kLagThreads) {  // cpsd.c:420-437, zero padding
+            const int i = e % ld, j = e / ld;
+            double v22 = 0.0, v21 = 0.0, v12 = 0.0, v11 = 0.0;
+            if (i < m && j < m) {
+                if (i == j) {
+                    v22 = (1.0 - M22[i * m + i]) * 0.5 / dte;
+                    v21 = (1.0 - M21[i * m + i]) * 0.5;
+                    v12 = v21;
+                    v11 = -M11[i * m + i] * 0.5 * dte;
+                } else {
+                    const int lo = i < j ? i : j, hi = i < j ? j : i;
+                    v22 = -M22[lo * m + hi] * 0.5 / dte;
+                    v21 = -M21[lo * m + hi] * 0.5;
+                    v12 = -M21[hi * m + lo] * 0.5;
+                    v11 = -M11[lo * m + hi] * 0.5 * dte;
+                }
             }
             s22[e] = v22;
             s21[e] = v21;
             s12[e] = v12;
             s11[e] = v11;
             X[0][e] = v22;
+            X[1][e] = 0.0;
+            st1[e] = 0.0;
         }
         __syncthreads();
         int cur = 0, iter = 0;
         bool done = false;
         while (!done && iter < 30) {
             ++iter;
-            double *c = X[cur], *nx = X[cur ^ 1];
-            for (int e = tid; e < kk; e += kLagThreads) {  // cpsd.c:444-462
-                const int i = e % m, j = e / m;
-                double t1 = 0.0, t2 = 0.0, t3 = 0.0;
-                for (int l = 0; l < m; ++l) {
-                    const double c_lj = c[l + j * m];
-                    t1 = fma(s21[i + l * m], c_lj, t1);
-                    t2 = fma(c[i + l * m], s12[l + j * m], t2);
-                    t3 = fma(s11[i + l * m], c_lj, t3);
+            const double *c = X[cur];
+            double *nx = X[cur ^ 1];
+            double part[TPW][2];
+            // X S12 + (S21 X + S22) and st1 = S11 X (cpsd.c:444-462)
+#pragma unroll
+            for (int u = 0; u < TPW; ++u) {
+                const int t = warp + u * NW;
+                if (t >= nt) break;
+                const int i0 = (t % (mp / 8)) * 8, j0 = (t / (mp / 8)) * 8;
+                double t1[2], t2[2], t3[2];
+                lag_tile_mma(s21, c, ld, mp, i0, j0, lane, t1);
+                lag_tile_mma(c, s12, ld, mp, i0, j0, lane, t2);
+                lag_tile_mma(s11, c, ld, mp, i0, j0, lane, t3);
+                const int i = i0 + (lane >> 2), j = j0 + 2 * (lane & 3);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    part[u][h] = t2[h] + (t1[h] + s22[i + (j + h) * ld]);
+                    st1[i + (j + h) * ld] = t3[h];
                 }
-                nx[e] = t2 + (t1 + s22[e]);
-                st1[e] = t3;
             }
             __syncthreads();
-            double keep[(MM + kLagThreads - 1) / kLagThreads];
-            int q = 0;
-            for (int e = tid; e < kk; e += kLagThreads, ++q) {  // cpsd.c:463-468
-                const int i = e % m, j = e / m;
-                double t4 = 0.0;
-                for (int l = 0; l < m; ++l) t4 = fma(c[i + l * m], st1[l + j * m], t4);
-                keep[q] = t4 + nx[e];
-            }
-            __syncthreads();
+            // sa1 = that + X st1, the differences and their largest entry (cpsd.c:463-470)
             double bestv = -1.0;
             int besti = 0x7fffffff;
-            q = 0;
-            for (int e = tid; e < kk; e += kLagThreads, ++q) {  // cpsd.c:469-470
-                nx[e] = keep[q];
-                const double d = keep[q] - c[e];
-                st1[e] = d;
-                const double ad = fabs(d);
-                if (ad > bestv || (ad == bestv && e < besti)) {
-                    bestv = ad;
-                    besti = e;
+#pragma unroll
+            for (int u = 0; u < TPW; ++u) {
+                const int t = warp + u * NW;
+                if (t >= nt) break;
+                const int i0 = (t % (mp / 8)) * 8, j0 = (t / (mp / 8)) * 8;
+                double t4[2];
+                lag_tile_mma(c, st1, ld, mp, i0, j0, lane, t4);
+                const int i = i0 + (lane >> 2), j = j0 + 2 * (lane & 3);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int o = i + (j + h) * ld;
+                    const double v = t4[h] + part[u][h];
+                    nx[o] = v;
+                    if (i < m && j + h < m) {
+                        const double d = v - c[o];
+                        const int e = i + (j + h) * m;
+                        dif[e] = d;
+                        const double ad = fabs(d);
+                        if (ad > bestv || (ad == bestv && e < besti)) {
+                            bestv = ad;
+                            besti = e;
+                        }
+                    }
                 }
             }
 #pragma unroll
@@ -995,33 +1043,36 @@ __global__ void __launch_bounds__(kLagThreads) lagrange_small_kernel(LagArgs a)
                     besti = oi;
                 }
             }
-            if ((tid & 31) == 0) {
-                shv[tid >> 5] = bestv;
-                shi[tid >> 5] = besti;
+            if (lane == 0) {
+                shv[warp] = bestv;
+                shi[warp] = besti;
             }
             __syncthreads();
-            if (tid == 0) {
-                for (int w = 1; w < kLagThreads / 32; ++w)
-                    if (shv[w] > bestv || (shv[w] == bestv && shi[w] < besti)) {
-                        bestv = shv[w];
-                        besti = shi[w];
-                    }
-                // idamax returns an index in 1..kk even when every entry is
-                // NaN: the sentinel must never reach the read below
-                if (besti < 0 || (long)besti >= kk) besti = 0;
-                // idamax's 1-based index used as 0-based (cpsd.c:471); past st1 lies sa1
-                const long nxi = (long)besti + 1;
-                const double adiff = fabs(nxi < ne02 ? st1[nxi] : nx[nxi - ne02]);
-                s_done = adiff < 1e-15;
-            }
-            __syncthreads();
-            done = s_done != 0;
+            // every thread combines the warp maxima in the same order and
+            // takes the same decision: no third barrier for a broadcast
+            bestv = shv[0];
+            besti = shi[0];
+#pragma unroll
+            for (int w = 1; w < NW; ++w)
+                if (shv[w] > bestv || (shv[w] == bestv && shi[w] < besti)) {
+                    bestv = shv[w];
+                    besti = shi[w];
+                }
+            // idamax returns an index in 1..kk even when every entry is
+            // NaN: the sentinel must never reach the read below
+            if (besti < 0 || (long)besti >= kk) besti = 0;
+            // idamax's 1-based index used as 0-based (cpsd.c:471); past st1 lies
+            // sa1, whose first entry is element (0, 0)
+            const long nxi = (long)besti + 1;
+            const double adiff = fabs(nxi < ne02 ? dif[nxi] : nx[nxi - ne02]);
+            done = adiff < 1e-15;
             if (!done) cur ^= 1;
+            // the next iteration writes st1, shv and shi only after its first barrier
         }
         if (!done && tid == 0) atomicAdd(a.fail, 1);
         // converged: sa1 is the buffer just written; stopped at 30: it was swapped into cur
         const double *fin = done ? X[cur ^ 1] : X[cur];
-        for (int e = tid; e < kk; e += kLagThreads) a.lmd[ms * ne02 + e] = fin[e];
+        for (long e = tid; e < kk; e += kLagThreads) a.lmd[ms * ne02 + e] = fin[(e % m) + (e / m) * ld];
         __syncthreads();
     }
 }
