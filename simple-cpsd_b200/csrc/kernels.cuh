@@ -472,19 +472,8 @@ CPSD_D void dmma(double &d0, double &d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-// The four k-steps of a lane's fragment row of a [row][k] tile.
-CPSD_D void dm_frag(const double *t, int row, int fq, double (&v)[4])
-{
-    const double2 x = *reinterpret_cast<const double2 *>(t + row * kDmS + 4 * fq);
-    const double2 y = *reinterpret_cast<const double2 *>(t + row * kDmS + 4 * fq + 2);
-    v[0] = x.x;
-    v[1] = x.y;
-    v[2] = y.x;
-    v[3] = y.y;
-}
-
 // part[prod][split][i][j] as above; grid (M tiles, N tiles, nprod * splits).
-__global__ void __launch_bounds__(kDmThreads)
+__global__ void __launch_bounds__(kDmThreads, 4)
 gemm_tn_dmma_kernel(int M, int N, int K, long lda, long ldb, const double *__restrict__ w, int kchunk,
                     const __grid_constant__ TnBatch bt, double *__restrict__ part)
 {
@@ -530,18 +519,25 @@ gemm_tn_dmma_kernel(int M, int N, int K, long lda, long ldb, const double *__res
     for (int kk = k0; kk < k1; kk += kDmK) {
         const bool more = kk + kDmK < k1;
         if (more) fetch(kk + kDmK);
-        double a[4][4], b[4][4];
+        // two halves of two k-steps each: one 16-byte fragment load per
+        // operand row per half keeps the fragments in 32 registers
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            dm_frag(As[buf], wr + 8 * f + fr, fq, a[f]);
-            dm_frag(Bs[buf], wc + 8 * f + fr, fq, b[f]);
-        }
+        for (int hh = 0; hh < 2; ++hh) {
+            double2 a[4], b[4];
 #pragma unroll
-        for (int s = 0; s < 4; ++s)
+            for (int f = 0; f < 4; ++f) {
+                a[f] = *reinterpret_cast<const double2 *>(As[buf] + (wr + 8 * f + fr) * kDmS + 4 * fq + 2 * hh);
+                b[f] = *reinterpret_cast<const double2 *>(Bs[buf] + (wc + 8 * f + fr) * kDmS + 4 * fq + 2 * hh);
+            }
 #pragma unroll
             for (int fi = 0; fi < 4; ++fi)
 #pragma unroll
-                for (int fj = 0; fj < 4; ++fj) dmma(acc[fi][fj][0], acc[fi][fj][1], a[fi][s], b[fj][s]);
+                for (int fj = 0; fj < 4; ++fj) dmma(acc[fi][fj][0], acc[fi][fj][1], a[fi].x, b[fj].x);
+#pragma unroll
+            for (int fi = 0; fi < 4; ++fi)
+#pragma unroll
+                for (int fj = 0; fj < 4; ++fj) dmma(acc[fi][fj][0], acc[fi][fj][1], a[fi].y, b[fj].y);
+        }
         if (more) stash(buf ^ 1);
         __syncthreads();
         buf ^= 1;
@@ -563,7 +559,7 @@ gemm_tn_dmma_kernel(int M, int N, int K, long lda, long ldb, const double *__res
 
 // Out[j*ldo+k] = beta*Out + alpha * sum_l
 // Mat[l + j*ldm] * B[l*ldb + k]; grid x over 64-wide k tiles, y over j tiles.
-__global__ void __launch_bounds__(kDmThreads)
+__global__ void __launch_bounds__(kDmThreads, 4)
 gemm_nn_dmma_kernel(int NJ, int K, int L, double alpha, const double *__restrict__ Mat, long ldm,
                     const double *__restrict__ B, long ldb, double beta, double *__restrict__ Out, long ldo)
 {
@@ -607,19 +603,24 @@ gemm_nn_dmma_kernel(int NJ, int K, int L, double alpha, const double *__restrict
     for (int l0 = 0; l0 < L; l0 += kDmK) {
         const bool more = l0 + kDmK < L;
         if (more) fetch(l0 + kDmK);
-        double a[4][4];
 #pragma unroll
-        for (int f = 0; f < 4; ++f) dm_frag(Ms[buf], wr + 8 * f + fr, fq, a[f]);
+        for (int hh = 0; hh < 2; ++hh) {  // two k-steps per half, as in the TN kernel
+            double2 a[4];
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const double *bs = Bs[buf] + (4 * fq + s) * kDmSB + wc + fr;
-            double b[4];
+            for (int f = 0; f < 4; ++f)
+                a[f] = *reinterpret_cast<const double2 *>(Ms[buf] + (wr + 8 * f + fr) * kDmS + 4 * fq + 2 * hh);
 #pragma unroll
-            for (int fj = 0; fj < 4; ++fj) b[fj] = bs[8 * fj];
+            for (int s2 = 0; s2 < 2; ++s2) {
+                const double *bs = Bs[buf] + (4 * fq + 2 * hh + s2) * kDmSB + wc + fr;
+                double b[4];
 #pragma unroll
-            for (int fi = 0; fi < 4; ++fi)
+                for (int fj = 0; fj < 4; ++fj) b[fj] = bs[8 * fj];
 #pragma unroll
-                for (int fj = 0; fj < 4; ++fj) dmma(acc[fi][fj][0], acc[fi][fj][1], a[fi][s], b[fj]);
+                for (int fi = 0; fi < 4; ++fi)
+#pragma unroll
+                    for (int fj = 0; fj < 4; ++fj)
+                        dmma(acc[fi][fj][0], acc[fi][fj][1], s2 ? a[fi].y : a[fi].x, b[fj]);
+            }
         }
         if (more) stash(buf ^ 1);
         __syncthreads();
