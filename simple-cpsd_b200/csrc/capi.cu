@@ -1,8 +1,12 @@
 // capi.cu -- the reference-facing entry points of include/cpsd_b200.h:
-// cpsd() / cpsd_gpu_cpsd() (ccpsdv3/cpsd.c:33-71) and the Fortran-ABI
-// cr_fft3b_ / rc_fft3f_ (fftpack3d/fftpack3d.f:22-196).
+// cpsd() / cpsd_gpu_cpsd() (ccpsdv3/cpsd.c:33-71), the Fortran-ABI
+// cr_fft3b_ / rc_fft3f_ (fftpack3d/fftpack3d.f:22-196), the input pipeline
+// (kbpp() of ckbppv3/dkbppv3.c, cmakepsi/dmakepsi.c) and the epilogue's
+// ELCOUT / IONOUT writers (ccpsdv3/main.c:537-566).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
