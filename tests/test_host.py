@@ -170,3 +170,23 @@ def test_replica_timing_takes_the_slowest_rank():
         p.join(timeout=120)
     res = dict(q.get(timeout=5) for _ in range(2))
     assert res == {0: 11.0, 1: 11.0}
+
+
+@pytest.mark.parametrize("threads", ["1", "3", "16"])
+def test_host_pool_runs_every_item_once(tmp_path, threads):
+    """The host thread pool behind the drop-in's layout conversion: thousands
+    of jobs back to back, each item exactly once, for 1, 3 and 16 threads."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    exe = str(tmp_path / "pool_check")
+    src = os.path.join(REPO, "tests", "host_pool_check.cpp")
+    inc = os.path.join(REPO, "simple-cpsd_b200", "csrc")
+    subprocess.run([cxx, "-O2", "-std=c++17", "-pthread", "-I", inc, src, "-o", exe], check=True)
+    env = dict(os.environ, CPSD_B200_HOST_THREADS=threads)
+    out = subprocess.run([exe], env=env, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.startswith("ok %s threads" % threads)
+
