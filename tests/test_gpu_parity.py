@@ -611,3 +611,23 @@ def test_pipeline_inputs_drive_the_sd_path(restatement):
     cell.get_state(st)
     cell.close()
     assert np.abs(st.c2 - so.c2).max() < 1e-10
+
+
+def test_max_bands_per_spin_matches_restatement(restatement):
+    """256 bands, the engine's limit per spin: the 16-CTA column-cluster
+    Lagrange solver chosen on its own (no override), 4 x 4 tiles of the FP64
+    tensor-core products, 256-band plane passes; one SD step against the
+    restatement on the same inputs."""
+    inp = inputs.build_inputs(configs.small_diamond(32, 256, ecut=40.0, seed=13))
+    so = oracle.State(inp)
+    restatement.run(inp, 1, so)
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    cell.run(1)
+    st = api.State(inp)
+    cell.get_state(st)
+    cell.close()
+    assert abs(cell.E[0] - so.E[0]) < 1e-12 * abs(so.E[0]) + 1e-9
+    assert np.abs(st.lmd - so.lmd).max() < 1e-10 * np.abs(so.lmd).max()
+    assert np.abs(st.hml - so.hml).max() < 1e-10 * np.abs(so.hml).max()
+    assert np.abs(st.c2 - so.c2).max() < 1e-10
