@@ -112,6 +112,29 @@ def small_diamond(nfft: int = 24, nb: int = 4, ecut: float = 20.0, seed: int = 3
                     species=[C_SP], katm=[0] * 8, positions=pos, ne=ne, ispin=ispin, seed=seed)
 
 
+def spin_h2(nfft: int = 16, ne=(2, 1)) -> CellSpec:
+    """Spin-polarised H2 from the reference's plane-wave start.  The
+    reference's Dirac exchange takes xi from the first two density values
+    (dirac_exchange.c:101) and returns NaN wherever |xi| > 1; near-uniform
+    plane-wave densities keep |xi| small for the first steps."""
+    spec = small_h2(nfft)
+    spec.name = "spin_h2_%d" % nfft
+    spec.ispin = 2
+    spec.ne = tuple(ne)
+    spec.start_waves = ((0, 0, 0, 0), (1, 0, 0, 1), (1, 0, 0, -1), (0, 1, 0, 1))[:max(ne)]
+    return spec
+
+
+def spin_diamond(nfft: int = 24, ne=(3, 2), ecut: float = 20.0) -> CellSpec:
+    """Spin-polarised 8-atom diamond from the plane-wave start (see spin_h2)."""
+    spec = small_diamond(nfft, ne[0], ecut=ecut)
+    spec.name = "spin_diamond_%d" % nfft
+    spec.ispin = 2
+    spec.ne = tuple(ne)
+    spec.start_waves = ((0, 0, 0, 0), (1, 0, 0, 1), (1, 0, 0, -1), (0, 1, 0, 1), (0, 1, 0, -1))[:max(ne)]
+    return spec
+
+
 def small_h2(nfft: int = 16, nb: int = 1, seed: int = 1) -> CellSpec:
     pos = np.array([[-0.7, 0.0, 0.0], [0.7, 0.0, 0.0]])
     return CellSpec(name="small_h2_%d" % nfft, unit=10.0, nfft=nfft, ecut_ry=12.0, species=[H_S],

@@ -16,7 +16,9 @@ seeded orbitals the workloads use in place of the reference's tabulated
   (read at ``ccpsdv3/main.c:264-284``), values from Gaussian model potentials
 * orbitals: complex normal coefficients on the half sphere with the kx=0
   plane Hermitian (``cmakepsi/makepsi.c:121-128`` layout), Gram-Schmidt
-  orthonormalised with the Gamma-point metric of ``ccpsdv3/gcdotc.c``.
+  orthonormalised with the Gamma-point metric of ``ccpsdv3/gcdotc.c``; or,
+  when a cell lists ``start_waves``, the reference's plane-wave start
+  (``cmakepsi/dmakepsi.c:93-140``).
 
 Complex arrays are float64 views of the half box: per band
 ``n2ft3d = (nfft+2)*nfft*nfft`` doubles, index ``2*(i + j*nh + k*nh*nfft)``
@@ -65,6 +67,9 @@ class CellSpec:
     dt: float = 5.8
     fmass: float = 400000.0
     move: int = 0
+    # PSI0.DAT rows (i, j, k, l) of a plane-wave start in place of the seeded
+    # orbitals; spin 1 reuses the first ne[1] rows, as dmakepsi does
+    start_waves: Tuple[Tuple[int, int, int, int], ...] = ()
 
 
 # ----------------------------------------------------------------- tables
@@ -166,6 +171,29 @@ def analytic_psp(sp: Species, G: np.ndarray, nfft3d: int):
 
 
 # ----------------------------------------------------------------- orbitals
+
+def plane_wave_orbitals(nfft: int, ispin: int, ne, rows) -> np.ndarray:
+    """The plane-wave start of cmakepsi/dmakepsi.c:93-140: band n of spin
+    ms is the wave of row n (coefficient 1 for l = 0, 1/sqrt(2) for l > 0,
+    i/sqrt(2) for l < 0), with its Hermitian partner on the kx = 0 plane."""
+    nh = nfft // 2 + 1
+    n2 = (nfft + 2) * nfft * nfft
+    s = 1.0 / math.sqrt(2.0)
+    out = np.zeros((int(ne[0]) + (int(ne[1]) if ispin == 2 else 0)) * n2)
+    b = 0
+    for ms in range(ispin):
+        for n in range(int(ne[ms])):
+            i, j, k, l = (int(v) for v in rows[n])
+            re, im = (0.0, s) if l < 0 else ((1.0, 0.0) if l == 0 else (s, 0.0))
+            k2, k3 = (j + nfft) % nfft, (k + nfft) % nfft
+            idx = b * n2 + 2 * (i + k2 * nh + k3 * nh * nfft)
+            out[idx], out[idx + 1] = re, im
+            if i == 0:
+                idx = b * n2 + 2 * (((nfft - k2) % nfft) * nh + ((nfft - k3) % nfft) * nh * nfft)
+                out[idx], out[idx + 1] = re, -im
+            b += 1
+    return out
+
 
 def gamma_weights(nfft: int) -> np.ndarray:
     """Per half-box point weight of the Gamma-point dot: 1 on kx=0, else 2."""
@@ -322,7 +350,10 @@ def build_inputs(spec: CellSpec) -> CpsdInputs:
         rcell[l], rcell[l + nsh], rcell[l + 2 * nsh] = v
 
     ne = np.array(spec.ne, dtype=np.int32)
-    c2 = random_orbitals(nfft, masker1, int(ne.sum()), spec.seed).reshape(-1)
+    if spec.start_waves:
+        c2 = plane_wave_orbitals(nfft, spec.ispin, ne, spec.start_waves)
+    else:
+        c2 = random_orbitals(nfft, masker1, int(ne.sum()), spec.seed).reshape(-1)
     r2 = np.asarray(spec.positions, dtype=np.float64).reshape(-1).copy()
     return CpsdInputs(spec=spec, nfft=nfft, nfft3d=nfft3d, n2ft3d=n2ft3d, ispin=spec.ispin,
                       ne=ne, nion=nion, unita=unita, unitg=unitg, omega=omega, dt=spec.dt,

@@ -58,12 +58,16 @@ CASES = [
     ("small_diamond_48", lambda: configs.small_diamond(48, 6, ecut=30.0), 2, 2, 6),
     ("h2_dimer_32", lambda: configs.h2_dimer_32(), 200, 1, 1),
     ("diamond8_64", lambda: configs.diamond8_64(), 4, 2, 4),
+    # spin-polarised, from the reference's plane-wave start (configs.spin_h2)
+    ("spin_h2_16", lambda: configs.spin_h2(16), 3, 2, 3),
+    ("spin_diamond_24", lambda: configs.spin_diamond(24, ne=(4, 3)), 3, 2, 7),
 ]
 
 # epilogue (main.c:452-487) after the calls: (name, spec builder, calls, inner)
 EPILOGUE_CASES = [
     ("small_diamond_24", lambda: configs.small_diamond(24, 4), 3, 2),
     ("small_diamond_32_40", lambda: configs.small_diamond(32, 40, ecut=25.0, seed=12), 2, 2),
+    ("spin_diamond_24", lambda: configs.spin_diamond(24, ne=(4, 3)), 3, 2),
 ]
 
 
