@@ -401,7 +401,8 @@ def main():
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-                "config": dict(config, step="one reference cpsd() call: 1 SD step + energies"),
+                "config": dict(config, step="one reference cpsd() call: 1 SD step + energies",
+                               l2="n/a: the reference runs on the host cores", precision="fp64", gemm="fp64"),
                 "cpu_baseline": {"value": v, "unit": "steps/s", "cores": ncores, "kind": kind,
                                  "sample": "%d reference cpsd() calls of inner=1 on %s" % (args.steps, args.workload)},
                 "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
