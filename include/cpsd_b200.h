@@ -150,7 +150,10 @@ int cpsd_gpu_set_state(cpsd_gpu_ctx *c, const double *c2, const double *r2);
 int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae, double *deltac,
                  double *deltar);
 
-/* Download the state cpsd() returns; any pointer may be NULL to skip it. */
+/* Download the state cpsd() returns; any pointer may be NULL to skip it.
+ * c1, c2 and cpsi are written on host threads in parallel (zeros, then the
+ * sphere's coefficients): they must be distinct, non-overlapping arrays, as
+ * the reference's driver allocates them (main.c:126-136). */
 int cpsd_gpu_get_state(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double *dn,
                        double *hml, double *lmd, double *r1, double *r2, double *fion);
 
