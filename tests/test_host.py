@@ -190,3 +190,38 @@ def test_host_pool_runs_every_item_once(tmp_path, threads):
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.startswith("ok %s threads" % threads)
 
+
+
+def test_new_entry_points_report_errors_without_a_gpu(tmp_path):
+    """Host-side checks of the epilogue writers and the input pipeline: bad
+    arguments and unwritable files come back as status codes, before any
+    device work (so they hold on a machine without a GPU)."""
+    from cpsd_b200 import api
+    L = lib.load()
+    assert "eigen" in lib.strerror(lib.CPSD_ERR_EIG)
+    assert "file" in lib.strerror(lib.CPSD_ERR_IO)
+    inp = inputs.build_inputs(configs.small_h2(16))
+    c1 = np.zeros(inp.nbands * inp.n2ft3d)
+    with pytest.raises(lib.CpsdError) as e:
+        api.write_elcout(str(tmp_path / "no_such_dir" / "ELCOUT"), inp, c1)
+    assert e.value.status == lib.CPSD_ERR_IO
+    with pytest.raises(ValueError):
+        api.write_elcout(str(tmp_path / "ELCOUT"), inp, c1[:-1])
+    ne = np.array([1, 0], dtype=np.int32)
+    assert L.cpsd_write_elcout(None, 1, 16, 20.0, 1, api._ptr(ne), api._ptr(c1)) == lib.CPSD_ERR_ARG
+    assert L.cpsd_write_ionout(str(tmp_path / "IONOUT").encode(), 1, None, None, 0, None, None) == lib.CPSD_ERR_ARG
+    # kbpp: lmax above 3, too few radial points, and missing outputs are refused up front
+    from cpsd_b200 import psp
+    t = psp.radial_table(2, seed=2)
+    G = inputs.get_g(16, inputs.get_cube(1, 10.26)[2])
+    nfft3d = 9 * 16 * 16
+    vp = t.vp.copy()
+    out = np.zeros(9 * nfft3d)
+    P = api._ptr
+    assert L.cpsd_gpu_kbpp(4.0, 4, t.nrho, t.drho, P(t.rho), P(vp), P(t.wp), nfft3d, P(G), P(out), P(out),
+                           P(out)) == lib.CPSD_ERR_ARG
+    assert L.cpsd_gpu_kbpp(4.0, 2, 1, t.drho, P(t.rho), P(vp), P(t.wp), nfft3d, P(G), P(out), P(out),
+                           P(out)) == lib.CPSD_ERR_ARG
+    assert L.cpsd_gpu_kbpp(4.0, 2, t.nrho, t.drho, P(t.rho), P(vp), P(t.wp), nfft3d, P(G), P(out), None,
+                           None) == lib.CPSD_ERR_ARG
+    assert np.array_equal(vp, t.vp)  # refused calls leave vp as it was
