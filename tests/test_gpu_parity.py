@@ -634,3 +634,20 @@ def test_max_bands_per_spin_matches_restatement(restatement):
     assert np.abs(st.lmd - so.lmd).max() < 1e-10 * np.abs(so.lmd).max()
     assert np.abs(st.hml - so.hml).max() < 1e-10 * np.abs(so.hml).max()
     assert np.abs(st.c2 - so.c2).max() < 1e-10
+
+
+def test_cell_shards_gpu_runner_equals_individual_cells():
+    """shards.run_cells with the GPU runner (one batched graph per SD step
+    for the rank's cells) gives each cell the energies of its own
+    resident run, bit for bit."""
+    from cpsd_b200 import shards
+    specs = [configs.small_h2(16, seed=3), configs.small_diamond(24, 4, seed=5), configs.small_h2(16, seed=4)]
+    E = shards.run_cells(specs, 2, 1)
+    for spec, e in zip(specs, E):
+        inp = inputs.build_inputs(spec)
+        cell = api.GpuCell(inp)
+        cell.set_state(inp.c2, inp.r2)
+        for _ in range(2):
+            cell.run(1)
+        assert np.array_equal(cell.E, e)
+        cell.close()

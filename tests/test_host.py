@@ -225,3 +225,70 @@ def test_new_entry_points_report_errors_without_a_gpu(tmp_path):
     assert L.cpsd_gpu_kbpp(4.0, 2, t.nrho, t.drho, P(t.rho), P(vp), P(t.wp), nfft3d, P(G), P(out), None,
                            None) == lib.CPSD_ERR_ARG
     assert np.array_equal(vp, t.vp)  # refused calls leave vp as it was
+
+
+def test_cell_shards_cover_every_cell_once_and_balance():
+    """config-4 style cells over 1..8 ranks: each cell on exactly one rank,
+    and no rank above the best balance the largest cell allows."""
+    from cpsd_b200 import shards
+    specs = configs.batched_cells(0)
+    costs = [shards.cell_cost(s) for s in specs]
+    for world in (1, 2, 3, 8):
+        parts = shards.assign(specs, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(specs)))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) <= sum(costs) / world + max(costs)
+    assert shards.assign(specs, 2) == shards.assign(specs, 2)  # deterministic
+
+
+def _restatement_runner(specs, calls, inner):
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    R = oracle.Restatement()
+    out = []
+    for spec in specs:
+        inp = inputs.build_inputs(spec)
+        st = oracle.State(inp)
+        for _ in range(calls):
+            R.run(inp, inner, st)
+        out.append(st.E.copy())
+    return np.array(out).reshape(len(specs), -1)
+
+
+def _shard_rank_main(rank, world, port, q):
+    import torch.distributed as dist
+    sys.path.insert(0, REPO)
+    from cpsd_b200 import shards
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    specs = [configs.small_h2(16, seed=3), configs.small_diamond(24, 4, seed=5), configs.small_h2(16, seed=4)]
+    E = shards.run_cells(specs, 2, 1, rank=rank, world=world, dist=dist, runner=_restatement_runner)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, E))
+
+
+def test_cell_shards_gather_equals_one_process():
+    """Two gloo ranks step their shares of three cells (the restatement
+    stands in for the GPU runner) and gather: every rank holds every cell's
+    energies, equal to one process stepping all of them."""
+    import multiprocessing as mp
+    import socket
+    from cpsd_b200 import shards
+    specs = [configs.small_h2(16, seed=3), configs.small_diamond(24, 4, seed=5), configs.small_h2(16, seed=4)]
+    want = shards.run_cells(specs, 2, 1, runner=_restatement_runner)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_shard_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    for _, E in got:
+        assert np.array_equal(E, want)
