@@ -36,6 +36,7 @@ MOVE_CASES = {
     "move_small_h2_16": (lambda: _moving(configs.small_h2(16)), 3, 2),
     "move_small_diamond_24": (lambda: _moving(configs.small_diamond(24, 4)), 3, 2),
     "move_small_diamond_32": (lambda: _moving(configs.small_diamond(32, 40, ecut=25.0, seed=12)), 2, 2),
+    "move_spin_diamond_24": (lambda: _moving(configs.spin_diamond(24, ne=(4, 3))), 3, 2),
 }
 E_TOL = 1e-9  # Ha, total energy parity bar
 F_TOL = 1e-9  # Ha/bohr, force parity bar
