@@ -1,7 +1,7 @@
 """GPU parity: the sm_100a path through the C ABI against the reference's
 golden vectors and the oracle restatement.
 
-Tolerance: the north star's FP64 bar, |E - E_ref| < 1e-9 Ha for the total
+Tolerance: the FP64 parity bar, |E - E_ref| < 1e-9 Ha for the total
 energy of every cpsd() call; matrices and orbitals to ~1e-10.
 """
 import os
