@@ -1,7 +1,7 @@
 /*
  * fft3d.c -- ORACLE / TEST INFRASTRUCTURE ONLY.  Nothing on the product path
  * links, loads or calls this file; only tests/, __graft_entry__.smoke() and
- * bench.py's cpu_baseline leg use it, as the checker.
+ * bench.py's cpu_baseline leg use it, as the oracle.
  *
  * C restatement of the reference's 3-D FFT wrapper and of the 1-D FFTPACK
  * transforms underneath it.  The reference's versions are Fortran 77 and no

@@ -1,4 +1,4 @@
-"""ORACLE / TEST INFRASTRUCTURE ONLY -- ctypes access to the CPU checkers.
+"""ORACLE / TEST INFRASTRUCTURE ONLY -- ctypes access to the CPU oracles.
 
 * ``Restatement``  -- oracle/_build/liboracle.so, the project's plain-C
   restatement of ccpsdv3/cpsd.c (cpsd_oracle.c + fft3d.c).
@@ -233,7 +233,7 @@ def epilogue(inp, st: State, gcdotc, sort=eigsrt, matmul=None) -> dict:
       layout (column-major, ld ne[ms]);
     * ``c1``: c2 V per spin (main.c:481-487), the orbitals ELCOUT holds.
 
-    ``gcdotc(nfft, a, b)`` is a checker's Gamma-point dot; ``sort(D, V)``
+    ``gcdotc(nfft, a, b)`` is an oracle's Gamma-point dot; ``sort(D, V)``
     orders the eigenpairs (V as an array, column i = vector i); ``matmul(C2, V)``
     returns C2 @ V for C2 of shape (n2ft3d, m) (numpy by default)."""
     from scipy.linalg import lapack
