@@ -245,7 +245,11 @@ int cpsd_gpu_phase_timing(cpsd_gpu_ctx *c, int on);
 int cpsd_gpu_phase_times(cpsd_gpu_ctx *c, float *ms, int max);
 const char *cpsd_gpu_phase_name(int i);
 
-/* The context the drop-in cpsd() keeps between calls (NULL before the first call). */
+/* The context the drop-in cpsd() keeps between calls (NULL before the first
+ * call).  The pointer stays valid only until the next cpsd() call whose
+ * arguments describe a different cell (grid, bands, ions or precision), which
+ * destroys that context and builds a new one; do not use it while another
+ * thread is inside cpsd(). */
 cpsd_gpu_ctx *cpsd_gpu_dropin_context(void);
 
 /* CUDA stream the context runs on (a cudaStream_t), for timing with events. */
@@ -368,6 +372,10 @@ int cpsd_overlap_tn(int method, int M, int N, int K, const double *A, long lda, 
  * looks up the array's device address (cudaGetSymbolAddress) and sets the
  * tensor-core kernel's shared-memory limit.  A caller that captures streams
  * into CUDA graphs should make that first call before any capture begins.
+ * The set-up is kept for the life of the process: a host program that calls
+ * cudaDeviceReset (or otherwise destroys the device's primary context) must
+ * not call this entry point on that device afterwards, since the cached
+ * address belonged to the destroyed context.
  * Every call on a device shares the one array, which keeps the last call's
  * contents: each call clears the status word, and every partial is written
  * before it is read.  Calls whose GPU work overlaps (on concurrent streams,

@@ -71,7 +71,11 @@ def run_cells(specs: Sequence, calls: int, inner: int, rank: int = 0, world: int
     are gathered, and every rank returns the full array in cell order."""
     runner = runner or gpu_runner
     mine = assign(specs, world)[rank]
-    local = np.asarray(runner([specs[i] for i in mine], calls, inner), dtype=np.float64).reshape(len(mine), -1)
+    if mine:
+        local = np.asarray(runner([specs[i] for i in mine], calls, inner), dtype=np.float64).reshape(len(mine), -1)
+    else:
+        # more ranks than cells: this rank runs nothing but still joins the gather
+        local = np.zeros((0, 10))
     if dist is None or world == 1:
         parts = [(mine, local)]
     else:

@@ -203,7 +203,11 @@ extern "C" int cpsd_gpu_kbpp(double zv, int lmax, int nrho, double drho, const d
     a.G = dG.p;
     a.vl = dvl.p;
     a.vnl = dvnl.p;
-    const long blocks = std::max<long>(1, std::min<long>((N + kKbppThreads - 1) / kKbppThreads, 148L * 16));
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return CPSD_ERR_CUDA;
+    const long blocks = std::max<long>(1, std::min<long>((N + kKbppThreads - 1) / kKbppThreads, (long)sms * 16));
     kbpp_kernel<<<(unsigned)blocks, kKbppThreads, smem, s>>>(a);
     if (cudaGetLastError() != cudaSuccess) return CPSD_ERR_CUDA;
     if (cudaMemcpyAsync(vl, dvl.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s) != cudaSuccess ||

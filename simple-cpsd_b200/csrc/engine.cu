@@ -8,6 +8,7 @@
 #endif
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -46,6 +47,20 @@ cudaError_t &last_cuda_error()
 }
 
 inline long cdiv(long a, long b) { return (a + b - 1) / b; }
+
+// Streaming multiprocessors of the current device (148 on a B200), looked up
+// once per device.
+int device_sms()
+{
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) return 148;
+    cache[dev].store(v, std::memory_order_relaxed);
+    return v;
+}
 
 // Allow a kernel the device's opt-in shared memory minus its static part.
 template <typename K>
@@ -347,6 +362,7 @@ struct cpsd_mlp {
 struct cpsd_gpu_ctx {
     cpsd_gpu_params prm{};
     int n = 0, nh = 0, nb = 0, ne0 = 0, ne1 = 0, nion = 0, nkatm = 0, nsh = 0, ispin = 1;
+    int sms = 148;  // streaming multiprocessors of the context's device
     long nfft3d = 0, n2ft3d = 0, n3 = 0;
     double scal1 = 0, scal2 = 0, dv = 0, dte = 0;
     cudaStream_t st = nullptr;
@@ -439,18 +455,19 @@ struct cpsd_gpu_ctx {
 
 namespace {
 
-// Split-K plan of a batch of weighted TN products: about two CTAs per SM,
-// each split at least 64 reals, partials within ws_elems.
+// Split-K plan of a batch of weighted TN products: about two CTAs per SM
+// (sms: the device's SM count), each split at least 64 reals, partials
+// within ws_elems.
 struct TnPlan {
     long splits;
     int kchunk;
 };
 
-TnPlan tn_plan(int M, int N, int K, int nprod, bool tc, size_t ws_elems)
+TnPlan tn_plan(int M, int N, int K, int nprod, bool tc, size_t ws_elems, int sms)
 {
     const int tm = tc ? kTcM : kDmT, tn = tc ? kTcN : kDmT, bk = tc ? kTcBK : kDmK;
     const long tiles = cdiv(M, tm) * cdiv(N, tn) * nprod;
-    long splits = std::max<long>(1, cdiv(2 * 148, tiles));
+    long splits = std::max<long>(1, cdiv(2L * sms, tiles));
     splits = std::min<long>(splits, std::max<long>(1, K / 64));
     while ((size_t)splits * M * N * nprod > ws_elems && splits > 1) --splits;
     const int kchunk = (int)(cdiv(cdiv(K, splits), bk) * bk);
@@ -464,7 +481,7 @@ int launch_tn(int M, int N, int K, int nprod, const double *const *A, long lda, 
               const double *w, double alpha, double beta, double *const *C, long ldc, bool tc, double *ws,
               size_t ws_elems, int *err, cudaStream_t s)
 {
-    const TnPlan pl = tn_plan(M, N, K, nprod, tc, ws_elems);
+    const TnPlan pl = tn_plan(M, N, K, nprod, tc, ws_elems, device_sms());
     TnBatch bt{};
     for (int q = 0; q < nprod; ++q) {
         bt.A[q] = A[q];
@@ -525,7 +542,7 @@ int overlaps3(cpsd_gpu_ctx *c, int m, int K, long ld, const double *C2, const do
                       ((uintptr_t)C2 % 16) == 0;
     if (!tc || !fits) return gemm_tn_batch(c, m, m, K, 3, As, ld, Bs, ld, c->w, 1.0, 0.0, Cs, m, TN_OVERLAPS);
     const long mm = (long)m * m;
-    long splits = std::min<long>(148, std::max<long>(1, K / 64));
+    long splits = std::min<long>(c->sms, std::max<long>(1, K / 64));
     while ((size_t)splits * 3 * mm > c->gemm_ws_elems && splits > 1) --splits;
     const int kchunk = (int)(cdiv(cdiv(K, splits), kOvBK) * kOvBK);
     splits = cdiv(K, kchunk);
@@ -1446,6 +1463,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     c->npw_pad = h.npw_pad;
     c->ldc = h.npw_pad;
     CK(cudaSetDevice(p->device));
+    c->sms = device_sms();
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
@@ -1526,9 +1544,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     // minimises waves x bands per CTA over the SMs' resident slots, the
     // smallest such count (fewer partial densities to add); never across spins
     {
-        int sms = 148;
-        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
-        const long slots = (long)sms * c->fft->plane_ctas_per_sm(PM_DENSITY);
+        const long slots = (long)c->sms * c->fft->plane_ctas_per_sm(PM_DENSITY);
         auto best_chunks = [&](int bands, int planes_per_chunk_group) {
             int best = 1;
             long best_cost = -1;
@@ -1578,11 +1594,11 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->Edev, 16));
     CK(ar.alloc(&c->flags, 4));
     c->gemm_splits_cap = 512;
-    // split-K partials: at least 32 MB, and room for 148 splits of the three
-    // overlaps of the largest spin
-    c->gemm_ws_elems = std::max<size_t>((size_t)4 << 20, (size_t)3 * c->ne0 * c->ne0 * 148);
+    // split-K partials: at least 32 MB, and room for one split per SM of the
+    // three overlaps of the largest spin
+    c->gemm_ws_elems = std::max<size_t>((size_t)4 << 20, (size_t)3 * c->ne0 * c->ne0 * c->sms);
     CK(ar.alloc(&c->gws, c->gemm_ws_elems));
-    c->pblocks = 148;
+    c->pblocks = c->sms;
     c->bblocks = (int)std::max<long>(1, std::min<long>(64, cdiv(c->npw, 256 * 8)));
     c->gblocks = 296;
     CK(ar.alloc(&c->ppart, 3 * c->pblocks));
@@ -2403,7 +2419,7 @@ int cpsd_overlap_tn(int method, int M, int N, int K, const double *A, long lda, 
     if (tc)
         CK(cudaFuncSetAttribute(tc_gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     const size_t cap = std::max<size_t>((size_t)M * N, (size_t)4 << 20);
-    const TnPlan pl = tn_plan(M, N, K, 1, tc, cap);
+    const TnPlan pl = tn_plan(M, N, K, 1, tc, cap, device_sms());
     struct Scratch {
         double *ws = nullptr;
         int *err = nullptr;

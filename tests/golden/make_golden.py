@@ -29,7 +29,8 @@ workloads and stores compact outputs:
   input builder is caught before parity is compared.
 
 Usage (needs the reference tree and ``make -C oracle ref``):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py NAME ...   # only these ref_<NAME> cases
 """
 from __future__ import annotations
 
@@ -61,7 +62,14 @@ CASES = [
     # spin-polarised, from the reference's plane-wave start (configs.spin_h2)
     ("spin_h2_16", lambda: configs.spin_h2(16), 3, 2, 3),
     ("spin_diamond_24", lambda: configs.spin_diamond(24, ne=(4, 3)), 3, 2, 7),
+    # the 128^3 / 64-atom / 128-band cell of the precision study: one call of
+    # two SD steps (about four minutes of reference CPU time)
+    ("diamond64_128", lambda: configs.diamond64_128(), 1, 2, 1),
 ]
+
+# cells of the 48-cell batched draw (configs.batched_cells(0)): one per grid
+# size, the most bands, mixed H/C kinds; (index in the draw, calls, inner, bands kept)
+BATCH_DRAW_CASES = [(0, 2, 2, 2), (9, 2, 2, 1), (13, 2, 2, 1), (45, 2, 2, 2)]
 
 # epilogue (main.c:452-487) after the calls: (name, spec builder, calls, inner)
 EPILOGUE_CASES = [
@@ -183,10 +191,14 @@ def run_case(ref, name, mk, ncalls, inner, keep):
         r2.append(st.r2.copy())
         fion.append(st.fion.copy())
     dn = st.dn.reshape(inp.ispin, inp.nfft, inp.nfft, inp.nfft + 2)[..., :inp.nfft]
+    c2all = packed(inp, st.c2, inp.nbands)
     out = dict(E=np.array(E), deltae=np.array(de), deltac=np.array(dc), hml=st.hml, lmd=st.lmd,
                c2=packed(inp, st.c2, keep), cpsi=packed(inp, st.cpsi, keep),
                dn_sum=dn.sum(axis=(1, 2, 3)), dn_sq=(dn * dn).sum(axis=(1, 2, 3)),
-               dn_plane0=np.ascontiguousarray(dn[:, 0]), inner=np.array(inner))
+               dn_plane0=np.ascontiguousarray(dn[:, 0]), inner=np.array(inner),
+               # every band, size-independent: sum of squares and of the
+               # coefficients over the sphere
+               c2_band_sq=(c2all * c2all).sum(axis=(1, 2)), c2_band_sum=c2all.sum(axis=(1, 2)))
     if spec.move:
         out.update(deltar=np.array(dr), r2=np.array(r2), fion=np.array(fion), r1=st.r1.copy())
     np.savez_compressed(os.path.join(HERE, "ref_%s.npz" % name), **out)
@@ -245,10 +257,27 @@ def run_main(name, mk, inner, outer):
     return input_digest(inp)
 
 
-def main():
+def batch_draw_case(index):
+    return lambda: configs.batched_cells(0)[index]
+
+
+def main(only=None):
     ref = oracle.ReferenceBuild()
+    path = os.path.join(HERE, "inputs.json")
     digests = {}
-    for name, mk, ncalls, inner, keep in CASES + MOVE_CASES:
+    if os.path.exists(path):
+        with open(path) as f:
+            digests = json.load(f)
+    cases = CASES + MOVE_CASES + [("batch0_%02d" % i, batch_draw_case(i), nc, inner, keep)
+                                  for i, nc, inner, keep in BATCH_DRAW_CASES]
+    if only:
+        for name, mk, ncalls, inner, keep in cases:
+            if name in only:
+                digests[name] = run_case(ref, name, mk, ncalls, inner, keep)
+        with open(path, "w") as f:
+            json.dump(digests, f, indent=1, sort_keys=True)
+        return
+    for name, mk, ncalls, inner, keep in cases:
         digests[name] = run_case(ref, name, mk, ncalls, inner, keep)
     for name, mk, ncalls, inner in EPILOGUE_CASES:
         digests["epi_" + name] = run_epilogue(ref, name, mk, ncalls, inner)
@@ -266,4 +295,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(set(sys.argv[1:]) or None)

@@ -29,7 +29,15 @@ CASES = {
     # spin-polarised, from the reference's plane-wave start
     "spin_h2_16": (lambda: configs.spin_h2(16), 3, 2),
     "spin_diamond_24": (lambda: configs.spin_diamond(24, ne=(4, 3)), 3, 2),
+    # the 128^3 / 64-atom / 128-band cell of the precision study
+    "diamond64_128": (lambda: configs.diamond64_128(), 1, 2),
+    # cells of the 48-cell batched draw, each on its own
+    "batch0_00": (lambda: configs.batched_cells(0)[0], 2, 2),
+    "batch0_09": (lambda: configs.batched_cells(0)[9], 2, 2),
+    "batch0_13": (lambda: configs.batched_cells(0)[13], 2, 2),
+    "batch0_45": (lambda: configs.batched_cells(0)[45], 2, 2),
 }
+BATCH_DRAW = {0: "batch0_00", 9: "batch0_09", 13: "batch0_13", 45: "batch0_45"}
 
 
 def packed(inp, c, nbands):
@@ -53,6 +61,10 @@ def check_against_golden(inp, g, rows, st):
     dn = dn[..., :inp.nfft]
     assert np.allclose(dn.sum(axis=(1, 2, 3)), g["dn_sum"], rtol=1e-12, atol=0)
     assert np.allclose(dn[:, 0], g["dn_plane0"], rtol=1e-11, atol=1e-15)
+    if "c2_band_sq" in g:  # every band: sums of squares and of the coefficients
+        c2 = packed(inp, st.c2, inp.nbands)
+        assert np.abs((c2 * c2).sum(axis=(1, 2)) - g["c2_band_sq"]).max() < 1e-10
+        assert np.abs(c2.sum(axis=(1, 2)) - g["c2_band_sum"]).max() < 1e-9
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -131,6 +143,8 @@ MOVE_CASES = {
     "move_small_h2_16": (lambda: _moving(configs.small_h2(16)), 3, 2),
     "move_small_diamond_24": (lambda: _moving(configs.small_diamond(24, 4)), 3, 2),
     "move_small_diamond_32": (lambda: _moving(configs.small_diamond(32, 40, ecut=25.0, seed=12)), 2, 2),
+    # spin-polarised: the nonlocal force factor is 1 instead of 2 (cpsd.c:287-304)
+    "move_spin_diamond_24": (lambda: _moving(configs.spin_diamond(24, ne=(4, 3))), 3, 2),
 }
 F_TOL = 1e-9  # Ha/bohr
 
@@ -435,6 +449,34 @@ def test_batched_cells_equal_individual_runs():
     E = batch.run(2)
     for i in range(len(inps)):
         assert np.array_equal(E[i], solo[i]), i
+    batch.close()
+    for c in cells:
+        c.close()
+
+
+def test_batched_draw_matches_reference(golden):
+    """The 48-cell batched workload (grids 32/48/64, 4-25 bands, H and C
+    kinds), all cells in one graph per SD step: the cells with fixtures from
+    the reference build match them call by call (energies, deltae, deltac)
+    and after the last call (hml, lmd, orbitals, density)."""
+    specs = configs.batched_cells(0)
+    inps = [inputs.build_inputs(s) for s in specs]
+    cells = []
+    for inp in inps:
+        cell = api.GpuCell(inp)
+        cell.set_state(inp.c2, inp.r2)
+        cells.append(cell)
+    batch = api.GpuBatch(cells)
+    rows = {i: [] for i in BATCH_DRAW}
+    for _ in range(2):
+        E = batch.run(2)
+        for i in BATCH_DRAW:
+            rows[i].append((E[i].copy(), batch.deltae[i], batch.deltac[i]))
+    for i, name in BATCH_DRAW.items():
+        st = api.State(inps[i])
+        cells[i].get_state(st)
+        check_against_golden(inps[i], golden(name), rows[i], st)
+    assert np.all(np.isfinite(batch.E))
     batch.close()
     for c in cells:
         c.close()

@@ -1,0 +1,87 @@
+"""Per-term error of the mixed-precision path against the FP64 reference.
+
+Every energy term E[0..9] of ccpsdv3/cpsd.c:497-647 (E[0] total at :638;
+E[1] eorbit, E[2] ehartr, E[3] exc, E[4] eion, E[5] eke, E[6] elocal,
+E[7] enlocal, E[8] 2 ehartr, E[9] pxc; :639-647) after the
+same cpsd() calls as the reference build's fixtures, for each precision
+mode of the engine:
+
+* ``fp32_fft``      FP32 transforms and plane passes, FP64 state, products,
+                    reductions and Lagrange solve;
+* ``tf32x3_proj``   + the KB projector contraction and back-projection as
+                    3xTF32 tcgen05 products;
+* ``tf32x3_ovl``    + the three Lagrange overlaps and the constraint
+                    correction as 3xTF32 tcgen05 products;
+* ``refined``       ``tf32x3_ovl`` for all calls but the last, then the
+                    last call in FP64 (the refinement sweep): its energies
+                    are FP64 evaluations of a state that carries the mixed
+                    steps' error.
+
+The fixtures are the reference's own serial C build (tests/golden), FP64
+throughout: diamond8_64 (64^3, 8 atoms, 16 bands; 4 calls of 2 steps) and
+diamond64_128 (128^3, 64 atoms, 128 bands; 1 call of 2 steps).  Bound per
+term: |dE_k| <= REL[mode] * (|E_k| + 1 Ha).  With CPSD_PRECISION_TABLE set
+to a file path the measured table is written there as JSON.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from cpsd_b200 import api, configs, inputs, lib
+
+pytestmark = pytest.mark.gpu
+
+TERMS = ["E", "eorbit", "ehartr", "exc", "eion", "eke", "elocal", "enlocal", "2ehartr", "pxc"]
+MODES = {
+    "fp32_fft": (lib.CPSD_GEMM_FP64, False),
+    "tf32x3_proj": (lib.CPSD_GEMM_TF32X3, False),
+    "tf32x3_ovl": (lib.CPSD_GEMM_TF32X3_OVERLAPS, False),
+    "refined": (lib.CPSD_GEMM_TF32X3_OVERLAPS, True),
+}
+# relative bound per term and mode (measured values are about 10x smaller)
+REL = {"fp32_fft": 1e-6, "tf32x3_proj": 1e-6, "tf32x3_ovl": 2e-5, "refined": 2e-5}
+WORKLOADS = {
+    "diamond8_64": (configs.diamond8_64, 4, 2),
+    "diamond64_128": (configs.diamond64_128, 1, 2),
+}
+_table = {}
+
+
+def _run_mode(inp, ncalls, inner, gemm, refine):
+    cell = api.GpuCell(inp, precision=lib.CPSD_PREC_MIXED)
+    cell.set_gemm(gemm)
+    cell.set_state(inp.c2, inp.r2)
+    rows = []
+    for k in range(ncalls):
+        if refine and k == ncalls - 1:
+            cell.set_precision(lib.CPSD_PREC_FP64)
+        cell.run(inner)
+        rows.append(cell.E.copy())
+    cell.close()
+    return np.array(rows)
+
+
+@pytest.mark.parametrize("workload", list(WORKLOADS))
+def test_per_term_error_of_mixed_modes(golden, workload):
+    mk, ncalls, inner = WORKLOADS[workload]
+    g = golden(workload)
+    assert g["E"].shape[0] == ncalls and int(g["inner"]) == inner
+    inp = inputs.build_inputs(mk())
+    ref = g["E"]
+    out, bad = {}, []
+    for mode, (gemm, refine) in MODES.items():
+        E = _run_mode(inp, ncalls, inner, gemm, refine)
+        dE = np.abs(E - ref).max(axis=0)  # worst call, per term
+        out[mode] = {t: float(d) for t, d in zip(TERMS, dE)}
+        out[mode]["E_per_atom"] = float(dE[0] / inp.nion)
+        bound = REL[mode] * (np.abs(ref).max(axis=0) + 1.0)
+        bad += [(mode, TERMS[k], float(dE[k]), float(bound[k])) for k in range(10) if not dE[k] <= bound[k]]
+    out["reference_E"] = {t: float(v) for t, v in zip(TERMS, ref[-1])}
+    _table[workload] = out
+    path = os.environ.get("CPSD_PRECISION_TABLE")
+    if path:
+        with open(path, "w") as f:
+            json.dump(_table, f, indent=1)
+    assert not bad, bad

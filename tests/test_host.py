@@ -256,34 +256,42 @@ def _restatement_runner(specs, calls, inner):
     return np.array(out).reshape(len(specs), -1)
 
 
+def _shard_specs():
+    return [configs.small_h2(16, seed=3), configs.small_diamond(24, 4, seed=5), configs.small_h2(16, seed=4)]
+
+
 def _shard_rank_main(rank, world, port, q):
+    import datetime
     import torch.distributed as dist
     sys.path.insert(0, REPO)
     from cpsd_b200 import shards
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    dist.init_process_group("gloo", rank=rank, world_size=world)
-    specs = [configs.small_h2(16, seed=3), configs.small_diamond(24, 4, seed=5), configs.small_h2(16, seed=4)]
-    E = shards.run_cells(specs, 2, 1, rank=rank, world=world, dist=dist, runner=_restatement_runner)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    E = shards.run_cells(_shard_specs(), 2, 1, rank=rank, world=world, dist=dist, runner=_restatement_runner)
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, E))
 
 
-def test_cell_shards_gather_equals_one_process():
-    """Two gloo ranks step their shares of three cells (the restatement
-    stands in for the GPU runner) and gather: every rank holds every cell's
-    energies, equal to one process stepping all of them."""
+@pytest.mark.parametrize("world", [2, 4])
+def test_cell_shards_gather_equals_one_process(world):
+    """gloo ranks step their shares of three cells (the restatement stands
+    in for the GPU runner) and gather: every rank holds every cell's
+    energies, equal to one process stepping all of them.  With 4 ranks one
+    rank has no cell and still joins the gather."""
     import multiprocessing as mp
     import socket
     from cpsd_b200 import shards
-    specs = [configs.small_h2(16, seed=3), configs.small_diamond(24, 4, seed=5), configs.small_h2(16, seed=4)]
+    specs = _shard_specs()
+    if world > len(specs):
+        assert any(not p for p in shards.assign(specs, world))
     want = shards.run_cells(specs, 2, 1, runner=_restatement_runner)
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_shard_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_shard_rank_main, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
     got = [q.get(timeout=300) for _ in procs]
@@ -292,3 +300,22 @@ def test_cell_shards_gather_equals_one_process():
     assert all(p.exitcode == 0 for p in procs)
     for _, E in got:
         assert np.array_equal(E, want)
+
+
+def test_cell_shards_rank_without_cells_runs_nothing():
+    """More ranks than cells: the empty rank never calls its runner and its
+    share is an empty (0 x 10) block, so it reaches the gather."""
+    from cpsd_b200 import shards
+    specs = _shard_specs()
+    calls = []
+
+    def runner(s, c, i):
+        calls.append(len(s))
+        return _restatement_runner(s, c, i)
+
+    parts = shards.assign(specs, 5)
+    empty = [r for r, p in enumerate(parts) if not p]
+    assert len(empty) == 2
+    with pytest.raises(RuntimeError):  # alone, an empty rank holds no cell's energies
+        shards.run_cells(specs, 1, 1, rank=empty[0], world=5, runner=runner)
+    assert calls == []

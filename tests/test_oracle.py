@@ -23,6 +23,12 @@ CASES = {
     "diamond8_64": (lambda: configs.diamond8_64(), 4, 2),
     "spin_h2_16": (lambda: configs.spin_h2(16), 3, 2),
     "spin_diamond_24": (lambda: configs.spin_diamond(24, ne=(4, 3)), 3, 2),
+    # cells of the 48-cell batched draw (make_golden.BATCH_DRAW_CASES): 32^3
+    # with H and C kinds, 48^3 / 19 bands, 64^3 / 14 ions, 32^3 / 25 bands
+    "batch0_00": (lambda: configs.batched_cells(0)[0], 2, 2),
+    "batch0_09": (lambda: configs.batched_cells(0)[9], 2, 2),
+    "batch0_13": (lambda: configs.batched_cells(0)[13], 2, 2),
+    "batch0_45": (lambda: configs.batched_cells(0)[45], 2, 2),
 }
 
 
@@ -120,6 +126,9 @@ def test_inputs_match_fixture_digests():
         assert input_digest(inputs.build_inputs(mk())) == want[name], name
     for name, mk in EPI_CASES.items():
         assert input_digest(inputs.build_inputs(mk())) == want["epi_" + name], name
+    # the 128^3 cell's fixture is checked against the GPU path only (one
+    # reference call of two steps takes minutes on the host)
+    assert input_digest(inputs.build_inputs(configs.diamond64_128())) == want["diamond64_128"]
 
 
 def test_orbitals_orthonormal_and_hermitian():
