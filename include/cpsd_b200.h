@@ -252,6 +252,73 @@ const char *cpsd_gpu_phase_name(int i);
  * thread is inside cpsd(). */
 cpsd_gpu_ctx *cpsd_gpu_dropin_context(void);
 
+/* ------------------------------------------------------ band-parallel SD
+ * One cell stepped by several ranks (one GPU each), every rank holding the
+ * whole state.  No counterpart in the serial reference; its MPI build
+ * (ccpsdv3-mpi) splits the FFT grid instead (d3db-mpi.c:817-1099, the
+ * reductions of Parallel.c:50-70 used at ccpsdv3-mpi/cpsd.c:385, 459-462).
+ * Here the bands are split: rank r transforms, densifies and steps bands
+ * [lo, hi) (phases 0 and 1), the caller sums the spin densities over the
+ * ranks between phases 0 and 1 and gathers every rank's rows of c2 between
+ * phases 1 and 2, and phase 2 (overlaps, Lagrange iteration, constraint,
+ * cpsd.c:415-488) runs on all bands on every rank.  The caller's exchange
+ * (an NCCL all-reduce and broadcasts over torch.distributed in
+ * cpsd_b200.bands) runs on the context's stream, between the calls. */
+
+/* Make the context step bands [lo, hi) only (hi < 0: every band again, the
+ * ordinary path).  Not with a learned preconditioner or ion motion
+ * (CPSD_ERR_ARG).  cpsd_gpu_run is refused while it is set. */
+int cpsd_gpu_set_band_range(cpsd_gpu_ctx *c, int lo, int hi);
+/* Enqueue phase 0, 1 or 2 of an SD step on the context's stream (without a
+ * band range the three phases back to back are one ordinary SD step). */
+int cpsd_gpu_step_phase(cpsd_gpu_ctx *c, int phase);
+/* Device arrays of the exchanges: dn_part (this rank's spin densities,
+ * ispin * nfft^3 doubles, after phase 0), dn (their sum, which the caller
+ * writes before phase 1), c2 and cpsi (the current step's new orbitals and
+ * -H psi, bands x ld doubles; after phase 1 rows [lo, hi) are this rank's). */
+int cpsd_gpu_bp_buffers(cpsd_gpu_ctx *c, double **dn_part, double **dn, double **c2, double **cpsi, long *ld);
+/* The energies of a call of `inner` band-parallel steps (cpsd.c:494-672),
+ * after the caller has gathered every rank's rows of cpsi of the last step;
+ * E[0] in: the previous total energy.  Every rank computes the same values. */
+int cpsd_gpu_bp_finish(cpsd_gpu_ctx *c, int inner, double *E, double *deltae, double *deltac);
+
+/* ------------------------------------------------------ tuning
+ * Kernel choices of a context that change speed, not the algorithm (results
+ * agree to rounding).  No counterpart in the reference.  The choices apply to
+ * the transforms of the precision the context runs at the time of the call;
+ * set them before batching the context (cpsd_gpu_batch_create). */
+typedef struct {
+    int plane_occupancy[4]; /* per plane pass (0 density, 1 V psi, 2 potential to r,
+                               3 density to G): 0 = the build for one CTA per SM (up to
+                               255 registers a thread), 1 = the one for two (128) */
+    int tn_ctas_per_sm;     /* split-K target of the weighted TN products: CTAs per SM, 1..8 */
+    int density_chunks;     /* band chunks per spin of the density pass */
+    int lagrange_solver;    /* more than 32 bands: 1 = 4 x 4 tiled cluster, 2 = column
+                               cluster; 0 for the single-CTA solver of <= 32 bands */
+} cpsd_gpu_tuning;
+int cpsd_gpu_get_tuning(const cpsd_gpu_ctx *c, cpsd_gpu_tuning *t);
+/* Largest accepted value of every field (lagrange_solver 1 needs a device that
+ * schedules its 16-CTA clusters). */
+int cpsd_gpu_tuning_limits(const cpsd_gpu_ctx *c, cpsd_gpu_tuning *max);
+/* CPSD_ERR_ARG for a value out of range (nothing is changed then). */
+int cpsd_gpu_set_tuning(cpsd_gpu_ctx *c, const cpsd_gpu_tuning *t);
+
+/*
+ * The project's autotuner: times `steps` SD steps (best of three, captured
+ * graphs) for the candidates of one field at a time on this context's own
+ * cell -- both plane builds per pass, density chunk counts around the SM-wave
+ * model, split-K targets 1, 2 and 4, the two cluster Lagrange solvers -- and
+ * keeps a choice that is at least 2% faster.  The result is cached per
+ * process by shape (device, grid, bands, sphere, projectors, precision,
+ * product engine, learned step, ion motion): a later context of the same
+ * shape takes it without timing unless `force`.  Needs the tables and a
+ * state; the orbitals and step counters are restored, so call it after
+ * cpsd_gpu_set_state and before cpsd_gpu_run (the other outputs of a run are
+ * not kept).  ms_before / ms_after (may be NULL): ms per SD step of the
+ * choices on entry and of the ones kept (-1 when taken from the cache).
+ */
+int cpsd_gpu_autotune(cpsd_gpu_ctx *c, int steps, int force, float *ms_before, float *ms_after);
+
 /* CUDA stream the context runs on (a cudaStream_t), for timing with events. */
 void *cpsd_gpu_stream(cpsd_gpu_ctx *c);
 

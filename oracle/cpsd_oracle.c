@@ -246,18 +246,18 @@ static double erfc_as(double w)
 
 /* -------------------------------------------------------------- the loop */
 
-int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
-                int nfft, int nfft3d, int n2ft3d, const double *unitg,
-                double omega, double dt, double fmass, const int *katm,
-                const double *amass, const double *zv, int nsh,
-                const double *rcell, double cewald, double rcut,
-                const int *masker, const double *G, const double *tg,
-                const double *vc, const double *vg, const int *lmmax,
-                const double *vnlnrm, const double *vl, const double *vnl,
-                double *r1, double *r2, double *fion, double *c1, double *c2,
-                double *cpsi, double *dn, double *hml, double *lmd, double *E,
-                double *deltae, double *deltac, double *deltar,
-                int *lagrange_fail)
+static int cpsd_impl(int inner, int move, int nion, int ispin, const int *ne,
+                     int nfft, int nfft3d, int n2ft3d, const double *unitg,
+                     double omega, double dt, double fmass, const int *katm,
+                     const double *amass, const double *zv, int nsh,
+                     const double *rcell, double cewald, double rcut,
+                     const int *masker, const double *G, const double *tg,
+                     const double *vc, const double *vg, const int *lmmax,
+                     const double *vnlnrm, const double *vl, const double *vnl,
+                     double *r1, double *r2, double *fion, double *c1, double *c2,
+                     double *cpsi, double *dn, double *hml, double *lmd, double *E,
+                     double *deltae, double *deltac, double *deltar,
+                     int *lagrange_fail, const oracle_bands *bp)
 {
     const double CERFC = 1.128379167;
     const int nbands = ne[0] + ne[1];
@@ -267,6 +267,9 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
     const double dv = omega * scal1;
     const double dte = dt / sqrt(fmass); /* cpsd.c:114 */
     int n1[2] = {0, ne[0]}, n2[2] = {ne[0] - 1, ne[0] + ne[1] - 1};
+    /* band-parallel: this rank transforms and steps bands [blo, bhi) only */
+    const int blo = bp ? bp->lo : 0, bhi = bp ? bp->hi : nbands;
+    if (bp && (move || blo < 0 || bhi > nbands || blo > bhi)) return -2;
     int inc2c = nfft / 2 + 1, inc3c = (nfft / 2 + 1) * nfft, inc2r = nfft + 2,
         inc3r = (nfft + 2) * nfft, naux = 0;
     int nf = nfft;
@@ -304,7 +307,7 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
 
         /* psi(G) -> psi(r), cpsd.c:177-181 */
         memcpy(cpsi, c1, sizeof(double) * (size_t)nn);
-        for (int i = 0; i < nbands; ++i)
+        for (int i = blo; i < bhi; ++i)
             cr_fft3b_(cpsi + (long)i * n2ft3d, &inc2c, &inc3c, &inc2r, &inc3r, &nf, &nf, &nf, NULL, &naux);
 
         /* spin densities, cpsd.c:185-194 */
@@ -312,6 +315,7 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
         for (int ms = 0; ms < ispin; ++ms) {
             double *d = dn + (long)ms * n2ft3d;
             for (int i = n1[ms]; i <= n2[ms]; ++i) {
+                if (i < blo || i >= bhi) continue;
                 const double *p = cpsi + (long)i * n2ft3d;
                 for (long k = 0; k < n2ft3d; ++k) d[k] += scal2 * (p[k] * p[k]);
             }
@@ -320,6 +324,8 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
                 d[l * inc2r + nfft + 1] = 0.0;
             }
         }
+        /* band-parallel: the spin densities summed over the ranks */
+        if (bp) bp->allreduce_sum(dn, (long)ispin * n2ft3d, bp->user);
 
         /* rho(G), cpsd.c:198-205 */
         for (long k = 0; k < n2ft3d; ++k) dng[k] = (dn[k] + dn[k + (long)(ispin - 1) * n2ft3d]) * scal1;
@@ -330,7 +336,7 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
         oracle_phafac(nfft, unitg, nion, r1, ex1, ex2, ex3);
 
         /* kinetic, cpsd.c:212-221 */
-        for (int i = 0; i < nbands; ++i) {
+        for (int i = blo; i < bhi; ++i) {
             const double *a = c1 + (long)i * n2ft3d;
             double *b = c2 + (long)i * n2ft3d;
             for (long k = 0; k < nfft3d; ++k) {
@@ -373,7 +379,7 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
                         vtmp[2 * k + 1] = exi[2 * k] * w[k];
                     }
                 }
-                for (int i = 0; i < nbands; ++i) { /* cpsd.c:287-305 */
+                for (int i = blo; i < bhi; ++i) { /* cpsd.c:287-305 */
                     const double *a = c1 + (long)i * n2ft3d;
                     double *b = c2 + (long)i * n2ft3d;
                     double sw1 = -oracle_gcdotc(nfft, vtmp, a) * scal2 / vnlnrm[ia * 9 + l];
@@ -438,6 +444,7 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
         /* V psi back to G and -H psi, cpsd.c:384-396 */
         for (int ms = 0; ms < ispin; ++ms)
             for (int i = n1[ms]; i <= n2[ms]; ++i) {
+                if (i < blo || i >= bhi) continue;
                 double *p = cpsi + (long)i * n2ft3d;
                 const double *x = xcp + (long)ms * n2ft3d;
                 for (long k = 0; k < n2ft3d; ++k) p[k] *= (vtmp[k] + x[k]);
@@ -447,7 +454,12 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
             }
 
         /* steepest descent, cpsd.c:399-411 */
-        for (long k = 0; k < nn; ++k) c2[k] = c1[k] + dte * cpsi[k];
+        for (long k = (long)blo * n2ft3d; k < (long)bhi * n2ft3d; ++k) c2[k] = c1[k] + dte * cpsi[k];
+        /* band-parallel: every rank's new orbitals (and -H psi) to every rank */
+        if (bp) {
+            bp->allgather_rows(c2, n2ft3d, bp->user);
+            bp->allgather_rows(cpsi, n2ft3d, bp->user);
+        }
         if (move)
             for (int ii = 0; ii < nion; ++ii)
                 for (int d = 0; d < 3; ++d) r2[3 * ii + d] = r1[3 * ii + d] + dti[ii] * fion[3 * ii + d];
@@ -641,4 +653,41 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
     free(dng); free(vall); free(vtmp); free(s); free(exi); free(xcp); free(xce);
     free(ex1); free(ex2); free(ex3); free(lag); free(dti);
     return 0;
+}
+
+int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
+                int nfft, int nfft3d, int n2ft3d, const double *unitg,
+                double omega, double dt, double fmass, const int *katm,
+                const double *amass, const double *zv, int nsh,
+                const double *rcell, double cewald, double rcut,
+                const int *masker, const double *G, const double *tg,
+                const double *vc, const double *vg, const int *lmmax,
+                const double *vnlnrm, const double *vl, const double *vnl,
+                double *r1, double *r2, double *fion, double *c1, double *c2,
+                double *cpsi, double *dn, double *hml, double *lmd, double *E,
+                double *deltae, double *deltac, double *deltar,
+                int *lagrange_fail)
+{
+    return cpsd_impl(inner, move, nion, ispin, ne, nfft, nfft3d, n2ft3d, unitg, omega, dt, fmass, katm, amass,
+                     zv, nsh, rcell, cewald, rcut, masker, G, tg, vc, vg, lmmax, vnlnrm, vl, vnl, r1, r2, fion,
+                     c1, c2, cpsi, dn, hml, lmd, E, deltae, deltac, deltar, lagrange_fail, NULL);
+}
+
+int oracle_cpsd_bands(int inner, int nion, int ispin, const int *ne,
+                      int nfft, int nfft3d, int n2ft3d, const double *unitg,
+                      double omega, double dt, double fmass, const int *katm,
+                      const double *amass, const double *zv, int nsh,
+                      const double *rcell, double cewald, double rcut,
+                      const int *masker, const double *G, const double *tg,
+                      const double *vc, const double *vg, const int *lmmax,
+                      const double *vnlnrm, const double *vl, const double *vnl,
+                      double *r1, double *r2, double *fion, double *c1, double *c2,
+                      double *cpsi, double *dn, double *hml, double *lmd, double *E,
+                      double *deltae, double *deltac, double *deltar,
+                      int *lagrange_fail, const oracle_bands *bp)
+{
+    if (!bp || !bp->allreduce_sum || !bp->allgather_rows) return -2;
+    return cpsd_impl(inner, 0, nion, ispin, ne, nfft, nfft3d, n2ft3d, unitg, omega, dt, fmass, katm, amass,
+                     zv, nsh, rcell, cewald, rcut, masker, G, tg, vc, vg, lmmax, vnlnrm, vl, vnl, r1, r2, fion,
+                     c1, c2, cpsi, dn, hml, lmd, E, deltae, deltac, deltar, lagrange_fail, bp);
 }

@@ -53,6 +53,36 @@ int oracle_cpsd(int inner, int move, int nion, int ispin, const int *ne,
                 double *deltae, double *deltac, double *deltar,
                 int *lagrange_fail);
 
+/*
+ * Band-parallel form of the same step (move = 0), the decomposition a
+ * multi-GPU run of one cell uses: this rank transforms, densifies and steps
+ * only bands [lo, hi); allreduce_sum adds the spin densities of all ranks in
+ * place (after the density, cpsd.c:185-194), allgather_rows gives every rank
+ * the rows of buf that each rank owns (its [lo, hi), row doubles each) after
+ * the steepest-descent update (cpsd.c:399-400), for c2 and for cpsi.  The
+ * overlaps, the Lagrange iteration, the constraint and the energies then run
+ * on the full arrays on every rank.  Returns -2 for a bad range.
+ */
+typedef struct {
+    int lo, hi;
+    void (*allreduce_sum)(double *buf, long n, void *user);
+    void (*allgather_rows)(double *buf, long row, void *user);
+    void *user;
+} oracle_bands;
+
+int oracle_cpsd_bands(int inner, int nion, int ispin, const int *ne,
+                      int nfft, int nfft3d, int n2ft3d, const double *unitg,
+                      double omega, double dt, double fmass, const int *katm,
+                      const double *amass, const double *zv, int nsh,
+                      const double *rcell, double cewald, double rcut,
+                      const int *masker, const double *G, const double *tg,
+                      const double *vc, const double *vg, const int *lmmax,
+                      const double *vnlnrm, const double *vl, const double *vnl,
+                      double *r1, double *r2, double *fion, double *c1, double *c2,
+                      double *cpsi, double *dn, double *hml, double *lmd, double *E,
+                      double *deltae, double *deltac, double *deltar,
+                      int *lagrange_fail, const oracle_bands *bp);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,16 @@ def _common_args(inp, inner: int, move: int):
     ]
 
 
+class _Bands(ctypes.Structure):
+    """oracle_bands of oracle.h."""
+    _fields_ = [("lo", ctypes.c_int), ("hi", ctypes.c_int), ("allreduce_sum", ctypes.c_void_p),
+                ("allgather_rows", ctypes.c_void_p), ("user", ctypes.c_void_p)]
+
+    def __init__(self, lo, hi, red, gat, user):
+        super().__init__(lo, hi, ctypes.cast(red, ctypes.c_void_p), ctypes.cast(gat, ctypes.c_void_p), user)
+        self._keep = (red, gat)
+
+
 class Restatement:
     def __init__(self, path: str = RESTATEMENT_SO):
         if not os.path.exists(path):
@@ -93,6 +103,32 @@ class Restatement:
                                   ctypes.byref(dd[1]), ctypes.byref(dd[2]), ctypes.byref(fail))
         if rc != 0:
             raise MemoryError("oracle_cpsd could not allocate scratch")
+        st.deltae, st.deltac, st.deltar = dd[0].value, dd[1].value, dd[2].value
+        st.lagrange_fail += fail.value
+        return st
+
+    def run_bands(self, inp, inner: int, st: State, lo: int, hi: int, allreduce_sum, allgather_rows) -> State:
+        """The band-parallel form (oracle_cpsd_bands, move = 0): this rank
+        steps bands [lo, hi); allreduce_sum(array) adds an array over the
+        ranks in place and allgather_rows(array2d) fills every rank's rows
+        of a (bands x row) array in place -- numpy views of the C buffers."""
+        ne, args = _common_args(inp, inner, 0)
+        del args[1]  # no move argument
+        dd = [ctypes.c_double() for _ in range(3)]
+        fail = ctypes.c_int()
+        RED = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_long, ctypes.c_void_p)
+        GAT = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_long, ctypes.c_void_p)
+        nb = inp.nbands
+        red = RED(lambda p, n, u: allreduce_sum(np.ctypeslib.as_array(p, shape=(n,))))
+        gat = GAT(lambda p, row, u: allgather_rows(np.ctypeslib.as_array(p, shape=(nb, row))))
+        bp = _Bands(lo, hi, red, gat, None)
+        rc = self.lib.oracle_cpsd_bands(*args, _ptr(st.r1), _ptr(st.r2), _ptr(st.fion), _ptr(st.c1),
+                                        _ptr(st.c2), _ptr(st.cpsi), _ptr(st.dn), _ptr(st.hml),
+                                        _ptr(st.lmd), _ptr(st.E), ctypes.byref(dd[0]),
+                                        ctypes.byref(dd[1]), ctypes.byref(dd[2]), ctypes.byref(fail),
+                                        ctypes.byref(bp))
+        if rc != 0:
+            raise ValueError("oracle_cpsd_bands: status %d" % rc)
         st.deltae, st.deltac, st.deltar = dd[0].value, dd[1].value, dd[2].value
         st.lagrange_fail += fail.value
         return st

@@ -101,6 +101,7 @@ class GpuCell:
         if rc:
             raise CpsdError(rc, "cpsd_gpu_create")
         self.h = h
+        self.device = device
         self._check(L.cpsd_gpu_set_tables(
             h, _ptr(inp.katm), _ptr(inp.amass), _ptr(inp.zv), _ptr(inp.rcell), _ptr(inp.G),
             _ptr(inp.tg), _ptr(inp.vc), _ptr(inp.vg), _ptr(inp.lmmax), _ptr(inp.vnlnrm),
@@ -158,6 +159,63 @@ class GpuCell:
         self._check(self._L.cpsd_gpu_set_preconditioner(self.h, mlp.h if mlp is not None else None),
                     "cpsd_gpu_set_preconditioner")
         self._mlp = mlp  # keep it alive while attached
+
+    # band-parallel SD (cpsd_b200.bands drives these)
+    def set_band_range(self, lo: int, hi: int) -> None:
+        self._check(self._L.cpsd_gpu_set_band_range(self.h, int(lo), int(hi)), "cpsd_gpu_set_band_range")
+
+    def step_phase(self, phase: int) -> None:
+        self._check(self._L.cpsd_gpu_step_phase(self.h, int(phase)), "cpsd_gpu_step_phase")
+
+    def bp_buffers(self):
+        """Device addresses (dn_part, dn, c2, cpsi) and the row length in doubles."""
+        p = [ctypes.c_void_p() for _ in range(4)]
+        ld = ctypes.c_long()
+        self._check(self._L.cpsd_gpu_bp_buffers(self.h, *[ctypes.byref(x) for x in p], ctypes.byref(ld)),
+                    "cpsd_gpu_bp_buffers")
+        return tuple(x.value for x in p) + (ld.value,)
+
+    def bp_finish(self, inner: int) -> np.ndarray:
+        de, dc = ctypes.c_double(), ctypes.c_double()
+        rc = self._L.cpsd_gpu_bp_finish(self.h, int(inner), _ptr(self.E), ctypes.byref(de), ctypes.byref(dc))
+        if rc == _l.CPSD_WARN_LAGRANGE:
+            self.lagrange_warnings += 1
+        elif rc != _l.CPSD_OK:
+            raise CpsdError(rc, "cpsd_gpu_bp_finish")
+        self.deltae, self.deltac = de.value, dc.value
+        return self.E
+
+    def tuning(self) -> dict:
+        """The kernel choices of this context (cpsd_gpu_get_tuning)."""
+        t = _l.Tuning()
+        self._check(self._L.cpsd_gpu_get_tuning(self.h, ctypes.byref(t)), "cpsd_gpu_get_tuning")
+        return t.as_dict()
+
+    def tuning_limits(self) -> dict:
+        t = _l.Tuning()
+        self._check(self._L.cpsd_gpu_tuning_limits(self.h, ctypes.byref(t)), "cpsd_gpu_tuning_limits")
+        return t.as_dict()
+
+    def set_tuning(self, **kw) -> None:
+        """Change some kernel choices (cpsd_gpu_set_tuning); unnamed fields keep their values."""
+        cur = self.tuning()
+        cur.update(kw)
+        t = _l.Tuning()
+        for i, v in enumerate(cur["plane_occupancy"]):
+            t.plane_occupancy[i] = int(v)
+        t.tn_ctas_per_sm = int(cur["tn_ctas_per_sm"])
+        t.density_chunks = int(cur["density_chunks"])
+        t.lagrange_solver = int(cur["lagrange_solver"])
+        self._check(self._L.cpsd_gpu_set_tuning(self.h, ctypes.byref(t)), "cpsd_gpu_set_tuning")
+
+    def autotune(self, steps: int = 10, force: bool = False) -> dict:
+        """Time the candidate kernel choices on this cell and keep the
+        fastest (cpsd_gpu_autotune); returns the choices and ms per SD step
+        before and after (-1 when the process cache had this shape)."""
+        b, a = ctypes.c_float(), ctypes.c_float()
+        self._check(self._L.cpsd_gpu_autotune(self.h, int(steps), int(force), ctypes.byref(b), ctypes.byref(a)),
+                    "cpsd_gpu_autotune")
+        return {"tuning": self.tuning(), "ms_per_step_before": b.value, "ms_per_step_after": a.value}
 
     def set_gemm(self, mode: int) -> None:
         """TN-product engine of the mixed path: CPSD_GEMM_FP64 or CPSD_GEMM_TF32X3."""

@@ -51,6 +51,8 @@ EXPORTS = [
     "cpsd_gpu_get_packed", "cpsd_gpu_set_packed", "cpsd_gpu_get_sphere", "cpsd_gpu_set_gemm",
     "cpsd_overlap_tn", "cpsd_overlap_tn_noalloc", "cpsd_gpu_epilogue", "cpsd_write_elcout",
     "cpsd_write_ionout", "cpsd_gpu_kbpp", "cpsd_makepsi",
+    "cpsd_gpu_get_tuning", "cpsd_gpu_set_tuning", "cpsd_gpu_tuning_limits", "cpsd_gpu_autotune",
+    "cpsd_gpu_set_band_range", "cpsd_gpu_step_phase", "cpsd_gpu_bp_buffers", "cpsd_gpu_bp_finish",
 ]
 
 
@@ -60,6 +62,16 @@ class Params(ctypes.Structure):
         ("precision", _I), ("device", _I), ("unitg", _D * 9), ("omega", _D), ("dt", _D),
         ("fmass", _D), ("cewald", _D), ("rcut", _D),
     ]
+
+
+class Tuning(ctypes.Structure):
+    """cpsd_gpu_tuning of include/cpsd_b200.h."""
+    _fields_ = [("plane_occupancy", _I * 4), ("tn_ctas_per_sm", _I), ("density_chunks", _I),
+                ("lagrange_solver", _I)]
+
+    def as_dict(self) -> dict:
+        return {"plane_occupancy": list(self.plane_occupancy), "tn_ctas_per_sm": self.tn_ctas_per_sm,
+                "density_chunks": self.density_chunks, "lagrange_solver": self.lagrange_solver}
 
 
 class CpsdError(RuntimeError):
@@ -132,6 +144,15 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_gpu_set_packed.argtypes = [_P, _P]
     lib.cpsd_gpu_get_sphere.argtypes = [_P, _P, _P, _P]
     lib.cpsd_gpu_set_gemm.argtypes = [_P, _I]
+    lib.cpsd_gpu_get_tuning.argtypes = [_P, ctypes.POINTER(Tuning)]
+    lib.cpsd_gpu_set_tuning.argtypes = [_P, ctypes.POINTER(Tuning)]
+    lib.cpsd_gpu_tuning_limits.argtypes = [_P, ctypes.POINTER(Tuning)]
+    lib.cpsd_gpu_set_band_range.argtypes = [_P, _I, _I]
+    lib.cpsd_gpu_step_phase.argtypes = [_P, _I]
+    lib.cpsd_gpu_bp_buffers.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                                        ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_long)]
+    lib.cpsd_gpu_bp_finish.argtypes = [_P, _I, _P, _P, _P]
+    lib.cpsd_gpu_autotune.argtypes = [_P, _I, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
     _L = ctypes.c_long
     lib.cpsd_overlap_tn.argtypes = [_I, _I, _I, _I, _P, _L, _P, _L, _P, _P, _L, _P]
     lib.cpsd_overlap_tn_noalloc.argtypes = [_I, _I, _I, _I, _P, _L, _P, _L, _P, _P, _L, _P]

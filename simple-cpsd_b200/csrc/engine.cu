@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -47,6 +48,8 @@ cudaError_t &last_cuda_error()
 }
 
 inline long cdiv(long a, long b) { return (a + b - 1) / b; }
+
+constexpr int kTuneMaxCtas = 8;  // largest split-K target (CTAs per SM) a tuning may set
 
 // Streaming multiprocessors of the current device (148 on a B200), looked up
 // once per device.
@@ -162,6 +165,10 @@ struct FftOps {
     virtual void fwd_z_sd(const Geom &g, const void *Tb, const ZEpilogue &e, int nb, cudaStream_t s) = 0;
     virtual void plane(int mode, const Geom &g, void *Tb, const PlaneArgs &a, int nchunks, cudaStream_t s) = 0;
     virtual int plane_ctas_per_sm(int mode) const = 0;  // resident CTAs of a plane pass
+    // occupancy builds of a plane pass (1 or 2) and the one that runs
+    virtual int plane_variants(int mode) const = 0;
+    virtual int plane_variant(int mode) const = 0;
+    virtual void set_plane_variant(int mode, int v) = 0;
 };
 
 template <typename T, int NF>
@@ -170,7 +177,8 @@ struct FftOpsT final : FftOps {
     int KX = 0;
     size_t zsmem = 0;
     size_t psmem[4] = {0, 0, 0, 0};
-    bool two_cta[4] = {false, false, false, false};  // launch the two-CTA build of a plane mode
+    bool hi_fits[4] = {false, false, false, false};  // the high-occupancy build's CTAs fit an SM
+    int occ[4] = {0, 0, 0, 0};                       // plane build that runs, per mode
 
     size_t elem() const override { return sizeof(cx<T>); }
 
@@ -228,11 +236,19 @@ struct FftOpsT final : FftOps {
         CK(allow_plane<PM_APPLYV>(optin));
         CK(allow_plane<PM_INVREAL>(optin));
         CK(allow_plane<PM_FWDREAL>(optin));
-        // two CTAs per SM when two planes (plus the per-CTA reserve) fit
+        // the high-occupancy build needs its CTAs' shared memory (plus the
+        // per-CTA reserve) to fit an SM; it starts as the default where it
+        // does, except where its register cap is known to spill (FP64 lines
+        // of 32 values and more per lane); a tuner may switch per mode
         int sm_bytes = 0, reserve = 0;
         CK(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
         CK(cudaDeviceGetAttribute(&reserve, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-        for (int m = 0; m < 4; ++m) two_cta[m] = 2 * (psmem[m] + (size_t)reserve) <= (size_t)sm_bytes;
+        const bool has_two[4] = {plane_has_two_cta_build<NF, PM_DENSITY>(), plane_has_two_cta_build<NF, PM_APPLYV>(),
+                                 plane_has_two_cta_build<NF, PM_INVREAL>(), plane_has_two_cta_build<NF, PM_FWDREAL>()};
+        for (int m = 0; m < 4; ++m) {
+            hi_fits[m] = has_two[m] && 2 * (psmem[m] + (size_t)reserve) <= (size_t)sm_bytes;
+            occ[m] = hi_fits[m] ? 1 : 0;
+        }
         return CPSD_OK;
     }
 
@@ -245,11 +261,12 @@ struct FftOpsT final : FftOps {
         return e;
     }
 
+    // occ 1: the two-CTA build (128 registers a thread), occ 0: one CTA per SM
     template <int MODE>
     void launch_plane(dim3 grid, int nt, const Geom &g, void *Tb, const PlaneArgs &a, cudaStream_t s)
     {
         if constexpr (plane_has_two_cta_build<NF, MODE>())
-            if (two_cta[MODE]) {
+            if (occ[MODE]) {
                 plane_kernel<T, NF, MODE, 2><<<grid, nt, psmem[MODE], s>>>(g, (cx<T> *)Tb, a, tw);
                 return;
             }
@@ -291,11 +308,12 @@ struct FftOpsT final : FftOps {
         }
     }
     bool mode_ok(int mode) const { return psmem[mode] != 0; }
-    int plane_ctas_per_sm(int mode) const override
+    int plane_ctas_per_sm(int mode) const override { return occ[mode & 3] ? 2 : 1; }
+    int plane_variants(int mode) const override { return hi_fits[mode & 3] ? 2 : 1; }
+    int plane_variant(int mode) const override { return occ[mode & 3]; }
+    void set_plane_variant(int mode, int v) override
     {
-        const bool two = (mode == PM_DENSITY) ? plane_has_two_cta_build<NF, PM_DENSITY>() && two_cta[mode]
-                                              : two_cta[mode];
-        return two ? 2 : 1;
+        if (mode >= 0 && mode < 4) occ[mode] = (v && hi_fits[mode]) ? 1 : 0;
     }
 };
 
@@ -390,6 +408,20 @@ struct cpsd_gpu_ctx {
     cudaEvent_t ev_fork = nullptr, ev_sf = nullptr, ev_side = nullptr;
     cudaStream_t cs = nullptr;  // the stream the GEMM helpers launch on
     bool lag_tile = false;  // 4 x 4 tiled solver (<= 128 bands, 16-CTA clusters schedulable)
+    bool lag_tile_ok = false;  // the tiled solver can run on this device for these bands
+    // tuning (cpsd_gpu_set_tuning / cpsd_gpu_autotune): split-K target of the
+    // TN products, density chunk capacity and the model's chunk counts
+    int tn_ctas = 2;
+    int dens_cap = 0;
+    int dens_model[2] = {0, 0};
+    // band-parallel SD (cpsd_gpu_set_band_range): this context transforms and
+    // steps bands [bp_lo, bp_hi); dn_part holds its spin densities before the
+    // caller sums them over the ranks; its density chunks in chunk_bp
+    bool bp = false;
+    int bp_lo = 0, bp_hi = 0;
+    double *dn_part = nullptr;
+    int *chunk_bp = nullptr;
+    int nchunk_bp[2] = {0, 0};
     int lag_cluster = 8;  // CTAs per cluster of the Lagrange solver (16 where schedulable)
     int lag_lb = 0;       // its row-tile width
     // learned preconditioner (optional): shells, stats, features, outputs
@@ -455,6 +487,16 @@ struct cpsd_gpu_ctx {
 
 namespace {
 
+// Band ranges of the density pass: n0 chunks of spin 0's ne0 bands, then
+// n1 chunks of spin 1's (starts, ends appended: n0 + n1 + 1 entries).
+std::vector<int> density_chunk_table(int ne0, int n0, int ne1, int n1)
+{
+    std::vector<int> b0;
+    for (int q = 0; q <= n0; ++q) b0.push_back((int)((long)ne0 * q / n0));
+    for (int q = 1; q <= n1; ++q) b0.push_back(ne0 + (int)((long)ne1 * q / n1));
+    return b0;
+}
+
 // Split-K plan of a batch of weighted TN products: about two CTAs per SM
 // (sms: the device's SM count), each split at least 64 reals, partials
 // within ws_elems.
@@ -463,11 +505,11 @@ struct TnPlan {
     int kchunk;
 };
 
-TnPlan tn_plan(int M, int N, int K, int nprod, bool tc, size_t ws_elems, int sms)
+TnPlan tn_plan(int M, int N, int K, int nprod, bool tc, size_t ws_elems, int sms, int ctas_per_sm = 2)
 {
     const int tm = tc ? kTcM : kDmT, tn = tc ? kTcN : kDmT, bk = tc ? kTcBK : kDmK;
     const long tiles = cdiv(M, tm) * cdiv(N, tn) * nprod;
-    long splits = std::max<long>(1, cdiv(2L * sms, tiles));
+    long splits = std::max<long>(1, cdiv((long)ctas_per_sm * sms, tiles));
     splits = std::min<long>(splits, std::max<long>(1, K / 64));
     while ((size_t)splits * M * N * nprod > ws_elems && splits > 1) --splits;
     const int kchunk = (int)(cdiv(cdiv(K, splits), bk) * bk);
@@ -479,9 +521,9 @@ TnPlan tn_plan(int M, int N, int K, int nprod, bool tc, size_t ws_elems, int sms
 // reduction.  Returns the number of launches.
 int launch_tn(int M, int N, int K, int nprod, const double *const *A, long lda, const double *const *B, long ldb,
               const double *w, double alpha, double beta, double *const *C, long ldc, bool tc, double *ws,
-              size_t ws_elems, int *err, cudaStream_t s)
+              size_t ws_elems, int *err, cudaStream_t s, int ctas_per_sm = 2)
 {
-    const TnPlan pl = tn_plan(M, N, K, nprod, tc, ws_elems, device_sms());
+    const TnPlan pl = tn_plan(M, N, K, nprod, tc, ws_elems, device_sms(), ctas_per_sm);
     TnBatch bt{};
     for (int q = 0; q < nprod; ++q) {
         bt.A[q] = A[q];
@@ -520,7 +562,7 @@ int gemm_tn_batch(cpsd_gpu_ctx *c, int M, int N, int K, int nprod, const double 
     if (nprod > kTnMaxProd) return CPSD_ERR_ARG;
     const bool tc = (c->gemm_mode & which) != 0 && c->precision == CPSD_PREC_MIXED;
     c->nlaunch += launch_tn(M, N, K, nprod, A, lda, B, ldb, w, alpha, beta, C, ldc, tc, c->gws, c->gemm_ws_elems,
-                            c->flags + 2, c->cs);
+                            c->flags + 2, c->cs, c->tn_ctas);
     return CPSD_OK;
 }
 
@@ -597,205 +639,255 @@ inline void mark(cpsd_gpu_ctx *c, int i)
     if (c->phase_timing) cudaEventRecordWithFlags(c->pev[i], c->st, cudaEventRecordExternal);
 }
 
-int one_step(cpsd_gpu_ctx *c)
+// Side-stream work of a step (or in order on `side` = the main stream):
+// phase factors, local psp and projectors (cpsd.c:208, 224-286) ...
+void issue_sf(cpsd_gpu_ctx *c, cudaStream_t side)
+{
+    if (c->nion > 0) {
+        phase_tables_kernel<<<(unsigned)cdiv(3 * c->nion, 128), 128, 0, side>>>(c->nion, c->n, c->unitg, c->r1,
+                                                                             c->ex1, c->ex2, c->ex3);
+        c->nlaunch += 1;
+    }
+    VlocArgs va{};
+    va.npw = c->npw;
+    va.npw_pad = c->npw_pad;
+    va.n = c->n;
+    va.nh = c->nh;
+    va.nion = c->nion;
+    va.pt_i = c->pt_i;
+    va.pt_j = c->pt_j;
+    va.pt_k = c->pt_k;
+    va.katm = c->katm;
+    va.zv = c->zv;
+    va.ex1 = c->ex1;
+    va.ex2 = c->ex2;
+    va.ex3 = c->ex3;
+    va.vl = c->vl;
+    va.vnl = c->vnl;
+    va.lmmax = c->lmmax;
+    va.proj_off = c->proj_off;
+    va.s = c->sfac;
+    va.vall = c->vall;
+    va.proj = c->proj;
+    vloc_proj_kernel<<<(unsigned)cdiv(c->npw_pad, 128), 128, 0, side>>>(va); c->nlaunch += 1;
+}
+
+// ... and the kinetic + nonlocal part of -H psi into c2 (cpsd.c:212-221,
+// 287-290) for the bands [lo, lo + nbl) this context steps
+int issue_knl(cpsd_gpu_ctx *c, cudaStream_t side, const cx<double> *c1, cx<double> *c2, int lo, int nbl)
+{
+    cudaStream_t s = c->st;
+    const int K = 2 * c->npw_pad;
+    const long ldr = 2L * c->npw_pad;
+    const cx<double> *c1l = c1 + (long)lo * c->ldc;
+    cx<double> *c2l = c2 + (long)lo * c->ldc;
+    c->cs = side;
+    if (nbl > 0) {
+        kinetic_kernel<<<(unsigned)cdiv((long)nbl * c->npw_pad, 256), 256, 0, side>>>(nbl, c->npw_pad, c->ldc,
+                                                                                     c->tg, c1l, c2l);
+        c->nlaunch += 1;
+    }
+    if (c->nproj > 0) {
+        int rc = gemm_tn(c, c->nproj, nbl, K, (const double *)c->proj, ldr, (const double *)c1l, ldr, c->w, 1.0,
+                         0.0, c->beta + lo, c->nb, TN_PROJECTOR);
+        if (rc) {
+            c->cs = s;
+            return rc;
+        }
+        kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, side>>>(
+            c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT, c->move ? c->coefP : nullptr);
+        c->nlaunch += 1;
+        gemm_nn(c, nbl, K, c->nproj, 1.0, c->coefT + (long)lo * c->nproj, c->nproj, (const double *)c->proj, ldr,
+                1.0, (double *)c2l, ldr, TN_PROJECTOR);
+        if (c->move) {  // nonlocal force: Y_P = sum_b sw1(P, b) c1_b, then sum_G G Im(conj(chi_P) Y_P)
+            gemm_nn(c, c->nproj, K, c->nb, 1.0, c->coefP, c->nb, (const double *)c1, ldr, 0.0, (double *)c->Ynl,
+                    ldr);
+            force_nonlocal_kernel<<<c->nproj, 256, 0, side>>>(c->npw, c->ldc, c->w, c->Gv, c->proj, c->Ynl,
+                                                             c->fnl);
+            c->nlaunch += 1;
+        }
+    }
+    c->cs = s;
+    return CPSD_OK;
+}
+
+// One SD step in three phases.  A context that steps every band runs them
+// back to back (one_step); a band-parallel context (c->bp) steps only its
+// bands [bp_lo, bp_hi) in phases 0 and 1, and its caller exchanges between
+// them: after phase 0 the spin densities of all ranks are summed into dn
+// (dn_part holds this rank's), after phase 1 every rank's new orbitals and
+// -H psi rows reach every rank.  Phase 2 (overlaps, Lagrange, constraint)
+// then runs on all bands everywhere.
+int step_phase(cpsd_gpu_ctx *c, int phase)
 {
     cudaStream_t s = c->st;
     cx<double> *c1 = c->cbuf[c->cur], *c2 = c->cbuf[c->cur ^ 1];
     const int K = 2 * c->npw_pad;
     const long ldr = 2L * c->npw_pad;
-    CK(cudaMemcpyAsync(c->r1, c->r2, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToDevice, s));  // cpsd.c:174
+    const int lo = c->bp ? c->bp_lo : 0, nbl = c->bp ? c->bp_hi - c->bp_lo : c->nb;
     // The structure factors, projectors and the kinetic + nonlocal part of
     // -H psi need only c1 and the ions: they run on a second stream beside
     // the density -> potential -> V psi chain, joined before the SD update.
     // With phase timing on, everything stays on one stream so the phases add up.
     const bool fork = !c->phase_timing;
     cudaStream_t side = fork ? c->st2 : s;
-    // phase factors, local psp and projectors: cpsd.c:208, 224-286
-    auto issue_sf = [&]() {
-        if (c->nion > 0) {
-            phase_tables_kernel<<<(unsigned)cdiv(3 * c->nion, 128), 128, 0, side>>>(c->nion, c->n, c->unitg, c->r1,
-                                                                                 c->ex1, c->ex2, c->ex3);
+    if (phase == 0) {
+        CK(cudaMemcpyAsync(c->r1, c->r2, sizeof(double) * 3 * c->nion, cudaMemcpyDeviceToDevice, s));  // cpsd.c:174
+        if (fork) {
+            CK(cudaEventRecord(c->ev_fork, s));
+            CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+            issue_sf(c, side);
+            CK(cudaEventRecord(c->ev_sf, c->st2));
+            int rc = issue_knl(c, side, c1, c2, lo, nbl);
+            if (rc) return rc;
+            CK(cudaEventRecord(c->ev_side, c->st2));
+        }
+
+        mark(c, 0);
+        // psi(G) -> psi(r) and the density, cpsd.c:177-194
+        if (nbl > 0) {
+            c->fft->inv_z(c->g, c1 + (long)lo * c->ldc, c->ldc, c->Tb, nbl, s);
             c->nlaunch += 1;
         }
-        VlocArgs va{};
-        va.npw = c->npw;
-        va.npw_pad = c->npw_pad;
-        va.n = c->n;
-        va.nh = c->nh;
-        va.nion = c->nion;
-        va.pt_i = c->pt_i;
-        va.pt_j = c->pt_j;
-        va.pt_k = c->pt_k;
-        va.katm = c->katm;
-        va.zv = c->zv;
-        va.ex1 = c->ex1;
-        va.ex2 = c->ex2;
-        va.ex3 = c->ex3;
-        va.vl = c->vl;
-        va.vnl = c->vnl;
-        va.lmmax = c->lmmax;
-        va.proj_off = c->proj_off;
-        va.s = c->sfac;
-        va.vall = c->vall;
-        va.proj = c->proj;
-        vloc_proj_kernel<<<(unsigned)cdiv(c->npw_pad, 128), 128, 0, side>>>(va); c->nlaunch += 1;
-    };
-    // kinetic + nonlocal part of -H psi into c2, cpsd.c:212-221, 287-290
-    auto issue_knl = [&]() -> int {
-        c->cs = side;
-        kinetic_kernel<<<(unsigned)cdiv((long)c->nb * c->npw_pad, 256), 256, 0, side>>>(c->nb, c->npw_pad, c->ldc,
-                                                                                       c->tg, c1, c2);
-        c->nlaunch += 1;
-        if (c->nproj > 0) {
-            int rc = gemm_tn(c, c->nproj, c->nb, K, (const double *)c->proj, ldr, (const double *)c1, ldr, c->w,
-                             1.0, 0.0, c->beta, c->nb, TN_PROJECTOR);
-            if (rc) {
-                c->cs = s;
-                return rc;
-            }
-            kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, side>>>(
-                c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT, c->move ? c->coefP : nullptr);
+        mark(c, 1);
+        PlaneArgs pa{};
+        pa.chunk_b0 = c->bp ? c->chunk_bp : c->chunk_dens;
+        pa.rho_part = c->rho_part;
+        const int ch0 = c->bp ? c->nchunk_bp[0] : c->nchunk0, ch1 = c->bp ? c->nchunk_bp[1] : c->nchunk1;
+        if (ch0 + ch1 > 0) {
+            c->fft->plane(PM_DENSITY, c->g, c->Tb, pa, ch0 + ch1, s);
             c->nlaunch += 1;
-            gemm_nn(c, c->nb, K, c->nproj, 1.0, c->coefT, c->nproj, (const double *)c->proj, ldr, 1.0,
-                    (double *)c2, ldr, TN_PROJECTOR);
-            if (c->move) {  // nonlocal force: Y_P = sum_b sw1(P, b) c1_b, then sum_G G Im(conj(chi_P) Y_P)
-                gemm_nn(c, c->nproj, K, c->nb, 1.0, c->coefP, c->nb, (const double *)c1, ldr, 0.0,
-                        (double *)c->Ynl, ldr);
-                force_nonlocal_kernel<<<c->nproj, 256, 0, side>>>(c->npw, c->ldc, c->w, c->Gv, c->proj, c->Ynl,
-                                                                 c->fnl);
+        }
+        mark(c, 2);
+        XcArgs xa{c->n3, c->ispin, ch0, ch1, c->rho_part, c->scal1, c->scal2, c->dn, c->xcp, c->xce, c->rfwd};
+        if (c->bp) {  // this rank's spin densities; the caller sums them into dn
+            density_sum_kernel<<<(unsigned)cdiv(c->n3, 256), 256, 0, s>>>(xa, c->dn_part);
+            c->nlaunch += 1;
+            CK(cudaGetLastError());
+            return CPSD_OK;
+        }
+        density_xc_kernel<<<(unsigned)cdiv(c->n3, 256), 256, 0, s>>>(xa); c->nlaunch += 1;
+        mark(c, 3);
+        return CPSD_OK;
+    }
+    if (phase == 1) {
+        if (c->bp) {  // dn holds the densities of all bands now
+            XcArgs xa{c->n3, c->ispin, 0, 0, nullptr, c->scal1, c->scal2, c->dn, c->xcp, c->xce, c->rfwd};
+            xc_from_density_kernel<<<(unsigned)cdiv(c->n3, 256), 256, 0, s>>>(xa);
+            c->nlaunch += 1;
+            mark(c, 3);
+        }
+        // rho(G), cpsd.c:198-205
+        PlaneArgs pf{};
+        pf.rin = c->rfwd;
+        c->fft->plane(PM_FWDREAL, c->g, c->Taux, pf, 1, s); c->nlaunch += 1;
+        c->fft->fwd_z_store(c->g, c->Taux, c->dng, c->ldc, 1.0, 1, s); c->nlaunch += 1;
+        mark(c, 4);
+        if (fork)
+            CK(cudaStreamWaitEvent(s, c->ev_sf, 0));
+        else
+            issue_sf(c, side);
+        // V(G), cpsd.c:373-379
+        vg_kernel<<<(unsigned)cdiv(c->npw, 128), 128, 0, s>>>(c->npw, c->vall, c->dng, c->vc, c->scal2, c->Vg);
+        c->nlaunch += 1;
+        if (c->move && c->nion > 0) {  // local, k-space and real-space Ewald forces
+            ForceArgs fa{};
+            fa.npw = c->npw;
+            fa.n = c->n;
+            fa.nh = c->nh;
+            fa.nion = c->nion;
+            fa.pt_i = c->pt_i;
+            fa.pt_j = c->pt_j;
+            fa.pt_k = c->pt_k;
+            fa.katm = c->katm;
+            fa.ex1 = c->ex1;
+            fa.ex2 = c->ex2;
+            fa.ex3 = c->ex3;
+            fa.w = c->w;
+            fa.G = c->Gv;
+            fa.vl = c->vl;
+            fa.vg = c->vg;
+            fa.zv = c->zv;
+            fa.dng = c->dng;
+            fa.s = c->sfac;
+            fa.scal2 = c->scal2;
+            fa.fpart = c->fpart;
+            force_local_ewald_kernel<<<dim3(kForceChunks, c->nion), 256, 0, s>>>(fa); c->nlaunch += 1;
+            if (c->nion > 1) {
+                force_ewald_pairs_kernel<<<c->nion, 256, 0, s>>>(c->nion, c->nsh, c->r1, c->rcell, c->zv, c->katm,
+                                                                 c->prm.rcut, c->ewp);
                 c->nlaunch += 1;
             }
         }
-        c->cs = s;
-        return CPSD_OK;
-    };
-    if (fork) {
-        CK(cudaEventRecord(c->ev_fork, s));
-        CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
-        issue_sf();
-        CK(cudaEventRecord(c->ev_sf, c->st2));
-        int rc = issue_knl();
-        if (rc) return rc;
-        CK(cudaEventRecord(c->ev_side, c->st2));
-    }
-
-    mark(c, 0);
-    // psi(G) -> psi(r) and the density, cpsd.c:177-194
-    c->fft->inv_z(c->g, c1, c->ldc, c->Tb, c->nb, s); c->nlaunch += 1;
-    mark(c, 1);
-    PlaneArgs pa{};
-    pa.chunk_b0 = c->chunk_dens;
-    pa.rho_part = c->rho_part;
-    c->fft->plane(PM_DENSITY, c->g, c->Tb, pa, c->nchunk0 + c->nchunk1, s); c->nlaunch += 1;
-    mark(c, 2);
-    XcArgs xa{c->n3, c->ispin, c->nchunk0, c->nchunk1, c->rho_part, c->scal1, c->scal2,
-              c->dn, c->xcp, c->xce, c->rfwd};
-    density_xc_kernel<<<(unsigned)cdiv(c->n3, 256), 256, 0, s>>>(xa); c->nlaunch += 1;
-    mark(c, 3);
-    // rho(G), cpsd.c:198-205
-    PlaneArgs pf{};
-    pf.rin = c->rfwd;
-    c->fft->plane(PM_FWDREAL, c->g, c->Taux, pf, 1, s); c->nlaunch += 1;
-    c->fft->fwd_z_store(c->g, c->Taux, c->dng, c->ldc, 1.0, 1, s); c->nlaunch += 1;
-    mark(c, 4);
-    if (fork)
-        CK(cudaStreamWaitEvent(s, c->ev_sf, 0));
-    else
-        issue_sf();
-    // V(G), cpsd.c:373-379
-    vg_kernel<<<(unsigned)cdiv(c->npw, 128), 128, 0, s>>>(c->npw, c->vall, c->dng, c->vc, c->scal2, c->Vg);
-    c->nlaunch += 1;
-    if (c->move && c->nion > 0) {  // local, k-space and real-space Ewald forces
-        ForceArgs fa{};
-        fa.npw = c->npw;
-        fa.n = c->n;
-        fa.nh = c->nh;
-        fa.nion = c->nion;
-        fa.pt_i = c->pt_i;
-        fa.pt_j = c->pt_j;
-        fa.pt_k = c->pt_k;
-        fa.katm = c->katm;
-        fa.ex1 = c->ex1;
-        fa.ex2 = c->ex2;
-        fa.ex3 = c->ex3;
-        fa.w = c->w;
-        fa.G = c->Gv;
-        fa.vl = c->vl;
-        fa.vg = c->vg;
-        fa.zv = c->zv;
-        fa.dng = c->dng;
-        fa.s = c->sfac;
-        fa.scal2 = c->scal2;
-        fa.fpart = c->fpart;
-        force_local_ewald_kernel<<<dim3(kForceChunks, c->nion), 256, 0, s>>>(fa); c->nlaunch += 1;
-        if (c->nion > 1) {
-            force_ewald_pairs_kernel<<<c->nion, 256, 0, s>>>(c->nion, c->nsh, c->r1, c->rcell, c->zv, c->katm,
-                                                             c->prm.rcut, c->ewp);
+        mark(c, 5);
+        // V_loc + V_H to real space, plus xc per spin (cpsd.c:380-388)
+        c->fft->inv_z(c->g, c->Vg, c->ldc, c->Taux, 1, s); c->nlaunch += 1;
+        PlaneArgs pv{};
+        pv.rout = c->Vr;
+        pv.xadd = c->xcp;
+        pv.nout = c->ispin;
+        c->fft->plane(PM_INVREAL, c->g, c->Taux, pv, 1, s); c->nlaunch += 1;
+        mark(c, 6);
+        if (!fork) {
+            int rc = issue_knl(c, side, c1, c2, lo, nbl);
+            if (rc) return rc;
+        }
+        mark(c, 7);
+        // (V + xc) psi back to G, -H psi and the SD step, cpsd.c:384-400
+        if (nbl > 0) {
+            PlaneArgs pp{};
+            pp.chunk_b0 = c->chunk_band;
+            pp.V = c->Vr;
+            pp.ne0 = (c->ispin == 2) ? std::max(0, c->ne0 - lo) : nbl;
+            c->fft->plane(PM_APPLYV, c->g, c->Tb, pp, nbl, s); c->nlaunch += 1;
+        }
+        mark(c, 8);
+        if (fork) CK(cudaStreamWaitEvent(s, c->ev_side, 0));  // kinetic + nonlocal c2 is in place
+        if (c->move && c->nion > 0) {  // total force and the ion step r2 = r1 + dti fion
+            force_total_kernel<<<(unsigned)cdiv(c->nion, 128), 128, 0, s>>>(
+                c->nion, 2.0 * (c->ispin == 1 ? 2.0 : 1.0), c->proj_off, c->lmmax, c->katm, c->fpart, c->fnl, c->ewp,
+                c->dti, c->r1, c->fion, c->r2);
             c->nlaunch += 1;
         }
-    }
-    mark(c, 5);
-    // V_loc + V_H to real space, plus xc per spin (cpsd.c:380-388)
-    c->fft->inv_z(c->g, c->Vg, c->ldc, c->Taux, 1, s); c->nlaunch += 1;
-    PlaneArgs pv{};
-    pv.rout = c->Vr;
-    pv.xadd = c->xcp;
-    pv.nout = c->ispin;
-    c->fft->plane(PM_INVREAL, c->g, c->Taux, pv, 1, s); c->nlaunch += 1;
-    mark(c, 6);
-    if (!fork) {
-        int rc = issue_knl();
-        if (rc) return rc;
-    }
-    mark(c, 7);
-    // (V + xc) psi back to G, -H psi and the SD step, cpsd.c:384-400
-    PlaneArgs pp{};
-    pp.chunk_b0 = c->chunk_band;
-    pp.V = c->Vr;
-    pp.ne0 = (c->ispin == 2) ? c->ne0 : c->nb;
-    c->fft->plane(PM_APPLYV, c->g, c->Tb, pp, c->nb, s); c->nlaunch += 1;
-    mark(c, 8);
-    if (fork) CK(cudaStreamWaitEvent(s, c->ev_side, 0));  // kinetic + nonlocal c2 is in place
-    if (c->move && c->nion > 0) {  // total force and the ion step r2 = r1 + dti fion
-        force_total_kernel<<<(unsigned)cdiv(c->nion, 128), 128, 0, s>>>(
-            c->nion, 2.0 * (c->ispin == 1 ? 2.0 : 1.0), c->proj_off, c->lmmax, c->katm, c->fpart, c->fnl, c->ewp,
-            c->dti, c->r1, c->fion, c->r2);
-        c->nlaunch += 1;
-    }
-    ZEpilogue e{};
-    e.c2 = c2;
-    e.c1 = c1;
-    e.cpsi = c->cpsi;
-    e.ldc = c->ldc;
-    e.scal1 = c->scal1;
-    e.dte = c->dte;
-    c->fft->fwd_z_sd(c->g, c->Tb, e, c->nb, s); c->nlaunch += 1;
-    if (c->mlp) {  // learned step scales per band and |G| shell
-        // The residual R = cpsi - C1 (C1' W cpsi) per spin: only R is
-        // preconditioned, so the update is plain SD wherever R = 0 and the
-        // fixed point H psi = psi Lambda is that of plain SD.
-        CK(cudaMemcpyAsync(c->pR, c->cpsi, sizeof(cx<double>) * c->nb * c->ldc, cudaMemcpyDeviceToDevice, s));
-        for (int ms = 0; ms < c->ispin; ++ms) {
-            const int m = ms ? c->ne1 : c->ne0;
-            const long off = (long)(ms ? c->ne0 : 0) * ldr;
-            double *Mt = c->pM + (long)ms * c->ne0 * c->ne0;  // Mt[b][a] = <cpsi_b|c1_a>
-            int rc = gemm_tn(c, m, m, K, (const double *)c->cpsi + off, ldr, (const double *)c1 + off, ldr, c->w,
-                             1.0, 0.0, Mt, m, TN_PROJECTOR);
-            if (rc) return rc;
-            gemm_nn(c, m, K, m, -1.0, Mt, m, (const double *)c1 + off, ldr, 1.0, (double *)c->pR + off, ldr,
-                    TN_PROJECTOR);
+        if (nbl > 0) {
+            ZEpilogue e{};
+            e.c2 = c2 + (long)lo * c->ldc;
+            e.c1 = c1 + (long)lo * c->ldc;
+            e.cpsi = c->cpsi + (long)lo * c->ldc;
+            e.ldc = c->ldc;
+            e.scal1 = c->scal1;
+            e.dte = c->dte;
+            c->fft->fwd_z_sd(c->g, c->Tb, e, nbl, s); c->nlaunch += 1;
         }
-        band_stats_kernel<<<c->nb, 256, 0, s>>>(c->npw, c->ldc, c->w, c->tg, c1, c->cpsi, c->pstats);
-        prec_features_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 256), 256, 0, s>>>(c->nb, c->tmax, c->pstats,
-                                                                                      c->dstep, c->pX);
-        mlp_forward_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 128), 128, 0, s>>>(
-            c->nb * kShells, c->pX, c->mlp->wq, c->mlp->p, c->py, nullptr);
-        prec_update_kernel<<<(unsigned)cdiv((long)c->nb * c->npw, 256), 256, 0, s>>>(
-            c->nb, c->npw, c->ldc, c->shell, c->py, c->pcap, c->dte, c->pR, c2, c->dstep);
-        c->nlaunch += 4;
+        if (c->mlp) {  // learned step scales per band and |G| shell
+            // The residual R = cpsi - C1 (C1' W cpsi) per spin: only R is
+            // preconditioned, so the update is plain SD wherever R = 0 and the
+            // fixed point H psi = psi Lambda is that of plain SD.
+            CK(cudaMemcpyAsync(c->pR, c->cpsi, sizeof(cx<double>) * c->nb * c->ldc, cudaMemcpyDeviceToDevice, s));
+            for (int ms = 0; ms < c->ispin; ++ms) {
+                const int m = ms ? c->ne1 : c->ne0;
+                const long off = (long)(ms ? c->ne0 : 0) * ldr;
+                double *Mt = c->pM + (long)ms * c->ne0 * c->ne0;  // Mt[b][a] = <cpsi_b|c1_a>
+                int rc = gemm_tn(c, m, m, K, (const double *)c->cpsi + off, ldr, (const double *)c1 + off, ldr, c->w,
+                                 1.0, 0.0, Mt, m, TN_PROJECTOR);
+                if (rc) return rc;
+                gemm_nn(c, m, K, m, -1.0, Mt, m, (const double *)c1 + off, ldr, 1.0, (double *)c->pR + off, ldr,
+                        TN_PROJECTOR);
+            }
+            band_stats_kernel<<<c->nb, 256, 0, s>>>(c->npw, c->ldc, c->w, c->tg, c1, c->cpsi, c->pstats);
+            prec_features_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 256), 256, 0, s>>>(c->nb, c->tmax, c->pstats,
+                                                                                          c->dstep, c->pX);
+            mlp_forward_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 128), 128, 0, s>>>(
+                c->nb * kShells, c->pX, c->mlp->wq, c->mlp->p, c->py, nullptr);
+            prec_update_kernel<<<(unsigned)cdiv((long)c->nb * c->npw, 256), 256, 0, s>>>(
+                c->nb, c->npw, c->ldc, c->shell, c->py, c->pcap, c->dte, c->pR, c2, c->dstep);
+            c->nlaunch += 4;
+        }
+        mark(c, 9);
+        CK(cudaGetLastError());
+        return CPSD_OK;
     }
-    mark(c, 9);
-    // overlaps and Lagrange multipliers, cpsd.c:415-479
+    // phase 2: overlaps and Lagrange multipliers, cpsd.c:415-479
     LagArgs la{};
     la.ispin = c->ispin;
     la.ne0 = c->ne0;
@@ -869,6 +961,15 @@ int one_step(cpsd_gpu_ctx *c)
     mark(c, 12);
     CK(cudaGetLastError());
     c->cur ^= 1;
+    return CPSD_OK;
+}
+
+int one_step(cpsd_gpu_ctx *c)
+{
+    for (int phase = 0; phase < 3; ++phase) {
+        int rc = step_phase(c, phase);
+        if (rc) return rc;
+    }
     return CPSD_OK;
 }
 
@@ -1564,15 +1665,18 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
             c->nchunk0 = best_chunks(c->ne0, 2 * c->n);
             c->nchunk1 = c->ne1 > 0 ? best_chunks(c->ne1, 2 * c->n) : 0;
         }
-        std::vector<int> b0;
-        for (int q = 0; q <= c->nchunk0; ++q) b0.push_back((int)((long)c->ne0 * q / c->nchunk0));
-        for (int q = 1; q <= c->nchunk1; ++q) b0.push_back(c->ne0 + (int)((long)c->ne1 * q / c->nchunk1));
+        c->dens_model[0] = c->nchunk0;
+        c->dens_model[1] = c->nchunk1;
+        // room for up to max(4, 2 x the model's count) chunks per spin (tuning)
+        c->dens_cap = std::min(std::max(4, 2 * std::max(c->nchunk0, c->nchunk1)), std::max(c->ne0, c->ne1));
+        std::vector<int> b0 = density_chunk_table(c->ne0, c->nchunk0, c->ne1, c->nchunk1);
+        b0.resize((size_t)2 * c->dens_cap + 1, 0);
         CK(upload(ar, &c->chunk_dens, b0));
         std::vector<int> bb(nb + 1);
         for (int b = 0; b <= nb; ++b) bb[b] = b;
         CK(upload(ar, &c->chunk_band, bb));
     }
-    CK(ar.alloc(&c->rho_part, (size_t)(c->nchunk0 + c->nchunk1) * c->n3));
+    CK(ar.alloc(&c->rho_part, (size_t)(std::min(c->dens_cap, c->ne0) + std::min(c->dens_cap, c->ne1)) * c->n3));
     CK(ar.alloc(&c->dn, (size_t)c->ispin * c->n3));
     CK(ar.alloc(&c->xcp, (size_t)c->ispin * c->n3));
     CK(ar.alloc(&c->xce, (size_t)c->n3));
@@ -1663,7 +1767,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
         // keeps the column solver, for comparisons)
         const char *lag_env = getenv("CPSD_B200_LAGRANGE");
         const size_t tsm = lagrange_tile_smem(c->ne0);
-        if (c->ne0 <= kLagTileMax && tsm <= limit && !(lag_env && !strcmp(lag_env, "cluster"))) {
+        if (c->ne0 <= kLagTileMax && tsm <= limit) {
             CK(cudaFuncSetAttribute(lagrange_tile_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
             CK(allow_max_smem(lagrange_tile_kernel, optin));
             cudaLaunchConfig_t cfg{};
@@ -1680,9 +1784,10 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
             int nclusters = 0;
             if (cudaOccupancyMaxActiveClusters(&nclusters, lagrange_tile_kernel, &cfg) == cudaSuccess &&
                 nclusters >= 1)
-                c->lag_tile = true;
+                c->lag_tile_ok = true;
             (void)cudaGetLastError();
         }
+        c->lag_tile = c->lag_tile_ok && !(lag_env && !strcmp(lag_env, "cluster"));
     }
     CK(cudaDeviceSynchronize());  // allocation memsets run on the legacy stream
     *out = c.release();
@@ -1834,6 +1939,8 @@ int cpsd_gpu_set_state(cpsd_gpu_ctx *c, const double *c2, const double *r2)
     return CPSD_OK;
 }
 
+static int finish_call(cpsd_gpu_ctx *c, int inner, double *E, double *deltae, double *deltac, double *deltar);
+
 int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae, double *deltac,
                  double *deltar)
 {
@@ -1856,6 +1963,7 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
         for (int ii = 0; ii < c->nion; ++ii) dti[ii] = c->prm.dt / sqrt(c->amass_h[katm[ii]]);
         CK(cudaMemcpy(c->dti, dti.data(), sizeof(double) * c->nion, cudaMemcpyHostToDevice));
     }
+    if (c->bp) return CPSD_ERR_ARG;  // band-parallel contexts step by phases
     cudaStream_t s = c->st;
     CK(cudaMemsetAsync(c->flags, 0, 3 * sizeof(int), s));
     CK(cudaMemcpyAsync(c->Edev, E, sizeof(double), cudaMemcpyHostToDevice, s));
@@ -1863,6 +1971,15 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
         int rc = run_step(c);
         if (rc) return rc;
     }
+    return finish_call(c, inner, E, deltae, deltac, deltar);
+}
+
+// The energies of a call and what cpsd() returns besides the orbitals
+// (cpsd.c:494-672), after its `inner` steps; E[0] on the device holds the
+// previous total energy.
+static int finish_call(cpsd_gpu_ctx *c, int inner, double *E, double *deltae, double *deltac, double *deltar)
+{
+    cudaStream_t s = c->st;
     int rc = energies(c, inner);
     if (rc) return rc;
     double Eh[16];
@@ -2039,6 +2156,7 @@ const char *cpsd_gpu_phase_name(int i) { return (i >= 0 && i < kNumPhases) ? kPh
 
 int cpsd_gpu_set_preconditioner(cpsd_gpu_ctx *c, cpsd_mlp *m)
 {
+    if (c && c->bp && m) return CPSD_ERR_ARG;
     if (!c) return CPSD_ERR_ARG;
     if (m && m->device != c->prm.device) return CPSD_ERR_ARG;
     if (m != c->mlp) drop_graphs(c);
@@ -2346,6 +2464,283 @@ int cpsd_gpu_use_graphs(cpsd_gpu_ctx *c, int on)
     if (!c) return CPSD_ERR_ARG;
     if (!on) drop_graphs(c);
     c->use_graph = on != 0;
+    return CPSD_OK;
+}
+
+// ------------------------------------------------------------ band-parallel SD
+int cpsd_gpu_set_band_range(cpsd_gpu_ctx *c, int lo, int hi)
+{
+    if (!c) return CPSD_ERR_ARG;
+    if (hi < 0) {  // back to stepping every band
+        c->bp = false;
+        drop_graphs(c);
+        return CPSD_OK;
+    }
+    if (lo < 0 || lo > hi || hi > c->nb || c->mlp || c->move) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    if (!c->dn_part) {
+        CK(c->ar.alloc(&c->dn_part, (size_t)c->ispin * c->n3));
+        CK(c->ar.alloc(&c->chunk_bp, (size_t)c->nb + 2));
+    }
+    // density chunks of this rank's bands: spin 0's [lo, min(hi, ne0)) then
+    // spin 1's, at most as many per spin as the whole-cell plan
+    const int n0 = std::max(0, std::min(hi, c->ne0) - lo), n1 = (hi - lo) - n0;
+    const int ch0 = n0 > 0 ? std::min(std::max(c->nchunk0, 1), n0) : 0;
+    const int ch1 = n1 > 0 ? std::min(std::max(c->nchunk1, 1), n1) : 0;
+    std::vector<int> tab;
+    tab.push_back(0);
+    for (int q = 1; q <= ch0; ++q) tab.push_back((int)((long)n0 * q / ch0));
+    for (int q = 1; q <= ch1; ++q) tab.push_back(n0 + (int)((long)n1 * q / ch1));
+    CK(cudaMemcpyAsync(c->chunk_bp, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->nchunk_bp[0] = ch0;
+    c->nchunk_bp[1] = ch1;
+    c->bp_lo = lo;
+    c->bp_hi = hi;
+    c->bp = true;
+    drop_graphs(c);
+    return CPSD_OK;
+}
+
+int cpsd_gpu_step_phase(cpsd_gpu_ctx *c, int phase)
+{
+    if (!c || phase < 0 || phase > 2) return CPSD_ERR_ARG;
+    if (!c->tables_ok || !c->state_ok) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    if (phase == 0 && c->move) {  // a band-parallel cell keeps its ions
+        drop_graphs(c);
+        c->move = 0;
+    }
+    return step_phase(c, phase);
+}
+
+int cpsd_gpu_bp_buffers(cpsd_gpu_ctx *c, double **dn_part, double **dn, double **c2, double **cpsi, long *ld)
+{
+    if (!c || !c->bp) return CPSD_ERR_ARG;
+    if (dn_part) *dn_part = c->dn_part;
+    if (dn) *dn = c->dn;
+    if (c2) *c2 = (double *)c->cbuf[c->cur ^ 1];
+    if (cpsi) *cpsi = (double *)c->cpsi;
+    if (ld) *ld = 2L * c->ldc;
+    return CPSD_OK;
+}
+
+int cpsd_gpu_bp_finish(cpsd_gpu_ctx *c, int inner, double *E, double *deltae, double *deltac)
+{
+    if (!c || !c->bp || !E || inner < 1) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    cudaStream_t s = c->st;
+    CK(cudaMemcpyAsync(c->Edev, E, sizeof(double), cudaMemcpyHostToDevice, s));
+    // the projector coefficients of every band (the steps formed only this
+    // rank's columns); c1 is the last step's orbitals of all bands
+    if (c->nproj > 0) {
+        const long ldr = 2L * c->npw_pad;
+        int rc = gemm_tn(c, c->nproj, c->nb, 2 * c->npw_pad, (const double *)c->proj, ldr,
+                         (const double *)c->cbuf[c->cur ^ 1], ldr, c->w, 1.0, 0.0, c->beta, c->nb, TN_PROJECTOR);
+        if (rc) return rc;
+    }
+    int rc = finish_call(c, inner, E, deltae, deltac, nullptr);
+    CK(cudaMemsetAsync(c->flags, 0, 3 * sizeof(int), s));
+    return rc;
+}
+
+// ------------------------------------------------------------ tuning
+int cpsd_gpu_get_tuning(const cpsd_gpu_ctx *c, cpsd_gpu_tuning *t)
+{
+    if (!c || !t) return CPSD_ERR_ARG;
+    for (int m = 0; m < 4; ++m) t->plane_occupancy[m] = c->fft->plane_variant(m);
+    t->tn_ctas_per_sm = c->tn_ctas;
+    t->density_chunks = c->nchunk0;
+    t->lagrange_solver = (c->ne0 <= kLagSmallMax) ? 0 : (c->lag_tile ? 1 : 2);
+    return CPSD_OK;
+}
+
+int cpsd_gpu_tuning_limits(const cpsd_gpu_ctx *c, cpsd_gpu_tuning *t)
+{
+    if (!c || !t) return CPSD_ERR_ARG;
+    for (int m = 0; m < 4; ++m) t->plane_occupancy[m] = c->fft->plane_variants(m) - 1;
+    t->tn_ctas_per_sm = kTuneMaxCtas;
+    t->density_chunks = std::min(c->dens_cap, c->ne0);
+    t->lagrange_solver = (c->ne0 <= kLagSmallMax) ? 0 : 2;
+    return CPSD_OK;
+}
+
+int cpsd_gpu_set_tuning(cpsd_gpu_ctx *c, const cpsd_gpu_tuning *t)
+{
+    if (!c || !t) return CPSD_ERR_ARG;
+    for (int m = 0; m < 4; ++m)
+        if (t->plane_occupancy[m] < 0 || t->plane_occupancy[m] >= c->fft->plane_variants(m)) return CPSD_ERR_ARG;
+    if (t->tn_ctas_per_sm < 1 || t->tn_ctas_per_sm > kTuneMaxCtas) return CPSD_ERR_ARG;
+    if (t->density_chunks < 1 || t->density_chunks > std::min(c->dens_cap, c->ne0)) return CPSD_ERR_ARG;
+    const bool small = c->ne0 <= kLagSmallMax;
+    if (small ? t->lagrange_solver != 0
+              : (t->lagrange_solver < 1 || t->lagrange_solver > 2 || (t->lagrange_solver == 1 && !c->lag_tile_ok)))
+        return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    const int n0 = t->density_chunks;
+    const int n1 = c->ispin == 2 && c->ne1 > 0 ? std::min(t->density_chunks, c->ne1) : 0;
+    if (n0 != c->nchunk0 || n1 != c->nchunk1) {
+        const std::vector<int> tab = density_chunk_table(c->ne0, n0, c->ne1, n1);
+        CK(cudaMemcpyAsync(c->chunk_dens, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        c->nchunk0 = n0;
+        c->nchunk1 = n1;
+    }
+    for (int m = 0; m < 4; ++m) c->fft->set_plane_variant(m, t->plane_occupancy[m]);
+    c->tn_ctas = t->tn_ctas_per_sm;
+    if (!small) c->lag_tile = t->lagrange_solver == 1;
+    drop_graphs(c);  // the step graphs hold the old choices
+    return CPSD_OK;
+}
+
+namespace {
+
+struct TuneKey {
+    int dev, n, ne0, ne1, npw, nproj, precision, gemm, mlp, move;
+    bool operator<(const TuneKey &o) const
+    {
+        return memcmp(this, &o, sizeof(TuneKey)) < 0;
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, cpsd_gpu_tuning> g_tune_cache;
+
+TuneKey tune_key(const cpsd_gpu_ctx *c)
+{
+    TuneKey k;
+    memset(&k, 0, sizeof(k));
+    k.dev = c->prm.device;
+    k.n = c->n;
+    k.ne0 = c->ne0;
+    k.ne1 = c->ne1;
+    k.npw = c->npw;
+    k.nproj = c->nproj;
+    k.precision = c->precision;
+    k.gemm = c->gemm_mode;
+    k.mlp = c->mlp != nullptr;
+    k.move = c->move;
+    return k;
+}
+
+}  // namespace
+
+int cpsd_gpu_autotune(cpsd_gpu_ctx *c, int steps, int force, float *ms_before, float *ms_after)
+{
+    if (!c || steps < 1) return CPSD_ERR_ARG;
+    if (!c->tables_ok || !c->state_ok) return CPSD_ERR_ARG;
+    CK(cudaSetDevice(c->prm.device));
+    if (ms_before) *ms_before = -1.0f;
+    if (ms_after) *ms_after = -1.0f;
+    const TuneKey key = tune_key(c);
+    if (!force) {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) return cpsd_gpu_set_tuning(c, &it->second);
+    }
+    // the orbitals and step counters are put back after every trial
+    const size_t bytes = sizeof(cx<double>) * c->nb * c->npw_pad;
+    struct Keep {
+        cx<double> *p = nullptr;
+        int *step = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Keep()
+        {
+            if (p) cudaFree(p);
+            if (step) cudaFree(step);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } keep;
+    CK(cudaMalloc(&keep.p, bytes));
+    CK(cudaMalloc(&keep.step, sizeof(int)));
+    CK(cudaEventCreate(&keep.e0));
+    CK(cudaEventCreate(&keep.e1));
+    const int cur0 = c->cur;
+    const long long steps0 = c->steps_run, nl0 = c->nlaunch;
+    cudaStream_t s = c->st;
+    CK(cudaMemcpyAsync(keep.p, c->cbuf[cur0], bytes, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(keep.step, c->dstep, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    auto restore = [&]() -> int {
+        c->cur = cur0;
+        CK(cudaMemcpyAsync(c->cbuf[cur0], keep.p, bytes, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(c->dstep, keep.step, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        return CPSD_OK;
+    };
+    // time `steps` SD steps of the current choice: best of three after a
+    // warm-up step that captures its graphs
+    auto trial = [&](float *ms) -> int {
+        drop_graphs(c);
+        int rc = restore();
+        if (!rc) rc = run_step(c);
+        float best = 0.0f;
+        for (int rep = 0; rep < 3 && !rc; ++rep) {
+            rc = restore();
+            if (rc) break;
+            CK(cudaEventRecord(keep.e0, s));
+            for (int k = 0; k < steps && !rc; ++k) rc = run_step(c);
+            CK(cudaEventRecord(keep.e1, s));
+            CK(cudaEventSynchronize(keep.e1));
+            float t = 0.0f;
+            CK(cudaEventElapsedTime(&t, keep.e0, keep.e1));
+            if (rep == 0 || t < best) best = t;
+        }
+        *ms = best / steps;
+        return rc;
+    };
+    cpsd_gpu_tuning cur{}, lim{};
+    cpsd_gpu_get_tuning(c, &cur);
+    cpsd_gpu_tuning_limits(c, &lim);
+    float t0 = 0.0f;
+    int rc = trial(&t0);
+    float best = t0;
+    // one knob at a time, a choice kept only when it is at least 2% faster
+    auto try_value = [&](int *field, int v) -> int {
+        const int old = *field;
+        if (v == old) return CPSD_OK;
+        *field = v;
+        if (cpsd_gpu_set_tuning(c, &cur) != CPSD_OK) {
+            *field = old;
+            return cpsd_gpu_set_tuning(c, &cur);
+        }
+        float t = 0.0f;
+        int r = trial(&t);
+        if (r) return r;
+        if (t < 0.98f * best) {
+            best = t;
+            return CPSD_OK;
+        }
+        *field = old;
+        return cpsd_gpu_set_tuning(c, &cur);
+    };
+    for (int m = 0; m < 4 && !rc; ++m)
+        for (int v = 0; v <= lim.plane_occupancy[m] && !rc; ++v) rc = try_value(&cur.plane_occupancy[m], v);
+    {
+        const int model = c->dens_model[0];
+        const int cand[4] = {1, std::max(1, model / 2), model + 1, 2 * model};
+        for (int q = 0; q < 4 && !rc; ++q)
+            if (cand[q] <= lim.density_chunks) rc = try_value(&cur.density_chunks, cand[q]);
+    }
+    for (int v : {1, 2, 4}) {
+        if (rc) break;
+        rc = try_value(&cur.tn_ctas_per_sm, v);
+    }
+    if (!rc && lim.lagrange_solver == 2)
+        for (int v = 1; v <= 2 && !rc; ++v) rc = try_value(&cur.lagrange_solver, v);
+    float t1 = best;
+    if (!rc) rc = trial(&t1);
+    const int rc2 = restore();
+    drop_graphs(c);
+    CK(cudaStreamSynchronize(s));
+    c->steps_run = steps0;
+    c->nlaunch = nl0;
+    if (rc) return rc;
+    if (rc2) return rc2;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_cache[key] = cur;
+    }
+    if (ms_before) *ms_before = t0;
+    if (ms_after) *ms_after = t1;
     return CPSD_OK;
 }
 

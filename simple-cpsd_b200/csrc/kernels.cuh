@@ -412,6 +412,53 @@ __global__ void density_xc_kernel(XcArgs a)
     a.rfwd[r] = (d[0] + d[a.ispin - 1]) * a.scal1;
 }
 
+// Band-parallel steps split density_xc_kernel at the exchange: this rank's
+// chunk sums (its bands only) -> dn_part, summed over the ranks into dn,
+// then the xc potential from dn.  The arithmetic per point is that of
+// density_xc_kernel, so one rank owning every band gets the same bits.
+__global__ void density_sum_kernel(XcArgs a, double *dn_part)
+{
+    const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.n3) return;
+    double d0 = 0.0, d1 = 0.0;
+    for (int c = 0; c < a.nchunk0; ++c) d0 += a.part[(long)c * a.n3 + r];
+    for (int c = a.nchunk0; c < a.nchunk0 + a.nchunk1; ++c) d1 += a.part[(long)c * a.n3 + r];
+    dn_part[r] = d0 * a.scal2;
+    if (a.ispin == 2) dn_part[a.n3 + r] = d1 * a.scal2;
+}
+
+__global__ void xc_from_density_kernel(XcArgs a)
+{
+    const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.n3) return;
+    const double d0 = a.dn[r], d1 = (a.ispin == 2) ? a.dn[a.n3 + r] : 0.0;
+    // the reference's xi of the spin-polarised exchange reads the first two
+    // spin-0 density values (dirac_exchange.c:101)
+    const double r0 = (a.ispin == 2) ? a.dn[0] : 0.0, r1 = (a.ispin == 2) ? a.dn[1] : 0.0;
+    double vx0, vx1, ex;
+    dirac_vosko(a.ispin, d0, d1, r0, r1, vx0, vx1, ex);
+    a.xcp[r] = vx0;
+    a.xce[r] = ex;
+    if (a.ispin == 2) a.xcp[a.n3 + r] = vx1;
+    a.rfwd[r] = (d0 + (a.ispin == 2 ? d1 : d0)) * a.scal1;
+}
+
+// dn = sum over the parts in their order (the ranks' spin densities of a
+// band-parallel step on one device)
+constexpr int kMaxGroupRanks = 8;
+struct PartSum {
+    const double *part[kMaxGroupRanks];
+    int nparts;
+};
+__global__ void sum_parts_kernel(PartSum p, long n, double *out)
+{
+    const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double acc = p.part[0][r];
+    for (int q = 1; q < p.nparts; ++q) acc += p.part[q][r];
+    out[r] = acc;
+}
+
 // ------------------------------------------------------------ FP64 GEMMs
 // part[prod][split][i][j] = sum_{k in chunk} w(k) A_prod[i*lda+k] B_prod[j*ldb+k];
 // K counts reals, the weight is per complex pair (w[k/2]): the Gamma-point

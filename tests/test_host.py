@@ -319,3 +319,94 @@ def test_cell_shards_rank_without_cells_runs_nothing():
     with pytest.raises(RuntimeError):  # alone, an empty rank holds no cell's energies
         shards.run_cells(specs, 1, 1, rank=empty[0], world=5, runner=runner)
     assert calls == []
+
+
+# ------------------------------------------------------------ band-parallel SD
+def test_band_ranges_cover_every_band_once():
+    from cpsd_b200 import bands
+    for nb in (1, 4, 7, 128):
+        for world in (1, 2, 3, 8):
+            r = bands.band_ranges(nb, world)
+            assert len(r) == world and r[0][0] == 0 and r[-1][1] == nb
+            assert all(a[1] == b[0] for a, b in zip(r, r[1:]))
+            sizes = [hi - lo for lo, hi in r]
+            assert max(sizes) - min(sizes) <= 1
+    assert bands.spin_split(3, 5, 4) == (1, 1)
+    assert bands.spin_split(0, 4, 4) == (4, 0)
+    assert bands.spin_split(5, 7, 4) == (0, 2)
+
+
+def _bands_specs():
+    return {"diamond": lambda: configs.small_diamond(24, 5), "spin": lambda: configs.spin_diamond(24, ne=(4, 3))}
+
+
+def test_band_parallel_restatement_one_rank_is_the_restatement(restatement):
+    """One rank owning every band, exchanges that do nothing: the same bits
+    as the plain restatement."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    for mk in _bands_specs().values():
+        inp = inputs.build_inputs(mk())
+        a, b = oracle.State(inp), oracle.State(inp)
+        for _ in range(2):
+            restatement.run(inp, 2, a)
+            restatement.run_bands(inp, 2, b, 0, inp.nbands, lambda x: None, lambda x: None)
+        for x, y in ((a.E, b.E), (a.c2, b.c2), (a.lmd, b.lmd), (a.dn, b.dn), (a.cpsi, b.cpsi)):
+            assert np.array_equal(x, y)
+
+
+def _bands_rank_main(rank, world, port, name, q):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    from cpsd_b200 import bands
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    inp = inputs.build_inputs(_bands_specs()[name]())
+    ranges = bands.band_ranges(inp.nbands, world)
+    red, gat = bands.torch_exchange(dist, ranges)
+    st = oracle.State(inp)
+    R = oracle.Restatement()
+    for _ in range(2):
+        R.run_bands(inp, 2, st, ranges[rank][0], ranges[rank][1], red, gat)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, st.E.copy(), st.c2.copy(), st.lmd.copy(), st.dn.copy()))
+
+
+@pytest.mark.parametrize("name,world", [("diamond", 2), ("spin", 2), ("spin", 3)])
+def test_band_parallel_restatement_gloo_ranks_equal_one_process(restatement, name, world):
+    """gloo ranks each step their bands of one cell (the restatement's
+    band-parallel form), exchanging the density sum and the new orbitals:
+    every rank ends with the state of one process stepping all bands, to
+    rounding (the density is summed in another order).  With 3 ranks over
+    4 + 3 spin bands one rank holds bands of both spins."""
+    import multiprocessing as mp
+    import socket
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    inp = inputs.build_inputs(_bands_specs()[name]())
+    want = oracle.State(inp)
+    for _ in range(2):
+        restatement.run(inp, 2, want)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_bands_rank_main, args=(r, world, port, name, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    first = got[0]
+    for _, E, c2, lmd, dn in got:
+        assert np.array_equal(E, first[1]) and np.array_equal(c2, first[2])  # replicated state
+        assert np.abs(E - want.E).max() < 1e-10
+        assert np.abs(c2 - want.c2).max() < 1e-12
+        assert np.abs(lmd - want.lmd).max() < 1e-11
+        assert np.abs(dn - want.dn).max() < 1e-12 * np.abs(want.dn).max()
