@@ -221,16 +221,19 @@ def time_kbpp(nfft=128, lmax=3, unit=20.5, reps=3, ref=True):
 
 
 # ----------------------------------------------------------------- GPU arm
-def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True, precision=0, gemm=0):
+def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True, precision=0, gemm=0, tune=True):
     """Device time of `steps` cpsd() calls of `inner` SD steps on a resident
-    cell.  The timed calls run the production schedule (no phase events: the
-    step's second stream overlaps the density chain); the per-phase times
-    come from two extra calls with phase events, which serialise the step."""
+    cell.  The kernel choices come from the library's autotuner (timed on
+    the cell before the warm-up, outside the timed region).  The timed calls
+    run the production schedule (no phase events: the step's second stream
+    overlaps the density chain); the per-phase times come from two extra
+    calls with phase events, which serialise the step."""
     from cpsd_b200 import api
     cell = api.GpuCell(inp, precision=precision)
     if gemm:
         cell.set_gemm(gemm)
     cell.set_state(inp.c2, inp.r2)
+    tuned = cell.autotune(steps=10 if inp.nbands <= 32 else 3) if tune else None
     stream = torch.cuda.ExternalStream(cell.stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(warmup):
@@ -262,9 +265,47 @@ def time_cell(inp, steps, warmup, inner, torch, dist, want_phases=True, precisio
                 phases.setdefault(name, []).append(ms)
         ph = {k: sum(v) / len(v) for k, v in phases.items()}
     geo = cell.geometry()
+    geo["tuning"] = tuned
     E = cell.E.copy()
     cell.close()
     return total_ms, launches, ph, geo, E
+
+
+def time_cufft(n, nb, torch, double=True, reps=5):
+    """The V psi application of every band through cuFFT (torch.fft), as a
+    cuFFT-based engine would run it on the full half box: batched 3-D c2r,
+    multiply by V(r), batched 3-D r2c.  A timed comparison only; the
+    engine's own transforms are the product."""
+    cdt = torch.complex128 if double else torch.complex64
+    rdt = torch.float64 if double else torch.float32
+    g = torch.Generator(device="cuda").manual_seed(1)
+    X = torch.randn(nb, n, n, n // 2 + 1, dtype=cdt, device="cuda", generator=g)
+    V = torch.randn(n, n, n, dtype=rdt, device="cuda", generator=g)
+    for _ in range(2):
+        torch.fft.rfftn(torch.fft.irfftn(X, s=(n, n, n), dim=(1, 2, 3)) * V, dim=(1, 2, 3))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        torch.fft.rfftn(torch.fft.irfftn(X, s=(n, n, n), dim=(1, 2, 3)) * V, dim=(1, 2, 3))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del X, V
+    torch.cuda.empty_cache()
+    return ms
+
+
+def cufft_entry(ph, n, nb, torch, double):
+    """cuFFT's batched full-box V psi against the engine's sphere-pruned
+    pass of the same work (kz inverse + the V psi plane pass + kz forward
+    with the SD epilogue), both device-timed."""
+    eng = sum(ph.get(k, 0.0) for k in ("inv_z_bands", "applyv_plane", "fwd_z_sd"))
+    cu = time_cufft(n, nb, torch, double)
+    return {"cufft_ms": round(cu, 4), "engine_ms": round(eng, 4), "engine_speedup": round(cu / eng, 2) if eng else None,
+            "work": "V psi of %d bands on %d^3: c2r, x V(r), r2c (%s)" % (nb, n, "FP64" if double else "FP32"),
+            "cufft": "torch.fft.irfftn / rfftn, batched, full half box",
+            "engine": "inv_z + plane V psi + fwd_z (sphere-pruned), phase times"}
 
 
 def time_batched(specs, inner, calls):
@@ -439,6 +480,9 @@ def main():
             "final_energy": float(E[0])}
     line["roofline"] = roofline_entry(ph, geo, inp.nbands, inp.nfft, inp.ispin, args.workload,
                                       total_ms / (args.steps * args.inner))
+    if geo.get("tuning"):
+        config["tuning"] = geo["tuning"]["tuning"]
+        config["autotune_ms_per_sd_step"] = [geo["tuning"]["ms_per_step_before"], geo["tuning"]["ms_per_step_after"]]
     line["phases_ms"] = {k: round(v, 5) for k, v in ph.items()}
 
     if rank == 0 and not args.no_e2e:
@@ -461,6 +505,8 @@ def main():
             "value": sd_steps / (tmx * 1e-3), "unit": "steps/s", "ms_per_step": tmx / args.steps,
             "final_energy": float(Em[0]), "abs_dE_vs_fp64_same_steps": abs(float(Em[0]) - float(E[0])),
             "phases_ms": {k: round(v, 5) for k, v in phm.items()}}
+        extra["cufft_" + args.workload] = cufft_entry(ph, inp.nfft, inp.nbands, torch, True)
+        extra["cufft_mixed_" + args.workload] = cufft_entry(phm, inp.nfft, inp.nbands, torch, False)
         # config 4: 48 uneven cells, one graph launch per SD step for all of them
         extra["batched_cells"] = time_batched(C.batched_cells(0), args.inner, 3)
         # the learned path (committed network, mixed precision with a final FP64
@@ -484,6 +530,8 @@ def main():
         extra["mixed_diamond64_128"] = {"value": 3 * args.inner / (tmm * 1e-3), "unit": "steps/s",
                                         "ms_per_sd_step": tmm / (3 * args.inner),
                                         "phases_ms": {k: round(v, 4) for k, v in ph3m.items()}}
+        extra["cufft_diamond64_128"] = cufft_entry(ph3, big.nfft, big.nbands, torch, True)
+        extra["cufft_mixed_diamond64_128"] = cufft_entry(ph3m, big.nfft, big.nbands, torch, False)
         # the same with the TN products on the tensor cores (3xTF32, tcgen05)
         for key, mode in (("mixed_tf32x3_diamond64_128", 1), ("mixed_tf32x3_overlaps_diamond64_128", 3)):
             tmt, _, ph3t, _, _ = time_cell(big, 3, 1, args.inner, torch, None, precision=1, gemm=mode)
@@ -496,6 +544,7 @@ def main():
         extra["diamond64_128"] = {
             "value": 3 * args.inner / (tms * 1e-3), "unit": "steps/s",
             "ms_per_sd_step": tms / (3 * args.inner), "npw": big.npw, "nbands": big.nbands,
+            "tuning": (geo3.get("tuning") or {}).get("tuning"),
             "phases_ms": {k: round(v, 4) for k, v in ph3.items()},
             "roofline": roofline_entry(ph3, geo3, big.nbands, big.nfft, big.ispin, "diamond64_128",
                                        tms / (3 * args.inner))}
