@@ -102,6 +102,33 @@ def batched_cells(seed: int = 0, count: int = 48) -> List[CellSpec]:
     return cells
 
 
+def h2_molecules(seed: int = 0, count: int = 4, a: float = 16.0, nfft: int = 32) -> CellSpec:
+    """`count` H2 molecules (bond 1.4 bohr, seeded centres at least 5 bohr
+    apart and seeded orientations) in an SC box: one doubly occupied band per
+    molecule, a large gap between the bonding and antibonding levels, so the
+    fixed-occupation SD minimum is unique (a control for path-dependent ends)."""
+    rng = np.random.default_rng(seed + 4241)
+    centres: List[np.ndarray] = []
+    while len(centres) < count:
+        p = rng.uniform(-0.5 * a, 0.5 * a, size=3)
+        ok = True
+        for q in centres:
+            d = p - q
+            d -= a * np.round(d / a)
+            if np.sqrt(d @ d) < 5.0:
+                ok = False
+                break
+        if ok:
+            centres.append(p)
+    pos = []
+    for c in centres:
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        pos += [c + 0.7 * u, c - 0.7 * u]
+    return CellSpec(name="h2_molecules_%d" % count, unit=a, nfft=nfft, ecut_ry=30.0, species=[H_S],
+                    katm=[0] * (2 * count), positions=_wrap(np.array(pos), a), ne=(count, 0), seed=seed)
+
+
 def small_diamond(nfft: int = 24, nb: int = 4, ecut: float = 20.0, seed: int = 3,
                   ispin: int = 1) -> CellSpec:
     """8-atom diamond cell on a small grid: s+p projectors, few bands."""
@@ -147,4 +174,5 @@ NAMED = {
     "diamond64_128": diamond64_128,
     # the 128^3 cell with 16 bands: small enough for a full ncu capture
     "diamond64_128_b16": lambda seed=0: diamond64_128(seed, nbands=16),
+    "h2_molecules": h2_molecules,
 }

@@ -370,6 +370,88 @@ def evaluate(inp, mlp: api.Mlp, inner: int, tol_per_ion: float, learned_steps: i
     return out
 
 
+def plain_to_convergence(inp, max_steps: int, inner: int = 200, tol: float = 1e-10,
+                         start_c2: Optional[np.ndarray] = None) -> dict:
+    """Plain FP64 SD until the energy changes by less than `tol` over each of
+    five consecutive blocks of `inner` steps: the converged energy E_conv
+    (the reference's own test, main.c:435, watches deltae the same way).
+    Returns E_conv, the steps taken (None if max_steps ran out) and the
+    energy and wall time after every block."""
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    if start_c2 is not None:
+        cell.set_packed(start_c2)
+    energies, seconds = [], []
+    prev, steps, quiet, conv = math.inf, 0, 0, None
+    t0 = time.perf_counter()
+    while steps < max_steps:
+        e = float(cell.run(inner)[0])
+        steps += inner
+        energies.append(e)
+        seconds.append(time.perf_counter() - t0)
+        quiet = quiet + 1 if abs(e - prev) < tol else 0
+        prev = e
+        if quiet >= 5:
+            conv = steps
+            break
+    cell.close()
+    return {"e_conv": energies[-1], "conv_step": conv, "energies": energies, "seconds": seconds, "inner": inner}
+
+
+def study_cell(inp, mlp: api.Mlp, tol_per_ion: float = 1e-6, plain_max: int = 600000, learned_max: int = 60000,
+               inner: int = 100, alt_start_seed: Optional[int] = None, verify_steps: int = 5000,
+               precision: int = 1, gemm: int = 3) -> dict:
+    """The learned path against plain SD on one cell, with plain SD's own
+    converged energy as the judge:
+
+    * plain FP64 SD from the cell's start orbitals to convergence -> E_conv,
+      and its time to |E - E_conv| <= tol_per_ion * nion;
+    * the learned mixed-precision path (FP64 refinement at the end, plain SD
+      as the fallback) from the same start until it is within the tolerance
+      of E_conv, or learned_max steps; plain FP64 SD continued from its end
+      state for verify_steps (a drift near zero: the end state is stationary
+      for plain SD);
+    * with alt_start_seed, plain SD from other seeded orbitals to convergence:
+      a different E_conv there shows that the cell's fixed-occupation energy
+      has several stationary points, and which one SD ends in depends on
+      the path."""
+    nion = inp.nion
+    tol = tol_per_ion * nion
+    pl = plain_to_convergence(inp, plain_max)
+    e_conv = pl["e_conv"]
+    p_steps, p_s = None, None
+    for k, e in enumerate(pl["energies"]):
+        if abs(e - e_conv) <= tol:
+            p_steps, p_s = (k + 1) * pl["inner"], pl["seconds"][k]
+            break
+    lr = run(inp, e_conv, tol_per_ion, learned_max, inner, mlp=mlp, precision=precision, gemm=gemm,
+             refine_per_ion=1e-8, keep_state=True)
+    ver = run(inp, None, tol_per_ion, verify_steps, inner, start_c2=lr.final_c2)
+    out = {"nion": nion, "nbands": int(inp.nbands), "nfft": int(inp.nfft), "tol_per_ion": tol_per_ion,
+           "plain": {"e_conv": e_conv, "conv_step": pl["conv_step"], "steps_to_tol": p_steps, "seconds_to_tol": p_s,
+                     "seconds_run": pl["seconds"][-1]},
+           "learned": {"steps_to_tol": lr.steps_to_tol, "seconds_to_tol": lr.seconds_to_tol, "steps_run": lr.steps,
+                       "final_energy": lr.energies[-1], "rejected_blocks": lr.rejected_blocks,
+                       "precision": "mixed" if precision else "fp64", "gemm": gemm,
+                       "fp64_refinement_from_step": lr.refine_step,
+                       "final_minus_e_conv_per_ion": (lr.energies[-1] - e_conv) / nion,
+                       "plain_continuation_drift_per_ion": abs(ver.energies[-1] - lr.energies[-1]) / nion}}
+    if p_s and lr.seconds_to_tol:
+        out["speedup_time"] = p_s / lr.seconds_to_tol
+        out["speedup_steps"] = p_steps / lr.steps_to_tol
+    if alt_start_seed is not None:
+        alt = inputs.random_orbitals(inp.nfft, inp.masker1, inp.nbands, alt_start_seed)
+        cell = api.GpuCell(inp)
+        pts = cell.sphere()[0]
+        cell.close()
+        c = alt.reshape(inp.nbands, inp.nfft3d, 2)[:, pts, :]
+        start = np.ascontiguousarray(c[..., 0] + 1j * c[..., 1])
+        pa = plain_to_convergence(inp, plain_max, start_c2=start)
+        out["plain_other_start"] = {"seed": alt_start_seed, "e_conv": pa["e_conv"], "conv_step": pa["conv_step"],
+                                    "minus_e_conv_per_ion": (pa["e_conv"] - e_conv) / nion}
+    return out
+
+
 def headline(n8: int = 6, n64: int = 2, traj8: int = 12000, traj64: int = 4000, inner: int = 100,
              train_steps: int = 3000, eval8: int = 2, eval64: int = 1, tol_per_ion: float = 1e-6,
              learned_steps8: int = 40000, plain_steps8: int = 250000, learned_steps64: int = 30000,
@@ -434,7 +516,27 @@ if __name__ == "__main__":
     ap.add_argument("--verify-steps", type=int, default=5000)
     ap.add_argument("--e-ref", type=float, default=None,
                     help="an energy of the same cell reached by another run (joins the reference minimum)")
+    ap.add_argument("--study", default=None,
+                    help="study_cell on held-out cells of a configs name (comma-separated seeds in --seeds)")
+    ap.add_argument("--seeds", default="5000,5001")
+    ap.add_argument("--plain-max", type=int, default=600000)
+    ap.add_argument("--fp64", action="store_true", help="study: the learned path in FP64 (no mixed precision)")
     a = ap.parse_args()
+    if a.study:
+        from . import configs
+        mlp = load_pretrained()
+        res = {}
+        for sd in (int(x) for x in a.seeds.split(",")):
+            r = study_cell(inputs.build_inputs(configs.NAMED[a.study](seed=sd)), mlp, plain_max=a.plain_max,
+                           learned_max=a.learned_steps, alt_start_seed=sd + 77,
+                           precision=0 if a.fp64 else 1, gemm=0 if a.fp64 else 3)
+            res["%s seed %d" % (a.study, sd)] = r
+            print(json.dumps({"cell": "%s seed %d" % (a.study, sd), **r}), flush=True)
+            if a.out:
+                with open(a.out, "w") as f:
+                    json.dump(res, f, indent=1)
+        mlp.close()
+        raise SystemExit(0)
     if a.headline:
         print(json.dumps(headline(out=a.out, weights=a.weights), indent=1))
         raise SystemExit(0)

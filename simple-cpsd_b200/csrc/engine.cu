@@ -402,6 +402,13 @@ struct cpsd_gpu_ctx {
     bool use_graph = true;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // one captured SD step per ping-pong parity
     int graph_launches = 0;
+    // several SD steps captured as one graph (the steps of a cpsd() call),
+    // per (steps, parity); a few kept
+    struct MultiGraph {
+        int steps, par, launches;
+        cudaGraphExec_t exec;
+    };
+    std::vector<MultiGraph> mgraphs;
     // second stream of a step: structure factors, projectors and the kinetic +
     // nonlocal part of -H psi run beside the density -> potential chain
     cudaStream_t st2 = nullptr;
@@ -980,6 +987,8 @@ void drop_graphs(cpsd_gpu_ctx *c)
             cudaGraphExecDestroy(g);
             g = nullptr;
         }
+    for (auto &m : c->mgraphs) cudaGraphExecDestroy(m.exec);
+    c->mgraphs.clear();
 }
 
 // One SD step, replayed from a CUDA graph captured on first use (one graph
@@ -1009,6 +1018,61 @@ int run_step(cpsd_gpu_ctx *c)
     CK(cudaGraphLaunch(c->gexec[par], c->st));
     c->nlaunch += c->graph_launches;
     c->cur ^= 1;
+    return CPSD_OK;
+}
+
+// `inner` SD steps as few graph launches: up to kStepsPerGraph steps are
+// captured into one graph (per step count and ping-pong parity, the last
+// kMultiGraphs kept), so a cpsd() call of 10 steps is one launch.
+constexpr int kStepsPerGraph = 32;
+constexpr size_t kMultiGraphs = 4;
+
+int run_steps(cpsd_gpu_ctx *c, int inner)
+{
+    if (!c->use_graph || c->phase_timing) {
+        for (int it = 0; it < inner; ++it) {
+            int rc = run_step(c);
+            if (rc) return rc;
+        }
+        return CPSD_OK;
+    }
+    while (inner > 0) {
+        const int k = std::min(inner, kStepsPerGraph);
+        const int par = c->cur;
+        cpsd_gpu_ctx::MultiGraph *m = nullptr;
+        for (auto &x : c->mgraphs)
+            if (x.steps == k && x.par == par) m = &x;
+        if (!m) {
+            cudaGraph_t g = nullptr;
+            const long long before = c->nlaunch;
+            CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+            int rc = CPSD_OK;
+            for (int it = 0; it < k && !rc; ++it) rc = one_step(c);
+            cudaError_t e = cudaStreamEndCapture(c->st, &g);
+            c->cur = par;  // capture launched nothing: undo the buffer flips
+            const int launches = (int)(c->nlaunch - before);
+            c->nlaunch = before;
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            CK(e);
+            cudaGraphExec_t ex = nullptr;
+            e = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            CK(e);
+            if (c->mgraphs.size() >= kMultiGraphs) {
+                cudaGraphExecDestroy(c->mgraphs.front().exec);
+                c->mgraphs.erase(c->mgraphs.begin());
+            }
+            c->mgraphs.push_back({k, par, launches, ex});
+            m = &c->mgraphs.back();
+        }
+        CK(cudaGraphLaunch(m->exec, c->st));
+        c->nlaunch += m->launches;
+        if (k & 1) c->cur ^= 1;
+        inner -= k;
+    }
     return CPSD_OK;
 }
 
@@ -1967,10 +2031,8 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
     cudaStream_t s = c->st;
     CK(cudaMemsetAsync(c->flags, 0, 3 * sizeof(int), s));
     CK(cudaMemcpyAsync(c->Edev, E, sizeof(double), cudaMemcpyHostToDevice, s));
-    for (int it = 0; it < inner; ++it) {
-        int rc = run_step(c);
-        if (rc) return rc;
-    }
+    int rc = run_steps(c, inner);
+    if (rc) return rc;
     return finish_call(c, inner, E, deltae, deltac, deltar);
 }
 
@@ -2671,13 +2733,13 @@ int cpsd_gpu_autotune(cpsd_gpu_ctx *c, int steps, int force, float *ms_before, f
     auto trial = [&](float *ms) -> int {
         drop_graphs(c);
         int rc = restore();
-        if (!rc) rc = run_step(c);
+        if (!rc) rc = run_steps(c, steps);
         float best = 0.0f;
         for (int rep = 0; rep < 3 && !rc; ++rep) {
             rc = restore();
             if (rc) break;
             CK(cudaEventRecord(keep.e0, s));
-            for (int k = 0; k < steps && !rc; ++k) rc = run_step(c);
+            rc = run_steps(c, steps);
             CK(cudaEventRecord(keep.e1, s));
             CK(cudaEventSynchronize(keep.e1));
             float t = 0.0f;

@@ -311,15 +311,17 @@ CPSD_D void dirac_vosko(int ispin, double nup_in, double ndn_in, double rho0, do
     const double two_to_onethird_d = 1.25992104989487319067;
     const double A_d = 0.25992104989487319067;
     const double pi_d = 3.14159265358979311600;
+    // cube roots of the (non-negative) density by cbrt: the reference's
+    // pow(x, 1/3) to within an ulp
     if (ispin == 1) {
         const double n = nup_in + nup_in;
-        const double n13 = pow(3.0 * n / pi_d, onethird_d);
+        const double n13 = cbrt(3.0 * n / pi_d);
         ex = -(9.0 / 8.0) * alpha * n13;
         vx0 = -(3.0 / 2.0) * alpha * n13;
         vx1 = vx0;
     } else {
         const double n = nup_in + ndn_in;
-        const double n13 = pow(3.0 * n / pi_d, onethird_d);
+        const double n13 = cbrt(3.0 * n / pi_d);
         // the reference's xi here uses the first two density values (dirac_exchange.c:101)
         const double xi = (n > 0.0) ? (rho0 - rho1) / n : 1.0;
         const double ex_p = -(9.0 / 8.0) * alpha * n13;
@@ -356,7 +358,7 @@ CPSD_D void dirac_vosko(int ispin, double nup_in, double ndn_in, double rho0, do
     const double nup = nup_in + small_number;
     const double ndown = ((ispin == 1) ? nup_in : ndn_in) + small_number;
     const double n = nup + ndown;
-    const double rs = rs_scale / pow(n, onethird);
+    const double rs = rs_scale / cbrt(n);
     const double xi = (nup - ndown) / n;
     const double x = sqrt(rs);
     const double xxp = rs + bp * x + cp;
