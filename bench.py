@@ -12,9 +12,13 @@ timed region.  ``--impl reference`` times the reference's own serial C
 (oracle/_ref, ccpsdv3/*.c compiled unmodified) on the host cores.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-Multi-GPU (torchrun, one process per GPU): every rank runs its own replica of
-the cell (the SD loop of one cell has no data-parallel split: replicas only);
-the timed region is bracketed by barriers and the time is the max over ranks.
+Multi-GPU (torchrun, one process per GPU): `value` is every rank running its
+own replica of the cell (weak scaling), timed between barriers, max over
+ranks; `extra` adds the 48-cell batched draw sharded over the ranks (no
+exchange in the step) and the 128^3 / 128-band cell stepped band-parallel by
+all ranks (densities all-reduced and orbital rows broadcast over NCCL, per
+SD step).  At one GPU the band-parallel extra runs two emulated ranks on the
+one device (the phases' overhead, not a speed-up).
 """
 from __future__ import annotations
 
@@ -342,6 +346,88 @@ def time_batched(specs, inner, calls):
             "speedup": t_seq / t_bat, "gpu_launches": launches, "timing": "host wall clock, synchronous calls"}
 
 
+def time_band_parallel(torch, dist, world, rank, calls=2, inner=2, emulate=1):
+    """Band-parallel SD of the 128^3 / 128-band cell: this rank steps its
+    bands, the densities are all-reduced and the orbital rows broadcast over
+    the process group (cpsd_b200.bands.TorchExchange, NCCL), device-timed on
+    the cell's stream, max over ranks.  With no process group, `emulate`
+    contexts on this GPU stand in for the ranks (LocalGroup, stepped phase by
+    phase): that measures the phases' overhead, not a speed-up."""
+    from cpsd_b200 import api, bands, configs, inputs
+    inp = inputs.build_inputs(configs.diamond64_128())
+    nr = world if dist is not None else emulate
+    ranges = bands.band_ranges(inp.nbands, nr)
+    mine = [rank] if dist is not None else list(range(nr))
+    cells = []
+    for r in mine:
+        c = api.GpuCell(inp)
+        c.set_state(inp.c2, inp.r2)
+        c.set_band_range(*ranges[r])
+        cells.append(c)
+    ex = bands.TorchExchange(torch, dist, cells[0], ranges) if dist is not None else \
+        bands.LocalGroup(torch, cells, ranges)
+    bands.run(cells, ex, inner)  # warm-up
+    stream = torch.cuda.ExternalStream(cells[0].stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(calls):
+        bands.run(cells, ex, inner)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        dist.barrier()
+    ms = max_over_ranks(ms, dist, torch, "cuda")
+    E = cells[0].E.copy()
+    for c in cells:
+        c.close()
+    return {"ranks": nr, "emulated": dist is None, "ms_per_sd_step": ms / (calls * inner),
+            "final_energy": float(E[0]), "bands_per_rank": [hi - lo for lo, hi in ranges],
+            "timing": "CUDA events on the stepping stream, %d calls of %d SD steps, max over ranks" % (calls, inner)}
+
+
+def time_cells_sharded(torch, dist, world, rank, calls=3, inner=10):
+    """The 48-cell batched draw sharded over the ranks (cpsd_b200.shards:
+    longest-processing-time split, one batched graph per SD step per rank,
+    no exchange in the step): SD steps of all cells per second, wall time
+    between barriers, max over ranks."""
+    from cpsd_b200 import api, configs, inputs, shards
+    specs = configs.batched_cells(0)
+    mine = shards.assign(specs, world)[rank]
+    cells = []
+    for i in mine:
+        inp = inputs.build_inputs(specs[i])
+        c = api.GpuCell(inp)
+        c.set_state(inp.c2, inp.r2)
+        cells.append(c)
+    batch = api.GpuBatch(cells) if cells else None
+    if batch:
+        batch.run(inner)  # warm-up (captures the batch graphs)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        if batch:
+            batch.run(inner)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    if dist is not None:
+        dist.barrier()
+    dt = max_over_ranks(dt, dist, torch, "cuda")
+    if batch:
+        batch.close()
+    for c in cells:
+        c.close()
+    sd = len(specs) * calls * inner
+    return {"cells": len(specs), "ranks": world, "value": sd / dt, "unit": "SD steps/s (all cells)",
+            "cells_on_rank0": len(shards.assign(specs, world)[0]), "scaling": "strong (fixed 48 cells)",
+            "timing": "host wall clock between barriers around synchronous batched calls, max over ranks"}
+
+
 def e2e_dropin(inp, calls, inner):
     """Through the reference-facing cpsd() with host buffers (copies timed)."""
     from cpsd_b200 import api
@@ -555,6 +641,14 @@ def main():
             "phases_ms": {k: round(v, 4) for k, v in ph3.items()},
             "roofline": roofline_entry(ph3, geo3, big.nbands, big.nfft, big.ispin, "diamond64_128",
                                        tms / (3 * args.inner))}
+    if world > 1 and not args.no_extra:
+        # multi-GPU: the 48-cell draw sharded over the ranks, and one 128^3
+        # cell stepped band-parallel by all of them (every rank takes part)
+        mg = {"cells_sharded": time_cells_sharded(torch, dist, world, rank),
+              "band_parallel_diamond64_128": time_band_parallel(torch, dist, world, rank)}
+        line.setdefault("extra", {}).update(mg)
+    elif rank == 0 and not args.no_extra:
+        line["extra"]["band_parallel_emulated_diamond64_128"] = time_band_parallel(torch, None, 1, 0, emulate=2)
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

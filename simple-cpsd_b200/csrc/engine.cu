@@ -165,6 +165,7 @@ struct FftOps {
     virtual void fwd_z_sd(const Geom &g, const void *Tb, const ZEpilogue &e, int nb, cudaStream_t s) = 0;
     virtual void plane(int mode, const Geom &g, void *Tb, const PlaneArgs &a, int nchunks, cudaStream_t s) = 0;
     virtual int plane_ctas_per_sm(int mode) const = 0;  // resident CTAs of a plane pass
+    virtual int plane_ctas_per_plane(int mode) const = 0;  // CTAs sharing one z plane (row split)
     // occupancy builds of a plane pass (1 or 2) and the one that runs
     virtual int plane_variants(int mode) const = 0;
     virtual int plane_variant(int mode) const = 0;
@@ -249,6 +250,10 @@ struct FftOpsT final : FftOps {
             hi_fits[m] = has_two[m] && 2 * (psmem[m] + (size_t)reserve) <= (size_t)sm_bytes;
             occ[m] = hi_fits[m] ? 1 : 0;
         }
+        // the row-split density build at NF >= 128 redoes each plane's y
+        // lines in two CTAs: measured slower than the whole-plane build, so
+        // it is only a candidate of the tuner
+        if (plane_row_split<NF, PM_DENSITY, 2>() > 1) occ[PM_DENSITY] = 0;
         return CPSD_OK;
     }
 
@@ -267,7 +272,9 @@ struct FftOpsT final : FftOps {
     {
         if constexpr (plane_has_two_cta_build<NF, MODE>())
             if (occ[MODE]) {
-                plane_kernel<T, NF, MODE, 2><<<grid, nt, psmem[MODE], s>>>(g, (cx<T> *)Tb, a, tw);
+                dim3 g2 = grid;
+                g2.z = plane_row_split<NF, MODE, 2>();  // the density pass's row halves
+                plane_kernel<T, NF, MODE, 2><<<g2, nt, psmem[MODE], s>>>(g, (cx<T> *)Tb, a, tw);
                 return;
             }
         plane_kernel<T, NF, MODE, 1><<<grid, nt, psmem[MODE], s>>>(g, (cx<T> *)Tb, a, tw);
@@ -309,6 +316,10 @@ struct FftOpsT final : FftOps {
     }
     bool mode_ok(int mode) const { return psmem[mode] != 0; }
     int plane_ctas_per_sm(int mode) const override { return occ[mode & 3] ? 2 : 1; }
+    int plane_ctas_per_plane(int mode) const override
+    {
+        return (mode == PM_DENSITY && occ[PM_DENSITY]) ? plane_row_split<NF, PM_DENSITY, 2>() : 1;
+    }
     int plane_variants(int mode) const override { return hi_fits[mode & 3] ? 2 : 1; }
     int plane_variant(int mode) const override { return occ[mode & 3]; }
     void set_plane_variant(int mode, int v) override
@@ -1709,7 +1720,8 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     // minimises waves x bands per CTA over the SMs' resident slots, the
     // smallest such count (fewer partial densities to add); never across spins
     {
-        const long slots = (long)c->sms * c->fft->plane_ctas_per_sm(PM_DENSITY);
+        const long slots = (long)c->sms * c->fft->plane_ctas_per_sm(PM_DENSITY) /
+                           c->fft->plane_ctas_per_plane(PM_DENSITY);
         auto best_chunks = [&](int bands, int planes_per_chunk_group) {
             int best = 1;
             long best_cost = -1;

@@ -175,10 +175,25 @@ struct PlaneShape {
     // exchange-buffer strides of the y-line groups and the x-row groups
     static constexpr int SY = group_stride<T, NF>();
     static constexpr int SX = group_stride<T, H>();
+    // FP64 lines of 8 lanes holding 2 outputs each (NF = 128): a lane stores
+    // its outputs 2 apart, so the 8 lanes of a 128-byte phase would meet in
+    // 4 of the 8 16-byte slots; one pad slot after every 8 y positions
+    // (ymap) spreads them over all 8
+    static constexpr bool YSWZ = sizeof(cx<T>) == 16 && LY::P >= 8 && LY::U >= 2;
+    static constexpr int YW = NF + (YSWZ ? NF / 8 : 0);
+    CPSD_HD static int ymap(int p) { return YSWZ ? p + (p >> 3) : p; }
     // y-line stride: lanes t of an x group read rows k = t + P m of one column
     // and the 8/P groups of a phase read neighbouring columns
-    static constexpr int YS = (LX::P >= kSlots<T>) ? pad_to(NF + 1, kSlots<T>, 1)
-                                                   : pad_to(NF + 1, kSlots<T>, kSlots<T> / LX::P);
+    static constexpr int YS = (LX::P >= kSlots<T>) ? pad_to(YW + 1, kSlots<T>, 1)
+                                                   : pad_to(YW + 1, kSlots<T>, kSlots<T> / LX::P);
+    // y-line groups that hold a line: all of them when there are at least as
+    // many lines as groups, else the lines rounded up to whole warps (the
+    // warps past them skip the y transforms and need no exchange buffer)
+    CPSD_HD static int y_groups(int KX, int ngy)
+    {
+        const int gpw = 32 / LY::P;
+        return KX >= ngy ? ngy : ((KX + gpw - 1) / gpw) * gpw;
+    }
     // density rows: one extra complex per row moves the next row's group
     static constexpr int RS = NF + 2;
 };
@@ -194,7 +209,7 @@ size_t plane_smem_bytes(int mode, int KX)
 {
     using S = PlaneShape<T, NF>;
     const int nt = plane_threads<T, NF>(mode);
-    const size_t ex_y = (size_t)(nt / S::LY::P) * S::SY, ex_x = (size_t)(nt / S::LX::P) * S::SX;
+    const size_t ex_y = (size_t)S::y_groups(KX, nt / S::LY::P) * S::SY, ex_x = (size_t)(nt / S::LX::P) * S::SX;
     size_t b = sizeof(cx<T>) * ((size_t)KX * S::YS + (ex_y > ex_x ? ex_y : ex_x));
     return (b + 15) / 16 * 16;
 }
@@ -202,11 +217,18 @@ size_t plane_smem_bytes(int mode, int KX)
 // Every plane variant is built for one and for two CTAs per SM (MINB); the
 // host launches the two-CTA build where two planes' shared memory fits an SM
 // (it caps registers at 128 per thread).  The density variant at n >= 128
-// keeps its per-lane sums in registers and is built for one CTA only.
+// keeps 64 per-lane sums in registers; its two-CTA build instead splits each
+// plane's x rows between two CTAs (blockIdx.z = the half): every CTA redoes
+// the plane's y lines (about a quarter of the work) and keeps half the sums.
 template <int NF, int MODE>
 constexpr bool plane_has_two_cta_build()
 {
-    return !(MODE == PM_DENSITY && NF >= 128);
+    return true;
+}
+template <int NF, int MODE, int MINB>
+constexpr int plane_row_split()
+{
+    return (MODE == PM_DENSITY && NF >= 128 && MINB == 2) ? 2 : 1;
 }
 
 template <typename T, int NF, int MODE, int MINB>
@@ -228,7 +250,10 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
     cx<T> *xball = Y + KX * YS;                       // group exchange buffers
     // DENSITY: each lane owns the same (row, x) points for every band, so the
     // sum of psi^2 over the band chunk stays in registers
-    constexpr int NIT = (NF + NGX - 1) / NGX;  // x-row iterations per lane
+    constexpr int RSPLIT = plane_row_split<NF, MODE, MINB>();
+    constexpr int NIT = (NF + NGX - 1) / NGX / RSPLIT;  // x-row iterations per lane (of this CTA's rows)
+    static_assert(RSPLIT == 1 || NIT * NGX * RSPLIT == NF, "row split");
+    const int it0 = (RSPLIT > 1) ? (int)blockIdx.z * NIT : 0;
     double rho[(MODE == PM_DENSITY) ? NIT : 1][(MODE == PM_DENSITY) ? 2 * QX : 1];
 
     const int z = blockIdx.x;
@@ -244,6 +269,7 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
     }
 
     const int gy = threadIdx.x / PY, ty = threadIdx.x % PY;
+    const int ngy_act = S::y_groups(KX, NGY);  // warp-uniform: whole warps skip the y lines
     const int gx = threadIdx.x / PX, tx = threadIdx.x % PX;
     cx<T> *xby = xball + gy * S::SY;
     cx<T> *xbx = xball + gx * S::SX;
@@ -252,7 +278,7 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
         cx<T> *Tplane = Tb + ((long)b * NF + z) * g.ncol;
         // ---- inverse along y (columns -> lines kx < KX) ------------------
         if constexpr (MODE != PM_FWDREAL) {
-            for (int base = 0; base < KX; base += NGY) {
+            for (int base = 0; base < KX && gy < ngy_act; base += NGY) {
                 const int i = base + gy;
                 const bool act = i < KX;
                 cx<T> v[QY];
@@ -266,7 +292,7 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
 #pragma unroll
                     for (int u = 0; u < UY; ++u)
 #pragma unroll
-                        for (int s = 0; s < PY; ++s) Y[i * YS + LY::out_index(ty, u, s)] = v[u * PY + s];
+                        for (int s = 0; s < PY; ++s) Y[i * YS + S::ymap(LY::out_index(ty, u, s))] = v[u * PY + s];
                 }
             }
             __syncthreads();
@@ -274,7 +300,7 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
         // ---- x rows --------------------------------------------------------
 #pragma unroll
         for (int it = 0; it < NIT; ++it) {
-            const int j = it * NGX + gx;
+            const int j = (it0 + it) * NGX + gx;
             const bool act = j < NF;
             const int jj = act ? j : 0;
             cx<T> v[QX];
@@ -284,8 +310,8 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
                 for (int m = 0; m < QX; ++m) {
                     const int k = LX::in_index(tx, m);
                     const int kk = H - k;
-                    cx<T> xa = (k < KX) ? Y[k * YS + jj] : cx<T>{0, 0};
-                    cx<T> xc = (kk < KX) ? Y[kk * YS + jj] : cx<T>{0, 0};
+                    cx<T> xa = (k < KX) ? Y[k * YS + S::ymap(jj)] : cx<T>{0, 0};
+                    cx<T> xc = (kk < KX) ? Y[kk * YS + S::ymap(jj)] : cx<T>{0, 0};
                     if (k == 0) {
                         xa.y = 0;
                         xc.y = 0;
@@ -370,7 +396,7 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
                     cx<T> O{D.y, -D.x};
                     cx<T> X = E + cmul(tw.r_fwd[k], O);
                     if (k == 0 || k == H) X.y = 0;
-                    if (act) Y[k * YS + j] = X;
+                    if (act) Y[k * YS + S::ymap(j)] = X;
                 }
                 __syncwarp();
             }
@@ -378,24 +404,24 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
         __syncthreads();
         // ---- forward along y, keep the columns -----------------------------
         if constexpr (MODE == PM_APPLYV || MODE == PM_FWDREAL) {
-            for (int base = 0; base < KX; base += NGY) {
+            for (int base = 0; base < KX && gy < ngy_act; base += NGY) {
                 const int i = base + gy;
                 const bool act = i < KX;
                 const int ii = act ? i : 0;
                 cx<T> v[QY];
 #pragma unroll
-                for (int m = 0; m < QY; ++m) v[m] = Y[ii * YS + LY::in_index(ty, m)];
+                for (int m = 0; m < QY; ++m) v[m] = Y[ii * YS + S::ymap(LY::in_index(ty, m))];
                 line_fft<NF, -1, T>(v, ty, xby, tw.n_fwd);
                 // each group reads and rewrites only its own line
                 if (act) {
 #pragma unroll
                     for (int u = 0; u < UY; ++u)
 #pragma unroll
-                        for (int s = 0; s < PY; ++s) Y[i * YS + LY::out_index(ty, u, s)] = v[u * PY + s];
+                        for (int s = 0; s < PY; ++s) Y[i * YS + S::ymap(LY::out_index(ty, u, s))] = v[u * PY + s];
                 }
             }
             __syncthreads();
-            for (int c = threadIdx.x; c < g.ncol; c += NT) Tplane[c] = Y[g.col_i[c] * YS + g.col_j[c]];
+            for (int c = threadIdx.x; c < g.ncol; c += NT) Tplane[c] = Y[g.col_i[c] * YS + S::ymap(g.col_j[c])];
             __syncthreads();
         }
     }
@@ -404,7 +430,7 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
         double *dst = a.rho_part + ((long)blockIdx.y * NF + z) * plane;
 #pragma unroll
         for (int it = 0; it < NIT; ++it) {
-            const int j = it * NGX + gx;
+            const int j = (it0 + it) * NGX + gx;
             if (j < NF) {
 #pragma unroll
                 for (int u = 0; u < UX; ++u)

@@ -67,6 +67,23 @@ def test_every_plane_build_keeps_parity(golden, mode):
         check_against_golden(inp, g, rows, st)
 
 
+@pytest.mark.parametrize("occ", [0, 1])
+def test_density_row_split_keeps_parity_at_128(golden, occ):
+    """The 128^3 density pass whole (one CTA per plane) and with its x rows
+    split between two CTAs per plane, against the reference build."""
+    inp = inputs.build_inputs(configs.diamond64_128())
+    cell = api.GpuCell(inp)
+    lim = cell.tuning_limits()["plane_occupancy"][0]
+    planes = cell.tuning()["plane_occupancy"]
+    cell.close()
+    if occ > lim:
+        pytest.skip("the row-split build does not fit this device")
+    planes[0] = occ
+    rows, st, t = _run(inp, 1, 2, plane_occupancy=planes)
+    assert t["plane_occupancy"][0] == occ
+    check_against_golden(inp, golden("diamond64_128"), rows, st)
+
+
 def test_density_chunks_split_k_and_solvers_keep_parity(restatement):
     """Other choices on a 40-band cell against the restatement: density chunk
     counts 1 and the largest, split-K targets 1 and 4, both cluster solvers."""
