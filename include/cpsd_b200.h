@@ -368,6 +368,21 @@ int cpsd_gpu_set_gemm(cpsd_gpu_ctx *c, int mode);
  * the device at every step, so it takes effect without re-capturing the
  * step graphs. */
 int cpsd_gpu_set_preconditioner_range(cpsd_gpu_ctx *c, double min_log_k, double max_log_k);
+/*
+ * The guarded learned loop with plain SD as the judge, in the library (no
+ * counterpart in the reference): `blocks` blocks of `inner` steps with the
+ * attached network (CPSD_ERR_ARG without one), the bound on log K at most
+ * *cap.  A block whose energy rises above the previous one (E[0] in), is not
+ * finite, or whose Lagrange iteration did not converge (more than one band
+ * per spin) is redone from its start with plain SD steps (K = 1: the
+ * reference's update), and *cap shrinks by 0.7; an accepted block grows it by
+ * 0.1 (within [-2, 4.5]).  E, deltae, deltac: those of the last block;
+ * *rejected (may be NULL) counts the redone blocks.  The rollback point is
+ * the device copy of cpsd_gpu_save_orbitals.
+ */
+int cpsd_gpu_run_guarded(cpsd_gpu_ctx *c, int blocks, int inner, double *cap, double *E, double *deltae,
+                         double *deltac, int *rejected);
+
 /* Keep a device copy of the current orbitals and step count / go back to it
  * (the rollback point of a guarded block, without a round trip through the
  * host). */

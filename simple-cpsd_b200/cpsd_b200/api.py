@@ -160,6 +160,21 @@ class GpuCell:
                     "cpsd_gpu_set_preconditioner")
         self._mlp = mlp  # keep it alive while attached
 
+    def run_guarded(self, inner: int, cap: float, blocks: int = 1):
+        """Blocks of learned steps with plain SD as the judge, in the library
+        (cpsd_gpu_run_guarded): returns (energy, rejected blocks, new cap)."""
+        c = np.array([cap], dtype=np.float64)
+        de, dc = ctypes.c_double(), ctypes.c_double()
+        rej = ctypes.c_int(0)
+        rc = self._L.cpsd_gpu_run_guarded(self.h, int(blocks), int(inner), _ptr(c), _ptr(self.E), ctypes.byref(de),
+                                          ctypes.byref(dc), ctypes.byref(rej))
+        if rc == _l.CPSD_WARN_LAGRANGE:
+            self.lagrange_warnings += 1
+        elif rc != _l.CPSD_OK:
+            raise CpsdError(rc, "cpsd_gpu_run_guarded")
+        self.deltae, self.deltac = de.value, dc.value
+        return float(self.E[0]), rej.value, float(c[0])
+
     # band-parallel SD (cpsd_b200.bands drives these)
     def set_band_range(self, lo: int, hi: int) -> None:
         self._check(self._L.cpsd_gpu_set_band_range(self.h, int(lo), int(hi)), "cpsd_gpu_set_band_range")

@@ -197,29 +197,17 @@ def run(spec_or_inp, e_conv: Optional[float], tol_per_ion: float, max_steps: int
     hit_step, hit_time, refine_step = None, None, None
     prev = math.inf
     cap = LOGK_MAX
-    min_bands = min(int(n) for n in inp.ne[:inp.ispin])
     t0 = time.perf_counter()
     if mlp is not None:
         cell.set_preconditioner(mlp)
     while steps < max_steps:
         if mlp is not None:
-            cell.save_orbitals()
-            warn0 = cell.lagrange_warnings
-            cell.set_preconditioner_range(LOGK_MIN, cap)
-            e = float(cell.run(inner)[0])
-            # (with one band per spin the reference's convergence test can never
-            # pass, so its warning says nothing there)
-            lag_failed = cell.lagrange_warnings > warn0 and min_bands > 1
-            if not math.isfinite(e) or e > prev or lag_failed:
-                # rejected: redo the block from its start with plain SD steps
-                # (K = 1 exactly: the update reduces to the reference's)
-                rejected += 1
-                cap = max(LOGK_MIN, cap - CAP_SHRINK)
-                cell.restore_orbitals()
-                cell.set_preconditioner_range(0.0, 0.0)
-                e = float(cell.run(inner)[0])
-            else:
-                cap = min(LOGK_MAX, cap + CAP_GROW)
+            # one guarded block in the library (cpsd_gpu_run_guarded): a block
+            # whose energy rises, is not finite or whose Lagrange iteration did
+            # not converge is redone from its start with plain SD steps
+            cell.E[0] = prev
+            e, rej, cap = cell.run_guarded(inner, cap)
+            rejected += rej
         else:
             e = float(cell.run(inner)[0])
         steps += inner

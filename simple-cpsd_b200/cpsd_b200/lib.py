@@ -53,6 +53,7 @@ EXPORTS = [
     "cpsd_write_ionout", "cpsd_gpu_kbpp", "cpsd_makepsi",
     "cpsd_gpu_get_tuning", "cpsd_gpu_set_tuning", "cpsd_gpu_tuning_limits", "cpsd_gpu_autotune",
     "cpsd_gpu_set_band_range", "cpsd_gpu_step_phase", "cpsd_gpu_bp_buffers", "cpsd_gpu_bp_finish",
+    "cpsd_gpu_run_guarded",
 ]
 
 
@@ -147,6 +148,7 @@ def load(path: str = LIB) -> ctypes.CDLL:
     lib.cpsd_gpu_get_tuning.argtypes = [_P, ctypes.POINTER(Tuning)]
     lib.cpsd_gpu_set_tuning.argtypes = [_P, ctypes.POINTER(Tuning)]
     lib.cpsd_gpu_tuning_limits.argtypes = [_P, ctypes.POINTER(Tuning)]
+    lib.cpsd_gpu_run_guarded.argtypes = [_P, _I, _I, _P, _P, _P, _P, _P]
     lib.cpsd_gpu_set_band_range.argtypes = [_P, _I, _I]
     lib.cpsd_gpu_step_phase.argtypes = [_P, _I]
     lib.cpsd_gpu_bp_buffers.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),

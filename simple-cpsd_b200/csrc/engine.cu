@@ -50,6 +50,10 @@ cudaError_t &last_cuda_error()
 inline long cdiv(long a, long b) { return (a + b - 1) / b; }
 
 constexpr int kTuneMaxCtas = 8;  // largest split-K target (CTAs per SM) a tuning may set
+// trust region of the guarded learned step (cpsd_gpu_run_guarded): the bound
+// on log K shrinks after a rejected block and grows after an accepted one
+// (steady state near one rejected block in eight)
+constexpr double kCapShrink = 0.7, kCapGrow = 0.1;
 
 // Streaming multiprocessors of the current device (148 on a B200), looked up
 // once per device.
@@ -2258,6 +2262,43 @@ int cpsd_gpu_set_preconditioner_range(cpsd_gpu_ctx *c, double min_log_k, double 
     CK(cudaMemcpyAsync(c->pcap, range, sizeof(range), cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
     return CPSD_OK;
+}
+
+int cpsd_gpu_run_guarded(cpsd_gpu_ctx *c, int blocks, int inner, double *cap, double *E, double *deltae,
+                         double *deltac, int *rejected)
+{
+    if (!c || !cap || !E || blocks < 1 || inner < 1) return CPSD_ERR_ARG;
+    if (!c->mlp) return CPSD_ERR_ARG;  // plain SD: cpsd_gpu_run
+    const int min_bands = (c->ispin == 2) ? std::min(c->ne0, c->ne1) : c->ne0;
+    int last = CPSD_OK;
+    for (int blk = 0; blk < blocks; ++blk) {
+        const double prev = E[0];
+        int rc = cpsd_gpu_save_orbitals(c);
+        if (rc) return rc;
+        rc = cpsd_gpu_set_preconditioner_range(c, kLogKMin, *cap);
+        if (rc) return rc;
+        last = cpsd_gpu_run(c, inner, 0, E, deltae, deltac, nullptr);
+        if (last != CPSD_OK && last != CPSD_WARN_LAGRANGE) return last;
+        // with one band per spin the reference's convergence test can never
+        // pass (cpsd.c:471), so its warning says nothing there
+        const bool lag_failed = last == CPSD_WARN_LAGRANGE && min_bands > 1;
+        if (!std::isfinite(E[0]) || E[0] > prev || lag_failed) {
+            // rejected: the block again from its start with plain SD steps
+            // (K = 1 exactly: the reference's update, cpsd.c:399-400)
+            if (rejected) ++*rejected;
+            *cap = std::max<double>(kLogKMin, *cap - kCapShrink);
+            rc = cpsd_gpu_restore_orbitals(c);
+            if (rc) return rc;
+            rc = cpsd_gpu_set_preconditioner_range(c, 0.0, 0.0);
+            if (rc) return rc;
+            E[0] = prev;
+            last = cpsd_gpu_run(c, inner, 0, E, deltae, deltac, nullptr);
+            if (last != CPSD_OK && last != CPSD_WARN_LAGRANGE) return last;
+        } else {
+            *cap = std::min<double>(kLogKMax, *cap + kCapGrow);
+        }
+    }
+    return last;
 }
 
 int cpsd_gpu_save_orbitals(cpsd_gpu_ctx *c)

@@ -122,6 +122,21 @@ tc_gemm_tn_kernel(int M, int N, int K, long lda, long ldb, const double *__restr
     // staging map: a warp covers 8 rows x 4 consecutive k (one 32-byte
     // sector per row in HBM, 32 consecutive words in shared memory)
     const int kq = tid & 3, rlo = (tid >> 2) & 7, chunk = tid >> 5;  // chunk 0..7 of the 32-wide slab
+    // the 32 global loads of a stage (and its weight), issued one stage
+    // ahead into the other register set so their latency overlaps the split
+    // and the MMAs of the stage before
+    double ra[16], rb[16], na[16], nb[16], wk = 1.0, nwk = 1.0;
+    auto load = [&](int st, double (&xa)[16], double (&xb)[16], double &xw) {
+        const int k = k0 + st * kTcBK + chunk * 4 + kq;
+        xw = (w && k < k1) ? w[k >> 1] : 1.0;
+#pragma unroll
+        for (int rhi = 0; rhi < 16; ++rhi) {
+            const int r = rhi * 8 + rlo;
+            xa[rhi] = (k < k1 && i0 + r < M) ? A[(long)(i0 + r) * lda + k] : 0.0;
+            xb[rhi] = (k < k1 && j0 + r < N) ? B[(long)(j0 + r) * ldb + k] : 0.0;
+        }
+    };
+    if (nst > 0) load(0, ra, rb, wk);
     bool fail = false;
     int issued = 0;  // stages whose MMAs were committed
     for (int it = 0; it < nst; ++it) {
@@ -134,16 +149,7 @@ tc_gemm_tn_kernel(int M, int N, int K, long lda, long ldb, const double *__restr
             fail = true;
             break;
         }
-        const int k = k0 + it * kTcBK + chunk * 4 + kq;
-        const double wk = (w && k < k1) ? w[k >> 1] : 1.0;
-        // all 32 loads of this thread first (memory-level parallelism), then split
-        double ra[16], rb[16];
-#pragma unroll
-        for (int rhi = 0; rhi < 16; ++rhi) {
-            const int r = rhi * 8 + rlo;
-            ra[rhi] = (k < k1 && i0 + r < M) ? A[(long)(i0 + r) * lda + k] : 0.0;
-            rb[rhi] = (k < k1 && j0 + r < N) ? B[(long)(j0 + r) * ldb + k] : 0.0;
-        }
+        if (it + 1 < nst) load(it + 1, na, nb, nwk);
 #pragma unroll
         for (int rhi = 0; rhi < 16; ++rhi) {
             const float a = (float)(ra[rhi] * wk), bv = (float)rb[rhi];
@@ -169,6 +175,14 @@ tc_gemm_tn_kernel(int M, int N, int K, long lda, long ldb, const double *__restr
             tc_commit(smem_u32(&mbar[b]));
         }
         issued = it + 1;
+        if (it + 1 < nst) {
+            wk = nwk;
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                ra[q] = na[q];
+                rb[q] = nb[q];
+            }
+        }
     }
     // the last commit tracks every MMA this block issued
     bool done = true;
@@ -463,6 +477,24 @@ tc_gemm_nn_kernel(int NJ, int K, int L, double alpha, const double *__restrict__
     const int kq = tid & 3, rlo = (tid >> 2) & 7, chunk = tid >> 5;
     // B slab map: thread -> column kk of the tile and 16 consecutive l
     const int kk = tid & 127, lq = tid >> 7;
+    // the global loads of a stage, issued one stage ahead into the other
+    // register set so their latency overlaps the split and the MMAs
+    double ra[16], rb[16], na[16], nb[16];
+    auto load = [&](int st, double (&xa)[16], double (&xb)[16]) {
+        const int l0 = st * kTcBK;
+        const int l = l0 + chunk * 4 + kq;
+#pragma unroll
+        for (int rhi = 0; rhi < 16; ++rhi) {
+            const int r = rhi * 8 + rlo;
+            xa[rhi] = (l < L && j0 + r < NJ) ? Mat[(long)(j0 + r) * ldm + l] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int lb = l0 + lq * 16 + q;
+            xb[q] = (lb < L && k0 + kk < K) ? B[(long)lb * ldb + k0 + kk] : 0.0;
+        }
+    };
+    if (nst > 0) load(0, ra, rb);
     bool fail = false;
     int issued = 0;
     for (int it = 0; it < nst; ++it) {
@@ -474,21 +506,7 @@ tc_gemm_nn_kernel(int NJ, int K, int L, double alpha, const double *__restrict__
             fail = true;
             break;
         }
-        const int l0 = it * kTcBK;
-        double ra[16], rb[16];
-        {
-            const int l = l0 + chunk * 4 + kq;
-#pragma unroll
-            for (int rhi = 0; rhi < 16; ++rhi) {
-                const int r = rhi * 8 + rlo;
-                ra[rhi] = (l < L && j0 + r < NJ) ? Mat[(long)(j0 + r) * ldm + l] : 0.0;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int l = l0 + lq * 16 + q;
-            rb[q] = (l < L && k0 + kk < K) ? B[(long)l * ldb + k0 + kk] : 0.0;
-        }
+        if (it + 1 < nst) load(it + 1, na, nb);
 #pragma unroll
         for (int rhi = 0; rhi < 16; ++rhi) {
             const float a = (float)ra[rhi];
@@ -521,6 +539,13 @@ tc_gemm_nn_kernel(int NJ, int K, int L, double alpha, const double *__restrict__
             tc_commit(smem_u32(&mbar[b]));
         }
         issued = it + 1;
+        if (it + 1 < nst) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                ra[q] = na[q];
+                rb[q] = nb[q];
+            }
+        }
     }
     bool done = true;
     if (issued > 0) {

@@ -149,3 +149,34 @@ def test_save_and_restore_orbitals_repeat_a_block():
     assert e1[0] == e2[0]
     cell.close()
     m.close()
+
+
+def test_guarded_block_in_the_library_rejects_and_redoes_with_plain_sd():
+    """cpsd_gpu_run_guarded: with the previous energy set to -inf every
+    learned block counts as a rise, so each is redone from its start with
+    plain SD steps -- the energies and orbitals are plain SD's, bit for bit,
+    and the trust region shrinks by 0.7 per rejected block."""
+    inp = inputs.build_inputs(configs.small_diamond(24, 4, ecut=16.0, seed=7))
+    plain = api.GpuCell(inp)
+    plain.set_state(inp.c2, inp.r2)
+    e_plain = [plain.run(5).copy() for _ in range(2)]
+    c_plain = plain.get_c2()
+    m = api.Mlp(seed=2)
+    cell = api.GpuCell(inp)
+    cell.set_state(inp.c2, inp.r2)
+    cell.set_preconditioner(m)
+    cap = learned.LOGK_MAX
+    for k in range(2):
+        cell.E[0] = -math.inf
+        e, rej, cap = cell.run_guarded(5, cap)
+        assert rej == 1
+        assert np.array_equal(cell.E[1:], e_plain[k][1:]) and e == e_plain[k][0]
+    assert cap == pytest.approx(learned.LOGK_MAX - 2 * learned.CAP_SHRINK)
+    assert np.array_equal(cell.get_c2(), c_plain)
+    # with the previous energy +inf a block is kept as the network made it
+    cell.E[0] = math.inf
+    e, rej, cap2 = cell.run_guarded(5, cap)
+    assert rej == 0 and math.isfinite(e) and cap2 == pytest.approx(cap + learned.CAP_GROW)
+    plain.close()
+    cell.close()
+    m.close()
