@@ -84,6 +84,7 @@ cudaError_t allow_max_smem(K kernel, int optin)
 struct HostGeom {
     int n = 0, nh = 0, KX = 0, ncol = 0, npw = 0, npw_pad = 0;
     std::vector<int> col_i, col_j, col_ptr, pt_k, pt_i, pt_j, pt_idx, colidx, inv_idx;
+    std::vector<int> yrun;  // 3 per line kx < KX (see Geom::yrun), empty if some line is not two runs
     std::vector<double> w;
 };
 
@@ -125,6 +126,30 @@ HostGeom build_geom(int n, const int *masker1, bool full)
     h.w.resize(h.npw_pad, 0.0);
     h.colidx.assign((size_t)std::max(h.KX, 1) * n, -1);
     for (int c = 0; c < h.ncol; ++c) h.colidx[(size_t)h.col_i[c] * n + h.col_j[c]] = c;
+    // The columns of one line kx are usually y in [0, a) and [b, n) (the
+    // sphere's |ky| range): then a line's column of y is arithmetic.
+    h.yrun.assign((size_t)3 * std::max(h.KX, 1), 0);
+    for (int i = 0; i < h.KX; ++i) {
+        const int *row = h.colidx.data() + (size_t)i * n;
+        int a = 0;
+        while (a < n && row[a] >= 0) ++a;
+        int b = n;
+        while (b > a && row[b - 1] >= 0) --b;
+        bool ok = true;
+        for (int j = a; j < b && ok; ++j) ok = row[j] < 0;
+        const int first = (a > 0) ? row[0] : (b < n ? row[b] : 0);
+        for (int j = 0; j < n && ok; ++j) {
+            const int want = j < a ? first + j : (j >= b ? first + a + (j - b) : -1);
+            ok = row[j] == want;
+        }
+        if (!ok) {
+            h.yrun.clear();
+            break;
+        }
+        h.yrun[3 * i] = first;
+        h.yrun[3 * i + 1] = a;
+        h.yrun[3 * i + 2] = b;
+    }
     return h;
 }
 
@@ -473,7 +498,7 @@ struct cpsd_gpu_ctx {
 
     // device
     int *pt_i = nullptr, *pt_j = nullptr, *pt_k = nullptr, *pt_idx = nullptr, *inv_idx = nullptr;
-    int *col_i = nullptr, *col_j = nullptr, *col_ptr = nullptr, *colidx = nullptr;
+    int *col_i = nullptr, *col_j = nullptr, *col_ptr = nullptr, *colidx = nullptr, *yrun = nullptr;
     double *w = nullptr, *tg = nullptr, *vc = nullptr, *vg = nullptr, *vl = nullptr, *vnl = nullptr;
     double *zv = nullptr, *rcell = nullptr, *unitg = nullptr, *vnlnrm_p = nullptr;
     int *katm = nullptr, *lmmax = nullptr, *proj_off = nullptr;
@@ -1680,6 +1705,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(upload(ar, &c->col_j, h.col_j));
     CK(upload(ar, &c->col_ptr, h.col_ptr));
     CK(upload(ar, &c->colidx, h.colidx));
+    if (!h.yrun.empty()) CK(upload(ar, &c->yrun, h.yrun));
     CK(upload(ar, &c->w, h.w));
     c->g.n = c->n;
     c->g.nh = c->nh;
@@ -1692,6 +1718,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     c->g.col_ptr = c->col_ptr;
     c->g.pt_k = c->pt_k;
     c->g.colidx = c->colidx;
+    c->g.yrun = c->yrun;
 
     const long P = c->npw_pad;
     const int nb = c->nb, nkatm = c->nkatm, nion = c->nion;

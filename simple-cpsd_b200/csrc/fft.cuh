@@ -28,6 +28,10 @@ struct Geom {
     const int *col_i, *col_j, *col_ptr;  // ncol, ncol, ncol+1
     const int *pt_k;                     // npw
     const int *colidx;                   // KX*n: column of (kx, y) or -1
+    // 3 per line kx: first column, a, b -- the line's columns are y in
+    // [0, a) then [b, n), column first + y or first + a + (y - b); null:
+    // use colidx
+    const int *yrun;
 };
 
 template <typename T>
@@ -282,10 +286,25 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
                 const int i = base + gy;
                 const bool act = i < KX;
                 cx<T> v[QY];
+                // the line's columns: arithmetic from its two runs (one small
+                // load per line), else the colidx table (one load per value).
+                // The density pass keeps the table: measured faster there (its
+                // band loop reuses the same columns for every band)
+                if (MODE != PM_DENSITY && g.yrun) {
+                    const int c0 = act ? g.yrun[3 * i] : 0, ra = act ? g.yrun[3 * i + 1] : 0;
+                    const int rb = act ? g.yrun[3 * i + 2] : NF;
 #pragma unroll
-                for (int m = 0; m < QY; ++m) {
-                    int c = act ? g.colidx[i * NF + LY::in_index(ty, m)] : -1;
-                    v[m] = (c >= 0) ? Tplane[c] : cx<T>{0, 0};
+                    for (int m = 0; m < QY; ++m) {
+                        const int y = LY::in_index(ty, m);
+                        const int c = y < ra ? c0 + y : (y >= rb ? c0 + ra + (y - rb) : -1);
+                        v[m] = (c >= 0) ? Tplane[c] : cx<T>{0, 0};
+                    }
+                } else {
+#pragma unroll
+                    for (int m = 0; m < QY; ++m) {
+                        const int c = act ? g.colidx[i * NF + LY::in_index(ty, m)] : -1;
+                        v[m] = (c >= 0) ? Tplane[c] : cx<T>{0, 0};
+                    }
                 }
                 line_fft<NF, +1, T>(v, ty, xby, tw.n_inv);
                 if (act) {
