@@ -1905,6 +1905,11 @@ int cpsd_gpu_set_scalars(cpsd_gpu_ctx *c, const double *unitg, double omega, dou
                          double cewald, double rcut)
 {
     if (!c || !unitg || omega <= 0 || fmass <= 0) return CPSD_ERR_ARG;
+    // the drop-in passes the same scalars on every call: keep the captured
+    // step graphs unless a value changes
+    const bool same = !memcmp(c->prm.unitg, unitg, sizeof(c->prm.unitg)) && c->prm.omega == omega &&
+                      c->prm.dt == dt && c->prm.fmass == fmass && c->prm.cewald == cewald && c->prm.rcut == rcut;
+    if (same) return CPSD_OK;
     memcpy(c->prm.unitg, unitg, sizeof(c->prm.unitg));
     c->prm.omega = omega;
     c->prm.dt = dt;
