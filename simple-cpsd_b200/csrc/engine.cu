@@ -924,7 +924,7 @@ int step_phase(cpsd_gpu_ctx *c, int phase)
             band_stats_kernel<<<c->nb, 256, 0, s>>>(c->npw, c->ldc, c->w, c->tg, c1, c->cpsi, c->pstats);
             prec_features_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 256), 256, 0, s>>>(c->nb, c->tmax, c->pstats,
                                                                                           c->dstep, c->pX);
-            mlp_forward_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 128), 128, 0, s>>>(
+            mlp_forward_kernel<<<mlp_forward_blocks((long)c->nb * kShells), kMlpTileThreads, 0, s>>>(
                 c->nb * kShells, c->pX, c->mlp->wq, c->mlp->p, c->py, nullptr);
             prec_update_kernel<<<(unsigned)cdiv((long)c->nb * c->npw, 256), 256, 0, s>>>(
                 c->nb, c->npw, c->ldc, c->shell, c->py, c->pcap, c->dte, c->pR, c2, c->dstep);
@@ -2464,7 +2464,7 @@ int mlp_reserve(cpsd_mlp *m, int n)
 int mlp_grad_batch(cpsd_mlp *m, const float *X, const float *T, int n)
 {
     const unsigned b128 = (unsigned)cdiv(n, 128);
-    mlp_forward_kernel<<<b128, 128, 0, m->st>>>(n, X, m->wq, m->p, m->y, m->H);
+    mlp_forward_kernel<<<mlp_forward_blocks(n), kMlpTileThreads, 0, m->st>>>(n, X, m->wq, m->p, m->y, m->H);
     mlp_backward_delta_kernel<<<b128, 128, 0, m->st>>>(n, m->y, T, m->wq, m->H, m->D, m->dy, m->lp);
     mlp_wgrad_kernel<<<3 * kMlpHid + 1, kMlpGradThreads, 0, m->st>>>(n, X, m->H, m->D, m->dy, m->g);
     CK(cudaGetLastError());
@@ -2479,7 +2479,7 @@ int cpsd_mlp_forward(cpsd_mlp *m, const float *X, int n, float *y)
     int rc = mlp_reserve(m, n);
     if (rc) return rc;
     CK(cudaMemcpyAsync(m->X, X, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice, m->st));
-    mlp_forward_kernel<<<(unsigned)cdiv(n, 128), 128, 0, m->st>>>(n, m->X, m->wq, m->p, m->y, nullptr);
+    mlp_forward_kernel<<<mlp_forward_blocks(n), kMlpTileThreads, 0, m->st>>>(n, m->X, m->wq, m->p, m->y, nullptr);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(y, m->y, sizeof(float) * n, cudaMemcpyDeviceToHost, m->st));
     CK(cudaStreamSynchronize(m->st));

@@ -32,61 +32,107 @@ struct MlpDev {
     const float *p;           // FP32 master parameters (biases read from here)
 };
 
-// one sample: x[4] -> y; optionally store activations h1,h2,h3 (each 64)
-template <bool STORE>
-CPSD_D float mlp_sample(const float *__restrict__ x, const __nv_bfloat16 *__restrict__ wq,
-                        const float *__restrict__ p, float *h1o, float *h2o, float *h3o)
+// Forward over a batch: y[s], and the activations when H is given
+// ([3][n][64]).  One CTA takes kMlpTile samples: the weights are staged once
+// per CTA in shared memory, transposed (Wt[i][o]) and widened to FP32, and
+// thread t computes output unit o = t % 64 of a hidden layer for
+// kMlpTile / 4 samples, so the 64-long dot products of all units run side by
+// side instead of one sample's 8k FMAs in a row.  Every unit's sum is
+// bias first, then one fmaf per input in ascending order (the order a
+// one-sample evaluation takes, so y does not depend on the tiling).
+constexpr int kMlpTile = 16;
+constexpr int kMlpTileThreads = 256;
+constexpr int kMlpTileSpt = kMlpTile / (kMlpTileThreads / kMlpHid);  // samples a thread: 4
+
+__global__ void __launch_bounds__(kMlpTileThreads) mlp_forward_kernel(int n, const float *__restrict__ X,
+                                                                      const __nv_bfloat16 *__restrict__ wq,
+                                                                      const float *__restrict__ p,
+                                                                      float *__restrict__ y, float *__restrict__ H)
 {
-    float a[kMlpHid], b[kMlpHid];
-#pragma unroll 4
-    for (int o = 0; o < kMlpHid; ++o) {
-        float s = p[kB1 + o];
+    __shared__ float w1t[kMlpIn][kMlpHid];
+    // a padded row (65) keeps the transposing writes and the unit-wise reads
+    // on distinct banks
+    __shared__ float w2t[kMlpHid][kMlpHid + 1], w3t[kMlpHid][kMlpHid + 1];
+    __shared__ float w4[kMlpHid], bias[3][kMlpHid];
+    __shared__ __align__(16) float act[3][kMlpTile][kMlpHid];  // h1, h2, h3
+    __shared__ float x0[kMlpTile][kMlpIn];
+    const int t = threadIdx.x;
+    const long s0 = (long)blockIdx.x * kMlpTile;
+    // stage: row-major W[o][i] read coalesced, written transposed
+    for (int k = t; k < kMlpHid * kMlpHid; k += kMlpTileThreads) {
+        const int o = k / kMlpHid, i = k % kMlpHid;
+        w2t[i][o] = __bfloat162float(wq[kW2 + k]);
+        w3t[i][o] = __bfloat162float(wq[kW3 + k]);
+    }
+    for (int k = t; k < kMlpHid * kMlpIn; k += kMlpTileThreads) w1t[k % kMlpIn][k / kMlpIn] = __bfloat162float(wq[kW1 + k]);
+    if (t < kMlpHid) {
+        w4[t] = __bfloat162float(wq[kW4 + t]);
+        bias[0][t] = p[kB1 + t];
+        bias[1][t] = p[kB2 + t];
+        bias[2][t] = p[kB3 + t];
+    }
+    if (t < kMlpTile * kMlpIn) {
+        const long e = s0 * kMlpIn + t;
+        x0[t / kMlpIn][t % kMlpIn] = (e < (long)n * kMlpIn) ? X[e] : 0.0f;
+    }
+    __syncthreads();
+    const int o = t % kMlpHid, sg = t / kMlpHid;
+    const long nr = (long)n;
+    // layer 1 (4 inputs)
 #pragma unroll
-        for (int i = 0; i < kMlpIn; ++i) s = fmaf(__bfloat162float(wq[kW1 + o * kMlpIn + i]), x[i], s);
-        a[o] = tanhf(s);
+    for (int k = 0; k < kMlpTileSpt; ++k) {
+        const int sl = sg * kMlpTileSpt + k;
+        float acc = bias[0][o];
+#pragma unroll
+        for (int i = 0; i < kMlpIn; ++i) acc = fmaf(w1t[i][o], x0[sl][i], acc);
+        act[0][sl][o] = tanhf(acc);
     }
-    if (STORE)
-        for (int o = 0; o < kMlpHid; ++o) h1o[o] = a[o];
-#pragma unroll 2
-    for (int o = 0; o < kMlpHid; ++o) {
-        float s = p[kB2 + o];
-#pragma unroll 8
-        for (int i = 0; i < kMlpHid; ++i) s = fmaf(__bfloat162float(wq[kW2 + o * kMlpHid + i]), a[i], s);
-        b[o] = tanhf(s);
+    __syncthreads();
+    // layers 2 and 3 (64 inputs): act[0] -> act[1] -> act[2]
+#pragma unroll
+    for (int layer = 0; layer < 2; ++layer) {
+        const float(*wt)[kMlpHid + 1] = layer ? w3t : w2t;
+        const float(*in)[kMlpHid] = act[layer];
+        float acc[kMlpTileSpt];
+#pragma unroll
+        for (int k = 0; k < kMlpTileSpt; ++k) acc[k] = bias[1 + layer][o];
+#pragma unroll 4
+        for (int i = 0; i < kMlpHid; i += 4) {
+            float w[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) w[j] = wt[i + j][o];
+#pragma unroll
+            for (int k = 0; k < kMlpTileSpt; ++k) {
+                const float4 h = *reinterpret_cast<const float4 *>(&in[sg * kMlpTileSpt + k][i]);
+                acc[k] = fmaf(w[0], h.x, acc[k]);
+                acc[k] = fmaf(w[1], h.y, acc[k]);
+                acc[k] = fmaf(w[2], h.z, acc[k]);
+                acc[k] = fmaf(w[3], h.w, acc[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kMlpTileSpt; ++k) act[1 + layer][sg * kMlpTileSpt + k][o] = tanhf(acc[k]);
+        __syncthreads();
     }
-    if (STORE)
-        for (int o = 0; o < kMlpHid; ++o) h2o[o] = b[o];
-#pragma unroll 2
-    for (int o = 0; o < kMlpHid; ++o) {
-        float s = p[kB3 + o];
-#pragma unroll 8
-        for (int i = 0; i < kMlpHid; ++i) s = fmaf(__bfloat162float(wq[kW3 + o * kMlpHid + i]), b[i], s);
-        a[o] = tanhf(s);
+    if (H) {  // training keeps the activations, one coalesced row per sample and layer
+#pragma unroll
+        for (int k = 0; k < kMlpTileSpt; ++k) {
+            const int sl = sg * kMlpTileSpt + k;
+            const long s = s0 + sl;
+            if (s >= nr) continue;
+#pragma unroll
+            for (int l = 0; l < 3; ++l) H[((long)l * nr + s) * kMlpHid + o] = act[l][sl][o];
+        }
     }
-    if (STORE)
-        for (int o = 0; o < kMlpHid; ++o) h3o[o] = a[o];
-    float y = p[kB4];
-#pragma unroll 8
-    for (int i = 0; i < kMlpHid; ++i) y = fmaf(__bfloat162float(wq[kW4 + i]), a[i], y);
-    return y;
+    // output unit: one thread per sample, 64 inputs in order
+    if (t < kMlpTile && s0 + t < nr) {
+        float acc = p[kB4];
+        for (int i = 0; i < kMlpHid; ++i) acc = fmaf(w4[i], act[2][t][i], acc);
+        y[s0 + t] = acc;
+    }
 }
 
-// forward over a batch: y[s], and the activations when H is given ([3][n][64])
-__global__ void mlp_forward_kernel(int n, const float *__restrict__ X, const __nv_bfloat16 *__restrict__ wq,
-                                   const float *__restrict__ p, float *__restrict__ y, float *__restrict__ H)
-{
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    float x[kMlpIn];
-#pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) x[i] = X[(long)s * kMlpIn + i];
-    if (H) {
-        y[s] = mlp_sample<true>(x, wq, p, H + (long)s * kMlpHid, H + ((long)n + s) * kMlpHid,
-                                H + (2L * n + s) * kMlpHid);
-    } else {
-        y[s] = mlp_sample<false>(x, wq, p, nullptr, nullptr, nullptr);
-    }
-}
+inline unsigned mlp_forward_blocks(long n) { return (unsigned)((n + kMlpTile - 1) / kMlpTile); }
 
 // MSE loss on y - t: dy = 2 (y - t) / n; deltas dZ3, dZ2, dZ1 ([3][n][64]);
 // loss partials per block
