@@ -234,8 +234,11 @@ struct Line {
 };
 
 // Two-level transform of one line by P lanes (see file header).
-// tw: table of W_N^m (m < N) for this SIGN.  xb: the group's exchange buffer
-// (Line<N>::XB entries).  All lanes of the warp must call it together.
+// tw: the twiddles in the order the lanes read them, tw[q*P + t] = W_N^{t q}
+// (q < Q, t < P) for this SIGN, so the P lanes of a group read P consecutive
+// entries for every q (no shared-memory bank conflicts).  xb: the group's
+// exchange buffer (Line<N>::XB entries).  All lanes of the warp must call it
+// together.
 template <int N, int SIGN, typename T>
 CPSD_D void line_fft(cx<T> *v, int t, cx<T> *xb, const cx<T> *__restrict__ tw)
 {
@@ -243,7 +246,7 @@ CPSD_D void line_fft(cx<T> *v, int t, cx<T> *xb, const cx<T> *__restrict__ tw)
     constexpr int P = L::P, Q = L::Q, U = L::U;
     DFT<Q, SIGN, T>::run(v);
 #pragma unroll
-    for (int q = 1; q < Q; ++q) v[q] = cmul(v[q], tw[t * q]);
+    for (int q = 1; q < Q; ++q) v[q] = cmul(v[q], tw[q * P + t]);
 #pragma unroll
     for (int q = 0; q < Q; ++q) xb[L::xb_index(q, t)] = v[q];
     __syncwarp();
@@ -264,6 +267,7 @@ CPSD_D void line_fft(cx<T> *v, int t, cx<T> *xb, const cx<T> *__restrict__ tw)
 // x[(t*U + u) + Q*s] in v[u*P + s] -- the output distribution of line_fft --
 // and ends with X[t + P*m] in v[m], its input distribution.  P-point DFTs,
 // twiddle W_N^{q t'}, one exchange, then the Q-point DFT in registers.
+// tw: tw[t'*Q + q] = W_N^{q t'} (t' < P, q < Q) for this SIGN.
 template <int N, int SIGN, typename T>
 CPSD_D void line_fft_dif(cx<T> *v, int t, cx<T> *xb, const cx<T> *__restrict__ tw)
 {
@@ -277,7 +281,7 @@ CPSD_D void line_fft_dif(cx<T> *v, int t, cx<T> *xb, const cx<T> *__restrict__ t
         DFT<P, SIGN, T>::run(w);
         const int q = t * U + u;
 #pragma unroll
-        for (int tp = 0; tp < P; ++tp) xb[L::xb_index(q, tp)] = (tp == 0) ? w[0] : cmul(w[tp], tw[q * tp]);
+        for (int tp = 0; tp < P; ++tp) xb[L::xb_index(q, tp)] = (tp == 0) ? w[0] : cmul(w[tp], tw[tp * Q + q]);
     }
     __syncwarp();
 #pragma unroll

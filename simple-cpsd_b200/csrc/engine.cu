@@ -170,7 +170,14 @@ struct DevArena {
         if (e != cudaSuccess) return e;
         ptrs.push_back(q);
         *p = static_cast<X *>(q);
-        return cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(X));
+        // Zero-filled before the caller sees it: the fill runs on the legacy
+        // stream, which the contexts' non-blocking streams do not wait for,
+        // so an asynchronous copy into the buffer on a context stream could
+        // otherwise be overwritten by the fill (a chunk table written right
+        // after its allocation read back as zeros).
+        e = cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(X), 0);
+        if (e != cudaSuccess) return e;
+        return cudaStreamSynchronize(0);
     }
 };
 
@@ -187,7 +194,7 @@ cudaError_t upload(DevArena &ar, X **d, const std::vector<X> &h)
 struct FftOps {
     virtual ~FftOps() = default;
     virtual size_t elem() const = 0;
-    virtual int init(DevArena &ar, int KX) = 0;
+    virtual int init(DevArena &ar, int KX, int ncol) = 0;
     virtual void inv_z(const Geom &g, const cx<double> *psi, long ldp, void *Tb, int nb, cudaStream_t s) = 0;
     virtual void fwd_z_store(const Geom &g, const void *Tb, cx<double> *out, long ldo, double scale,
                              int nb, cudaStream_t s) = 0;
@@ -207,56 +214,68 @@ struct FftOpsT final : FftOps {
     int KX = 0;
     size_t zsmem = 0;
     size_t psmem[4] = {0, 0, 0, 0};
+    size_t psmem_split = 0;  // the row-split density build (no staged columns)
     bool hi_fits[4] = {false, false, false, false};  // the high-occupancy build's CTAs fit an SM
     int occ[4] = {0, 0, 0, 0};                       // plane build that runs, per mode
 
     size_t elem() const override { return sizeof(cx<T>); }
 
-    static void fill(std::vector<cx<T>> &v, int N, int sign, int count)
+    static cx<T> turn(int m, int N, int sign)  // e^{sign 2 pi i m / N}
     {
-        for (int m = 0; m < count; ++m) {
-            long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)N;
-            v.push_back(cx<T>{(T)cosl(a), (T)(sign * sinl(a))});
-        }
+        long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)N;
+        return cx<T>{(T)cosl(a), (T)(sign * sinl(a))};
+    }
+    // count values e^{sign 2 pi i m / N}, m < count, at v[at..]
+    static void fill(std::vector<cx<T>> &v, int at, int N, int sign, int count)
+    {
+        for (int m = 0; m < count; ++m) v[at + m] = turn(m, N, sign);
+    }
+    // line_fft's table of Line<N>: v[at + q*P + t] = W_N^{t q}
+    template <int N>
+    static void fill_line(std::vector<cx<T>> &v, int at, int sign)
+    {
+        using L = Line<N>;
+        for (int q = 0; q < L::Q; ++q)
+            for (int t = 0; t < L::P; ++t) v[at + q * L::P + t] = turn(t * q, N, sign);
+    }
+    // line_fft_dif's table of Line<N>: v[at + t*Q + q] = W_N^{q t}
+    template <int N>
+    static void fill_dif(std::vector<cx<T>> &v, int at, int sign)
+    {
+        using L = Line<N>;
+        for (int t = 0; t < L::P; ++t)
+            for (int q = 0; q < L::Q; ++q) v[at + t * L::Q + q] = turn(q * t, N, sign);
     }
 
-    int init(DevArena &ar, int kx) override
+    int init(DevArena &ar, int kx, int ncol) override
     {
         KX = kx;
         constexpr int H = NF / 2;
-        std::vector<cx<T>> tab;
-        size_t o_ninv = tab.size();
-        fill(tab, NF, +1, NF);
-        size_t o_nfwd = tab.size();
-        fill(tab, NF, -1, NF);
-        size_t o_hinv = tab.size();
-        fill(tab, H, +1, H);
-        size_t o_hfwd = tab.size();
-        fill(tab, H, -1, H);
-        size_t o_rinv = tab.size();
-        fill(tab, NF, +1, H + 1);
-        size_t o_rfwd = tab.size();
-        fill(tab, NF, -1, H + 1);
+        using TL = TwLayout<NF>;
+        std::vector<cx<T>> tab(TL::total);
+        fill_line<NF>(tab, TL::n_inv, +1);
+        fill_line<NF>(tab, TL::n_fwd, -1);
+        fill_line<H>(tab, TL::h_inv, +1);
+        fill_line<H>(tab, TL::h_fwd, -1);
+        fill_dif<H>(tab, TL::h_fwd_dif, -1);
+        fill(tab, TL::r_inv, NF, +1, H + 1);
+        fill(tab, TL::r_fwd, NF, -1, H + 1);
         cx<T> *d = nullptr;
         CK(upload(ar, &d, tab));
-        tw.n_inv = d + o_ninv;
-        tw.n_fwd = d + o_nfwd;
-        tw.h_inv = d + o_hinv;
-        tw.h_fwd = d + o_hfwd;
-        tw.r_inv = d + o_rinv;
-        tw.r_fwd = d + o_rfwd;
+        tw = Twiddles<T>::template at<NF>(d);
 
         using L = Line<NF>;
         constexpr int P = L::P, CPB = kThreads / P;
         constexpr int TILE = (CPB * (NF + 1) > NF * (CPB + 1)) ? CPB * (NF + 1) : NF * (CPB + 1);
-        zsmem = sizeof(cx<T>) * ((size_t)TILE + (size_t)CPB * group_stride<T, NF>());
+        zsmem = sizeof(cx<T>) * ((size_t)TILE + (size_t)CPB * group_stride<T, NF>() + (size_t)NF);
         int dev = 0, optin = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         CK(cudaFuncSetAttribute(inv_z_kernel<T, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem));
         CK(cudaFuncSetAttribute(fwd_z_kernel<T, NF, ZEPI_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem));
         CK(cudaFuncSetAttribute(fwd_z_kernel<T, NF, ZEPI_SD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem));
-        for (int m = 0; m < 4; ++m) psmem[m] = plane_smem_bytes<T, NF>(m, KX);
+        for (int m = 0; m < 4; ++m) psmem[m] = plane_smem_bytes<T, NF>(m, KX, ncol);
+        psmem_split = plane_smem_bytes<T, NF>(PM_DENSITY, KX, 0);
         for (int m = 0; m < 4; ++m)
             if ((int)psmem[m] > optin) psmem[m] = 0;  // mode unavailable for this sphere
         // The limit is a per-kernel (process-wide) attribute shared by every
@@ -276,7 +295,8 @@ struct FftOpsT final : FftOps {
         const bool has_two[4] = {plane_has_two_cta_build<NF, PM_DENSITY>(), plane_has_two_cta_build<NF, PM_APPLYV>(),
                                  plane_has_two_cta_build<NF, PM_INVREAL>(), plane_has_two_cta_build<NF, PM_FWDREAL>()};
         for (int m = 0; m < 4; ++m) {
-            hi_fits[m] = has_two[m] && 2 * (psmem[m] + (size_t)reserve) <= (size_t)sm_bytes;
+            const size_t hi = (m == PM_DENSITY && plane_row_split<NF, PM_DENSITY, 2>() > 1) ? psmem_split : psmem[m];
+            hi_fits[m] = has_two[m] && psmem[m] != 0 && 2 * (hi + (size_t)reserve) <= (size_t)sm_bytes;
             occ[m] = hi_fits[m] ? 1 : 0;
         }
         // the row-split density build at NF >= 128 redoes each plane's y
@@ -303,7 +323,8 @@ struct FftOpsT final : FftOps {
             if (occ[MODE]) {
                 dim3 g2 = grid;
                 g2.z = plane_row_split<NF, MODE, 2>();  // the density pass's row halves
-                plane_kernel<T, NF, MODE, 2><<<g2, nt, psmem[MODE], s>>>(g, (cx<T> *)Tb, a, tw);
+                const size_t sm = (g2.z > 1) ? psmem_split : psmem[MODE];
+                plane_kernel<T, NF, MODE, 2><<<g2, nt, sm, s>>>(g, (cx<T> *)Tb, a, tw);
                 return;
             }
         plane_kernel<T, NF, MODE, 1><<<grid, nt, psmem[MODE], s>>>(g, (cx<T> *)Tb, a, tw);
@@ -384,21 +405,21 @@ std::unique_ptr<FftOps> make_fft(int n, int precision = CPSD_PREC_FP64)
 }
 
 template <typename T>
-size_t plane_need_t(int n, int mode, int KX)
+size_t plane_need_t(int n, int mode, int KX, int ncol)
 {
     switch (n) {
-    case 16: return plane_smem_bytes<T, 16>(mode, KX);
-    case 24: return plane_smem_bytes<T, 24>(mode, KX);
-    case 32: return plane_smem_bytes<T, 32>(mode, KX);
-    case 48: return plane_smem_bytes<T, 48>(mode, KX);
-    case 64: return plane_smem_bytes<T, 64>(mode, KX);
-    default: return plane_smem_bytes<T, 128>(mode, KX);
+    case 16: return plane_smem_bytes<T, 16>(mode, KX, ncol);
+    case 24: return plane_smem_bytes<T, 24>(mode, KX, ncol);
+    case 32: return plane_smem_bytes<T, 32>(mode, KX, ncol);
+    case 48: return plane_smem_bytes<T, 48>(mode, KX, ncol);
+    case 64: return plane_smem_bytes<T, 64>(mode, KX, ncol);
+    default: return plane_smem_bytes<T, 128>(mode, KX, ncol);
     }
 }
 
-size_t plane_need(int n, int mode, int KX, int precision = CPSD_PREC_FP64)
+size_t plane_need(int n, int mode, int KX, int ncol, int precision = CPSD_PREC_FP64)
 {
-    return precision == CPSD_PREC_MIXED ? plane_need_t<float>(n, mode, KX) : plane_need_t<double>(n, mode, KX);
+    return precision == CPSD_PREC_MIXED ? plane_need_t<float>(n, mode, KX, ncol) : plane_need_t<double>(n, mode, KX, ncol);
 }
 
 }  // namespace
@@ -1200,9 +1221,9 @@ int cpsd_fft_run_full(int n, int dir, const Geom &g, double *grid, cx<double> *p
         if (!c->ops) return CPSD_ERR_GRID;
         int optin = 0;
         CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        c->inv_ok = (int)plane_need(n, PM_INVREAL, kx) <= optin;
-        c->fwd_ok = (int)plane_need(n, PM_FWDREAL, kx) <= optin;
-        int rc = c->ops->init(c->ar, kx);
+        c->inv_ok = (int)plane_need(n, PM_INVREAL, kx, 0) <= optin;
+        c->fwd_ok = (int)plane_need(n, PM_FWDREAL, kx, 0) <= optin;
+        int rc = c->ops->init(c->ar, kx, 0);
         if (rc) return rc;
         e = c.get();
         cache.push_back(std::move(c));
@@ -1680,15 +1701,15 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
     if (p->precision != CPSD_PREC_FP64 && p->precision != CPSD_PREC_MIXED) return CPSD_ERR_ARG;
     for (int m = 0; m < 4; ++m)
-        if ((int)plane_need(c->n, m, h.KX, p->precision) > optin) return CPSD_ERR_GRID;
+        if ((int)plane_need(c->n, m, h.KX, h.ncol, p->precision) > optin) return CPSD_ERR_GRID;
     DevArena &ar = c->ar;
     c->fft64 = make_fft(c->n, CPSD_PREC_FP64);
     if (!c->fft64) return CPSD_ERR_GRID;
-    int rc = c->fft64->init(ar, h.KX);
+    int rc = c->fft64->init(ar, h.KX, h.ncol);
     if (rc) return rc;
     if (p->precision == CPSD_PREC_MIXED) {
         c->fft32 = make_fft(c->n, CPSD_PREC_MIXED);
-        rc = c->fft32->init(ar, h.KX);
+        rc = c->fft32->init(ar, h.KX, h.ncol);
         if (rc) return rc;
         CK(cudaFuncSetAttribute(tc_gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
         CK(cudaFuncSetAttribute(tc_overlaps3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOvSmem));

@@ -34,11 +34,29 @@ struct Geom {
     const int *yrun;
 };
 
+// The twiddle tables of the y/z length NF, one allocation in this order:
+// the line-transform tables of Line<NF> (line_fft order) for the signs +1
+// and -1, those of Line<H> (H = NF/2) for both signs, the Line<H> table of
+// the transposed transform (line_fft_dif order, sign -1), and the
+// real-transform factors e^{+-2 pi i k/NF} (k <= H).
+template <int NF>
+struct TwLayout {
+    static constexpr int H = NF / 2;
+    static constexpr int n_inv = 0, n_fwd = NF, h_inv = 2 * NF, h_fwd = 2 * NF + H, h_fwd_dif = 2 * NF + 2 * H,
+                         r_inv = 2 * NF + 3 * H, r_fwd = 2 * NF + 4 * H + 1, total = 2 * NF + 5 * H + 2;
+};
+
 template <typename T>
 struct Twiddles {
-    // W_N^m for the y/z length n and the half length h, both signs, and the
-    // real-transform factors e^{+-2 pi i k/n}, k <= h
-    const cx<T> *n_inv, *n_fwd, *h_inv, *h_fwd, *r_inv, *r_fwd;
+    const cx<T> *n_inv, *n_fwd, *h_inv, *h_fwd, *h_fwd_dif, *r_inv, *r_fwd;
+    // the tables of one TwLayout<NF> allocation starting at base
+    template <int NF>
+    CPSD_HD static Twiddles at(const cx<T> *base)
+    {
+        using L = TwLayout<NF>;
+        return Twiddles{base + L::n_inv, base + L::n_fwd,     base + L::h_inv, base + L::h_fwd,
+                        base + L::h_fwd_dif, base + L::r_inv, base + L::r_fwd};
+    }
 };
 
 constexpr int kThreads = 256;
@@ -58,6 +76,8 @@ inv_z_kernel(Geom g, const cx<double> *__restrict__ psi, long ldp, cx<T> *__rest
     extern __shared__ unsigned char smem_raw[];
     cx<T> *tile = reinterpret_cast<cx<T> *>(smem_raw);
     cx<T> *xb = tile + TILE;
+    cx<T> *twz = xb + CPB * XS;  // W_NF^m staged once per CTA (read by every line)
+    for (int i = threadIdx.x; i < NF; i += kThreads) twz[i] = tw.n_inv[i];
 
     const int b = blockIdx.y;
     const int c0 = blockIdx.x * CPB;
@@ -73,11 +93,11 @@ inv_z_kernel(Geom g, const cx<double> *__restrict__ psi, long ldp, cx<T> *__rest
             row[g.pt_k[p]] = cx<T>{(T)vv.x, (T)vv.y};
         }
     }
-    __syncwarp();
+    __syncthreads();  // the rows and the staged table
     cx<T> v[Q];
 #pragma unroll
     for (int m = 0; m < Q; ++m) v[m] = row[L::in_index(t, m)];
-    line_fft<NF, +1, T>(v, t, xb + grp * XS, tw.n_inv);
+    line_fft<NF, +1, T>(v, t, xb + grp * XS, twz);
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < U; ++u)
@@ -124,6 +144,8 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
     const int c0 = blockIdx.x * CPB;
     const int grp = threadIdx.x / P, t = threadIdx.x % P;
     const int c = c0 + grp;
+    cx<T> *twz = xb + CPB * XS;  // W_NF^-m staged once per CTA
+    for (int i = threadIdx.x; i < NF; i += kThreads) twz[i] = tw.n_fwd[i];
     const cx<T> *src = Tb + (long)b * NF * g.ncol;
     for (int idx = threadIdx.x; idx < NF * CPB; idx += kThreads) {
         int z = idx / CPB, cl = idx % CPB;
@@ -133,7 +155,7 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
     cx<T> v[Q];
 #pragma unroll
     for (int m = 0; m < Q; ++m) v[m] = tile[L::in_index(t, m) * CS + grp];
-    line_fft<NF, -1, T>(v, t, xb + grp * XS, tw.n_fwd);
+    line_fft<NF, -1, T>(v, t, xb + grp * XS, twz);
     __syncthreads();
     cx<T> *row = tile + grp * RS;
 #pragma unroll
@@ -208,13 +230,38 @@ __host__ __device__ constexpr int plane_threads(int mode)
     return kThreads;
 }
 
+// one complex value global -> shared without a register round trip
+// (cp.async: 16 bytes bypassing L1 for FP64, 8 bytes for FP32)
+template <typename T>
+CPSD_D void cp_async_cx(cx<T> *dst, const cx<T> *src)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(cx<T>) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+CPSD_D void cp_async_commit_all() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+CPSD_D void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// The density pass stages the next band's columns of its plane in shared
+// memory (ncol values, rounded to 16 bytes); the other passes take one band
+// per CTA and read the columns directly, and so does the density build that
+// splits a plane's rows between two CTAs (its two CTAs must fit one SM).
+template <typename T>
+constexpr size_t stage_elems(int mode, int ncol)
+{
+    return mode == PM_DENSITY ? ((size_t)ncol * sizeof(cx<T>) + 15) / 16 * 16 / sizeof(cx<T>) : 0;
+}
+
 template <typename T, int NF>
-size_t plane_smem_bytes(int mode, int KX)
+size_t plane_smem_bytes(int mode, int KX, int ncol)
 {
     using S = PlaneShape<T, NF>;
     const int nt = plane_threads<T, NF>(mode);
     const size_t ex_y = (size_t)S::y_groups(KX, nt / S::LY::P) * S::SY, ex_x = (size_t)(nt / S::LX::P) * S::SX;
-    size_t b = sizeof(cx<T>) * ((size_t)KX * S::YS + (ex_y > ex_x ? ex_y : ex_x));
+    size_t b = sizeof(cx<T>) * ((size_t)TwLayout<NF>::total + stage_elems<T>(mode, ncol) + (size_t)KX * S::YS +
+                                (ex_y > ex_x ? ex_y : ex_x));
     return (b + 15) / 16 * 16;
 }
 
@@ -237,7 +284,7 @@ constexpr int plane_row_split()
 
 template <typename T, int NF, int MODE, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB)
-plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
+plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> twg)
 {
     using S = PlaneShape<T, NF>;
     using LY = typename S::LY;
@@ -250,11 +297,19 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
     constexpr int EXB = (NGY * S::SY > NGX * S::SX) ? NGY * S::SY : NGX * S::SX;
     extern __shared__ unsigned char smem_raw[];
     const int KX = g.KX;
-    cx<T> *Y = reinterpret_cast<cx<T> *>(smem_raw);  // [KX][YS]
+    // the twiddle tables, staged once per CTA: shared-memory reads instead of
+    // L1 hits in every line transform, and 32-bit addresses (fewer registers)
+    cx<T> *tws = reinterpret_cast<cx<T> *>(smem_raw);
+    constexpr int RSPLIT = plane_row_split<NF, MODE, MINB>();
+    constexpr bool STAGE = MODE == PM_DENSITY && RSPLIT == 1;
+    cx<T> *stage = tws + TwLayout<NF>::total;                          // STAGE: one band's columns
+    cx<T> *Y = stage + stage_elems<T>(STAGE ? MODE : -1, g.ncol);  // [KX][YS]
     cx<T> *xball = Y + KX * YS;                       // group exchange buffers
+    for (int i = threadIdx.x; i < TwLayout<NF>::total; i += NT) tws[i] = twg.n_inv[i];
+    const Twiddles<T> tw = Twiddles<T>::template at<NF>(tws);
+    __syncthreads();
     // DENSITY: each lane owns the same (row, x) points for every band, so the
     // sum of psi^2 over the band chunk stays in registers
-    constexpr int RSPLIT = plane_row_split<NF, MODE, MINB>();
     constexpr int NIT = (NF + NGX - 1) / NGX / RSPLIT;  // x-row iterations per lane (of this CTA's rows)
     static_assert(RSPLIT == 1 || NIT * NGX * RSPLIT == NF, "row split");
     const int it0 = (RSPLIT > 1) ? (int)blockIdx.z * NIT : 0;
@@ -278,8 +333,22 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
     cx<T> *xby = xball + gy * S::SY;
     cx<T> *xbx = xball + gx * S::SX;
 
+    // STAGE: band bb's columns of this plane -> stage, asynchronously; the
+    // copy of band b+1 is issued once band b's y lines have read the stage
+    // and lands while band b's x rows run
+    auto prefetch = [&](int bb) {
+        const cx<T> *src = Tb + ((long)bb * NF + z) * g.ncol;
+        for (int c = threadIdx.x; c < g.ncol; c += NT) cp_async_cx(stage + c, src + c);
+        cp_async_commit_all();
+    };
+    if (STAGE && b0 < b1) prefetch(b0);
     for (int b = b0; b < b1; ++b) {
         cx<T> *Tplane = Tb + ((long)b * NF + z) * g.ncol;
+        const cx<T> *Tcol = STAGE ? stage : Tplane;
+        if (STAGE) {
+            cp_async_wait_all();
+            __syncthreads();
+        }
         // ---- inverse along y (columns -> lines kx < KX) ------------------
         if constexpr (MODE != PM_FWDREAL) {
             for (int base = 0; base < KX && gy < ngy_act; base += NGY) {
@@ -303,7 +372,7 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
 #pragma unroll
                     for (int m = 0; m < QY; ++m) {
                         const int c = act ? g.colidx[i * NF + LY::in_index(ty, m)] : -1;
-                        v[m] = (c >= 0) ? Tplane[c] : cx<T>{0, 0};
+                        v[m] = (c >= 0) ? Tcol[c] : cx<T>{0, 0};
                     }
                 }
                 line_fft<NF, +1, T>(v, ty, xby, tw.n_inv);
@@ -315,6 +384,7 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
                 }
             }
             __syncthreads();
+            if (STAGE && b + 1 < b1) prefetch(b + 1);
         }
         // ---- x rows --------------------------------------------------------
 #pragma unroll
@@ -392,7 +462,7 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> tw)
                 }
             }
             if constexpr (MODE == PM_APPLYV) {
-                line_fft_dif<H, -1, T>(v, tx, xbx, tw.h_fwd);
+                line_fft_dif<H, -1, T>(v, tx, xbx, tw.h_fwd_dif);
 #pragma unroll
                 for (int m = 0; m < QX; ++m) xbx[LX::in_index(tx, m)] = v[m];
                 __syncwarp();
