@@ -264,10 +264,7 @@ struct FftOpsT final : FftOps {
         CK(upload(ar, &d, tab));
         tw = Twiddles<T>::template at<NF>(d);
 
-        using L = Line<NF>;
-        constexpr int P = L::P, CPB = kThreads / P;
-        constexpr int TILE = (CPB * (NF + 1) > NF * (CPB + 1)) ? CPB * (NF + 1) : NF * (CPB + 1);
-        zsmem = sizeof(cx<T>) * ((size_t)TILE + (size_t)CPB * group_stride<T, NF>() + (size_t)NF);
+        zsmem = z_smem_bytes<T, NF>();
         int dev = 0, optin = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));

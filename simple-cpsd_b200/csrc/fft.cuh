@@ -61,6 +61,23 @@ struct Twiddles {
 
 constexpr int kThreads = 256;
 
+// Shared memory of the z passes: one region (complex values) that holds the
+// CTA's column tile ([CPB][NF + 1] or [NF][CPB + 1]) and, once the lines are
+// in registers, the line groups' exchange buffers; the twiddle table after it.
+template <typename T, int NF>
+constexpr int z_tile_elems()
+{
+    constexpr int CPB = kThreads / Line<NF>::P;
+    constexpr int TILE = (CPB * (NF + 1) > NF * (CPB + 1)) ? CPB * (NF + 1) : NF * (CPB + 1);
+    constexpr int XB = CPB * group_stride<T, NF>();
+    return TILE > XB ? TILE : XB;
+}
+template <typename T, int NF>
+constexpr size_t z_smem_bytes()
+{
+    return sizeof(cx<T>) * ((size_t)z_tile_elems<T, NF>() + NF);
+}
+
 // ------------------------------------------------------------------ inv_z
 // packed psi (double) -> T (type T), one CTA = CPB columns of one band
 template <typename T, int NF>
@@ -70,13 +87,13 @@ inv_z_kernel(Geom g, const cx<double> *__restrict__ psi, long ldp, cx<T> *__rest
 {
     using L = Line<NF>;
     constexpr int P = L::P, Q = L::Q, U = L::U, CPB = kThreads / P;
-    constexpr int RS = NF + 1, CS = CPB + 1;  // row / column strides of the tile
-    constexpr int TILE = (CPB * RS > NF * CS) ? CPB * RS : NF * CS;
     constexpr int XS = group_stride<T, NF>();
+    constexpr int RS = NF + 1, CS = CPB + 1;  // row / column strides of the tile
     extern __shared__ unsigned char smem_raw[];
+    // the exchange buffers reuse the tile once every line is in registers
     cx<T> *tile = reinterpret_cast<cx<T> *>(smem_raw);
-    cx<T> *xb = tile + TILE;
-    cx<T> *twz = xb + CPB * XS;  // W_NF^m staged once per CTA (read by every line)
+    cx<T> *xb = tile;
+    cx<T> *twz = tile + z_tile_elems<T, NF>();  // W_NF^m staged once per CTA (read by every line)
     for (int i = threadIdx.x; i < NF; i += kThreads) twz[i] = tw.n_inv[i];
 
     const int b = blockIdx.y;
@@ -97,6 +114,7 @@ inv_z_kernel(Geom g, const cx<double> *__restrict__ psi, long ldp, cx<T> *__rest
     cx<T> v[Q];
 #pragma unroll
     for (int m = 0; m < Q; ++m) v[m] = row[L::in_index(t, m)];
+    __syncthreads();  // every row read: the exchange buffers overwrite the tile
     line_fft<NF, +1, T>(v, t, xb + grp * XS, twz);
     __syncthreads();
 #pragma unroll
@@ -134,17 +152,16 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
     using L = Line<NF>;
     constexpr int P = L::P, Q = L::Q, U = L::U, CPB = kThreads / P;
     constexpr int RS = NF + 1, CS = CPB + 1;
-    constexpr int TILE = (CPB * RS > NF * CS) ? CPB * RS : NF * CS;
     constexpr int XS = group_stride<T, NF>();
     extern __shared__ unsigned char smem_raw[];
     cx<T> *tile = reinterpret_cast<cx<T> *>(smem_raw);
-    cx<T> *xb = tile + TILE;
+    cx<T> *xb = tile;  // reuses the tile once every line is in registers
 
     const int b = blockIdx.y;
     const int c0 = blockIdx.x * CPB;
     const int grp = threadIdx.x / P, t = threadIdx.x % P;
     const int c = c0 + grp;
-    cx<T> *twz = xb + CPB * XS;  // W_NF^-m staged once per CTA
+    cx<T> *twz = tile + z_tile_elems<T, NF>();  // W_NF^-m staged once per CTA
     for (int i = threadIdx.x; i < NF; i += kThreads) twz[i] = tw.n_fwd[i];
     const cx<T> *src = Tb + (long)b * NF * g.ncol;
     for (int idx = threadIdx.x; idx < NF * CPB; idx += kThreads) {
@@ -155,6 +172,7 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
     cx<T> v[Q];
 #pragma unroll
     for (int m = 0; m < Q; ++m) v[m] = tile[L::in_index(t, m) * CS + grp];
+    __syncthreads();  // every column read: the exchange buffers overwrite the tile
     line_fft<NF, -1, T>(v, t, xb + grp * XS, twz);
     __syncthreads();
     cx<T> *row = tile + grp * RS;
