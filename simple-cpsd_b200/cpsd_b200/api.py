@@ -51,22 +51,43 @@ class State:
         self.lagrange_fail = 0
 
 
+_DROPIN_INP = ("unitg", "katm", "amass", "zv", "rcell", "masker", "G", "tg", "vc", "vg", "lmmax", "vnlnrm",
+               "vl", "vnl")
+_DROPIN_ST = ("r1", "r2", "fion", "c1", "c2", "cpsi", "dn", "hml", "lmd", "E")
+
+
+def _dropin_args(inp, st: State, inner: int, move: int):
+    """The C arguments of one drop-in call, built once per (inputs, state)
+    and reused while every array object and scalar they name is the same
+    (marshalling 40 arguments costs about as much as a small cell's step)."""
+    key = (id(inp), inner, move, int(inp.nion), int(inp.ispin), int(inp.nfft), int(inp.nfft3d), int(inp.n2ft3d),
+           float(inp.omega), float(inp.dt), float(inp.fmass), int(inp.nsh), float(inp.cewald), float(inp.rcut),
+           tuple(int(x) for x in inp.ne), tuple(id(getattr(inp, n)) for n in _DROPIN_INP),
+           tuple(id(getattr(st, n)) for n in _DROPIN_ST))
+    cached = getattr(st, "_dropin", None)
+    if cached is not None and cached[0] == key:
+        return cached[1], cached[2]
+    ne = np.ascontiguousarray(inp.ne, dtype=np.int32)
+    dd = [ctypes.c_double() for _ in range(3)]
+    args = (ctypes.c_int(inner), ctypes.c_int(move), ctypes.c_int(inp.nion), ctypes.c_int(inp.ispin),
+            _ptr(ne), ctypes.c_int(inp.nfft), ctypes.c_int(inp.nfft3d), ctypes.c_int(inp.n2ft3d),
+            _ptr(inp.unitg), ctypes.c_double(inp.omega), ctypes.c_double(inp.dt),
+            ctypes.c_double(inp.fmass), _ptr(inp.katm), _ptr(inp.amass), _ptr(inp.zv),
+            ctypes.c_int(inp.nsh), _ptr(inp.rcell), ctypes.c_double(inp.cewald),
+            ctypes.c_double(inp.rcut), _ptr(inp.masker), _ptr(inp.G), _ptr(inp.tg), _ptr(inp.vc),
+            _ptr(inp.vg), _ptr(inp.lmmax), _ptr(inp.vnlnrm), _ptr(inp.vl), _ptr(inp.vnl),
+            _ptr(st.r1), _ptr(st.r2), _ptr(st.fion), _ptr(st.c1), _ptr(st.c2), _ptr(st.cpsi),
+            _ptr(st.dn), _ptr(st.hml), _ptr(st.lmd), _ptr(st.E), ctypes.byref(dd[0]),
+            ctypes.byref(dd[1]), ctypes.byref(dd[2]))
+    st._dropin = (key, args, dd, ne)  # ne stays alive with the pointer to it
+    return args, dd
+
+
 def cpsd(inp, st: State, inner: int, move: int = 0) -> State:
     """The drop-in: exactly the reference's cpsd() call with host buffers."""
     L = _l.load()
-    ne = np.ascontiguousarray(inp.ne, dtype=np.int32)
-    dd = [ctypes.c_double() for _ in range(3)]
-    rc = L.cpsd_gpu_cpsd(
-        ctypes.c_int(inner), ctypes.c_int(move), ctypes.c_int(inp.nion), ctypes.c_int(inp.ispin),
-        _ptr(ne), ctypes.c_int(inp.nfft), ctypes.c_int(inp.nfft3d), ctypes.c_int(inp.n2ft3d),
-        _ptr(inp.unitg), ctypes.c_double(inp.omega), ctypes.c_double(inp.dt),
-        ctypes.c_double(inp.fmass), _ptr(inp.katm), _ptr(inp.amass), _ptr(inp.zv),
-        ctypes.c_int(inp.nsh), _ptr(inp.rcell), ctypes.c_double(inp.cewald),
-        ctypes.c_double(inp.rcut), _ptr(inp.masker), _ptr(inp.G), _ptr(inp.tg), _ptr(inp.vc),
-        _ptr(inp.vg), _ptr(inp.lmmax), _ptr(inp.vnlnrm), _ptr(inp.vl), _ptr(inp.vnl),
-        _ptr(st.r1), _ptr(st.r2), _ptr(st.fion), _ptr(st.c1), _ptr(st.c2), _ptr(st.cpsi),
-        _ptr(st.dn), _ptr(st.hml), _ptr(st.lmd), _ptr(st.E), ctypes.byref(dd[0]),
-        ctypes.byref(dd[1]), ctypes.byref(dd[2]))
+    args, dd = _dropin_args(inp, st, inner, move)
+    rc = L.cpsd_gpu_cpsd(*args)
     if rc == _l.CPSD_WARN_LAGRANGE:
         st.lagrange_fail += 1
     elif rc != _l.CPSD_OK:

@@ -25,15 +25,31 @@ cpsd_gpu_ctx *g_ctx = nullptr;
 struct Signature {
     int nfft = 0, ispin = 0, ne0 = 0, ne1 = 0, nion = 0, nkatm = 0, nsh = 0, device = -1;
     std::vector<int> masker1;
-    bool operator==(const Signature &o) const
+    bool same_shape(const Signature &o) const
     {
         return nfft == o.nfft && ispin == o.ispin && ne0 == o.ne0 && ne1 == o.ne1 && nion == o.nion &&
-               nkatm == o.nkatm && nsh == o.nsh && device == o.device && masker1 == o.masker1;
+               nkatm == o.nkatm && nsh == o.nsh && device == o.device;
+    }
+    // the reference's masker holds every value twice (main.c:189-195)
+    bool same_mask(const int *masker, int nfft3d) const
+    {
+        if ((int)masker1.size() != nfft3d) return false;
+        for (int k = 0; k < nfft3d; ++k)
+            if (masker[2 * k] != masker1[k]) return false;
+        return true;
     }
 };
 Signature g_sig;
 
+
 }  // namespace
+
+// engine.cu: the drop-in's state upload, steps and host-layout outputs, with
+// the check that c2 is zero outside the sphere overlapping the steps.
+int cpsd_dropin_state_run_fetch(cpsd_gpu_ctx *c, const double *r2in, int inner, int move, double *E,
+                                double *deltae, double *deltac, double *deltar, double *c1, double *c2,
+                                double *cpsi, double *dn, double *hml, double *lmd, double *r1, double *r2,
+                                double *fion);
 
 // engine.cu: cpsd_gpu_run, then the host-layout outputs, with c1 and cpsi
 // zeroed on host threads during the run (c2 must have just gone through
@@ -66,11 +82,11 @@ extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, co
     sig.nkatm = nkatm;
     sig.nsh = nsh;
     cudaGetDevice(&sig.device);
-    sig.masker1.resize(nfft3d);
-    for (int k = 0; k < nfft3d; ++k) sig.masker1[k] = masker[2 * k];  // main.c:189-195 duplicates it
 
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_ctx || !(sig == g_sig)) {
+    if (!g_ctx || !sig.same_shape(g_sig) || !g_sig.same_mask(masker, nfft3d)) {
+        sig.masker1.resize(nfft3d);
+        for (int k = 0; k < nfft3d; ++k) sig.masker1[k] = masker[2 * k];
         if (g_ctx) cpsd_gpu_destroy(g_ctx);
         g_ctx = nullptr;
         cpsd_gpu_params p{};
@@ -99,10 +115,8 @@ extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, co
     if (rc) return rc;
     rc = cpsd_gpu_set_tables(c, katm, amass, zv, rcell, G, tg, vc, vg, lmmax, vnlnrm, vl, vnl);
     if (rc) return rc;
-    rc = cpsd_gpu_set_state(c, c2, r2);
-    if (rc) return rc;
-    return cpsd_dropin_run_fetch(c, inner, move, E, deltae, deltac, deltar, c1, c2, cpsi, dn, hml, lmd, r1, r2,
-                                 fion);
+    return cpsd_dropin_state_run_fetch(c, r2, inner, move, E, deltae, deltac, deltar, c1, c2, cpsi, dn, hml, lmd,
+                                       r1, r2, fion);
 }
 
 extern "C" cpsd_gpu_ctx *cpsd_gpu_dropin_context(void)

@@ -545,6 +545,7 @@ struct cpsd_gpu_ctx {
     } hstage;
     Pinned tstage;  // packed tables of cpsd_gpu_set_tables
     size_t tstage_bytes = 0;
+    std::vector<char> tables_last;  // the staged bytes of the last upload (a repeat is not sent again)
     Pinned dstage;  // the density (ispin * n^3) on its way to the padded host layout
     int pblocks = 0, bblocks = 0, gblocks = 0;
     double *ppart = nullptr, *bpart = nullptr, *gpart = nullptr;
@@ -1382,6 +1383,34 @@ long host_gather(cpsd_gpu_ctx *c, const double *full)
     return outside.load();
 }
 
+// c->hstage[b][p] = full[b][pt_idx[p]], zero past npw: the sphere only (the
+// rest of the grid is checked separately, see count_outside).
+void host_gather_sphere(cpsd_gpu_ctx *c, const double *full)
+{
+    const cx<double> *src = reinterpret_cast<const cx<double> *>(full);
+    const int *pt = c->hg.pt_idx.data();
+    cpsd_host::Pool::get().run(c->nb, [&](int b) {
+        const cx<double> *sb = src + (long)b * c->nfft3d;
+        cx<double> *d = c->hstage.p + (long)b * c->ldc;
+        for (int p = 0; p < c->npw; ++p) d[p] = sb[pt[p]];
+        for (long p = c->npw; p < c->ldc; ++p) d[p] = cx<double>{0.0, 0.0};
+    });
+}
+
+// Nonzero values outside the sphere in slice t of the band grids (the
+// slicing of grid_slices).
+long count_outside(const cpsd_gpu_ctx *c, const double *full, int t)
+{
+    const cx<double> *src = reinterpret_cast<const cx<double> *>(full);
+    const int *inv = c->hg.inv_idx.data();
+    const long S = grid_slices(c), per = cdiv(c->nfft3d, S);
+    const long b = t / S, g0 = (t % S) * per, g1 = std::min(c->nfft3d, g0 + per);
+    const cx<double> *sb = src + b * c->nfft3d;
+    long bad = 0;
+    for (long g = g0; g < g1; ++g) bad += (inv[g] < 0) & (sb[g].x != 0.0 || sb[g].y != 0.0);
+    return bad;
+}
+
 // Zero n doubles.  On x86-64 with non-temporal stores: the lines are only
 // written, so they need not be read for ownership first; scalar stores at
 // the unaligned ends, and a store fence so that later stores from other
@@ -1530,6 +1559,81 @@ int cpsd_dropin_run_fetch(cpsd_gpu_ctx *c, int inner, int move, double *E, doubl
     if (run != CPSD_OK && run != CPSD_WARN_LAGRANGE) return run;
     const unsigned zeroed = separate ? (ZERO_C1 | ZERO_C2 | ZERO_CPSI) : 0u;
     const int rc = get_state_host(c, c1, c2, cpsi, dn, hml, lmd, r1, r2, fion, zeroed);
+    return rc ? rc : run;
+}
+
+// The drop-in's whole call after the tables: c2's sphere is gathered and
+// uploaded and the steps start at once; host threads meanwhile check that c2
+// is zero outside the sphere (the reference keeps it masked, and the pruned
+// transforms rely on it) and only then zero c1 and cpsi for the outputs.  A
+// c2 with values outside the sphere returns CPSD_ERR_UNMASKED_PSI with every
+// output untouched; the context's device state is then that of a discarded
+// run and the next call uploads its own.  Outputs that share memory take the
+// serial path (check, run, then zero and scatter).
+int cpsd_dropin_state_run_fetch(cpsd_gpu_ctx *c, const double *r2in, int inner, int move, double *E,
+                                double *deltae, double *deltac, double *deltar, double *c1, double *c2,
+                                double *cpsi, double *dn, double *hml, double *lmd, double *r1, double *r2,
+                                double *fion)
+{
+    if (!c || !c2 || (c->nion > 0 && !r2in)) return CPSD_ERR_ARG;
+    const size_t gb = sizeof(double) * c->nb * c->n2ft3d;
+    auto apart = [gb](const double *x, const double *y) {
+        return !x || !y || (const char *)x + gb <= (const char *)y || (const char *)y + gb <= (const char *)x;
+    };
+    if (!(apart(c1, c2) && apart(cpsi, c2) && apart(c1, cpsi))) {
+        const int rc = cpsd_gpu_set_state(c, c2, r2in);
+        if (rc) return rc;
+        return cpsd_dropin_run_fetch(c, inner, move, E, deltae, deltac, deltar, c1, c2, cpsi, dn, hml, lmd, r1,
+                                     r2, fion);
+    }
+    CK(cudaSetDevice(c->prm.device));
+    cudaStream_t s = c->st;
+    CK(cudaStreamSynchronize(s));  // the staging buffer may still feed an earlier copy
+    host_gather_sphere(c, c2);
+    const size_t pb = sizeof(cx<double>) * c->nb * c->ldc;
+    CK(cudaMemcpyAsync(c->cbuf[c->cur], c->hstage.p, pb, cudaMemcpyHostToDevice, s));
+    if (c->nion > 0) CK(cudaMemcpyAsync(c->r2, r2in, sizeof(double) * 3 * c->nion, cudaMemcpyHostToDevice, s));
+    c->h2d += (long long)pb + (long long)sizeof(double) * 3 * c->nion;
+    c->state_ok = true;
+    // items [0, nv): the check of c2; [nv, nv + nz): the zeroing of c1 and
+    // cpsi, each of which first waits for the whole check (the items are
+    // claimed in order, so every check item is running or done by then)
+    const long S = grid_slices(c);
+    const int nv = (int)(c->nb * S);
+    std::vector<double *> zero;
+    if (c1) zero.push_back(c1);
+    if (cpsi) zero.push_back(cpsi);
+    int nz = 0;
+    auto ztask = zero.empty() ? std::function<void(int)>() : zero_grids_task(c, zero, &nz);
+    std::atomic<long> bad{0};
+    std::atomic<int> checked{0};
+    auto &pool = cpsd_host::Pool::get();
+    pool.start(nv + nz, [&](int t) {
+        if (t < nv) {
+            const long n = count_outside(c, c2, t);
+            if (n) bad += n;
+            checked.fetch_add(1, std::memory_order_release);
+            return;
+        }
+        while (checked.load(std::memory_order_acquire) < nv) std::this_thread::yield();
+        if (bad.load() == 0) ztask(t - nv);
+    });
+    // the energies go to the caller only once the check has passed (E[0]
+    // comes in as the previous call's energy, for deltae)
+    double Et[10], dt3[3] = {0.0, 0.0, 0.0};
+    memcpy(Et, E, sizeof(Et));
+    const int run = cpsd_gpu_run(c, inner, move, Et, &dt3[0], &dt3[1], &dt3[2]);
+    pool.wait();
+    if (bad.load()) {
+        c->state_ok = false;
+        return CPSD_ERR_UNMASKED_PSI;
+    }
+    memcpy(E, Et, sizeof(Et));
+    if (deltae) *deltae = dt3[0];
+    if (deltac) *deltac = dt3[1];
+    if (deltar) *deltar = dt3[2];
+    if (run != CPSD_OK && run != CPSD_WARN_LAGRANGE) return run;
+    const int rc = get_state_host(c, c1, c2, cpsi, dn, hml, lmd, r1, r2, fion, ZERO_C1 | ZERO_C2 | ZERO_CPSI);
     return rc ? rc : run;
 }
 
@@ -1968,6 +2072,7 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
             if (!(amass[ia] > 0)) return CPSD_ERR_ARG;
     if (np != c->nproj || !c->proj) {
         drop_graphs(c);
+        c->tables_last.clear();
         if (np > 0) {
             CK(c->ar.alloc(&c->proj, (size_t)np * c->npw_pad));
             CK(c->ar.alloc(&c->beta, (size_t)np * c->nb));
@@ -2024,6 +2129,13 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
     if (motion)
         for (int d = 0; d < 3; ++d)
             for (int p = 0; p < npw; ++p) pg[(size_t)d * npw + p] = G[(size_t)d * c->nfft3d + pt[p]];
+    // a driver passes the same tables every call (ccpsdv3/main.c:422-426):
+    // the device copies are current when the staged bytes are unchanged
+    if (motion) c->amass_h.assign(amass, amass + nkatm);
+    if (c->tables_ok && c->tables_last.size() == sg.off && !memcmp(c->tables_last.data(), c->tstage.p, sg.off)) {
+        c->motion_ok = motion;
+        return CPSD_OK;
+    }
     sg.put(c->tg, ptg, npw_pad);
     sg.put(c->shell, sh, npw_pad);
     sg.put(c->vc, pvc, npw_pad);
@@ -2043,12 +2155,13 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
     c->motion_ok = false;
     if (motion) {
         sg.put(c->Gv, pg, (size_t)3 * npw);
-        c->amass_h.assign(amass, amass + nkatm);
         c->motion_ok = true;
     }
+    c->tables_last.clear();
     CK(sg.err);
     CK(cudaStreamSynchronize(c->st));
     c->h2d += sg.bytes;
+    c->tables_last.assign(reinterpret_cast<const char *>(c->tstage.p), reinterpret_cast<const char *>(c->tstage.p) + sg.off);
     c->tables_ok = true;
     return CPSD_OK;
 }

@@ -312,7 +312,7 @@ def test_full_size_cell_properties():
     cell2.close()
 
 
-def test_error_paths():
+def test_error_paths(golden):
     """Bad inputs come back as status codes, never as a device fault."""
     inp = inputs.build_inputs(configs.small_h2(16))
     # move = 1 without the G vectors and masses it needs
@@ -332,9 +332,24 @@ def test_error_paths():
     out_of_mask = np.flatnonzero(bad.masker1 == 0)[5]
     bad.c2[2 * out_of_mask] = 1.0
     st = api.State(bad)
+    st.c1[:] = -2.0
+    st.cpsi[:] = 5.0
+    before = {n: getattr(st, n).copy() for n in ("c1", "c2", "cpsi", "dn", "hml", "lmd", "E", "r1", "r2")}
     with pytest.raises(lib.CpsdError) as e:
         api.cpsd(bad, st, 1)
     assert e.value.status == lib.CPSD_ERR_UNMASKED_PSI
+    # the check runs beside the steps, but no output is written on a refusal
+    for n, v in before.items():
+        assert np.array_equal(getattr(st, n), v), n
+    # and the next call with masked orbitals is the reference's
+    mk, ncalls, inner = CASES["small_h2_16"]
+    good = inputs.build_inputs(mk())
+    sg = api.State(good)
+    rows = []
+    for _ in range(ncalls):
+        api.cpsd(good, sg, inner)
+        rows.append((sg.E.copy(), sg.deltae, sg.deltac))
+    check_against_golden(good, golden("small_h2_16"), rows, sg)
     cell = api.GpuCell(inp)
     with pytest.raises(lib.CpsdError) as e:
         cell.run(0)
