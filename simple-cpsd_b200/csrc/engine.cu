@@ -84,6 +84,10 @@ cudaError_t allow_max_smem(K kernel, int optin)
 struct HostGeom {
     int n = 0, nh = 0, KX = 0, ncol = 0, npw = 0, npw_pad = 0;
     std::vector<int> col_i, col_j, col_ptr, pt_k, pt_i, pt_j, pt_idx, colidx, inv_idx;
+    // the sphere points in ascending full-box index (pt_idx[pt_ord[q]] grows
+    // with q): host loops over the reference's grids walk them in memory
+    // order instead of one column (stride nh*n) at a time
+    std::vector<int> pt_ord;
     std::vector<int> yrun;  // 3 per line kx < KX (see Geom::yrun), empty if some line is not two runs
     std::vector<double> w;
 };
@@ -122,6 +126,9 @@ HostGeom build_geom(int n, const int *masker1, bool full)
         }
     h.ncol = (int)h.col_i.size();
     h.npw = (int)h.pt_k.size();
+    h.pt_ord.reserve(h.npw);
+    for (long idx = 0; idx < nfft3d; ++idx)
+        if (h.inv_idx[idx] >= 0) h.pt_ord.push_back(h.inv_idx[idx]);
     h.npw_pad = (int)cdiv(std::max(h.npw, 1), 32) * 32;
     h.w.resize(h.npw_pad, 0.0);
     h.colidx.assign((size_t)std::max(h.KX, 1) * n, -1);
@@ -471,6 +478,11 @@ struct cpsd_gpu_ctx {
     // nonlocal part of -H psi run beside the density -> potential chain
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_sf = nullptr, ev_side = nullptr;
+    // early fetch (the drop-in): once the steps are done, c1, c2 and the
+    // density go to the pinned staging on the side stream while the
+    // energies run; get_state_host then only waits for ev_fetch
+    bool early_fetch = false, fetched = false;
+    cudaEvent_t ev_steps = nullptr, ev_fetch = nullptr;
     cudaStream_t cs = nullptr;  // the stream the GEMM helpers launch on
     bool lag_tile = false;  // 4 x 4 tiled solver (<= 128 bands, 16-CTA clusters schedulable)
     bool lag_tile_ok = false;  // the tiled solver can run on this device for these bands
@@ -1388,11 +1400,14 @@ long host_gather(cpsd_gpu_ctx *c, const double *full)
 void host_gather_sphere(cpsd_gpu_ctx *c, const double *full)
 {
     const cx<double> *src = reinterpret_cast<const cx<double> *>(full);
-    const int *pt = c->hg.pt_idx.data();
+    const int *pt = c->hg.pt_idx.data(), *ord = c->hg.pt_ord.data();
     cpsd_host::Pool::get().run(c->nb, [&](int b) {
         const cx<double> *sb = src + (long)b * c->nfft3d;
         cx<double> *d = c->hstage.p + (long)b * c->ldc;
-        for (int p = 0; p < c->npw; ++p) d[p] = sb[pt[p]];
+        for (int q = 0; q < c->npw; ++q) {
+            const int p = ord[q];
+            d[p] = sb[pt[p]];
+        }
         for (long p = c->npw; p < c->ldc; ++p) d[p] = cx<double>{0.0, 0.0};
     });
 }
@@ -1454,20 +1469,25 @@ int get_state_host(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double
     const size_t pb = sizeof(cx<double>) * P;
     const cx<double> *cc2 = c->cbuf[c->cur], *cc1 = c->ran ? c->cbuf[c->cur ^ 1] : cc2;
     cx<double> *h2 = c->hstage.p, *h1 = c->hstage.p + P;
-    if (c2 || cpsi) {
-        CK(cudaMemcpyAsync(h2, cc2, pb, cudaMemcpyDeviceToHost, s));
-        c->d2h += (long long)pb;
-    }
-    if (c1 || cpsi) {
-        CK(cudaMemcpyAsync(h1, cc1, pb, cudaMemcpyDeviceToHost, s));
-        c->d2h += (long long)pb;
+    double *dst = reinterpret_cast<double *>(c->dstage.p);
+    if (c->fetched) {  // c1, c2 and the density are in the staging already
+        CK(cudaEventSynchronize(c->ev_fetch));
+        c->fetched = false;
+    } else {
+        if (c2 || cpsi) {
+            CK(cudaMemcpyAsync(h2, cc2, pb, cudaMemcpyDeviceToHost, s));
+            c->d2h += (long long)pb;
+        }
+        if (c1 || cpsi) {
+            CK(cudaMemcpyAsync(h1, cc1, pb, cudaMemcpyDeviceToHost, s));
+            c->d2h += (long long)pb;
+        }
+        if (dn) {  // unpadded into pinned staging; the host adds the two pad reals per x line
+            CK(cudaMemcpyAsync(dst, c->dn, sizeof(double) * c->ispin * c->n3, cudaMemcpyDeviceToHost, s));
+            c->d2h += (long long)sizeof(double) * c->ispin * c->n3;
+        }
     }
     const long ne02 = (long)c->ne0 * c->ne0, ne12 = (long)c->ne1 * c->ne1;
-    double *dst = reinterpret_cast<double *>(c->dstage.p);
-    if (dn) {  // unpadded into pinned staging; the host adds the two pad reals per x line
-        CK(cudaMemcpyAsync(dst, c->dn, sizeof(double) * c->ispin * c->n3, cudaMemcpyDeviceToHost, s));
-        c->d2h += (long long)sizeof(double) * c->ispin * c->n3;
-    }
     c->d2h += (long long)sizeof(double) * ((hml ? ne02 + ne12 : 0) + (lmd ? ne02 + ne12 : 0) +
                                           (c->nion > 0 ? ((r1 ? 3 : 0) + (r2 ? 3 : 0)) * c->nion : 0));
     if (hml) CK(cudaMemcpyAsync(hml, c->hml, sizeof(double) * (ne02 + ne12), cudaMemcpyDeviceToHost, s));
@@ -1512,7 +1532,7 @@ int get_state_host(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double
     std::vector<Out> todo;
     for (const Out &o : outs)
         if (o.host) todo.push_back(o);
-    const int *pt = c->hg.pt_idx.data();
+    const int *pt = c->hg.pt_idx.data(), *ord = c->hg.pt_ord.data();
     pool.run((int)(todo.size() * c->nb), [&](int t) {
         const Out &o = todo[t / c->nb];
         const long b = t % c->nb;
@@ -1520,9 +1540,15 @@ int get_state_host(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double
         const cx<double> *a = o.a + b * c->ldc;
         if (o.sub) {
             const cx<double> *u = o.sub + b * c->ldc;
-            for (int p = 0; p < c->npw; ++p) d[pt[p]] = cx<double>{a[p].x - u[p].x, a[p].y - u[p].y};
+            for (int q = 0; q < c->npw; ++q) {
+                const int p = ord[q];
+                d[pt[p]] = cx<double>{a[p].x - u[p].x, a[p].y - u[p].y};
+            }
         } else {
-            for (int p = 0; p < c->npw; ++p) d[pt[p]] = a[p];
+            for (int q = 0; q < c->npw; ++q) {
+                const int p = ord[q];
+                d[pt[p]] = a[p];
+            }
         }
     });
     return CPSD_OK;
@@ -1622,8 +1648,16 @@ int cpsd_dropin_state_run_fetch(cpsd_gpu_ctx *c, const double *r2in, int inner, 
     // comes in as the previous call's energy, for deltae)
     double Et[10], dt3[3] = {0.0, 0.0, 0.0};
     memcpy(Et, E, sizeof(Et));
+    c->early_fetch = true;
     const int run = cpsd_gpu_run(c, inner, move, Et, &dt3[0], &dt3[1], &dt3[2]);
+    c->early_fetch = false;
     pool.wait();
+    if (bad.load() || (run != CPSD_OK && run != CPSD_WARN_LAGRANGE)) {
+        if (c->fetched) {  // the staging is free again only once those copies are done
+            CK(cudaEventSynchronize(c->ev_fetch));
+            c->fetched = false;
+        }
+    }
     if (bad.load()) {
         c->state_ok = false;
         return CPSD_ERR_UNMASKED_PSI;
@@ -2094,28 +2128,43 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
     int *plm = sg.slice<int>(nkatm), *pk = sg.slice<int>(c->nion), *po = sg.slice<int>(c->nion);
     double *pn = sg.slice<double>(np), *pg = sg.slice<double>(motion ? (size_t)3 * npw : 0);
     if (!sg.ok()) return CPSD_ERR_ARG;  // more kinds / ions than the context was created for
+    // gathered in the grids' memory order (pt_ord), each table on a host thread
+    const int *ord = h.pt_ord.data();
+    for (int p = npw; p < npw_pad; ++p) ptg[p] = pvc[p] = pvg[p] = 0.0;
+    const int ntab = 3 + nkatm * 10 + (motion ? 3 : 0);
+    cpsd_host::Pool::get().run(ntab, [&](int t) {
+        const double *src;
+        double *d;
+        if (t < 3) {
+            src = t == 0 ? tg : (t == 1 ? vc : vg);
+            d = t == 0 ? ptg : (t == 1 ? pvc : pvg);
+        } else if (t < 3 + nkatm * 10) {
+            const int ia = (t - 3) / 10, l = (t - 3) % 10;  // l = 0: vl, else vnl channel l - 1
+            if (l == 0) {
+                src = vl + (size_t)ia * c->nfft3d;
+                d = pvl + (size_t)ia * npw;
+            } else {
+                d = pvnl + ((size_t)ia * 9 + l - 1) * npw;
+                if (l - 1 >= lmmax[ia]) {
+                    memset(d, 0, sizeof(double) * npw);
+                    return;
+                }
+                src = vnl + ((size_t)ia * 9 + l - 1) * c->nfft3d;
+            }
+        } else {
+            const int dd = t - 3 - nkatm * 10;
+            src = G + (size_t)dd * c->nfft3d;
+            d = pg + (size_t)dd * npw;
+        }
+        for (int q = 0; q < npw; ++q) {
+            const int p = ord[q];
+            d[p] = src[pt[p]];
+        }
+    });
     double tmax = 0.0;
-    for (int p = 0; p < npw_pad; ++p) {
-        const bool in = p < npw;
-        ptg[p] = in ? tg[pt[p]] : 0.0;
-        pvc[p] = in ? vc[pt[p]] : 0.0;
-        pvg[p] = in ? vg[pt[p]] : 0.0;
-        tmax = std::max(tmax, ptg[p]);
-    }
+    for (int p = 0; p < npw; ++p) tmax = std::max(tmax, ptg[p]);
     c->tmax = tmax > 0 ? tmax : 1.0;
     for (int p = 0; p < npw_pad; ++p) sh[p] = p < npw ? std::min(kShells - 1, (int)(ptg[p] / c->tmax * kShells)) : 0;
-    for (int ia = 0; ia < nkatm; ++ia) {
-        for (int p = 0; p < npw; ++p) pvl[(size_t)ia * npw + p] = vl[(size_t)ia * c->nfft3d + pt[p]];
-        for (int l = 0; l < 9; ++l) {
-            double *d = pvnl + ((size_t)ia * 9 + l) * npw;
-            if (l < lmmax[ia]) {
-                const double *src = vnl + ((size_t)ia * 9 + l) * c->nfft3d;
-                for (int p = 0; p < npw; ++p) d[p] = src[pt[p]];
-            } else {
-                memset(d, 0, sizeof(double) * npw);
-            }
-        }
-    }
     memcpy(pzv, zv, sizeof(double) * nkatm);
     memcpy(pug, c->prm.unitg, sizeof(double) * 9);
     if (c->nsh > 0) memcpy(prc, rcell, sizeof(double) * 3 * c->nsh);
@@ -2126,9 +2175,6 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
     }
     for (int ii = 0, q = 0; ii < c->nion; ++ii)
         for (int l = 0; l < lmmax[hk[ii]]; ++l) pn[q++] = vnlnrm[hk[ii] * 9 + l];
-    if (motion)
-        for (int d = 0; d < 3; ++d)
-            for (int p = 0; p < npw; ++p) pg[(size_t)d * npw + p] = G[(size_t)d * c->nfft3d + pt[p]];
     // a driver passes the same tables every call (ccpsdv3/main.c:422-426):
     // the device copies are current when the staged bytes are unchanged
     if (motion) c->amass_h.assign(amass, amass + nkatm);
@@ -2212,6 +2258,22 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
     CK(cudaMemcpyAsync(c->Edev, E, sizeof(double), cudaMemcpyHostToDevice, s));
     int rc = run_steps(c, inner);
     if (rc) return rc;
+    if (c->early_fetch) {  // the energies below only read c1, c2 and the density
+        const size_t pb = sizeof(cx<double>) * c->nb * c->ldc;
+        if (!c->ev_steps) {
+            CK(cudaEventCreateWithFlags(&c->ev_steps, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c->ev_fetch, cudaEventDisableTiming));
+        }
+        CK(cudaEventRecord(c->ev_steps, s));
+        CK(cudaStreamWaitEvent(c->st2, c->ev_steps, 0));
+        CK(cudaMemcpyAsync(c->hstage.p, c->cbuf[c->cur], pb, cudaMemcpyDeviceToHost, c->st2));
+        CK(cudaMemcpyAsync(c->hstage.p + (long)c->nb * c->ldc, c->cbuf[c->cur ^ 1], pb, cudaMemcpyDeviceToHost,
+                           c->st2));
+        CK(cudaMemcpyAsync(c->dstage.p, c->dn, sizeof(double) * c->ispin * c->n3, cudaMemcpyDeviceToHost, c->st2));
+        CK(cudaEventRecord(c->ev_fetch, c->st2));
+        c->d2h += 2LL * (long long)pb + (long long)sizeof(double) * c->ispin * c->n3;
+        c->fetched = true;
+    }
     return finish_call(c, inner, E, deltae, deltac, deltar);
 }
 
@@ -3033,7 +3095,8 @@ void cpsd_gpu_destroy(cpsd_gpu_ctx *c)
     for (auto &e : c->pev)
         if (e) cudaEventDestroy(e);
     c->ar.release();
-    for (cudaEvent_t e : {c->ev_fork, c->ev_sf, c->ev_side})
+    if (c->st2) cudaStreamSynchronize(c->st2);
+    for (cudaEvent_t e : {c->ev_fork, c->ev_sf, c->ev_side, c->ev_steps, c->ev_fetch})
         if (e) cudaEventDestroy(e);
     if (c->st2) cudaStreamDestroy(c->st2);
     if (c->st) cudaStreamDestroy(c->st);
