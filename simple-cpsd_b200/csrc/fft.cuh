@@ -61,6 +61,20 @@ struct Twiddles {
 
 constexpr int kThreads = 256;
 
+// one complex value global -> shared without a register round trip
+// (cp.async: 16 bytes bypassing L1 for FP64, 8 bytes for FP32)
+template <typename T>
+CPSD_D void cp_async_cx(cx<T> *dst, const cx<T> *src)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(cx<T>) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+CPSD_D void cp_async_commit_all() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+CPSD_D void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // Shared memory of the z passes: one region (complex values) that holds the
 // CTA's column tile ([CPB][NF + 1] or [NF][CPB + 1]) and, once the lines are
 // in registers, the line groups' exchange buffers; the twiddle table after it.
@@ -104,10 +118,21 @@ inv_z_kernel(Geom g, const cx<double> *__restrict__ psi, long ldp, cx<T> *__rest
     for (int k = t; k < NF; k += P) row[k] = cx<T>{0, 0};
     __syncwarp();
     if (c < g.ncol) {
+        // four points per lane in flight: their loads before their stores
         const cx<double> *src = psi + (long)b * ldp;
-        for (int p = g.col_ptr[c] + t; p < g.col_ptr[c + 1]; p += P) {
-            cx<double> vv = src[p];
-            row[g.pt_k[p]] = cx<T>{(T)vv.x, (T)vv.y};
+        const int pe = g.col_ptr[c + 1];
+        for (int p0 = g.col_ptr[c] + t; p0 < pe; p0 += 4 * P) {
+            cx<double> vv[4];
+            int kk[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int p = p0 + u * P;
+                kk[u] = (p < pe) ? g.pt_k[p] : -1;
+                if (p < pe) vv[u] = src[p];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (kk[u] >= 0) row[kk[u]] = cx<T>{(T)vv[u].x, (T)vv[u].y};
         }
     }
     __syncthreads();  // the rows and the staged table
@@ -163,11 +188,17 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
     const int c = c0 + grp;
     cx<T> *twz = tile + z_tile_elems<T, NF>();  // W_NF^-m staged once per CTA
     for (int i = threadIdx.x; i < NF; i += kThreads) twz[i] = tw.n_fwd[i];
+    // the column tile by cp.async: every element of a thread in flight at once
     const cx<T> *src = Tb + (long)b * NF * g.ncol;
     for (int idx = threadIdx.x; idx < NF * CPB; idx += kThreads) {
         int z = idx / CPB, cl = idx % CPB;
-        tile[z * CS + cl] = (c0 + cl < g.ncol) ? src[(long)z * g.ncol + c0 + cl] : cx<T>{0, 0};
+        if (c0 + cl < g.ncol)
+            cp_async_cx(tile + z * CS + cl, src + (long)z * g.ncol + c0 + cl);
+        else
+            tile[z * CS + cl] = cx<T>{0, 0};
     }
+    cp_async_commit_all();
+    cp_async_wait_all();
     __syncthreads();
     cx<T> v[Q];
 #pragma unroll
@@ -182,16 +213,36 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
         for (int s = 0; s < P; ++s) row[L::out_index(t, u, s)] = v[u * P + s];
     __syncwarp();
     if (c < g.ncol) {
-        for (int p = g.col_ptr[c] + t; p < g.col_ptr[c + 1]; p += P) {
-            cx<T> F = row[g.pt_k[p]];
-            if constexpr (EPI == ZEPI_STORE) {
-                e.out[(long)b * e.ldo + p] = cx<double>{e.scale * (double)F.x, e.scale * (double)F.y};
-            } else {
-                long o = (long)b * e.ldc + p;
-                cx<double> c2k = e.c2[o], c1v = e.c1[o];
-                cx<double> cp{-e.scal1 * (double)F.x + c2k.x, -e.scal1 * (double)F.y + c2k.y};
-                e.cpsi[o] = cp;
-                e.c2[o] = cx<double>{c1v.x + e.dte * cp.x, c1v.y + e.dte * cp.y};
+        // four points per lane in flight: every load of the four before any
+        // store (the stores to c2 would otherwise keep the next loads back)
+        const int pe = g.col_ptr[c + 1];
+        for (int p0 = g.col_ptr[c] + t; p0 < pe; p0 += 4 * P) {
+            int kk[4];
+            cx<double> c2k[4], c1v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int p = p0 + u * P;
+                kk[u] = (p < pe) ? g.pt_k[p] : -1;
+                if constexpr (EPI == ZEPI_SD)
+                    if (p < pe) {
+                        const long o = (long)b * e.ldc + p;
+                        c2k[u] = e.c2[o];
+                        c1v[u] = e.c1[o];
+                    }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (kk[u] < 0) continue;
+                const int p = p0 + u * P;
+                const cx<T> F = row[kk[u]];
+                if constexpr (EPI == ZEPI_STORE) {
+                    e.out[(long)b * e.ldo + p] = cx<double>{e.scale * (double)F.x, e.scale * (double)F.y};
+                } else {
+                    const long o = (long)b * e.ldc + p;
+                    const cx<double> cp{-e.scal1 * (double)F.x + c2k[u].x, -e.scal1 * (double)F.y + c2k[u].y};
+                    e.cpsi[o] = cp;
+                    e.c2[o] = cx<double>{c1v[u].x + e.dte * cp.x, c1v[u].y + e.dte * cp.y};
+                }
             }
         }
     }
@@ -247,20 +298,6 @@ __host__ __device__ constexpr int plane_threads(int mode)
 {
     return kThreads;
 }
-
-// one complex value global -> shared without a register round trip
-// (cp.async: 16 bytes bypassing L1 for FP64, 8 bytes for FP32)
-template <typename T>
-CPSD_D void cp_async_cx(cx<T> *dst, const cx<T> *src)
-{
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-    if constexpr (sizeof(cx<T>) == 16)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
-}
-CPSD_D void cp_async_commit_all() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-CPSD_D void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // The density pass stages the next band's columns of its plane in shared
 // memory (ncol values, rounded to 16 bytes); the other passes take one band
