@@ -359,13 +359,16 @@ struct FftOpsT final : FftOps {
     }
     void plane(int mode, const Geom &g, void *Tb, const PlaneArgs &a, int nchunks, cudaStream_t s) override
     {
-        dim3 grid(NF, (unsigned)nchunks);
+        // a CTA takes plane_bands_per_cta chunks (one band each for V psi)
+        dim3 grid(NF, (unsigned)cdiv(nchunks, plane_bands_per_cta(NF, mode)));
+        PlaneArgs pa = a;
+        pa.nchunks = nchunks;
         const int nt = plane_threads<T, NF>(mode);
         switch (mode) {
-        case PM_DENSITY: launch_plane<PM_DENSITY>(grid, nt, g, Tb, a, s); break;
-        case PM_APPLYV: launch_plane<PM_APPLYV>(grid, nt, g, Tb, a, s); break;
-        case PM_INVREAL: launch_plane<PM_INVREAL>(grid, nt, g, Tb, a, s); break;
-        default: launch_plane<PM_FWDREAL>(grid, nt, g, Tb, a, s); break;
+        case PM_DENSITY: launch_plane<PM_DENSITY>(grid, nt, g, Tb, pa, s); break;
+        case PM_APPLYV: launch_plane<PM_APPLYV>(grid, nt, g, Tb, pa, s); break;
+        case PM_INVREAL: launch_plane<PM_INVREAL>(grid, nt, g, Tb, pa, s); break;
+        default: launch_plane<PM_FWDREAL>(grid, nt, g, Tb, pa, s); break;
         }
     }
     bool mode_ok(int mode) const { return psmem[mode] != 0; }

@@ -260,6 +260,7 @@ struct PlaneArgs {
     const double *xadd;
     int nout;
     const double *rin;    // FWDREAL: real input grid
+    int nchunks;          // APPLYV with two bands a CTA: chunk_b0 has nchunks + 1 entries
 };
 
 template <typename T, int NF>
@@ -309,13 +310,24 @@ constexpr size_t stage_elems(int mode, int ncol)
     return mode == PM_DENSITY ? ((size_t)ncol * sizeof(cx<T>) + 15) / 16 * 16 / sizeof(cx<T>) : 0;
 }
 
+// Bands one CTA of a plane pass takes together.  The V psi pass on grids up
+// to 64 takes two: a small plane has few y lines (11 at 64^3 for 32 line
+// groups), so with one band most warps wait at the barriers around its y
+// phases; two bands fill twice the groups and share each barrier (and each
+// V row).  At 128 the second band's line buffer would leave one CTA per SM.
+__host__ __device__ constexpr int plane_bands_per_cta(int NF, int mode)
+{
+    return (mode == PM_APPLYV && NF <= 64) ? 2 : 1;
+}
+
 template <typename T, int NF>
 size_t plane_smem_bytes(int mode, int KX, int ncol)
 {
     using S = PlaneShape<T, NF>;
     const int nt = plane_threads<T, NF>(mode);
-    const size_t ex_y = (size_t)S::y_groups(KX, nt / S::LY::P) * S::SY, ex_x = (size_t)(nt / S::LX::P) * S::SX;
-    size_t b = sizeof(cx<T>) * ((size_t)TwLayout<NF>::total + stage_elems<T>(mode, ncol) + (size_t)KX * S::YS +
+    const int lines = plane_bands_per_cta(NF, mode) * KX;
+    const size_t ex_y = (size_t)S::y_groups(lines, nt / S::LY::P) * S::SY, ex_x = (size_t)(nt / S::LX::P) * S::SX;
+    size_t b = sizeof(cx<T>) * ((size_t)TwLayout<NF>::total + stage_elems<T>(mode, ncol) + (size_t)lines * S::YS +
                                 (ex_y > ex_x ? ex_y : ex_x));
     return (b + 15) / 16 * 16;
 }
@@ -358,8 +370,9 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> twg)
     constexpr int RSPLIT = plane_row_split<NF, MODE, MINB>();
     constexpr bool STAGE = MODE == PM_DENSITY && RSPLIT == 1;
     cx<T> *stage = tws + TwLayout<NF>::total;                          // STAGE: one band's columns
-    cx<T> *Y = stage + stage_elems<T>(STAGE ? MODE : -1, g.ncol);  // [KX][YS]
-    cx<T> *xball = Y + KX * YS;                       // group exchange buffers
+    constexpr int BPC = plane_bands_per_cta(NF, MODE);
+    cx<T> *Y = stage + stage_elems<T>(STAGE ? MODE : -1, g.ncol);  // [BPC][KX][YS]
+    cx<T> *xball = Y + BPC * KX * YS;                               // group exchange buffers
     for (int i = threadIdx.x; i < TwLayout<NF>::total; i += NT) tws[i] = twg.n_inv[i];
     const Twiddles<T> tw = Twiddles<T>::template at<NF>(tws);
     __syncthreads();
@@ -371,8 +384,10 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> twg)
     double rho[(MODE == PM_DENSITY) ? NIT : 1][(MODE == PM_DENSITY) ? 2 * QX : 1];
 
     const int z = blockIdx.x;
-    const int b0 = (MODE == PM_DENSITY || MODE == PM_APPLYV) ? a.chunk_b0[blockIdx.y] : 0;
-    const int b1 = (MODE == PM_DENSITY || MODE == PM_APPLYV) ? a.chunk_b0[blockIdx.y + 1] : 1;
+    // this CTA's bands: chunk blockIdx.y, or chunks BPC y .. BPC y + BPC - 1
+    const int cb = (int)blockIdx.y * BPC, ce = (BPC > 1) ? min(cb + BPC, a.nchunks) : cb + 1;
+    const int b0 = (MODE == PM_DENSITY || MODE == PM_APPLYV) ? a.chunk_b0[cb] : 0;
+    const int b1 = (MODE == PM_DENSITY || MODE == PM_APPLYV) ? a.chunk_b0[ce] : 1;
     const long plane = (long)NF * NF;
 
     if constexpr (MODE == PM_DENSITY) {
@@ -383,7 +398,6 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> twg)
     }
 
     const int gy = threadIdx.x / PY, ty = threadIdx.x % PY;
-    const int ngy_act = S::y_groups(KX, NGY);  // warp-uniform: whole warps skip the y lines
     const int gx = threadIdx.x / PX, tx = threadIdx.x % PX;
     cx<T> *xby = xball + gy * S::SY;
     cx<T> *xbx = xball + gx * S::SX;
@@ -397,18 +411,25 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> twg)
         cp_async_commit_all();
     };
     if (STAGE && b0 < b1) prefetch(b0);
-    for (int b = b0; b < b1; ++b) {
-        cx<T> *Tplane = Tb + ((long)b * NF + z) * g.ncol;
-        const cx<T> *Tcol = STAGE ? stage : Tplane;
+    // bands b .. b + nbg - 1 together (nbg = 1 unless BPC > 1); line li of
+    // the group is line li % KX of band b + li / KX
+    for (int b = b0; b < b1; b += BPC) {
+        const int nbg = (BPC == 1) ? 1 : min(BPC, b1 - b);
+        const int nl = nbg * KX;
+        const int ngy_act = S::y_groups(nl, NGY);  // warp-uniform: whole warps skip the y lines
+        const cx<T> *Tcol = STAGE ? stage : Tb + ((long)b * NF + z) * g.ncol;
         if (STAGE) {
             cp_async_wait_all();
             __syncthreads();
         }
         // ---- inverse along y (columns -> lines kx < KX) ------------------
         if constexpr (MODE != PM_FWDREAL) {
-            for (int base = 0; base < KX && gy < ngy_act; base += NGY) {
-                const int i = base + gy;
-                const bool act = i < KX;
+            for (int base = 0; base < nl && gy < ngy_act; base += NGY) {
+                const int li = base + gy;
+                const bool act = li < nl;
+                const int kb = (BPC == 1 || !act) ? 0 : li / KX;
+                const int i = act ? li - kb * KX : 0;
+                const cx<T> *Tp = (BPC == 1) ? Tcol : Tb + ((long)(b + kb) * NF + z) * g.ncol;
                 cx<T> v[QY];
                 // the line's columns: arithmetic from its two runs (one small
                 // load per line), else the colidx table (one load per value).
@@ -421,151 +442,158 @@ plane_kernel(Geom g, cx<T> *__restrict__ Tb, PlaneArgs a, Twiddles<T> twg)
                     for (int m = 0; m < QY; ++m) {
                         const int y = LY::in_index(ty, m);
                         const int c = y < ra ? c0 + y : (y >= rb ? c0 + ra + (y - rb) : -1);
-                        v[m] = (c >= 0) ? Tplane[c] : cx<T>{0, 0};
+                        v[m] = (c >= 0) ? Tp[c] : cx<T>{0, 0};
                     }
                 } else {
 #pragma unroll
                     for (int m = 0; m < QY; ++m) {
                         const int c = act ? g.colidx[i * NF + LY::in_index(ty, m)] : -1;
-                        v[m] = (c >= 0) ? Tcol[c] : cx<T>{0, 0};
+                        v[m] = (c >= 0) ? Tp[c] : cx<T>{0, 0};
                     }
                 }
                 line_fft<NF, +1, T>(v, ty, xby, tw.n_inv);
                 if (act) {
+                    cx<T> *Yl = Y + (kb * KX + i) * YS;
 #pragma unroll
                     for (int u = 0; u < UY; ++u)
 #pragma unroll
-                        for (int s = 0; s < PY; ++s) Y[i * YS + S::ymap(LY::out_index(ty, u, s))] = v[u * PY + s];
+                        for (int s = 0; s < PY; ++s) Yl[S::ymap(LY::out_index(ty, u, s))] = v[u * PY + s];
                 }
             }
             __syncthreads();
             if (STAGE && b + 1 < b1) prefetch(b + 1);
         }
         // ---- x rows --------------------------------------------------------
+        for (int kb = 0; kb < nbg; ++kb) {
+            cx<T> *Yb = Y + kb * KX * YS;
 #pragma unroll
-        for (int it = 0; it < NIT; ++it) {
-            const int j = (it0 + it) * NGX + gx;
-            const bool act = j < NF;
-            const int jj = act ? j : 0;
-            cx<T> v[QX];
-            if constexpr (MODE != PM_FWDREAL) {
-                // c2r pre-processing: Z_k = E_k + i O_k (half-length packing)
+            for (int it = 0; it < NIT; ++it) {
+                const int j = (it0 + it) * NGX + gx;
+                const bool act = j < NF;
+                const int jj = act ? j : 0;
+                cx<T> v[QX];
+                if constexpr (MODE != PM_FWDREAL) {
+                    // c2r pre-processing: Z_k = E_k + i O_k (half-length packing)
 #pragma unroll
-                for (int m = 0; m < QX; ++m) {
-                    const int k = LX::in_index(tx, m);
-                    const int kk = H - k;
-                    cx<T> xa = (k < KX) ? Y[k * YS + S::ymap(jj)] : cx<T>{0, 0};
-                    cx<T> xc = (kk < KX) ? Y[kk * YS + S::ymap(jj)] : cx<T>{0, 0};
-                    if (k == 0) {
-                        xa.y = 0;
-                        xc.y = 0;
+                    for (int m = 0; m < QX; ++m) {
+                        const int k = LX::in_index(tx, m);
+                        const int kk = H - k;
+                        cx<T> xa = (k < KX) ? Yb[k * YS + S::ymap(jj)] : cx<T>{0, 0};
+                        cx<T> xc = (kk < KX) ? Yb[kk * YS + S::ymap(jj)] : cx<T>{0, 0};
+                        if (k == 0) {
+                            xa.y = 0;
+                            xc.y = 0;
+                        }
+                        cx<T> E = xa + conj(xc);
+                        cx<T> O = cmul(xa - conj(xc), tw.r_inv[k]);
+                        v[m] = cx<T>{E.x - O.y, E.y + O.x};
                     }
-                    cx<T> E = xa + conj(xc);
-                    cx<T> O = cmul(xa - conj(xc), tw.r_inv[k]);
-                    v[m] = cx<T>{E.x - O.y, E.y + O.x};
-                }
-                line_fft<H, +1, T>(v, tx, xbx, tw.h_inv);
-                // v[u*PX+s] = (psi(2m), psi(2m+1)), m = out_index
-                if constexpr (MODE == PM_DENSITY) {
+                    line_fft<H, +1, T>(v, tx, xbx, tw.h_inv);
+                    // v[u*PX+s] = (psi(2m), psi(2m+1)), m = out_index
+                    if constexpr (MODE == PM_DENSITY) {
 #pragma unroll
-                    for (int q = 0; q < QX; ++q) {
-                        const cx<T> w = v[q];
-                        rho[it][2 * q] += (double)w.x * (double)w.x;
-                        rho[it][2 * q + 1] += (double)w.y * (double)w.y;
-                    }
-                } else if constexpr (MODE == PM_INVREAL) {
-                    if (act) {
+                        for (int q = 0; q < QX; ++q) {
+                            const cx<T> w = v[q];
+                            rho[it][2 * q] += (double)w.x * (double)w.x;
+                            rho[it][2 * q + 1] += (double)w.y * (double)w.y;
+                        }
+                    } else if constexpr (MODE == PM_INVREAL) {
+                        if (act) {
+#pragma unroll
+                            for (int u = 0; u < UX; ++u)
+#pragma unroll
+                                for (int s = 0; s < PX; ++s) {
+                                    const int m = LX::out_index(tx, u, s);
+                                    cx<T> w = v[u * PX + s];
+                                    const long o = (long)z * plane + (long)j * NF + 2 * m;
+                                    for (int ms = 0; ms < a.nout; ++ms) {
+                                        double *ro = a.rout + ms * NF * plane;
+                                        if (a.xadd) {
+                                            const double *xa = a.xadd + ms * NF * plane;
+                                            ro[o] = (double)w.x + xa[o];
+                                            ro[o + 1] = (double)w.y + xa[o + 1];
+                                        } else {
+                                            ro[o] = (double)w.x;
+                                            ro[o + 1] = (double)w.y;
+                                        }
+                                    }
+                                }
+                        }
+                    } else {  // APPLYV: multiply in place; the DIF forward takes this distribution
+                        const double *V = a.V + ((b + kb >= a.ne0) ? NF * plane : 0);
 #pragma unroll
                         for (int u = 0; u < UX; ++u)
 #pragma unroll
                             for (int s = 0; s < PX; ++s) {
                                 const int m = LX::out_index(tx, u, s);
-                                cx<T> w = v[u * PX + s];
-                                const long o = (long)z * plane + (long)j * NF + 2 * m;
-                                for (int ms = 0; ms < a.nout; ++ms) {
-                                    double *ro = a.rout + ms * NF * plane;
-                                    if (a.xadd) {
-                                        const double *xa = a.xadd + ms * NF * plane;
-                                        ro[o] = (double)w.x + xa[o];
-                                        ro[o + 1] = (double)w.y + xa[o + 1];
-                                    } else {
-                                        ro[o] = (double)w.x;
-                                        ro[o + 1] = (double)w.y;
-                                    }
-                                }
+                                const long o = (long)z * plane + (long)jj * NF + 2 * m;
+                                const double2 vv = *reinterpret_cast<const double2 *>(V + o);
+                                cx<T> &w = v[u * PX + s];
+                                w = cx<T>{(T)((double)w.x * vv.x), (T)((double)w.y * vv.y)};
                             }
                     }
-                } else {  // APPLYV: multiply in place; the DIF forward takes this distribution
-                    const double *V = a.V + ((b >= a.ne0) ? NF * plane : 0);
+                } else {  // FWDREAL: load the real row directly in DIT order
+                    const double *r = a.rin + (long)z * plane + (long)jj * NF;
+#pragma unroll
+                    for (int m = 0; m < QX; ++m) {
+                        const int mm = LX::in_index(tx, m);
+                        v[m] = cx<T>{(T)r[2 * mm], (T)r[2 * mm + 1]};
+                    }
+                }
+                if constexpr (MODE == PM_APPLYV) {
+                    line_fft_dif<H, -1, T>(v, tx, xbx, tw.h_fwd_dif);
+#pragma unroll
+                    for (int m = 0; m < QX; ++m) xbx[LX::in_index(tx, m)] = v[m];
+                    __syncwarp();
+                }
+                if constexpr (MODE == PM_FWDREAL) {
+                    line_fft<H, -1, T>(v, tx, xbx, tw.h_fwd);
 #pragma unroll
                     for (int u = 0; u < UX; ++u)
 #pragma unroll
-                        for (int s = 0; s < PX; ++s) {
-                            const int m = LX::out_index(tx, u, s);
-                            const long o = (long)z * plane + (long)jj * NF + 2 * m;
-                            const double2 vv = *reinterpret_cast<const double2 *>(V + o);
-                            cx<T> &w = v[u * PX + s];
-                            w = cx<T>{(T)((double)w.x * vv.x), (T)((double)w.y * vv.y)};
-                        }
+                        for (int s = 0; s < PX; ++s) xbx[LX::out_index(tx, u, s)] = v[u * PX + s];
+                    __syncwarp();
                 }
-            } else {  // FWDREAL: load the real row directly in DIT order
-                const double *r = a.rin + (long)z * plane + (long)jj * NF;
-#pragma unroll
-                for (int m = 0; m < QX; ++m) {
-                    const int mm = LX::in_index(tx, m);
-                    v[m] = cx<T>{(T)r[2 * mm], (T)r[2 * mm + 1]};
+                if constexpr (MODE == PM_APPLYV || MODE == PM_FWDREAL) {
+                    // r2c post-processing for the kx < KX that are kept
+                    for (int k = tx; k < KX; k += PX) {
+                        cx<T> zk = xbx[k % H];
+                        cx<T> zc = conj(xbx[(H - k) % H]);
+                        cx<T> E = (T)0.5 * (zk + zc);
+                        cx<T> D = (T)0.5 * (zk - zc);
+                        cx<T> O{D.y, -D.x};
+                        cx<T> X = E + cmul(tw.r_fwd[k], O);
+                        if (k == 0 || k == H) X.y = 0;
+                        if (act) Yb[k * YS + S::ymap(j)] = X;
+                    }
+                    __syncwarp();
                 }
-            }
-            if constexpr (MODE == PM_APPLYV) {
-                line_fft_dif<H, -1, T>(v, tx, xbx, tw.h_fwd_dif);
-#pragma unroll
-                for (int m = 0; m < QX; ++m) xbx[LX::in_index(tx, m)] = v[m];
-                __syncwarp();
-            }
-            if constexpr (MODE == PM_FWDREAL) {
-                line_fft<H, -1, T>(v, tx, xbx, tw.h_fwd);
-#pragma unroll
-                for (int u = 0; u < UX; ++u)
-#pragma unroll
-                    for (int s = 0; s < PX; ++s) xbx[LX::out_index(tx, u, s)] = v[u * PX + s];
-                __syncwarp();
-            }
-            if constexpr (MODE == PM_APPLYV || MODE == PM_FWDREAL) {
-                // r2c post-processing for the kx < KX that are kept
-                for (int k = tx; k < KX; k += PX) {
-                    cx<T> zk = xbx[k % H];
-                    cx<T> zc = conj(xbx[(H - k) % H]);
-                    cx<T> E = (T)0.5 * (zk + zc);
-                    cx<T> D = (T)0.5 * (zk - zc);
-                    cx<T> O{D.y, -D.x};
-                    cx<T> X = E + cmul(tw.r_fwd[k], O);
-                    if (k == 0 || k == H) X.y = 0;
-                    if (act) Y[k * YS + S::ymap(j)] = X;
-                }
-                __syncwarp();
             }
         }
         __syncthreads();
         // ---- forward along y, keep the columns -----------------------------
         if constexpr (MODE == PM_APPLYV || MODE == PM_FWDREAL) {
-            for (int base = 0; base < KX && gy < ngy_act; base += NGY) {
-                const int i = base + gy;
-                const bool act = i < KX;
-                const int ii = act ? i : 0;
+            for (int base = 0; base < nl && gy < ngy_act; base += NGY) {
+                const int li = base + gy;
+                const bool act = li < nl;
+                const int lii = act ? li : 0;  // line kb * KX + i of Y
                 cx<T> v[QY];
 #pragma unroll
-                for (int m = 0; m < QY; ++m) v[m] = Y[ii * YS + S::ymap(LY::in_index(ty, m))];
+                for (int m = 0; m < QY; ++m) v[m] = Y[lii * YS + S::ymap(LY::in_index(ty, m))];
                 line_fft<NF, -1, T>(v, ty, xby, tw.n_fwd);
                 // each group reads and rewrites only its own line
                 if (act) {
 #pragma unroll
                     for (int u = 0; u < UY; ++u)
 #pragma unroll
-                        for (int s = 0; s < PY; ++s) Y[i * YS + S::ymap(LY::out_index(ty, u, s))] = v[u * PY + s];
+                        for (int s = 0; s < PY; ++s) Y[li * YS + S::ymap(LY::out_index(ty, u, s))] = v[u * PY + s];
                 }
             }
             __syncthreads();
-            for (int c = threadIdx.x; c < g.ncol; c += NT) Tplane[c] = Y[g.col_i[c] * YS + S::ymap(g.col_j[c])];
+            for (int c = threadIdx.x; c < g.ncol; c += NT) {
+                const int yo = g.col_i[c] * YS + S::ymap(g.col_j[c]);
+                for (int kb = 0; kb < nbg; ++kb) Tb[((long)(b + kb) * NF + z) * g.ncol + c] = Y[kb * KX * YS + yo];
+            }
             __syncthreads();
         }
     }
