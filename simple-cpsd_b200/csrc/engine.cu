@@ -486,6 +486,11 @@ struct cpsd_gpu_ctx {
     // energies run; get_state_host then only waits for ev_fetch
     bool early_fetch = false, fetched = false;
     cudaEvent_t ev_steps = nullptr, ev_fetch = nullptr;
+    // the density of a call's last step is final once its density pass has
+    // run: ev_dn is recorded there (in the last step of each captured graph)
+    // so that its copy to the host can start during the rest of the step
+    cudaEvent_t ev_dn = nullptr;
+    bool rec_dn = false;
     cudaStream_t cs = nullptr;  // the stream the GEMM helpers launch on
     bool lag_tile = false;  // 4 x 4 tiled solver (<= 128 bands, 16-CTA clusters schedulable)
     bool lag_tile_ok = false;  // the tiled solver can run on this device for these bands
@@ -848,6 +853,15 @@ int step_phase(cpsd_gpu_ctx *c, int phase)
             return CPSD_OK;
         }
         density_xc_kernel<<<(unsigned)cdiv(c->n3, 256), 256, 0, s>>>(xa); c->nlaunch += 1;
+        if (c->rec_dn) {
+            // while capturing, an external record: a plain one would only be a
+            // dependency inside the graph, invisible to a wait outside it (the
+            // flag is refused outside a capture)
+            cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+            CK(cudaStreamIsCapturing(s, &cap));
+            CK(cap == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(c->ev_dn, s, cudaEventRecordExternal)
+                                                    : cudaEventRecord(c->ev_dn, s));
+        }
         mark(c, 3);
         return CPSD_OK;
     }
@@ -1104,10 +1118,15 @@ constexpr size_t kMultiGraphs = 4;
 int run_steps(cpsd_gpu_ctx *c, int inner)
 {
     if (!c->use_graph || c->phase_timing) {
+        c->rec_dn = true;
         for (int it = 0; it < inner; ++it) {
             int rc = run_step(c);
-            if (rc) return rc;
+            if (rc) {
+                c->rec_dn = false;
+                return rc;
+            }
         }
+        c->rec_dn = false;
         return CPSD_OK;
     }
     while (inner > 0) {
@@ -1121,7 +1140,11 @@ int run_steps(cpsd_gpu_ctx *c, int inner)
             const long long before = c->nlaunch;
             CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
             int rc = CPSD_OK;
-            for (int it = 0; it < k && !rc; ++it) rc = one_step(c);
+            for (int it = 0; it < k && !rc; ++it) {
+                c->rec_dn = it == k - 1;  // one record of ev_dn per graph, in its last step
+                rc = one_step(c);
+            }
+            c->rec_dn = false;
             cudaError_t e = cudaStreamEndCapture(c->st, &g);
             c->cur = par;  // capture launched nothing: undo the buffer flips
             const int launches = (int)(c->nlaunch - before);
@@ -1833,6 +1856,7 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c->ev_sf, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c->ev_side, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_dn, cudaEventDisableTiming));
     c->cs = c->st;
     // the fused density plane must fit in shared memory
     int optin = 0;
@@ -2267,12 +2291,15 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
             CK(cudaEventCreateWithFlags(&c->ev_steps, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&c->ev_fetch, cudaEventDisableTiming));
         }
+        // the density as soon as the last step's density pass is done, the
+        // orbitals once the steps are
+        CK(cudaStreamWaitEvent(c->st2, c->ev_dn, 0));
+        CK(cudaMemcpyAsync(c->dstage.p, c->dn, sizeof(double) * c->ispin * c->n3, cudaMemcpyDeviceToHost, c->st2));
         CK(cudaEventRecord(c->ev_steps, s));
         CK(cudaStreamWaitEvent(c->st2, c->ev_steps, 0));
         CK(cudaMemcpyAsync(c->hstage.p, c->cbuf[c->cur], pb, cudaMemcpyDeviceToHost, c->st2));
         CK(cudaMemcpyAsync(c->hstage.p + (long)c->nb * c->ldc, c->cbuf[c->cur ^ 1], pb, cudaMemcpyDeviceToHost,
                            c->st2));
-        CK(cudaMemcpyAsync(c->dstage.p, c->dn, sizeof(double) * c->ispin * c->n3, cudaMemcpyDeviceToHost, c->st2));
         CK(cudaEventRecord(c->ev_fetch, c->st2));
         c->d2h += 2LL * (long long)pb + (long long)sizeof(double) * c->ispin * c->n3;
         c->fetched = true;
@@ -3099,7 +3126,7 @@ void cpsd_gpu_destroy(cpsd_gpu_ctx *c)
         if (e) cudaEventDestroy(e);
     c->ar.release();
     if (c->st2) cudaStreamSynchronize(c->st2);
-    for (cudaEvent_t e : {c->ev_fork, c->ev_sf, c->ev_side, c->ev_steps, c->ev_fetch})
+    for (cudaEvent_t e : {c->ev_fork, c->ev_sf, c->ev_side, c->ev_steps, c->ev_fetch, c->ev_dn})
         if (e) cudaEventDestroy(e);
     if (c->st2) cudaStreamDestroy(c->st2);
     if (c->st) cudaStreamDestroy(c->st);
