@@ -1542,7 +1542,7 @@ int get_state_host(cpsd_gpu_ctx *c, double *c1, double *c2, double *cpsi, double
     CK(cudaStreamSynchronize(s));
     if (dn) {  // [ms][z][y][x] -> the reference's [ms][z][y][x(n+2)], pads zero (cpsd.c:185-194)
         const int n = c->n;
-        const long lines = (long)c->ispin * n * n, per = 1024;
+        const long lines = (long)c->ispin * n * n, per = 128;  // enough items for every host thread
         pool.run((int)cdiv(lines, per), [&](int t) {
             for (long l = t * per; l < std::min(lines, (t + 1) * per); ++l) {
                 memcpy(dn + l * (n + 2), dst + l * n, sizeof(double) * n);
@@ -2291,15 +2291,15 @@ int cpsd_gpu_run(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae
             CK(cudaEventCreateWithFlags(&c->ev_steps, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&c->ev_fetch, cudaEventDisableTiming));
         }
-        // the density as soon as the last step's density pass is done, the
-        // orbitals once the steps are
+        // the density and c1 (the last step's input orbitals) as soon as the
+        // last step's density pass is done, c2 once the steps are
         CK(cudaStreamWaitEvent(c->st2, c->ev_dn, 0));
         CK(cudaMemcpyAsync(c->dstage.p, c->dn, sizeof(double) * c->ispin * c->n3, cudaMemcpyDeviceToHost, c->st2));
+        CK(cudaMemcpyAsync(c->hstage.p + (long)c->nb * c->ldc, c->cbuf[c->cur ^ 1], pb, cudaMemcpyDeviceToHost,
+                           c->st2));
         CK(cudaEventRecord(c->ev_steps, s));
         CK(cudaStreamWaitEvent(c->st2, c->ev_steps, 0));
         CK(cudaMemcpyAsync(c->hstage.p, c->cbuf[c->cur], pb, cudaMemcpyDeviceToHost, c->st2));
-        CK(cudaMemcpyAsync(c->hstage.p + (long)c->nb * c->ldc, c->cbuf[c->cur ^ 1], pb, cudaMemcpyDeviceToHost,
-                           c->st2));
         CK(cudaEventRecord(c->ev_fetch, c->st2));
         c->d2h += 2LL * (long long)pb + (long long)sizeof(double) * c->ispin * c->n3;
         c->fetched = true;
