@@ -18,7 +18,7 @@ LIBDIR = os.path.join(PKG_ROOT, "lib")
 LIB = os.path.join(LIBDIR, "libcpsd_b200.so")
 
 SOURCES = ["engine.cu", "capi.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "host_pool.h", "kernels.cuh", "mlp.cuh", "pipeline.cuh", "tc_gemm.cuh"]
+HEADERS = ["common.cuh", "dropin.h", "fft.cuh", "host_pool.h", "kernels.cuh", "mlp.cuh", "pipeline.cuh", "tc_gemm.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "cpsd_b200.h"
 #include "fft.cuh"
+#include "dropin.h"
 #include "host_pool.h"
 #include "pipeline.cuh"
 
@@ -53,20 +54,6 @@ Signature g_sig;
 
 }  // namespace
 
-// engine.cu: the drop-in's state upload, steps and host-layout outputs, with
-// the check that c2 is zero outside the sphere overlapping the steps.
-int cpsd_dropin_state_run_fetch(cpsd_gpu_ctx *c, const double *r2in, int inner, int move, double *E,
-                                double *deltae, double *deltac, double *deltar, double *c1, double *c2,
-                                double *cpsi, double *dn, double *hml, double *lmd, double *r1, double *r2,
-                                double *fion);
-
-// engine.cu: cpsd_gpu_run, then the host-layout outputs, with c1 and cpsi
-// zeroed on host threads during the run (c2 must have just gone through
-// cpsd_gpu_set_state).
-int cpsd_dropin_run_fetch(cpsd_gpu_ctx *c, int inner, int move, double *E, double *deltae, double *deltac,
-                          double *deltar, double *c1, double *c2, double *cpsi, double *dn, double *hml,
-                          double *lmd, double *r1, double *r2, double *fion);
-
 extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, const int ispin, const int *ne,
                              const int nfft, const int nfft3d, const int n2ft3d, const double *unitg,
                              const double omega, const double dt, const double fmass, const int *katm,
@@ -93,6 +80,19 @@ extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, co
     cudaGetDevice(&sig.device);
 
     std::lock_guard<std::mutex> lk(g_mu);
+    if (g_ctx && sig.same_shape(g_sig)) {
+        // a driver's loop passes the same mask and tables every call
+        // (main.c:422-426): run on the context's, and check them on host
+        // threads beside the steps; a mismatch discards the run and takes
+        // the full path below
+        int rc = cpsd_gpu_set_scalars(g_ctx, unitg, omega, dt, fmass, cewald, rcut);
+        if (rc) return rc;
+        const DropinCheck check{masker, g_sig.masker.data(), g_sig.masker.size(),
+                                TableArgs{katm, amass, zv, rcell, G, tg, vc, vg, lmmax, vnlnrm, vl, vnl}};
+        rc = cpsd_dropin_state_run_fetch(g_ctx, r2, inner, move, E, deltae, deltac, deltar, c1, c2, cpsi, dn, hml,
+                                         lmd, r1, r2, fion, &check);
+        if (rc != kDropinRedo) return rc;
+    }
     if (!g_ctx || !sig.same_shape(g_sig) || !g_sig.same_mask(masker, nfft3d)) {
         sig.masker1.resize(nfft3d);
         for (int k = 0; k < nfft3d; ++k) sig.masker1[k] = masker[2 * k];
@@ -126,7 +126,7 @@ extern "C" int cpsd_gpu_cpsd(const int inner, const int move, const int nion, co
     rc = cpsd_gpu_set_tables(c, katm, amass, zv, rcell, G, tg, vc, vg, lmmax, vnlnrm, vl, vnl);
     if (rc) return rc;
     return cpsd_dropin_state_run_fetch(c, r2, inner, move, E, deltae, deltac, deltar, c1, c2, cpsi, dn, hml, lmd,
-                                       r1, r2, fion);
+                                       r1, r2, fion, nullptr);
 }
 
 extern "C" cpsd_gpu_ctx *cpsd_gpu_dropin_context(void)

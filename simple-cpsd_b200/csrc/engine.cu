@@ -21,6 +21,7 @@
 #include "common.cuh"
 #include "cpsd_b200.h"
 #include "fft.cuh"
+#include "dropin.h"
 #include "host_pool.h"
 #include "kernels.cuh"
 #include "mlp.cuh"
@@ -1393,6 +1394,132 @@ long grid_slices(const cpsd_gpu_ctx *c)
     return std::max<long>(1, cdiv(c->nfft3d * (long)sizeof(cx<double>), 512L << 10));
 }
 
+// The packed form of the tables (TableArgs, dropin.h): the sphere's values
+// in one staging buffer, slices 16-byte aligned in a fixed order.
+struct TablePack {
+    double *tg, *vc, *vg, *vl, *vnl, *zv, *ug, *rc, *n, *g;
+    int *sh, *lm, *k, *o;
+    size_t bytes;  // of the buffer used
+    int np;        // projectors
+    bool motion;   // G vectors and masses given
+    double tmax;
+};
+
+// Checks the arguments and packs the tables into base (cap bytes): the
+// gathers in the grids' memory order (pt_ord), on the host threads when
+// threads is set (each table an item), else on the calling thread.
+int pack_tables(const cpsd_gpu_ctx *c, const TableArgs &t, char *base, size_t cap, bool threads, TablePack *pk)
+{
+    if (!t.zv || !t.tg || !t.vc || !t.vg || !t.lmmax || !t.vnlnrm || !t.vl || !t.vnl) return CPSD_ERR_ARG;
+    if (c->nion > 0 && (!t.katm || !t.rcell)) return CPSD_ERR_ARG;
+    const HostGeom &h = c->hg;
+    const int nkatm = c->nkatm;
+    for (int ia = 0; ia < nkatm; ++ia)
+        if (t.lmmax[ia] < 0 || t.lmmax[ia] > 9) return CPSD_ERR_ARG;
+    std::vector<int> off(std::max(c->nion, 1), 0), hk(std::max(c->nion, 1), 0);
+    int np = 0;
+    for (int ii = 0; ii < c->nion; ++ii) {
+        const int ia = t.katm[ii];
+        if (ia < 0 || ia >= nkatm) return CPSD_ERR_ARG;
+        hk[ii] = ia;
+        off[ii] = np;
+        np += t.lmmax[ia];
+    }
+    const bool motion = t.G && t.amass && c->nion > 0;
+    if (motion)
+        for (int ia = 0; ia < nkatm; ++ia)
+            if (!(t.amass[ia] > 0)) return CPSD_ERR_ARG;
+    Stager sg{base, cap, nullptr};
+    const int npw = c->npw, npw_pad = c->npw_pad;
+    const int *pt = h.pt_idx.data();
+    TablePack &p = *pk;
+    p.tg = sg.slice<double>(npw_pad);
+    p.vc = sg.slice<double>(npw_pad);
+    p.vg = sg.slice<double>(npw_pad);
+    p.sh = sg.slice<int>(npw_pad);
+    p.vl = sg.slice<double>((size_t)nkatm * npw);
+    p.vnl = sg.slice<double>((size_t)nkatm * 9 * npw);
+    p.zv = sg.slice<double>(nkatm);
+    p.ug = sg.slice<double>(9);
+    p.rc = sg.slice<double>(3 * c->nsh);
+    p.lm = sg.slice<int>(nkatm);
+    p.k = sg.slice<int>(c->nion);
+    p.o = sg.slice<int>(c->nion);
+    p.n = sg.slice<double>(np);
+    p.g = sg.slice<double>(motion ? (size_t)3 * npw : 0);
+    if (!sg.ok()) return CPSD_ERR_ARG;  // more kinds / ions than the context was created for
+    p.bytes = sg.off;
+    p.np = np;
+    p.motion = motion;
+    const int *ord = h.pt_ord.data();
+    for (int q = npw; q < npw_pad; ++q) p.tg[q] = p.vc[q] = p.vg[q] = 0.0;
+    const int ntab = 3 + nkatm * 10 + (motion ? 3 : 0);
+    auto gather = [&](int i) {
+        const double *src;
+        double *d;
+        if (i < 3) {
+            src = i == 0 ? t.tg : (i == 1 ? t.vc : t.vg);
+            d = i == 0 ? p.tg : (i == 1 ? p.vc : p.vg);
+        } else if (i < 3 + nkatm * 10) {
+            const int ia = (i - 3) / 10, l = (i - 3) % 10;  // l = 0: vl, else vnl channel l - 1
+            if (l == 0) {
+                src = t.vl + (size_t)ia * c->nfft3d;
+                d = p.vl + (size_t)ia * npw;
+            } else {
+                d = p.vnl + ((size_t)ia * 9 + l - 1) * npw;
+                if (l - 1 >= t.lmmax[ia]) {
+                    memset(d, 0, sizeof(double) * npw);
+                    return;
+                }
+                src = t.vnl + ((size_t)ia * 9 + l - 1) * c->nfft3d;
+            }
+        } else {
+            const int dd = i - 3 - nkatm * 10;
+            src = t.G + (size_t)dd * c->nfft3d;
+            d = p.g + (size_t)dd * npw;
+        }
+        for (int q = 0; q < npw; ++q) {
+            const int pp = ord[q];
+            d[pp] = src[pt[pp]];
+        }
+    };
+    if (threads)
+        cpsd_host::Pool::get().run(ntab, gather);
+    else
+        for (int i = 0; i < ntab; ++i) gather(i);
+    double tmax = 0.0;
+    for (int q = 0; q < npw; ++q) tmax = std::max(tmax, p.tg[q]);
+    p.tmax = tmax > 0 ? tmax : 1.0;
+    for (int q = 0; q < npw_pad; ++q) p.sh[q] = q < npw ? std::min(kShells - 1, (int)(p.tg[q] / p.tmax * kShells)) : 0;
+    memcpy(p.zv, t.zv, sizeof(double) * nkatm);
+    memcpy(p.ug, c->prm.unitg, sizeof(double) * 9);
+    if (c->nsh > 0) memcpy(p.rc, t.rcell, sizeof(double) * 3 * c->nsh);
+    memcpy(p.lm, t.lmmax, sizeof(int) * nkatm);
+    if (c->nion > 0) {
+        memcpy(p.k, hk.data(), sizeof(int) * c->nion);
+        memcpy(p.o, off.data(), sizeof(int) * c->nion);
+    }
+    for (int ii = 0, q = 0; ii < c->nion; ++ii)
+        for (int l = 0; l < t.lmmax[hk[ii]]; ++l) p.n[q++] = t.vnlnrm[hk[ii] * 9 + l];
+    return CPSD_OK;
+}
+
+// Whether tables passed now equal the ones the device holds (the packed
+// bytes of the last upload, the masses kept on the host): packed into
+// scratch on the calling thread.
+bool tables_current(const cpsd_gpu_ctx *c, const TableArgs &t, std::vector<char> &scratch)
+{
+    if (!c->tables_ok || c->tables_last.empty()) return false;
+    scratch.resize(c->tstage_bytes);
+    TablePack pk{};
+    if (pack_tables(c, t, scratch.data(), scratch.size(), false, &pk)) return false;
+    if (pk.np != c->nproj || pk.motion != c->motion_ok) return false;
+    if (pk.motion && (c->amass_h.size() != (size_t)c->nkatm ||
+                      memcmp(c->amass_h.data(), t.amass, sizeof(double) * c->nkatm)))
+        return false;
+    return pk.bytes == c->tables_last.size() && !memcmp(scratch.data(), c->tables_last.data(), pk.bytes);
+}
+
 // c->hstage[b][p] = full[b][pt_idx[p]], zero past npw; returns the number of
 // nonzero points outside the sphere.
 long host_gather(cpsd_gpu_ctx *c, const double *full)
@@ -1625,7 +1752,7 @@ int cpsd_dropin_run_fetch(cpsd_gpu_ctx *c, int inner, int move, double *E, doubl
 int cpsd_dropin_state_run_fetch(cpsd_gpu_ctx *c, const double *r2in, int inner, int move, double *E,
                                 double *deltae, double *deltac, double *deltar, double *c1, double *c2,
                                 double *cpsi, double *dn, double *hml, double *lmd, double *r1, double *r2,
-                                double *fion)
+                                double *fion, const DropinCheck *check)
 {
     if (!c || !c2 || (c->nion > 0 && !r2in)) return CPSD_ERR_ARG;
     const size_t gb = sizeof(double) * c->nb * c->n2ft3d;
@@ -1633,6 +1760,7 @@ int cpsd_dropin_state_run_fetch(cpsd_gpu_ctx *c, const double *r2in, int inner, 
         return !x || !y || (const char *)x + gb <= (const char *)y || (const char *)y + gb <= (const char *)x;
     };
     if (!(apart(c1, c2) && apart(cpsi, c2) && apart(c1, cpsi))) {
+        if (check) return kDropinRedo;  // the serial path checks first: no speculation
         const int rc = cpsd_gpu_set_state(c, c2, r2in);
         if (rc) return rc;
         return cpsd_dropin_run_fetch(c, inner, move, E, deltae, deltac, deltar, c1, c2, cpsi, dn, hml, lmd, r1,
@@ -1647,28 +1775,40 @@ int cpsd_dropin_state_run_fetch(cpsd_gpu_ctx *c, const double *r2in, int inner, 
     if (c->nion > 0) CK(cudaMemcpyAsync(c->r2, r2in, sizeof(double) * 3 * c->nion, cudaMemcpyHostToDevice, s));
     c->h2d += (long long)pb + (long long)sizeof(double) * 3 * c->nion;
     c->state_ok = true;
-    // items [0, nv): the check of c2; [nv, nv + nz): the zeroing of c1 and
-    // cpsi, each of which first waits for the whole check (the items are
-    // claimed in order, so every check item is running or done by then)
+    // items [0, ns): the DropinCheck (mask and tables, one item); [ns, ns +
+    // nv): the check of c2; then the zeroing of c1 and cpsi, each of which
+    // first waits for every check (the items are claimed in order, so every
+    // check item is running or done by then) and is skipped after a failed
+    // one, so that a refused or redone call leaves the outputs untouched
     const long S = grid_slices(c);
-    const int nv = (int)(c->nb * S);
+    const int ns = check ? 1 : 0, nv = (int)(c->nb * S);
     std::vector<double *> zero;
     if (c1) zero.push_back(c1);
     if (cpsi) zero.push_back(cpsi);
     int nz = 0;
     auto ztask = zero.empty() ? std::function<void(int)>() : zero_grids_task(c, zero, &nz);
     std::atomic<long> bad{0};
-    std::atomic<int> checked{0};
+    std::atomic<int> checked{0}, stale{0};
+    std::vector<char> scratch;
     auto &pool = cpsd_host::Pool::get();
-    pool.start(nv + nz, [&](int t) {
+    pool.start(ns + nv + nz, [&](int t) {
+        if (t < ns) {
+            const bool same = check->masker_n == (size_t)2 * c->nfft3d &&
+                              !memcmp(check->masker, check->masker_ref, sizeof(int) * check->masker_n) &&
+                              tables_current(c, check->tables, scratch);
+            if (!same) stale = 1;
+            checked.fetch_add(1, std::memory_order_release);
+            return;
+        }
+        t -= ns;
         if (t < nv) {
             const long n = count_outside(c, c2, t);
             if (n) bad += n;
             checked.fetch_add(1, std::memory_order_release);
             return;
         }
-        while (checked.load(std::memory_order_acquire) < nv) std::this_thread::yield();
-        if (bad.load() == 0) ztask(t - nv);
+        while (checked.load(std::memory_order_acquire) < ns + nv) std::this_thread::yield();
+        if (bad.load() == 0 && stale.load() == 0) ztask(t - nv);
     });
     // the energies go to the caller only once the check has passed (E[0]
     // comes in as the previous call's energy, for deltae)
@@ -1678,11 +1818,15 @@ int cpsd_dropin_state_run_fetch(cpsd_gpu_ctx *c, const double *r2in, int inner, 
     const int run = cpsd_gpu_run(c, inner, move, Et, &dt3[0], &dt3[1], &dt3[2]);
     c->early_fetch = false;
     pool.wait();
-    if (bad.load() || (run != CPSD_OK && run != CPSD_WARN_LAGRANGE)) {
+    if (stale.load() || bad.load() || (run != CPSD_OK && run != CPSD_WARN_LAGRANGE)) {
         if (c->fetched) {  // the staging is free again only once those copies are done
             CK(cudaEventSynchronize(c->ev_fetch));
             c->fetched = false;
         }
+    }
+    if (stale.load()) {  // the steps ran on another mask or other tables: discarded
+        c->state_ok = false;
+        return kDropinRedo;
     }
     if (bad.load()) {
         c->state_ok = false;
@@ -2111,26 +2255,16 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
                         const double *vg, const int *lmmax, const double *vnlnrm, const double *vl,
                         const double *vnl)
 {
-    if (!c || !zv || !tg || !vc || !vg || !lmmax || !vnlnrm || !vl || !vnl) return CPSD_ERR_ARG;
-    if (c->nion > 0 && (!katm || !rcell)) return CPSD_ERR_ARG;
+    if (!c) return CPSD_ERR_ARG;
+    const TableArgs t{katm, amass, zv, rcell, G, tg, vc, vg, lmmax, vnlnrm, vl, vnl};
     CK(cudaSetDevice(c->prm.device));
-    const HostGeom &h = c->hg;
-    const int nkatm = c->nkatm;
-    for (int ia = 0; ia < nkatm; ++ia)
-        if (lmmax[ia] < 0 || lmmax[ia] > 9) return CPSD_ERR_ARG;
-    std::vector<int> off(std::max(c->nion, 1), 0), hk(std::max(c->nion, 1), 0);
-    int np = 0;
-    for (int ii = 0; ii < c->nion; ++ii) {
-        const int ia = katm[ii];
-        if (ia < 0 || ia >= nkatm) return CPSD_ERR_ARG;
-        hk[ii] = ia;
-        off[ii] = np;
-        np += lmmax[ia];
-    }
-    const bool motion = G && amass && c->nion > 0;
-    if (motion)
-        for (int ia = 0; ia < nkatm; ++ia)
-            if (!(amass[ia] > 0)) return CPSD_ERR_ARG;
+    // pack into pinned staging (the previous upload from it has finished
+    // once the stream is idle), then one asynchronous copy per table
+    CK(cudaStreamSynchronize(c->st));
+    TablePack pk{};
+    int rc = pack_tables(c, t, reinterpret_cast<char *>(c->tstage.p), c->tstage_bytes, true, &pk);
+    if (rc) return rc;
+    const int np = pk.np, nkatm = c->nkatm, npw = c->npw, npw_pad = c->npw_pad;
     if (np != c->nproj || !c->proj) {
         drop_graphs(c);
         c->tables_last.clear();
@@ -2142,99 +2276,42 @@ int cpsd_gpu_set_tables(cpsd_gpu_ctx *c, const int *katm, const double *amass, c
         }
         c->nproj = np;
     }
-    // pack into pinned staging (the previous upload from it has finished
-    // once the stream is idle), then one asynchronous copy per table
-    CK(cudaStreamSynchronize(c->st));
-    Stager sg{reinterpret_cast<char *>(c->tstage.p), c->tstage_bytes, c->st};
-    const int npw = c->npw, npw_pad = c->npw_pad;
-    const int *pt = h.pt_idx.data();
-    double *ptg = sg.slice<double>(npw_pad), *pvc = sg.slice<double>(npw_pad), *pvg = sg.slice<double>(npw_pad);
-    int *sh = sg.slice<int>(npw_pad);
-    double *pvl = sg.slice<double>((size_t)nkatm * npw), *pvnl = sg.slice<double>((size_t)nkatm * 9 * npw);
-    double *pzv = sg.slice<double>(nkatm), *pug = sg.slice<double>(9), *prc = sg.slice<double>(3 * c->nsh);
-    int *plm = sg.slice<int>(nkatm), *pk = sg.slice<int>(c->nion), *po = sg.slice<int>(c->nion);
-    double *pn = sg.slice<double>(np), *pg = sg.slice<double>(motion ? (size_t)3 * npw : 0);
-    if (!sg.ok()) return CPSD_ERR_ARG;  // more kinds / ions than the context was created for
-    // gathered in the grids' memory order (pt_ord), each table on a host thread
-    const int *ord = h.pt_ord.data();
-    for (int p = npw; p < npw_pad; ++p) ptg[p] = pvc[p] = pvg[p] = 0.0;
-    const int ntab = 3 + nkatm * 10 + (motion ? 3 : 0);
-    cpsd_host::Pool::get().run(ntab, [&](int t) {
-        const double *src;
-        double *d;
-        if (t < 3) {
-            src = t == 0 ? tg : (t == 1 ? vc : vg);
-            d = t == 0 ? ptg : (t == 1 ? pvc : pvg);
-        } else if (t < 3 + nkatm * 10) {
-            const int ia = (t - 3) / 10, l = (t - 3) % 10;  // l = 0: vl, else vnl channel l - 1
-            if (l == 0) {
-                src = vl + (size_t)ia * c->nfft3d;
-                d = pvl + (size_t)ia * npw;
-            } else {
-                d = pvnl + ((size_t)ia * 9 + l - 1) * npw;
-                if (l - 1 >= lmmax[ia]) {
-                    memset(d, 0, sizeof(double) * npw);
-                    return;
-                }
-                src = vnl + ((size_t)ia * 9 + l - 1) * c->nfft3d;
-            }
-        } else {
-            const int dd = t - 3 - nkatm * 10;
-            src = G + (size_t)dd * c->nfft3d;
-            d = pg + (size_t)dd * npw;
-        }
-        for (int q = 0; q < npw; ++q) {
-            const int p = ord[q];
-            d[p] = src[pt[p]];
-        }
-    });
-    double tmax = 0.0;
-    for (int p = 0; p < npw; ++p) tmax = std::max(tmax, ptg[p]);
-    c->tmax = tmax > 0 ? tmax : 1.0;
-    for (int p = 0; p < npw_pad; ++p) sh[p] = p < npw ? std::min(kShells - 1, (int)(ptg[p] / c->tmax * kShells)) : 0;
-    memcpy(pzv, zv, sizeof(double) * nkatm);
-    memcpy(pug, c->prm.unitg, sizeof(double) * 9);
-    if (c->nsh > 0) memcpy(prc, rcell, sizeof(double) * 3 * c->nsh);
-    memcpy(plm, lmmax, sizeof(int) * nkatm);
-    if (c->nion > 0) {
-        memcpy(pk, hk.data(), sizeof(int) * c->nion);
-        memcpy(po, off.data(), sizeof(int) * c->nion);
-    }
-    for (int ii = 0, q = 0; ii < c->nion; ++ii)
-        for (int l = 0; l < lmmax[hk[ii]]; ++l) pn[q++] = vnlnrm[hk[ii] * 9 + l];
+    c->tmax = pk.tmax;
     // a driver passes the same tables every call (ccpsdv3/main.c:422-426):
     // the device copies are current when the staged bytes are unchanged
-    if (motion) c->amass_h.assign(amass, amass + nkatm);
-    if (c->tables_ok && c->tables_last.size() == sg.off && !memcmp(c->tables_last.data(), c->tstage.p, sg.off)) {
-        c->motion_ok = motion;
+    if (pk.motion) c->amass_h.assign(amass, amass + nkatm);
+    if (c->tables_ok && c->tables_last.size() == pk.bytes && !memcmp(c->tables_last.data(), c->tstage.p, pk.bytes)) {
+        c->motion_ok = pk.motion;
         return CPSD_OK;
     }
-    sg.put(c->tg, ptg, npw_pad);
-    sg.put(c->shell, sh, npw_pad);
-    sg.put(c->vc, pvc, npw_pad);
-    sg.put(c->vg, pvg, npw_pad);
-    sg.put(c->vl, pvl, (size_t)nkatm * npw);
-    sg.put(c->vnl, pvnl, (size_t)nkatm * 9 * npw);
-    sg.put(c->zv, pzv, nkatm);
-    sg.put(c->lmmax, plm, nkatm);
-    sg.put(c->unitg, pug, 9);
+    Stager sg{reinterpret_cast<char *>(c->tstage.p), c->tstage_bytes, c->st};
+    sg.put(c->tg, pk.tg, npw_pad);
+    sg.put(c->shell, pk.sh, npw_pad);
+    sg.put(c->vc, pk.vc, npw_pad);
+    sg.put(c->vg, pk.vg, npw_pad);
+    sg.put(c->vl, pk.vl, (size_t)nkatm * npw);
+    sg.put(c->vnl, pk.vnl, (size_t)nkatm * 9 * npw);
+    sg.put(c->zv, pk.zv, nkatm);
+    sg.put(c->lmmax, pk.lm, nkatm);
+    sg.put(c->unitg, pk.ug, 9);
     if (c->nion > 0) {
-        sg.put(c->katm, pk, c->nion);
-        sg.put(c->proj_off, po, c->nion);
+        sg.put(c->katm, pk.k, c->nion);
+        sg.put(c->proj_off, pk.o, c->nion);
     }
-    if (c->nsh > 0) sg.put(c->rcell, prc, 3 * c->nsh);
-    if (np > 0) sg.put(c->vnlnrm_p, pn, np);
+    if (c->nsh > 0) sg.put(c->rcell, pk.rc, 3 * c->nsh);
+    if (np > 0) sg.put(c->vnlnrm_p, pk.n, np);
     // ion motion needs the G vectors (packed like tg) and the masses
     c->motion_ok = false;
-    if (motion) {
-        sg.put(c->Gv, pg, (size_t)3 * npw);
+    if (pk.motion) {
+        sg.put(c->Gv, pk.g, (size_t)3 * npw);
         c->motion_ok = true;
     }
     c->tables_last.clear();
     CK(sg.err);
     CK(cudaStreamSynchronize(c->st));
     c->h2d += sg.bytes;
-    c->tables_last.assign(reinterpret_cast<const char *>(c->tstage.p), reinterpret_cast<const char *>(c->tstage.p) + sg.off);
+    c->tables_last.assign(reinterpret_cast<const char *>(c->tstage.p),
+                          reinterpret_cast<const char *>(c->tstage.p) + pk.bytes);
     c->tables_ok = true;
     return CPSD_OK;
 }

@@ -103,6 +103,43 @@ def _outside_sphere(inp, x):
     return x.reshape(-1, inp.nfft3d, 2)[:, inp.masker1 == 0, :]
 
 
+def _resident_call(inp, c2, r2, inner):
+    """One call of `inner` steps on a fresh resident context."""
+    cell = api.GpuCell(inp)
+    cell.set_state(c2, r2)
+    cell.run(inner)
+    st = api.State(inp)
+    cell.get_state(st)
+    E = cell.E.copy()
+    cell.close()
+    return E, st
+
+
+def test_dropin_notices_changed_tables_and_mask():
+    """The drop-in reuses its context and runs on the tables and mask it
+    holds while host threads compare them with the caller's: tables changed
+    in place between calls, and a cell of the same shape with another mask,
+    give what a fresh context gives for the new inputs."""
+    inp = inputs.build_inputs(configs.small_diamond(24, 4, ecut=20.0))
+    st = api.State(inp)
+    api.cpsd(inp, st, 2)
+    inp.vg *= 1.0 + 1e-3  # the Hartree kernel, in place: same array, new values
+    c2, r2 = st.c2.copy(), st.r2.copy()
+    api.cpsd(inp, st, 2)
+    E_ref, s_ref = _resident_call(inp, c2, r2, 2)
+    assert np.array_equal(st.E, E_ref)
+    assert np.array_equal(st.c2, s_ref.c2)
+    # same nfft, bands, ions and kinds, another cutoff: another mask
+    other = inputs.build_inputs(configs.small_diamond(24, 4, ecut=16.0))
+    assert not np.array_equal(other.masker1, inp.masker1)
+    so = api.State(other)
+    api.cpsd(other, so, 2)
+    E_ref, s_ref = _resident_call(other, other.c2, other.r2, 2)
+    assert np.array_equal(so.E, E_ref)
+    assert np.array_equal(so.c2, s_ref.c2)
+    assert np.array_equal(so.dn, s_ref.dn)
+
+
 def test_host_layout_outputs_overwrite_every_grid_point():
     """c1 and cpsi are outputs only: NaN or other values in those buffers
     before a call leave no trace (only the sphere crosses PCIe; host threads
