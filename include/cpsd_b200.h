@@ -49,6 +49,15 @@ const char *cpsd_gpu_strerror(int status);
  * hml/lmd the Hamiltonian and Lagrange matrices.  cpsdwork is accepted and
  * not used (scratch lives on the GPU).  Errors are printed like the
  * reference's and the call returns; use cpsd_gpu_cpsd() for a status.
+ *
+ * The library keeps one device context per shape (grid, bands, ions, kinds,
+ * mask).  A call of the same shape as the last one starts its steps on the
+ * mask and tables the context holds and compares them with the ones passed
+ * (and c2 with zero outside the mask) on host threads meanwhile; if
+ * anything differs the steps are discarded and the call runs again on the
+ * new inputs, so the outputs are always those of the inputs passed.  c2
+ * with values outside the mask is refused (CPSD_ERR_UNMASKED_PSI) with
+ * every output left untouched.
  */
 void cpsd(const int inner, const int move, const int nion, const int ispin, const int *ne,
           const int nfft, const int nfft3d, const int n2ft3d, const double *unitg,
