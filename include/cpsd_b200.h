@@ -378,7 +378,7 @@ int cpsd_gpu_set_gemm(cpsd_gpu_ctx *c, int mode);
  * step graphs. */
 int cpsd_gpu_set_preconditioner_range(cpsd_gpu_ctx *c, double min_log_k, double max_log_k);
 /*
- * The guarded learned loop with plain SD as the judge, in the library (no
+ * The guarded learned loop with plain SD as the arbiter, in the library (no
  * counterpart in the reference): `blocks` blocks of `inner` steps with the
  * attached network (CPSD_ERR_ARG without one), the bound on log K at most
  * *cap.  A block whose energy rises above the previous one (E[0] in), is not

@@ -182,7 +182,7 @@ class GpuCell:
         self._mlp = mlp  # keep it alive while attached
 
     def run_guarded(self, inner: int, cap: float, blocks: int = 1):
-        """Blocks of learned steps with plain SD as the judge, in the library
+        """Blocks of learned steps with plain SD as the arbiter, in the library
         (cpsd_gpu_run_guarded): returns (energy, rejected blocks, new cap)."""
         c = np.array([cap], dtype=np.float64)
         de, dc = ctypes.c_double(), ctypes.c_double()

@@ -390,7 +390,7 @@ def study_cell(inp, mlp: api.Mlp, tol_per_ion: float = 1e-6, plain_max: int = 60
                inner: int = 100, alt_start_seed: Optional[int] = None, verify_steps: int = 5000,
                precision: int = 1, gemm: int = 3) -> dict:
     """The learned path against plain SD on one cell, with plain SD's own
-    converged energy as the judge:
+    converged energy as the yardstick:
 
     * plain FP64 SD from the cell's start orbitals to convergence -> E_conv,
       and its time to |E - E_conv| <= tol_per_ion * nion;
