@@ -769,11 +769,6 @@ int issue_knl(cpsd_gpu_ctx *c, cudaStream_t side, const cx<double> *c1, cx<doubl
     const cx<double> *c1l = c1 + (long)lo * c->ldc;
     cx<double> *c2l = c2 + (long)lo * c->ldc;
     c->cs = side;
-    if (nbl > 0) {
-        kinetic_kernel<<<(unsigned)cdiv((long)nbl * c->npw_pad, 256), 256, 0, side>>>(nbl, c->npw_pad, c->ldc,
-                                                                                     c->tg, c1l, c2l);
-        c->nlaunch += 1;
-    }
     if (c->nproj > 0) {
         int rc = gemm_tn(c, c->nproj, nbl, K, (const double *)c->proj, ldr, (const double *)c1l, ldr, c->w, 1.0,
                          0.0, c->beta + lo, c->nb, TN_PROJECTOR);
@@ -784,8 +779,9 @@ int issue_knl(cpsd_gpu_ctx *c, cudaStream_t side, const cx<double> *c1, cx<doubl
         kb_coef_kernel<<<(unsigned)cdiv((long)c->nproj * c->nb, 256), 256, 0, side>>>(
             c->nproj, c->nb, c->beta, c->vnlnrm_p, c->scal2, c->coefT, c->move ? c->coefP : nullptr);
         c->nlaunch += 1;
+        // the nonlocal part alone; the SD epilogue adds the kinetic term
         gemm_nn(c, nbl, K, c->nproj, 1.0, c->coefT + (long)lo * c->nproj, c->nproj, (const double *)c->proj, ldr,
-                1.0, (double *)c2l, ldr, TN_PROJECTOR);
+                0.0, (double *)c2l, ldr, TN_PROJECTOR);
         if (c->move) {  // nonlocal force: Y_P = sum_b sw1(P, b) c1_b, then sum_G G Im(conj(chi_P) Y_P)
             gemm_nn(c, c->nproj, K, c->nb, 1.0, c->coefP, c->nb, (const double *)c1, ldr, 0.0, (double *)c->Ynl,
                     ldr);
@@ -953,6 +949,8 @@ int step_phase(cpsd_gpu_ctx *c, int phase)
             e.ldc = c->ldc;
             e.scal1 = c->scal1;
             e.dte = c->dte;
+            e.tg = c->tg;
+            e.has_nl = c->nproj > 0;
             c->fft->fwd_z_sd(c->g, c->Tb, e, nbl, s); c->nlaunch += 1;
         }
         if (c->mlp) {  // learned step scales per band and |G| shell

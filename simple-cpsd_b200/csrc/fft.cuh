@@ -162,12 +162,16 @@ struct ZEpilogue {
     cx<double> *out;
     long ldo;
     double scale;
-    // SD (ccpsdv3/cpsd.c:394-400): cpsi = -scal1*F + c2; c2 = c1 + dte*cpsi
-    cx<double> *c2;        // in: kinetic + nonlocal part; out: steepest-descent iterate
+    // SD (ccpsdv3/cpsd.c:212-221, 394-400): cpsi = -scal1*F + (-tg c1 + nl);
+    // c2 = c1 + dte*cpsi, the kinetic term -tg c1 formed here from the c1
+    // the epilogue reads anyway
+    cx<double> *c2;        // in: the nonlocal part nl (when has_nl); out: steepest-descent iterate
     const cx<double> *c1;
     cx<double> *cpsi;
+    const double *tg;      // G^2/2 per sphere point
     long ldc;
     double scal1, dte;
+    int has_nl;            // 0: no projectors, nl = 0 and c2 is not read
 };
 
 template <typename T, int NF, int EPI>
@@ -219,6 +223,7 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
         for (int p0 = g.col_ptr[c] + t; p0 < pe; p0 += 4 * P) {
             int kk[4];
             cx<double> c2k[4], c1v[4];
+            double t[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int p = p0 + u * P;
@@ -226,8 +231,9 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
                 if constexpr (EPI == ZEPI_SD)
                     if (p < pe) {
                         const long o = (long)b * e.ldc + p;
-                        c2k[u] = e.c2[o];
                         c1v[u] = e.c1[o];
+                        t[u] = e.tg[p];
+                        c2k[u] = e.has_nl ? e.c2[o] : cx<double>{0.0, 0.0};
                     }
             }
 #pragma unroll
@@ -239,7 +245,10 @@ fwd_z_kernel(Geom g, const cx<T> *__restrict__ Tb, ZEpilogue e, Twiddles<T> tw)
                     e.out[(long)b * e.ldo + p] = cx<double>{e.scale * (double)F.x, e.scale * (double)F.y};
                 } else {
                     const long o = (long)b * e.ldc + p;
-                    const cx<double> cp{-e.scal1 * (double)F.x + c2k[u].x, -e.scal1 * (double)F.y + c2k[u].y};
+                    // kinetic + nonlocal: -t c1 + nl (nl absent: the kinetic term alone)
+                    const cx<double> kin{-t[u] * c1v[u].x, -t[u] * c1v[u].y};
+                    const cx<double> h = e.has_nl ? cx<double>{c2k[u].x + kin.x, c2k[u].y + kin.y} : kin;
+                    const cx<double> cp{-e.scal1 * (double)F.x + h.x, -e.scal1 * (double)F.y + h.y};
                     e.cpsi[o] = cp;
                     e.c2[o] = cx<double>{c1v[u].x + e.dte * cp.x, c1v[u].y + e.dte * cp.y};
                 }

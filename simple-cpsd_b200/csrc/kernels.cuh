@@ -261,18 +261,6 @@ __global__ void force_total_kernel(int nion, double nl_factor, const int *__rest
     }
 }
 
-// kinetic part of -H psi: c2 = -tg c1, ccpsdv3/cpsd.c:212-221
-__global__ void kinetic_kernel(int nb, int npw_pad, long ldc, const double *__restrict__ tg,
-                               const cx<double> *__restrict__ c1, cx<double> *__restrict__ c2)
-{
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= (long)nb * npw_pad) return;
-    const int b = (int)(id / npw_pad), p = (int)(id % npw_pad);
-    const double t = tg[p];
-    cx<double> v = c1[(long)b * ldc + p];
-    c2[(long)b * ldc + p] = cx<double>{-t * v.x, -t * v.y};
-}
-
 // coefficients of the KB back-projection, ccpsdv3/cpsd.c:289:
 // coefT[b][P] = -beta[P][b] * scal2 / vnlnrm[P]
 // (and, for the nonlocal force, the same in [P][b] order when coefP is given)
