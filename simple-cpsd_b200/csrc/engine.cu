@@ -528,7 +528,7 @@ struct cpsd_gpu_ctx {
     double *pM = nullptr;      // <cpsi_b|c1_a> per spin
     double *pstats = nullptr, tmax = 0.0;
     long long steps_run = 0;  // SD steps taken by this context
-    float *pX = nullptr, *py = nullptr;
+    float *py = nullptr;
     // optional phase timing: events recorded between the phases of a step
     // (captured into the step graphs), read back by cpsd_gpu_phase_times()
     bool phase_timing = false;
@@ -957,7 +957,6 @@ int step_phase(cpsd_gpu_ctx *c, int phase)
             // The residual R = cpsi - C1 (C1' W cpsi) per spin: only R is
             // preconditioned, so the update is plain SD wherever R = 0 and the
             // fixed point H psi = psi Lambda is that of plain SD.
-            CK(cudaMemcpyAsync(c->pR, c->cpsi, sizeof(cx<double>) * c->nb * c->ldc, cudaMemcpyDeviceToDevice, s));
             for (int ms = 0; ms < c->ispin; ++ms) {
                 const int m = ms ? c->ne1 : c->ne0;
                 const long off = (long)(ms ? c->ne0 : 0) * ldr;
@@ -965,17 +964,16 @@ int step_phase(cpsd_gpu_ctx *c, int phase)
                 int rc = gemm_tn(c, m, m, K, (const double *)c->cpsi + off, ldr, (const double *)c1 + off, ldr, c->w,
                                  1.0, 0.0, Mt, m, TN_PROJECTOR);
                 if (rc) return rc;
-                gemm_nn(c, m, K, m, -1.0, Mt, m, (const double *)c1 + off, ldr, 1.0, (double *)c->pR + off, ldr,
+                // pR = -C1 Mt; the update adds cpsi (R = cpsi + pR)
+                gemm_nn(c, m, K, m, -1.0, Mt, m, (const double *)c1 + off, ldr, 0.0, (double *)c->pR + off, ldr,
                         TN_PROJECTOR);
             }
             band_stats_kernel<<<c->nb, 256, 0, s>>>(c->npw, c->ldc, c->w, c->tg, c1, c->cpsi, c->pstats);
-            prec_features_kernel<<<(unsigned)cdiv((long)c->nb * kShells, 256), 256, 0, s>>>(c->nb, c->tmax, c->pstats,
-                                                                                          c->dstep, c->pX);
-            mlp_forward_kernel<<<mlp_forward_blocks((long)c->nb * kShells), kMlpTileThreads, 0, s>>>(
-                c->nb * kShells, c->pX, c->mlp->wq, c->mlp->p, c->py, nullptr);
+            prec_mlp_kernel<<<mlp_forward_blocks((long)c->nb * kShells), kMlpTileThreads, 0, s>>>(
+                c->nb, c->tmax, c->pstats, c->dstep, c->mlp->wq, c->mlp->p, c->py);
             prec_update_kernel<<<(unsigned)cdiv((long)c->nb * c->npw, 256), 256, 0, s>>>(
-                c->nb, c->npw, c->ldc, c->shell, c->py, c->pcap, c->dte, c->pR, c2, c->dstep);
-            c->nlaunch += 4;
+                c->nb, c->npw, c->ldc, c->shell, c->py, c->pcap, c->dte, c->cpsi, c->pR, c2, c->dstep);
+            c->nlaunch += 3;
         }
         mark(c, 9);
         CK(cudaGetLastError());
@@ -2161,7 +2159,6 @@ int cpsd_gpu_create(const cpsd_gpu_params *p, const int *masker1, cpsd_gpu_ctx *
     CK(ar.alloc(&c->pR, (size_t)nb * P));
     CK(ar.alloc(&c->pM, (size_t)c->ispin * c->ne0 * c->ne0));
     CK(ar.alloc(&c->pstats, (size_t)3 * nb));
-    CK(ar.alloc(&c->pX, (size_t)4 * nb * kShells));
     CK(ar.alloc(&c->py, (size_t)nb * kShells));
     if (c->ne0 <= kLagSmallMax)
         CK(cudaFuncSetAttribute(lagrange_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -44,10 +44,11 @@ constexpr int kMlpTile = 16;
 constexpr int kMlpTileThreads = 256;
 constexpr int kMlpTileSpt = kMlpTile / (kMlpTileThreads / kMlpHid);  // samples a thread: 4
 
-__global__ void __launch_bounds__(kMlpTileThreads) mlp_forward_kernel(int n, const float *__restrict__ X,
-                                                                      const __nv_bfloat16 *__restrict__ wq,
-                                                                      const float *__restrict__ p,
-                                                                      float *__restrict__ y, float *__restrict__ H)
+// One CTA's tile of the forward pass; xin(e) is input value e = 4 s + k of
+// sample s (s < n).
+template <typename XIn>
+CPSD_D void mlp_tile(int n, const XIn &xin, const __nv_bfloat16 *__restrict__ wq, const float *__restrict__ p,
+                     float *__restrict__ y, float *__restrict__ H)
 {
     __shared__ float w1t[kMlpIn][kMlpHid];
     // a padded row (65) keeps the transposing writes and the unit-wise reads
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(kMlpTileThreads) mlp_forward_kernel(int n, con
     }
     if (t < kMlpTile * kMlpIn) {
         const long e = s0 * kMlpIn + t;
-        x0[t / kMlpIn][t % kMlpIn] = (e < (long)n * kMlpIn) ? X[e] : 0.0f;
+        x0[t / kMlpIn][t % kMlpIn] = (e < (long)n * kMlpIn) ? xin(e) : 0.0f;
     }
     __syncthreads();
     const int o = t % kMlpHid, sg = t / kMlpHid;
@@ -130,6 +131,14 @@ __global__ void __launch_bounds__(kMlpTileThreads) mlp_forward_kernel(int n, con
         for (int i = 0; i < kMlpHid; ++i) acc = fmaf(w4[i], act[2][t][i], acc);
         y[s0 + t] = acc;
     }
+}
+
+__global__ void __launch_bounds__(kMlpTileThreads) mlp_forward_kernel(int n, const float *__restrict__ X,
+                                                                      const __nv_bfloat16 *__restrict__ wq,
+                                                                      const float *__restrict__ p,
+                                                                      float *__restrict__ y, float *__restrict__ H)
+{
+    mlp_tile(n, [X](long e) { return X[e]; }, wq, p, y, H);
 }
 
 inline unsigned mlp_forward_blocks(long n) { return (unsigned)((n + kMlpTile - 1) / kMlpTile); }
@@ -303,34 +312,49 @@ __global__ void band_stats_kernel(int npw, long ldc, const double *__restrict__ 
     }
 }
 
-// network inputs for (band, shell): tshell/KE, log KE, log |residual|^2, step
-// feature (the step counter advances in prec_update_kernel, a later launch)
-__global__ void prec_features_kernel(int nb, double tmax, const double *__restrict__ stats,
-                                     const int *__restrict__ step, float *__restrict__ X)
+// network input k of sample id = (band b, shell s): tshell/KE, log KE,
+// log |residual|^2, step feature (the step counter advances in
+// prec_update_kernel, a later launch)
+CPSD_D float prec_feature(double tmax, const double *__restrict__ stats, const int *__restrict__ step, long id,
+                          int k)
 {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= nb * kShells) return;
-    const int b = id / kShells, s = id % kShells;
+    const int b = (int)(id / kShells), s = (int)(id % kShells);
     const double ke = fmax(stats[3 * b], 1e-12);
-    const double hh = stats[3 * b + 1], qq = stats[3 * b + 2];
-    const double res = fmax(qq - hh * hh, 1e-30);  // |cpsi - <c1|cpsi> c1|^2
-    const double ts = (s + 0.5) * tmax / kShells;
-    X[4 * id + 0] = (float)(ts / ke);
-    X[4 * id + 1] = (float)log(ke);
-    X[4 * id + 2] = (float)log(res);
-    X[4 * id + 3] = (float)(log1p((double)*step) / 10.0);
+    switch (k) {
+    case 0: return (float)((s + 0.5) * tmax / kShells / ke);
+    case 1: return (float)log(ke);
+    case 2: {
+        const double hh = stats[3 * b + 1], qq = stats[3 * b + 2];
+        return (float)log(fmax(qq - hh * hh, 1e-30));  // |cpsi - <c1|cpsi> c1|^2
+    }
+    default: return (float)(log1p((double)*step) / 10.0);
+    }
+}
+
+// The step's network pass: the inputs of each (band, shell) formed from the
+// band statistics as the tile is staged, then the tiled forward pass.
+__global__ void __launch_bounds__(kMlpTileThreads) prec_mlp_kernel(int nb, double tmax,
+                                                                   const double *__restrict__ stats,
+                                                                   const int *__restrict__ step,
+                                                                   const __nv_bfloat16 *__restrict__ wq,
+                                                                   const float *__restrict__ p,
+                                                                   float *__restrict__ y)
+{
+    mlp_tile(nb * kShells, [=](long e) { return prec_feature(tmax, stats, step, e / kMlpIn, (int)(e % kMlpIn)); },
+             wq, p, y, nullptr);
 }
 
 // c2 (= c1 + dte cpsi, the plain SD update) += dte (K[b][shell(p)] - 1) R,
-// with R the residual of cpsi outside the occupied subspace: the residual is
+// with R = cpsi + Pm the residual of cpsi outside the occupied subspace (Pm =
+// -C1 (C1' W cpsi), the projection's product): the residual is
 // stepped by dte K, the part inside the subspace exactly as plain SD.  log K
 // is the network output clamped to [range[0], range[1]] (inside [kLogKMin,
 // kLogKMax]): the host narrows the upper end after a rejected block (a trust
 // region) and sets [0, 0] for plain SD steps (K = 1, c2 unchanged here).
 __global__ void prec_update_kernel(int nb, int npw, long ldc, const int *__restrict__ shell,
                                    const float *__restrict__ y, const float *__restrict__ range, double dte,
-                                   const cx<double> *__restrict__ R, cx<double> *__restrict__ c2,
-                                   int *__restrict__ step)
+                                   const cx<double> *__restrict__ cpsi, const cx<double> *__restrict__ Pm,
+                                   cx<double> *__restrict__ c2, int *__restrict__ step)
 {
     const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (id == 0) atomicAdd(step, 1);
@@ -340,6 +364,7 @@ __global__ void prec_update_kernel(int nb, int npw, long ldc, const int *__restr
     const float lk = fminf(fmaxf(y[b * kShells + shell[p]], lo), hi);
     const double f = dte * (exp((double)lk) - 1.0);
     const long o = (long)b * ldc + p;
-    const cx<double> r = R[o], u = c2[o];
+    const cx<double> q = cpsi[o], m = Pm[o], u = c2[o];
+    const cx<double> r{q.x + m.x, q.y + m.y};
     c2[o] = cx<double>{u.x + f * r.x, u.y + f * r.y};
 }
