@@ -72,7 +72,8 @@ def sphere_of(cell: api.GpuCell) -> Sphere:
 
 
 def features(sp: Sphere, c1: np.ndarray, cpsi: np.ndarray, step: int) -> np.ndarray:
-    """(nb*NSHELL, 4) float32 inputs, as prec_features_kernel builds them."""
+    """(nb*NSHELL, 4) float32 inputs, as the step's network pass forms them
+    (prec_feature in csrc/mlp.cuh)."""
     w = sp.w
     ke = np.maximum((w * sp.tg * (c1.real ** 2 + c1.imag ** 2)).sum(1), 1e-12)
     h = (w * (c1.real * cpsi.real + c1.imag * cpsi.imag)).sum(1)
